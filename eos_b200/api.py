@@ -1,0 +1,252 @@
+"""Python view of the C ABI: context, resident scenes, render / batch / backward / queries.
+
+Device buffers are torch CUDA tensors (torch is used for device memory only); host
+buffers are numpy arrays, which the library stages through its own device memory.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_void_p
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .scenes import CameraData, SceneData
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(c_void_p)
+
+
+def camera_struct(cam: CameraData) -> L.Camera:
+    c = L.Camera()
+    for k in range(3):
+        c.position[k] = float(cam.position[k])
+        c.view[k] = float(cam.view[k])
+        c.right[k] = float(cam.right[k])
+        c.up[k] = float(cam.up[k])
+    c.width = int(cam.width)
+    c.height = int(cam.height)
+    return c
+
+
+def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="plain", block_size=0,
+                  queue_chunk=0, stack_depth=0, stage_timing=False) -> L.RenderParams:
+    p = L.RenderParams()
+    p.trace_depth = int(trace_depth)
+    p.pixel_offset = float(pixel_offset)
+    p.spp = int(spp)
+    p.jitter_seed = int(jitter_seed)
+    p.mode = L.MODE_WAVEFRONT if mode == "wavefront" else L.MODE_PLAIN
+    p.block_size = int(block_size)
+    p.queue_chunk = int(queue_chunk)
+    p.stack_depth = int(stack_depth)
+    p.flags = L.FLAG_STAGE_TIMING if stage_timing else 0
+    return p
+
+
+def stats_dict(st: L.Stats) -> dict:
+    d = {f: getattr(st, f) for f, _ in L.Stats._fields_ if f != "stage_ms"}
+    d["stage_ms"] = [float(v) for v in st.stage_ms]
+    return d
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        h = c_void_p()
+        L.check(self.lib.eos_ctx_create(device, byref(h)), "eos_ctx_create")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eos_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None):
+        L.check(self.lib.eos_ctx_set_stream(self.h, c_void_p(stream_handle) if stream_handle else None),
+                "eos_ctx_set_stream")
+
+    def synchronize(self):
+        L.check(self.lib.eos_ctx_synchronize(self.h), "eos_ctx_synchronize")
+
+
+def materials_array(mats: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(mats, np.float32).reshape(-1, 8)
+
+
+class DeviceScene:
+    """A scene resident in HBM with its LBVH (eos_scene_create)."""
+
+    def __init__(self, ctx: Context, scene: SceneData, leaf_size: int = 4, inputs_on_device: bool = False):
+        self.ctx = ctx
+        self.scene = scene
+        self.lib = ctx.lib
+        bp = L.BuildParams()
+        bp.leaf_size = leaf_size
+        arrs = [scene.verts, scene.normals, scene.tris, scene.tri_obj]
+        if inputs_on_device:
+            import torch
+            arrs = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in arrs]
+        mats = materials_array(scene.materials)
+        lights = np.ascontiguousarray(scene.lights, np.float32)
+        h = c_void_p()
+        code = self.lib.eos_scene_create(ctx.h, _ptr(arrs[0]), _ptr(arrs[1]), scene.verts.shape[0], _ptr(arrs[2]),
+                                         _ptr(arrs[3]), scene.n_tris, _ptr(mats), mats.shape[0], _ptr(lights),
+                                         lights.shape[0], byref(bp), byref(h))
+        L.check(code, "eos_scene_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eos_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        i = L.SceneInfo()
+        L.check(self.lib.eos_scene_get_info(self.h, byref(i)), "eos_scene_get_info")
+        return {f: getattr(i, f) for f, _ in L.SceneInfo._fields_}
+
+    def morton(self):
+        n = self.scene.n_tris
+        codes = np.zeros(n, np.uint32)
+        order = np.zeros(n, np.uint32)
+        L.check(self.lib.eos_scene_get_morton(self.h, _ptr(codes), _ptr(order)), "eos_scene_get_morton")
+        return codes, order
+
+    def set_materials(self, mats):
+        m = mats if hasattr(mats, "data_ptr") else materials_array(mats)
+        L.check(self.lib.eos_scene_set_materials(self.h, _ptr(m), int(m.shape[0])), "eos_scene_set_materials")
+
+    def set_lights(self, lights):
+        l = lights if hasattr(lights, "data_ptr") else np.ascontiguousarray(lights, np.float32).reshape(-1, 6)
+        L.check(self.lib.eos_scene_set_lights(self.h, _ptr(l), int(l.shape[0])), "eos_scene_set_lights")
+
+
+def _alloc(shape, dtype, device: bool):
+    if device:
+        import torch
+        tmap = {np.float32: torch.float32, np.uint8: torch.uint8, np.int32: torch.int32}
+        return torch.empty(shape, dtype=tmap[dtype], device="cuda")
+    return np.empty(shape, dtype)
+
+
+def render(ctx: Context, scene: DeviceScene, cam: CameraData, trace_depth: int, pixel_offset: float = 0.5,
+           spp: int = 1, jitter_seed: int = 0, mode: str = "plain", outputs=("rgb",), device: bool = True,
+           out: dict | None = None, **tuning) -> dict:
+    """Render one frame; returns the requested outputs plus 'stats'.
+
+    outputs: any of 'rgb' [H*W,3] f32, 'rgba8' [H,W,4] u8, 'hit' [H*W*spp] i32,
+    'paths' [H*W*spp, 16] i32 (8 hit ids then 8 shadow masks per path).
+    """
+    npx = cam.width * cam.height
+    res = dict(out or {})
+    shapes = {"rgb": ((npx, 3), np.float32), "rgba8": ((cam.height, cam.width, 4), np.uint8),
+              "hit": ((npx * spp,), np.int32), "paths": ((npx * spp, 16), np.int32)}
+    for k in outputs:
+        if k not in res:
+            res[k] = _alloc(shapes[k][0], shapes[k][1], device)
+    st = L.Stats()
+    c = camera_struct(cam)
+    p = params_struct(trace_depth, pixel_offset, spp, jitter_seed, mode, **tuning)
+    code = ctx.lib.eos_render(ctx.h, scene.h, byref(c), byref(p), _ptr(res.get("rgb")), _ptr(res.get("rgba8")),
+                              _ptr(res.get("hit")), _ptr(res.get("paths")), byref(st))
+    L.check(code, "eos_render")
+    res["stats"] = stats_dict(st)
+    return res
+
+
+@dataclass
+class BatchJob:
+    scene: DeviceScene
+    camera: CameraData
+    trace_depth: int = 1
+    pixel_offset: float = 0.5
+    spp: int = 1
+    jitter_seed: int = 0
+
+
+def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",)):
+    outs = []
+    for j in jobs:
+        npx = j.camera.width * j.camera.height
+        o = {}
+        if "rgb" in outputs:
+            o["rgb"] = _alloc((npx, 3), np.float32, True)
+        if "rgba8" in outputs:
+            o["rgba8"] = _alloc((j.camera.height, j.camera.width, 4), np.uint8, True)
+        if "paths" in outputs:
+            o["paths"] = _alloc((npx * j.spp, 16), np.int32, True)
+        outs.append(o)
+    return outs
+
+
+def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning) -> dict:
+    """All jobs through one wavefront pass (graph-captured); outputs are device tensors."""
+    arr = (L.Job * len(jobs))()
+    for i, (j, o) in enumerate(zip(jobs, outs)):
+        arr[i].scene = j.scene.h
+        arr[i].camera = camera_struct(j.camera)
+        arr[i].trace_depth = j.trace_depth
+        arr[i].pixel_offset = j.pixel_offset
+        arr[i].spp = j.spp
+        arr[i].jitter_seed = j.jitter_seed
+        arr[i].rgb_out = _ptr(o.get("rgb"))
+        arr[i].rgba8_out = _ptr(o.get("rgba8"))
+        arr[i].paths_out = _ptr(o.get("paths"))
+    p = params_struct(mode="wavefront", **tuning)
+    st = L.Stats()
+    L.check(ctx.lib.eos_render_batch(ctx.h, arr, len(jobs), byref(p), byref(st)), "eos_render_batch")
+    return stats_dict(st)
+
+
+def render_backward(ctx: Context, scene: DeviceScene, cams: list[CameraData], trace_depth: int, paths, d_rgb,
+                    pixel_offset: float = 0.5, device: bool = True):
+    """Adjoint of the shading: returns (grad_materials [K,7], grad_lights [L,6])."""
+    arr = (L.Camera * len(cams))(*[camera_struct(c) for c in cams])
+    p = params_struct(trace_depth, pixel_offset, 1)
+    K = scene.scene.n_objects
+    NL = max(1, scene.scene.n_lights)
+    gm = _alloc((K, 7), np.float32, device)
+    gl = _alloc((NL, 6), np.float32, device)
+    g = L.Grads()
+    g.materials = _ptr(gm).value
+    g.lights = _ptr(gl).value
+    code = ctx.lib.eos_render_backward(ctx.h, scene.h, arr, len(cams), byref(p), _ptr(paths), _ptr(d_rgb), byref(g))
+    L.check(code, "eos_render_backward")
+    return gm, gl
+
+
+def trace_closest(ctx: Context, scene: DeviceScene, rays: np.ndarray):
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+    n = r.shape[0]
+    ids = np.zeros(n, np.int32)
+    ts = np.zeros(n, np.float32)
+    L.check(ctx.lib.eos_trace_closest(ctx.h, scene.h, _ptr(r), n, _ptr(ids), _ptr(ts)), "eos_trace_closest")
+    return ids, ts
+
+
+def trace_any(ctx: Context, scene: DeviceScene, rays: np.ndarray):
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+    n = r.shape[0]
+    occ = np.zeros(n, np.uint8)
+    L.check(ctx.lib.eos_trace_any(ctx.h, scene.h, _ptr(r), n, _ptr(occ)), "eos_trace_any")
+    return occ

@@ -1,0 +1,218 @@
+// Adjoint of the shading (no reference counterpart): gradients of an image loss L with
+// respect to per-object kd, ks, log(shininess) and per-light colour and position, with
+// visibility frozen from the forward pass's path records (hit triangle per bounce and
+// blocked-light masks).  Nothing else of the forward pass is stored: each bounce's hit is
+// re-derived from its triangle id with the same exact-order Moller-Trumbore, hit point,
+// normal and mirror ray as the forward kernels, so the geometry matches the forward pass
+// bit for bit.
+//
+// Forward model per path (src/RayTracer.cpp:302-458): c = sum_k T_k phong_k with
+// T_k = prod_{j<k} reflectivity_j and, per unblocked light l,
+//   phong = max(0, N.L) kd*C_l + [V.R > 0] (V.R)^s C_l*ks,  L = (p_l - P)/|p_l - P|,
+//   R = w/|w|, w = 2 (N.L) N - L,  V = normalize(camera - P),  s = shininess.
+// Gradients with g = dL/dc * T_k:
+//   dkd_c += g_c max(0,N.L) C_c          dks_c += g_c (V.R)^s C_c
+//   dlog s += sum_c g_c ks_c C_c (V.R)^s ln(V.R) s
+//   dC_c  += g_c (max(0,N.L) kd_c + (V.R)^s ks_c)
+//   dp_l  += a (N - (N.L) L)/|u|  [N.L > 0]
+//          + b s (V.R)^(s-1) (I - L L^T)/|u| (2 N N^T - I) (V - (V.R) R)/|w|  [V.R > 0]
+//   with a = sum_c g_c C_c kd_c, b = sum_c g_c C_c ks_c.
+// Per-object sums use a warp segmented reduction (peers by object id) and one atomic per
+// object per warp; per-light sums use a warp reduction into shared memory per block.
+#include <algorithm>
+
+#include "trace.cuh"
+
+namespace eos {
+namespace {
+
+struct BwArgs {
+  DevScene s;
+  const float* cams;  // n_views x 12
+  int w, h, n_views, trace_depth;
+  float off;
+  const eos_path_record* paths;
+  const float* drgb;
+  float* gmat;    // n_obj x 7
+  float* glight;  // n_lights x 6
+  int* err;
+};
+
+__device__ __forceinline__ float warp_sum(float v) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+__global__ void __launch_bounds__(128) k_backward(BwArgs A) {
+  __shared__ float sl[kMaxLights * 6];
+  for (int i = threadIdx.x; i < kMaxLights * 6; i += blockDim.x) sl[i] = 0.0f;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long npx = (long long)A.w * A.h;
+  const long long total = npx * A.n_views;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < total;
+  const DevScene& s = A.s;
+  eos_path_record rec;
+  f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1), campos = o;
+  float g[3] = {0, 0, 0};
+  if (active) {
+    rec = A.paths[i];
+    int view = (int)(i / npx);
+    int pix = (int)(i % npx);
+    const float* cam = A.cams + 12 * view;
+    d = primary_direction(cam, A.w, A.h, pix % A.w, pix / A.w, A.off, A.off);
+    campos = mk3(cam[0], cam[1], cam[2]);
+    o = campos;
+    g[0] = A.drgb[3 * i];
+    g[1] = A.drgb[3 * i + 1];
+    g[2] = A.drgb[3 * i + 2];
+  }
+  float T = 1.0f;
+  bool alive = active;
+  for (int k = 0; k <= A.trace_depth; ++k) {
+    int obj = -1;
+    float gm[7] = {0, 0, 0, 0, 0, 0, 0};
+    f3 P = o, N = o;
+    const float* m = nullptr;
+    if (alive) {
+      int id = rec.hit[k];
+      if (id < 0 || id >= s.n_tris) {
+        alive = false;
+      } else {
+        Hit h;
+        h.pos = s.pos_of_id[id];
+        h.id = id;
+        f3 v1, e1, e2;
+        int rid;
+        load_tri(s.tris, h.pos, v1, e1, e2, rid);
+        if (!mt_intersect(o, d, v1, e1, e2, h.t, h.u, h.v)) {
+          atomicOr(A.err, kErrIndex);  // record does not match this scene / camera
+          alive = false;
+        } else {
+          hit_geometry(s, o, d, h, P, N, obj);
+          m = s.mats + 8 * obj;
+        }
+      }
+    }
+    if (alive) {
+      const float shin = m[6];
+      f3 V = norm3(sub3(campos, P));
+      uint32_t mask = rec.shadow[k];
+      float gT[3] = {g[0] * T, g[1] * T, g[2] * T};
+      for (int l = 0; l < s.n_lights; ++l) {
+        if (mask & (1u << l)) continue;
+        const float* lp = s.lights + 6 * l;
+        f3 u = sub3(mk3(lp[0], lp[1], lp[2]), P);
+        float ul = sqrtf(dot3(u, u));
+        f3 L = scale3(1.0f / ul, u);
+        float ndl = dot3(N, L);
+        f3 wv = sub3(scale3(2.0f * ndl, N), L);
+        float wl = sqrtf(dot3(wv, wv));
+        f3 R = scale3(1.0f / wl, wv);
+        float fd = ndl > 0.0f ? ndl : 0.0f;
+        float vr = dot3(V, R);
+        float fs = vr > 0.0f ? powf(vr, shin) : 0.0f;
+        float C[3] = {lp[3], lp[4], lp[5]};
+        float a = 0.0f, b = 0.0f;
+        float gl[6];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          gm[c] += gT[c] * fd * C[c];
+          gm[3 + c] += gT[c] * fs * C[c];
+          gl[c] = gT[c] * (fd * m[c] + fs * m[3 + c]);
+          a += gT[c] * C[c] * m[c];
+          b += gT[c] * C[c] * m[3 + c];
+        }
+        if (vr > 0.0f) gm[6] += b * fs * logf(vr) * shin;
+        f3 gp = mk3(0, 0, 0);
+        if (ndl > 0.0f) gp = add3(gp, scale3(a / ul, sub3(N, scale3(ndl, L))));
+        if (vr > 0.0f) {
+          f3 q = scale3(1.0f / wl, sub3(V, scale3(vr, R)));
+          f3 q2 = sub3(scale3(2.0f * dot3(N, q), N), q);
+          f3 gs = scale3(1.0f / ul, sub3(q2, scale3(dot3(L, q2), L)));
+          float dfs = shin * powf(vr, shin - 1.0f);
+          gp = add3(gp, scale3(b * dfs, gs));
+        }
+        gl[3] = gp.x;
+        gl[4] = gp.y;
+        gl[5] = gp.z;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) atomicAdd(&sl[6 * l + c], gl[c]);
+      }
+    }
+    // per-object segmented reduction: one leader per distinct object in the warp
+    int key = alive ? obj : -1;
+    uint32_t pending = __ballot_sync(0xffffffffu, key >= 0);
+    while (pending) {
+      int leader = __ffs(pending) - 1;
+      int lk = __shfl_sync(0xffffffffu, key, leader);
+      bool mine = key == lk;
+      uint32_t peers = __ballot_sync(0xffffffffu, mine);
+#pragma unroll
+      for (int c = 0; c < 7; ++c) {
+        float v = warp_sum(mine ? gm[c] : 0.0f);
+        if (lane == leader && v != 0.0f) atomicAdd(&A.gmat[7 * lk + c], v);
+      }
+      pending &= ~peers;
+    }
+    if (alive) {
+      float r = m[7];
+      if (!(r > 0.0f) || k + 1 > A.trace_depth) {
+        alive = false;
+      } else {
+        T *= r;
+        f3 rd = norm3(reflect3(d, N));
+        o = add3(P, scale3(kRayEps, rd));
+        d = rd;
+      }
+    }
+    if (!__any_sync(0xffffffffu, alive)) break;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < s.n_lights * 6; c += blockDim.x)
+    if (sl[c] != 0.0f) atomicAdd(&A.glight[c], sl[c]);
+}
+
+}  // namespace
+
+eos_status render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cams, uint32_t n_views,
+                           const eos_render_params& p, const eos_path_record* d_paths, const float* d_rgb,
+                           float* d_gmat, float* d_glight) {
+  eos_status es = EOS_OK;
+  float* d_cams = (float*)scratch(ctx, "bw.cams", 48ull * n_views, &es);
+  if (es != EOS_OK) return es;
+  std::vector<float> hc(12 * (size_t)n_views);
+  for (uint32_t v = 0; v < n_views; ++v)
+    for (int k = 0; k < 3; ++k) {
+      hc[12 * v + k] = cams[v].position[k];
+      hc[12 * v + 3 + k] = cams[v].view[k];
+      hc[12 * v + 6 + k] = cams[v].right[k];
+      hc[12 * v + 9 + k] = cams[v].up[k];
+    }
+  EOS_CUDA(cudaMemcpyAsync(d_cams, hc.data(), hc.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  EOS_CUDA(cudaMemsetAsync(d_gmat, 0, 28ull * sc->dev.n_obj, ctx->stream));
+  EOS_CUDA(cudaMemsetAsync(d_glight, 0, 24ull * std::max(1, sc->dev.n_lights), ctx->stream));
+  BwArgs A;
+  A.s = sc->dev;
+  A.cams = d_cams;
+  A.w = cams[0].width;
+  A.h = cams[0].height;
+  A.n_views = (int)n_views;
+  A.trace_depth = p.trace_depth;
+  A.off = p.pixel_offset;
+  A.paths = d_paths;
+  A.drgb = d_rgb;
+  A.gmat = d_gmat;
+  A.glight = d_glight;
+  A.err = ctx->d_err;
+  long long total = (long long)A.w * A.h * n_views;
+  int grid = (int)((total + 127) / 128);
+  k_backward<<<grid, 128, 0, ctx->stream>>>(A);
+  EOS_CUDA(cudaGetLastError());
+  // the hc vector must outlive the async copy: wait for it
+  EOS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EOS_OK;
+}
+
+}  // namespace eos

@@ -1,0 +1,470 @@
+// C ABI of the render library (include/eos_c.h): argument checking, host/device buffer
+// staging, error words and statistics.  The kernels live in lbvh.cu, render.cu,
+// wavefront.cu and adjoint.cu.
+#include <algorithm>
+#include <cstring>
+
+#include "eos_internal.cuh"
+
+using namespace eos;
+
+eos_ctx::~eos_ctx() {
+  for (auto& kv : scratch)
+    if (kv.second.ptr) cudaFree(kv.second.ptr);
+  if (pinned) cudaFreeHost(pinned);
+  if (d_err) cudaFree(d_err);
+  if (d_counts) cudaFree(d_counts);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+namespace eos {
+
+void* scratch(eos_ctx* ctx, const char* name, size_t bytes, eos_status* st) {
+  DevBuffer& b = ctx->scratch[name];
+  if (b.bytes >= bytes && b.ptr) return b.ptr;
+  if (b.ptr) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 256);
+  if (cudaMalloc(&b.ptr, want) != cudaSuccess) {
+    cudaGetLastError();
+    b.ptr = nullptr;
+    if (st) *st = EOS_ERR_OOM;
+    return nullptr;
+  }
+  b.bytes = want;
+  return b.ptr;
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace eos
+
+namespace {
+
+// Device view of a caller buffer: device pointers pass through, host buffers are copied
+// into a named scratch buffer on the context stream.
+const void* stage_in(eos_ctx* ctx, const char* name, const void* p, size_t bytes, eos_status* st) {
+  if (!p || bytes == 0) return p;
+  if (is_device_ptr(p)) return p;
+  void* d = scratch(ctx, name, bytes, st);
+  if (!d) return nullptr;
+  if (cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+    *st = EOS_ERR_CUDA;
+    return nullptr;
+  }
+  return d;
+}
+
+struct OutBuf {
+  void* user = nullptr;
+  void* dev = nullptr;
+  size_t bytes = 0;
+  bool host = false;
+};
+
+eos_status out_buf(eos_ctx* ctx, const char* name, void* user, size_t bytes, OutBuf& o) {
+  o.user = user;
+  o.bytes = bytes;
+  if (!user) return EOS_OK;
+  if (is_device_ptr(user)) {
+    o.dev = user;
+    return EOS_OK;
+  }
+  eos_status st = EOS_OK;
+  o.dev = scratch(ctx, name, bytes, &st);
+  o.host = true;
+  return o.dev ? EOS_OK : st;
+}
+
+eos_status copy_out(eos_ctx* ctx, const OutBuf& o) {
+  if (o.user && o.host) EOS_CUDA(cudaMemcpyAsync(o.user, o.dev, o.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return EOS_OK;
+}
+
+// Clears the error word and counters before a call.
+eos_status begin_call(eos_ctx* ctx) {
+  ctx->launches = 0;
+  ctx->stage_ms[0] = ctx->stage_ms[1] = ctx->stage_ms[2] = 0.0f;
+  EOS_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+  EOS_CUDA(cudaMemsetAsync(ctx->d_counts, 0, kCounters * sizeof(unsigned long long), ctx->stream));
+  return EOS_OK;
+}
+
+eos_status err_to_status(int e) {
+  if (e & kErrStack) return EOS_ERR_STACK_OVERFLOW;
+  if (e & kErrQueue) return EOS_ERR_QUEUE_OVERFLOW;
+  if (e & kErrIndex) return EOS_ERR_INVALID_ARG;
+  if (e & kErrTimeout) return EOS_ERR_TIMEOUT;
+  if (e & kErrDepth) return EOS_ERR_STACK_OVERFLOW;
+  return EOS_OK;
+}
+
+// Waits for the call, reads the error word (and counters into stats).
+eos_status end_call(eos_ctx* ctx, eos_stats* stats) {
+  struct {
+    unsigned long long c[kCounters];
+    int err;
+  } h;
+  EOS_CUDA(cudaMemcpyAsync(h.c, ctx->d_counts, sizeof h.c, cudaMemcpyDeviceToHost, ctx->stream));
+  EOS_CUDA(cudaMemcpyAsync(&h.err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EOS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (stats) {
+    stats->primary_rays = h.c[0];
+    stats->shadow_rays = h.c[1];
+    stats->secondary_rays = h.c[2];
+    stats->nodes_closest = h.c[3];
+    stats->tests_closest = h.c[4];
+    stats->nodes_shadow = h.c[5];
+    stats->tests_shadow = h.c[6];
+    stats->shaded_hits = h.c[7];
+    stats->error_flags = h.err;
+    stats->kernel_launches = ctx->launches;
+    for (int k = 0; k < 3; ++k) stats->stage_ms[k] = ctx->stage_ms[k];
+  }
+  return err_to_status(h.err);
+}
+
+bool valid_camera(const eos_camera* c) {
+  return c && c->width > 0 && c->height > 0 && (long long)c->width * c->height <= (1ll << 28);
+}
+
+eos_status check_params(const eos_render_params* p) {
+  if (!p) return EOS_ERR_INVALID_ARG;
+  if (p->trace_depth < 0 || p->trace_depth >= EOS_MAX_BOUNCES) return EOS_ERR_INVALID_ARG;
+  if (p->spp < 1 || p->spp > 1024) return EOS_ERR_INVALID_ARG;
+  if (p->mode != EOS_MODE_PLAIN && p->mode != EOS_MODE_WAVEFRONT) return EOS_ERR_INVALID_ARG;
+  return EOS_OK;
+}
+
+eos_status set_device(eos_ctx* ctx) {
+  EOS_CUDA(cudaSetDevice(ctx->device));
+  return EOS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t eos_abi_version(void) { return EOS_ABI_VERSION; }
+
+const char* eos_status_string(eos_status s) {
+  switch (s) {
+    case EOS_OK: return "ok";
+    case EOS_ERR_INVALID_ARG: return "invalid argument";
+    case EOS_ERR_OOM: return "out of device memory";
+    case EOS_ERR_CUDA: return "CUDA error";
+    case EOS_ERR_TIMEOUT: return "device loop ran out of iterations";
+    case EOS_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+    case EOS_ERR_QUEUE_OVERFLOW: return "ray queue overflow";
+    case EOS_ERR_UNSUPPORTED: return "unsupported";
+    case EOS_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+eos_status eos_ctx_create(int32_t device, eos_ctx** out) {
+  if (!out) return EOS_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return EOS_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return EOS_ERR_INVALID_ARG;
+  eos_ctx* ctx = new eos_ctx();
+  ctx->device = device;
+  eos_status st = EOS_OK;
+  do {
+    if (cudaSetDevice(device) != cudaSuccess) { st = EOS_ERR_CUDA; break; }
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) { st = EOS_ERR_CUDA; break; }
+    ctx->stream = ctx->own_stream;
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) { st = EOS_ERR_CUDA; break; }
+    if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) { st = EOS_ERR_OOM; break; }
+    if (cudaMalloc(&ctx->d_counts, kCounters * sizeof(unsigned long long)) != cudaSuccess) { st = EOS_ERR_OOM; break; }
+    cudaMemset(ctx->d_err, 0, sizeof(int));
+    cudaMemset(ctx->d_counts, 0, kCounters * sizeof(unsigned long long));
+  } while (0);
+  if (st != EOS_OK) {
+    cudaGetLastError();
+    delete ctx;
+    return st;
+  }
+  *out = ctx;
+  return EOS_OK;
+}
+
+eos_status eos_ctx_destroy(eos_ctx* ctx) {
+  if (!ctx) return EOS_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+  return EOS_OK;
+}
+
+eos_status eos_ctx_set_stream(eos_ctx* ctx, void* stream) {
+  if (!ctx) return EOS_ERR_INVALID_ARG;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return EOS_OK;
+}
+
+eos_status eos_ctx_synchronize(eos_ctx* ctx) {
+  if (!ctx) return EOS_ERR_INVALID_ARG;
+  EOS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EOS_OK;
+}
+
+eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* normals, uint32_t n_verts,
+                            const uint32_t* tris, const uint32_t* tri_obj, uint32_t n_tris,
+                            const eos_material* materials, uint32_t n_materials, const eos_light* lights,
+                            uint32_t n_lights, const eos_build_params* build, eos_scene** out) {
+  if (!ctx || !out) return EOS_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (n_tris > 0 && (!verts || !normals || !tris || !tri_obj || n_verts == 0)) return EOS_ERR_INVALID_ARG;
+  if (n_tris > (1u << 28) || n_materials == 0 || !materials || n_lights > EOS_MAX_LIGHTS ||
+      (n_lights > 0 && !lights))
+    return EOS_ERR_INVALID_ARG;
+  int leaf = build && build->leaf_size > 0 ? build->leaf_size : 4;
+  if (leaf > 64) return EOS_ERR_INVALID_ARG;
+  eos_status st = set_device(ctx);
+  if (st != EOS_OK) return st;
+  eos_scene* sc = new eos_scene();
+  sc->ctx = ctx;
+  sc->leaf_size = leaf;
+  auto fail = [&](eos_status s) {
+    eos_scene_destroy(sc);
+    return s;
+  };
+  if ((st = begin_call(ctx)) != EOS_OK) return fail(st);
+  const float* dv = (const float*)stage_in(ctx, "in.verts", verts, 12ull * n_verts, &st);
+  const float* dn = (const float*)stage_in(ctx, "in.normals", normals, 12ull * n_verts, &st);
+  const uint32_t* dt = (const uint32_t*)stage_in(ctx, "in.tris", tris, 12ull * n_tris, &st);
+  const uint32_t* dob = (const uint32_t*)stage_in(ctx, "in.obj", tri_obj, 4ull * n_tris, &st);
+  if (st != EOS_OK) return fail(st);
+  if (cudaMalloc(&sc->d_mats, sizeof(eos_material) * n_materials) != cudaSuccess) return fail(EOS_ERR_OOM);
+  if (cudaMalloc(&sc->d_lights, sizeof(eos_light) * std::max<uint32_t>(1, n_lights)) != cudaSuccess)
+    return fail(EOS_ERR_OOM);
+  sc->device_bytes += sizeof(eos_material) * n_materials + sizeof(eos_light) * std::max<uint32_t>(1, n_lights);
+  sc->dev.n_obj = (int)n_materials;
+  sc->dev.n_lights = (int)n_lights;
+  sc->dev.n_tris = (int)n_tris;
+  if ((st = eos_scene_set_materials(sc, materials, n_materials)) != EOS_OK) return fail(st);
+  if (n_lights && (st = eos_scene_set_lights(sc, lights, n_lights)) != EOS_OK) return fail(st);
+  if ((st = build_scene(ctx, sc, dv, dn, n_verts, dt, dob, n_tris)) != EOS_OK) return fail(st);
+  sc->dev.nodes = (const float4*)sc->d_nodes;
+  sc->dev.tris = (const float4*)sc->d_tris;
+  sc->dev.shade = (const float4*)sc->d_shade;
+  sc->dev.pos_of_id = (const int32_t*)sc->d_pos_of_id;
+  sc->dev.mats = (const float*)sc->d_mats;
+  sc->dev.lights = (const float*)sc->d_lights;
+  if ((st = end_call(ctx, nullptr)) != EOS_OK) return fail(st);
+  // object ids must index the material table: checked on the device copy
+  {
+    std::vector<uint32_t> probe;
+    (void)probe;
+  }
+  *out = sc;
+  return EOS_OK;
+}
+
+eos_status eos_scene_destroy(eos_scene* sc) {
+  if (!sc) return EOS_ERR_INVALID_ARG;
+  if (sc->ctx) {
+    cudaSetDevice(sc->ctx->device);
+    cudaStreamSynchronize(sc->ctx->stream);
+  }
+  void* bufs[] = {sc->d_nodes, sc->d_tris, sc->d_shade, sc->d_pos_of_id, sc->d_mats, sc->d_lights, sc->d_codes,
+                  sc->d_order};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  delete sc;
+  return EOS_OK;
+}
+
+eos_status eos_scene_set_materials(eos_scene* sc, const eos_material* m, uint32_t n) {
+  if (!sc || !m || n != (uint32_t)sc->dev.n_obj) return EOS_ERR_INVALID_ARG;
+  EOS_CUDA(cudaSetDevice(sc->ctx->device));
+  cudaMemcpyKind kind = is_device_ptr(m) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  EOS_CUDA(cudaMemcpyAsync(sc->d_mats, m, sizeof(eos_material) * n, kind, sc->ctx->stream));
+  EOS_CUDA(cudaStreamSynchronize(sc->ctx->stream));
+  return EOS_OK;
+}
+
+eos_status eos_scene_set_lights(eos_scene* sc, const eos_light* l, uint32_t n) {
+  if (!sc || (!l && n) || n != (uint32_t)sc->dev.n_lights) return EOS_ERR_INVALID_ARG;
+  if (n == 0) return EOS_OK;
+  EOS_CUDA(cudaSetDevice(sc->ctx->device));
+  cudaMemcpyKind kind = is_device_ptr(l) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  EOS_CUDA(cudaMemcpyAsync(sc->d_lights, l, sizeof(eos_light) * n, kind, sc->ctx->stream));
+  EOS_CUDA(cudaStreamSynchronize(sc->ctx->stream));
+  return EOS_OK;
+}
+
+eos_status eos_scene_get_info(const eos_scene* sc, eos_scene_info* info) {
+  if (!sc || !info) return EOS_ERR_INVALID_ARG;
+  info->n_tris = (uint32_t)sc->dev.n_tris;
+  info->n_nodes = sc->n_nodes;
+  info->leaf_size = (uint32_t)sc->leaf_size;
+  info->n_objects = (uint32_t)sc->dev.n_obj;
+  info->n_lights = (uint32_t)sc->dev.n_lights;
+  info->build_ms = sc->build_ms;
+  info->device_bytes = sc->device_bytes;
+  return EOS_OK;
+}
+
+eos_status eos_scene_get_morton(const eos_scene* sc, uint32_t* codes, uint32_t* order) {
+  if (!sc) return EOS_ERR_INVALID_ARG;
+  EOS_CUDA(cudaSetDevice(sc->ctx->device));
+  size_t b = 4ull * sc->dev.n_tris;
+  if (b == 0) return EOS_OK;
+  if (codes) EOS_CUDA(cudaMemcpyAsync(codes, sc->d_codes, b, cudaMemcpyDefault, sc->ctx->stream));
+  if (order) EOS_CUDA(cudaMemcpyAsync(order, sc->d_order, b, cudaMemcpyDefault, sc->ctx->stream));
+  EOS_CUDA(cudaStreamSynchronize(sc->ctx->stream));
+  return EOS_OK;
+}
+
+eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, const eos_render_params* p,
+                      float* rgb_out, uint8_t* rgba8_out, int32_t* hit_out, eos_path_record* paths_out,
+                      eos_stats* stats) {
+  if (!ctx || !sc || !valid_camera(cam)) return EOS_ERR_INVALID_ARG;
+  eos_status st = check_params(p);
+  if (st != EOS_OK) return st;
+  if ((st = set_device(ctx)) != EOS_OK) return st;
+  const size_t npx = (size_t)cam->width * cam->height;
+  const size_t npath = npx * p->spp;
+  OutBuf o_rgb, o_q, o_hit, o_paths;
+  if ((st = out_buf(ctx, "out.rgb", rgb_out, 12 * npx, o_rgb)) != EOS_OK) return st;
+  if ((st = out_buf(ctx, "out.rgba8", rgba8_out, 4 * npx, o_q)) != EOS_OK) return st;
+  if ((st = out_buf(ctx, "out.hit", hit_out, 4 * npath, o_hit)) != EOS_OK) return st;
+  if ((st = out_buf(ctx, "out.paths", paths_out, sizeof(eos_path_record) * npath, o_paths)) != EOS_OK) return st;
+  if ((st = begin_call(ctx)) != EOS_OK) return st;
+  EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (p->mode == EOS_MODE_PLAIN) {
+    st = render_plain(ctx, sc, *cam, *p, (float*)o_rgb.dev, (uint8_t*)o_q.dev, (int32_t*)o_hit.dev,
+                      (eos_path_record*)o_paths.dev);
+  } else {
+    if (hit_out) return EOS_ERR_UNSUPPORTED;  // per-path hits come from paths_out in this mode
+    eos_job job;
+    job.scene = sc;
+    job.camera = *cam;
+    job.trace_depth = p->trace_depth;
+    job.pixel_offset = p->pixel_offset;
+    job.spp = p->spp;
+    job.jitter_seed = p->jitter_seed;
+    job.rgb_out = (float*)o_rgb.dev;
+    job.rgba8_out = (uint8_t*)o_q.dev;
+    job.paths_out = (eos_path_record*)o_paths.dev;
+    st = render_wavefront(ctx, &job, 1, *p, false);
+  }
+  if (st != EOS_OK) return st;
+  EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  if ((st = copy_out(ctx, o_rgb)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, o_q)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, o_hit)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, o_paths)) != EOS_OK) return st;
+  st = end_call(ctx, stats);
+  if (stats) cudaEventElapsedTime(&stats->gpu_ms, ctx->ev0, ctx->ev1);
+  return st;
+}
+
+eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, const eos_render_params* p,
+                            eos_stats* stats) {
+  if (!ctx || !jobs || n_jobs == 0) return EOS_ERR_INVALID_ARG;
+  eos_status st = check_params(p);
+  if (st != EOS_OK) return st;
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const eos_job& jb = jobs[j];
+    if (!jb.scene || !valid_camera(&jb.camera) || jb.trace_depth < 0 || jb.trace_depth >= EOS_MAX_BOUNCES ||
+        jb.spp < 1 || jb.spp > 1024)
+      return EOS_ERR_INVALID_ARG;
+    if ((jb.rgb_out && !is_device_ptr(jb.rgb_out)) || (jb.rgba8_out && !is_device_ptr(jb.rgba8_out)) ||
+        (jb.paths_out && !is_device_ptr(jb.paths_out)))
+      return EOS_ERR_INVALID_ARG;
+  }
+  if ((st = set_device(ctx)) != EOS_OK) return st;
+  if ((st = begin_call(ctx)) != EOS_OK) return st;
+  EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  st = render_wavefront(ctx, jobs, n_jobs, *p, (p->flags & EOS_FLAG_STAGE_TIMING) == 0);
+  if (st != EOS_OK) return st;
+  EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  st = end_call(ctx, stats);
+  if (stats) cudaEventElapsedTime(&stats->gpu_ms, ctx->ev0, ctx->ev1);
+  return st;
+}
+
+eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cams, uint32_t n_views,
+                               const eos_render_params* p, const eos_path_record* paths, const float* d_rgb,
+                               eos_grads* grads) {
+  if (!ctx || !sc || !cams || n_views == 0 || !paths || !d_rgb || !grads || !grads->materials || !grads->lights)
+    return EOS_ERR_INVALID_ARG;
+  eos_status st = check_params(p);
+  if (st != EOS_OK) return st;
+  if (p->spp != 1) return EOS_ERR_UNSUPPORTED;
+  for (uint32_t v = 0; v < n_views; ++v)
+    if (!valid_camera(&cams[v]) || cams[v].width != cams[0].width || cams[v].height != cams[0].height)
+      return EOS_ERR_INVALID_ARG;
+  if ((st = set_device(ctx)) != EOS_OK) return st;
+  const size_t npx = (size_t)n_views * cams[0].width * cams[0].height;
+  if ((st = begin_call(ctx)) != EOS_OK) return st;
+  const eos_path_record* dp =
+      (const eos_path_record*)stage_in(ctx, "bw.paths", paths, sizeof(eos_path_record) * npx, &st);
+  const float* dg = (const float*)stage_in(ctx, "bw.drgb", d_rgb, 12 * npx, &st);
+  if (st != EOS_OK) return st;
+  OutBuf o_m, o_l;
+  if ((st = out_buf(ctx, "bw.gm", grads->materials, 28ull * sc->dev.n_obj, o_m)) != EOS_OK) return st;
+  if ((st = out_buf(ctx, "bw.gl", grads->lights, 24ull * std::max(1, sc->dev.n_lights), o_l)) != EOS_OK) return st;
+  EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  st = render_backward(ctx, sc, cams, n_views, *p, dp, dg, (float*)o_m.dev, (float*)o_l.dev);
+  if (st != EOS_OK) return st;
+  EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  if ((st = copy_out(ctx, o_m)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, o_l)) != EOS_OK) return st;
+  return end_call(ctx, nullptr);
+}
+
+eos_status eos_trace_closest(eos_ctx* ctx, const eos_scene* sc, const float* rays, uint32_t n, int32_t* ids,
+                             float* t) {
+  if (!ctx || !sc || (n && (!rays || !ids))) return EOS_ERR_INVALID_ARG;
+  eos_status st = set_device(ctx);
+  if (st != EOS_OK) return st;
+  if ((st = begin_call(ctx)) != EOS_OK) return st;
+  const float* dr = (const float*)stage_in(ctx, "q.rays", rays, 24ull * n, &st);
+  if (st != EOS_OK) return st;
+  OutBuf oi, ot;
+  if ((st = out_buf(ctx, "q.ids", ids, 4ull * n, oi)) != EOS_OK) return st;
+  if ((st = out_buf(ctx, "q.t", t, 4ull * n, ot)) != EOS_OK) return st;
+  if ((st = trace_closest(ctx, sc, dr, n, (int32_t*)oi.dev, (float*)ot.dev)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, oi)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, ot)) != EOS_OK) return st;
+  return end_call(ctx, nullptr);
+}
+
+eos_status eos_trace_any(eos_ctx* ctx, const eos_scene* sc, const float* rays, uint32_t n, uint8_t* occluded) {
+  if (!ctx || !sc || (n && (!rays || !occluded))) return EOS_ERR_INVALID_ARG;
+  eos_status st = set_device(ctx);
+  if (st != EOS_OK) return st;
+  if ((st = begin_call(ctx)) != EOS_OK) return st;
+  const float* dr = (const float*)stage_in(ctx, "q.rays", rays, 24ull * n, &st);
+  if (st != EOS_OK) return st;
+  OutBuf oo;
+  if ((st = out_buf(ctx, "q.occ", occluded, n, oo)) != EOS_OK) return st;
+  if ((st = trace_any(ctx, sc, dr, n, (uint8_t*)oo.dev)) != EOS_OK) return st;
+  if ((st = copy_out(ctx, oo)) != EOS_OK) return st;
+  return end_call(ctx, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// Internal types of the render library: device scene layout, context and error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/eos_c.h"
+#include "eos_math.cuh"
+
+namespace eos {
+
+constexpr int kMaxBounces = EOS_MAX_BOUNCES;
+constexpr int kMaxLights = EOS_MAX_LIGHTS;
+constexpr int kStackMax = 64;  // >= LBVH depth bound: 30 code bits + 32 index bits + 2
+constexpr float kInf = __builtin_huge_valf();
+constexpr int kCounters = 8;  // ray / traversal counters per call (see trace.cuh)
+
+// Device error word bits (atomicOr'ed by kernels, read back by the host).
+enum : int {
+  kErrStack = 1 << 0,
+  kErrQueue = 1 << 1,
+  kErrIndex = 1 << 2,
+  kErrTimeout = 1 << 3,
+  kErrDepth = 1 << 4,
+};
+
+// ---------------------------------------------------------------------------------
+// HBM layout of a scene (all 16-byte aligned, read with 128-bit loads):
+//
+//  BVH node, 64 B = 4 x float4, both children's boxes in the parent:
+//    [0] c0.lo.x c0.lo.y c0.lo.z c0.hi.x
+//    [1] c0.hi.y c0.hi.z c1.lo.x c1.lo.y
+//    [2] c1.lo.z c1.hi.x c1.hi.y c1.hi.z
+//    [3] ref0 ref1 count0 count1          (int)
+//  count > 0: leaf, triangles [ref, ref + count) in sorted order
+//  count == 0: interior node `ref`;  count < 0: empty child
+//
+//  Triangle record (intersection), 48 B = 3 x float4, sorted (Morton) order:
+//    [0] v1.x v1.y v1.z e1.x   [1] e1.y e1.z e2.x e2.y   [2] e2.z id(int) - -
+//  Shading record, 48 B = 3 x float4, same order:
+//    [0] n1.x n1.y n1.z n2.x   [1] n2.y n2.z n3.x n3.y   [2] n3.z obj(int) - -
+// ---------------------------------------------------------------------------------
+struct DevScene {
+  const float4* nodes;
+  const float4* tris;
+  const float4* shade;
+  const int32_t* pos_of_id;  // triangle id -> sorted position
+  const float* mats;         // n_obj x 8: kd rgb, ks rgb, shininess, reflectivity
+  const float* lights;       // n_lights x 6: position xyz, colour rgb
+  int32_t n_tris;
+  int32_t n_obj;
+  int32_t n_lights;
+  int32_t pad;
+};
+
+struct DevBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace eos
+
+struct eos_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int* d_err = nullptr;                   // device error word
+  unsigned long long* d_counts = nullptr; // ray / traversal counters [kCounters]
+  std::map<std::string, eos::DevBuffer> scratch;
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  // per-call bookkeeping reported in eos_stats
+  uint32_t launches = 0;
+  float stage_ms[3] = {0, 0, 0};
+  // batched-render graph cache: one instantiated graph per batch shape
+  struct BatchGraph {
+    std::vector<long long> key;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t launches = 0;  // kernel nodes in the graph
+    ~BatchGraph() {
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+  };
+  std::vector<std::unique_ptr<BatchGraph>> graphs;
+  ~eos_ctx();
+};
+
+struct eos_scene {
+  eos_ctx* ctx = nullptr;
+  eos::DevScene dev{};
+  void* d_nodes = nullptr;
+  void* d_tris = nullptr;
+  void* d_shade = nullptr;
+  void* d_pos_of_id = nullptr;
+  void* d_mats = nullptr;
+  void* d_lights = nullptr;
+  void* d_codes = nullptr;  // sorted Morton codes (kept for the test hook)
+  void* d_order = nullptr;  // sorted triangle ids
+  uint32_t n_nodes = 0;
+  int leaf_size = 4;
+  float build_ms = 0.0f;
+  size_t device_bytes = 0;
+};
+
+namespace eos {
+
+// Scratch buffers owned by the context, grown on demand and reused across calls.
+void* scratch(eos_ctx* ctx, const char* name, size_t bytes, eos_status* st);
+// Pointer classification (cudaPointerGetAttributes): true for device/managed memory.
+bool is_device_ptr(const void* p);
+
+// LBVH build (lbvh.cu).  verts/normals/tris/tri_obj are device pointers.
+eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const float* d_normals,
+                       uint32_t n_verts, const uint32_t* d_tris, const uint32_t* d_obj, uint32_t n_tris);
+
+// Renderers (render.cu).
+struct RenderArgs {
+  const float* cam;  // 12 floats, device-visible via kernel params copy
+  int width, height;
+  int trace_depth;
+  float pixel_offset;
+  int spp;
+  uint32_t jitter_seed;
+  float* rgb;
+  uint8_t* rgba8;
+  int32_t* hit;
+  eos_path_record* paths;
+};
+eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam,
+                        const eos_render_params& p, float* rgb, uint8_t* rgba8, int32_t* hit,
+                        eos_path_record* paths);
+eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs,
+                            const eos_render_params& p, bool use_graph);
+eos_status trace_closest(eos_ctx* ctx, const eos_scene* sc, const float* d_rays, uint32_t n,
+                         int32_t* d_ids, float* d_t);
+eos_status trace_any(eos_ctx* ctx, const eos_scene* sc, const float* d_rays, uint32_t n,
+                     uint8_t* d_occ);
+eos_status render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cams, uint32_t n_views,
+                           const eos_render_params& p, const eos_path_record* d_paths,
+                           const float* d_rgb, float* d_gmat, float* d_glight);
+
+}  // namespace eos
+
+#define EOS_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) {                             \
+      if (e_ == cudaErrorMemoryAllocation) return EOS_ERR_OOM; \
+      return EOS_ERR_CUDA;                               \
+    }                                                    \
+  } while (0)

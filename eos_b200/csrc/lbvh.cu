@@ -1,0 +1,413 @@
+// GPU LBVH build: Morton codes -> stable radix sort -> Karras hierarchy -> atomic refit
+// -> 64-byte node / 48-byte triangle records.
+//
+// Replaces the reference's CPU top-down median/SAH build (src/BVH.cpp:97-111,549-606) and
+// its SoA upload (src/cudaStructures.cu:36-174,274-405).  The Morton encoder is the
+// reference's 30-bit EncodeMorton3 (src/morton.h:45-48); the centroid is the reference
+// triangle centroid ((v1 + v2) + v3) / 3 (src/Triangle.h:37), quantised per axis over the
+// centroid bounds as q = min(1023, (uint)((1024 * (c - lo)) / (hi - lo))).
+// Primitive order = stable sort by (code, triangle id).
+#include <algorithm>
+
+#include "eos_internal.cuh"
+
+namespace eos {
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per block
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+__device__ __forceinline__ uint32_t float_to_ordered(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ordered_to_float(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ __forceinline__ f3 load_vert(const float* v, uint32_t i) {
+  return mk3(v[3 * (size_t)i], v[3 * (size_t)i + 1], v[3 * (size_t)i + 2]);
+}
+
+// Centroids and their bounds.  bounds: [6] ordered uints (min xyz, max xyz).
+__global__ void k_centroids(const float* __restrict__ verts, uint32_t n_verts,
+                            const uint32_t* __restrict__ tris, int n, float4* __restrict__ cent,
+                            uint32_t* __restrict__ bounds, int* err) {
+  float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t a = tris[3 * (size_t)i], b = tris[3 * (size_t)i + 1], c = tris[3 * (size_t)i + 2];
+    if (a >= n_verts || b >= n_verts || c >= n_verts) {
+      atomicOr(err, kErrIndex);
+      a = b = c = 0;
+    }
+    f3 s = add3(add3(load_vert(verts, a), load_vert(verts, b)), load_vert(verts, c));
+    f3 m = mk3(s.x / 3.0f, s.y / 3.0f, s.z / 3.0f);
+    cent[i] = make_float4(m.x, m.y, m.z, 0.0f);
+    lo[0] = fminf(lo[0], m.x); lo[1] = fminf(lo[1], m.y); lo[2] = fminf(lo[2], m.z);
+    hi[0] = fmaxf(hi[0], m.x); hi[1] = fmaxf(hi[1], m.y); hi[2] = fmaxf(hi[2], m.z);
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 3; ++k) {
+      if (lo[k] <= hi[k]) {
+        atomicMin(&bounds[k], float_to_ordered(lo[k]));
+        atomicMax(&bounds[3 + k], float_to_ordered(hi[k]));
+      }
+    }
+  }
+}
+
+__global__ void k_morton(const float4* __restrict__ cent, int n, const uint32_t* __restrict__ bounds,
+                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 c = cent[i];
+  float cc[3] = {c.x, c.y, c.z};
+  uint32_t q[3];
+  for (int k = 0; k < 3; ++k) {
+    float lo = ordered_to_float(bounds[k]);
+    float hi = ordered_to_float(bounds[3 + k]);
+    float ext = hi - lo;
+    if (ext > 0.0f) {
+      float f = (1024.0f * (cc[k] - lo)) / ext;
+      uint32_t u = (uint32_t)f;
+      q[k] = u > 1023u ? 1023u : u;
+    } else {
+      q[k] = 0u;
+    }
+  }
+  keys[i] = morton3(q[0], q[1], q[2]);
+  vals[i] = (uint32_t)i;
+}
+
+// ------------------------------------------------------------------ stable LSD radix sort
+// Per pass: per-tile digit histogram -> per-digit exclusive scan over tiles -> scan of the
+// digit totals -> stable scatter.  Inside a tile, warp w owns keys [w*256, w*256+256) in
+// 8 rounds of 32; peers with the same digit are found with __match_any_sync and ranked
+// with popc, so the scatter keeps the input order (stability gives the (code, id) order).
+__global__ void k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift, uint32_t* __restrict__ counts,
+                            int n_tiles) {
+  __shared__ uint32_t h[kRadix];
+  for (int i = threadIdx.x; i < kRadix; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  int base = blockIdx.x * kSortTile;
+  for (int j = threadIdx.x; j < kSortTile; j += blockDim.x) {
+    int idx = base + j;
+    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & (kRadix - 1)], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) counts[(size_t)d * n_tiles + blockIdx.x] = h[d];
+}
+
+// One block per digit: exclusive scan of that digit's per-tile counts (in place).
+__global__ void k_sort_scan_rows(uint32_t* __restrict__ counts, int n_tiles, uint32_t* __restrict__ totals) {
+  __shared__ uint32_t s[kSortThreads];
+  __shared__ uint32_t carry;
+  uint32_t* row = counts + (size_t)blockIdx.x * n_tiles;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b = 0; b < n_tiles; b += blockDim.x) {
+    int i = b + threadIdx.x;
+    uint32_t v = i < n_tiles ? row[i] : 0u;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < blockDim.x; off <<= 1) {
+      uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    uint32_t incl = s[threadIdx.x];
+    if (i < n_tiles) row[i] = carry + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+__global__ void k_sort_scan_digits(uint32_t* __restrict__ totals) {
+  __shared__ uint32_t s[kRadix];
+  uint32_t v = totals[threadIdx.x];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < kRadix; off <<= 1) {
+    uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  totals[threadIdx.x] = s[threadIdx.x] - v;
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(
+    const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+    uint32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ counts, int n_tiles,
+    const uint32_t* __restrict__ digit_base) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t wh[kWarps][kRadix];
+  __shared__ uint32_t tile_base[kRadix];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kWarps * kRadix; i += blockDim.x) (&wh[0][0])[i] = 0;
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x)
+    tile_base[d] = digit_base[d] + counts[(size_t)d * n_tiles + blockIdx.x];
+  __syncthreads();
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t key[kSortItems], val[kSortItems], local[kSortItems];
+  int base = blockIdx.x * kSortTile + w * 32 * kSortItems;
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    int idx = base + r * 32 + lane;
+    bool valid = idx < n;
+    key[r] = valid ? kin[idx] : 0u;
+    val[r] = valid ? vin[idx] : 0u;
+    uint32_t digit = valid ? ((key[r] >> shift) & (kRadix - 1)) : (uint32_t)kRadix + lane;
+    uint32_t peers = __match_any_sync(0xffffffffu, digit);
+    uint32_t rank = __popc(peers & lt_mask);
+    uint32_t pre = valid ? wh[w][digit] : 0u;
+    __syncwarp();
+    if (valid && rank == 0) wh[w][digit] = pre + __popc(peers);
+    __syncwarp();
+    local[r] = pre + rank;
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+    uint32_t s = 0;
+    for (int ww = 0; ww < kWarps; ++ww) {
+      uint32_t t = wh[ww][d];
+      wh[ww][d] = s;
+      s += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    int idx = base + r * 32 + lane;
+    if (idx < n) {
+      uint32_t digit = (key[r] >> shift) & (kRadix - 1);
+      uint32_t pos = tile_base[digit] + wh[w][digit] + local[r];
+      kout[pos] = key[r];
+      vout[pos] = val[r];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ Karras hierarchy
+__device__ __forceinline__ int common_prefix(const uint32_t* __restrict__ k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = k[i], b = k[j];
+  if (a == b) return 32 + __clz((uint32_t)(i ^ j));
+  return __clz(a ^ b);
+}
+
+// Internal node i of n-1 (Karras 2012, "Maximizing parallelism in the construction of
+// BVHs, octrees and k-d trees").  Node numbering: interior 0..n-2, leaf p -> n-1+p.
+__global__ void k_karras(const uint32_t* __restrict__ k, int n, int2* __restrict__ child,
+                         int2* __restrict__ range, int* __restrict__ parent) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = (common_prefix(k, n, i, i + 1) - common_prefix(k, n, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = common_prefix(k, n, i, i - d);
+  int lmax = 2;
+  while (common_prefix(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (common_prefix(k, n, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int dnode = common_prefix(k, n, i, j);
+  int s = 0;
+  int t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (common_prefix(k, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  int gamma = i + s * d + min(d, 0);
+  int first = min(i, j), last = max(i, j);
+  int left = (first == gamma) ? (n - 1 + gamma) : gamma;
+  int right = (last == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
+  child[i] = make_int2(left, right);
+  range[i] = make_int2(first, last);
+  parent[left] = i;
+  parent[right] = i;
+}
+
+// Triangle records in sorted order, leaf boxes, id -> position map.
+__global__ void k_records(const float* __restrict__ verts, const float* __restrict__ normals, uint32_t n_verts,
+                          const uint32_t* __restrict__ tris, const uint32_t* __restrict__ obj,
+                          const uint32_t* __restrict__ order, int n, uint32_t n_obj, float4* __restrict__ trec,
+                          float4* __restrict__ srec, int32_t* __restrict__ pos_of_id, float4* __restrict__ blo,
+                          float4* __restrict__ bhi, int* err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  uint32_t id = order[p];
+  uint32_t a = tris[3 * (size_t)id], b = tris[3 * (size_t)id + 1], c = tris[3 * (size_t)id + 2];
+  if (a >= n_verts || b >= n_verts || c >= n_verts) a = b = c = 0;  // flagged in k_centroids
+  f3 v1 = load_vert(verts, a), v2 = load_vert(verts, b), v3 = load_vert(verts, c);
+  f3 e1 = sub3(v2, v1), e2 = sub3(v3, v1);
+  trec[3 * (size_t)p] = make_float4(v1.x, v1.y, v1.z, e1.x);
+  trec[3 * (size_t)p + 1] = make_float4(e1.y, e1.z, e2.x, e2.y);
+  trec[3 * (size_t)p + 2] = make_float4(e2.z, __int_as_float((int)id), 0.0f, 0.0f);
+  f3 n1 = load_vert(normals, a), n2 = load_vert(normals, b), n3 = load_vert(normals, c);
+  srec[3 * (size_t)p] = make_float4(n1.x, n1.y, n1.z, n2.x);
+  srec[3 * (size_t)p + 1] = make_float4(n2.y, n2.z, n3.x, n3.y);
+  uint32_t ob = obj[id];
+  if (ob >= n_obj) {
+    atomicOr(err, kErrIndex);
+    ob = 0;
+  }
+  srec[3 * (size_t)p + 2] = make_float4(n3.z, __int_as_float((int)ob), 0.0f, 0.0f);
+  pos_of_id[id] = p;
+  size_t leaf = (size_t)(n - 1) + p;
+  blo[leaf] = make_float4(fminf(fminf(v1.x, v2.x), v3.x), fminf(fminf(v1.y, v2.y), v3.y),
+                          fminf(fminf(v1.z, v2.z), v3.z), 0.0f);
+  bhi[leaf] = make_float4(fmaxf(fmaxf(v1.x, v2.x), v3.x), fmaxf(fmaxf(v1.y, v2.y), v3.y),
+                          fmaxf(fmaxf(v1.z, v2.z), v3.z), 0.0f);
+}
+
+__device__ __forceinline__ void child_ref(int c, int n, const int2* __restrict__ range, int leaf_size, int& ref,
+                                          int& cnt) {
+  if (c >= n - 1) {
+    ref = c - (n - 1);
+    cnt = 1;
+    return;
+  }
+  int2 r = range[c];
+  int size = r.y - r.x + 1;
+  if (size <= leaf_size) {
+    ref = r.x;
+    cnt = size;
+  } else {
+    ref = c;
+    cnt = 0;
+  }
+}
+
+// Bottom-up refit: one thread per leaf walks to the root; the second thread to reach an
+// interior node merges the two child boxes and writes the node record.  Bounded walk:
+// the tree depth is at most kStackMax.
+__global__ void k_refit(int n, const int2* __restrict__ child, const int2* __restrict__ range,
+                        const int* __restrict__ parent, float4* blo, float4* bhi, int* __restrict__ arrive,
+                        float4* __restrict__ nodes, int leaf_size, int* err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  int node = parent[n - 1 + p];
+  for (int step = 0; node >= 0; ++step) {
+    if (step > kStackMax) {
+      atomicOr(err, kErrDepth);
+      return;
+    }
+    __threadfence();
+    if (atomicAdd(&arrive[node], 1) == 0) return;
+    __threadfence();
+    int2 c = child[node];
+    float4 l0 = __ldcg(&blo[c.x]), h0 = __ldcg(&bhi[c.x]);
+    float4 l1 = __ldcg(&blo[c.y]), h1 = __ldcg(&bhi[c.y]);
+    blo[node] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+    bhi[node] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+    int r0, n0, r1, n1;
+    child_ref(c.x, n, range, leaf_size, r0, n0);
+    child_ref(c.y, n, range, leaf_size, r1, n1);
+    float4* o = nodes + 4 * (size_t)node;
+    o[0] = make_float4(l0.x, l0.y, l0.z, h0.x);
+    o[1] = make_float4(h0.y, h0.z, l1.x, l1.y);
+    o[2] = make_float4(l1.z, h1.x, h1.y, h1.z);
+    o[3] = make_float4(__int_as_float(r0), __int_as_float(r1), __int_as_float(n0), __int_as_float(n1));
+    node = parent[node];
+  }
+}
+
+// Root record for scenes of 0 or 1 triangle (no interior node exists).
+__global__ void k_small_root(int n, const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                             float4* __restrict__ nodes) {
+  float4 l = n == 1 ? blo[0] : make_float4(0, 0, 0, 0);
+  float4 h = n == 1 ? bhi[0] : make_float4(0, 0, 0, 0);
+  nodes[0] = make_float4(l.x, l.y, l.z, h.x);
+  nodes[1] = make_float4(h.y, h.z, 0.0f, 0.0f);
+  nodes[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  nodes[3] = make_float4(__int_as_float(0), __int_as_float(0), __int_as_float(n == 1 ? 1 : -1), __int_as_float(-1));
+}
+
+inline int grid_for(size_t n, int block) { return (int)std::max<size_t>(1, (n + block - 1) / block); }
+
+}  // namespace
+
+eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const float* d_normals,
+                       uint32_t n_verts, const uint32_t* d_tris, const uint32_t* d_obj, uint32_t n_tris) {
+  cudaStream_t st = ctx->stream;
+  const int n = (int)n_tris;
+  const size_t nn = std::max<size_t>(1, n);
+  eos_status es = EOS_OK;
+  const size_t n_nodes = std::max<size_t>(1, nn - 1);
+  // persistent scene buffers
+  EOS_CUDA(cudaMalloc(&sc->d_nodes, 64 * n_nodes));
+  EOS_CUDA(cudaMalloc(&sc->d_tris, 48 * nn));
+  EOS_CUDA(cudaMalloc(&sc->d_shade, 48 * nn));
+  EOS_CUDA(cudaMalloc(&sc->d_pos_of_id, 4 * nn));
+  EOS_CUDA(cudaMalloc(&sc->d_codes, 4 * nn));
+  EOS_CUDA(cudaMalloc(&sc->d_order, 4 * nn));
+  sc->device_bytes += 64 * n_nodes + 48 * nn * 2 + 4 * nn * 3;
+  sc->n_nodes = (uint32_t)n_nodes;
+  // temporaries
+  float4* cent = (float4*)scratch(ctx, "lbvh.cent", 16 * nn, &es);
+  uint32_t* bounds = (uint32_t*)scratch(ctx, "lbvh.bounds", 64, &es);
+  uint32_t* k2 = (uint32_t*)scratch(ctx, "lbvh.k2", 4 * nn, &es);
+  uint32_t* v2 = (uint32_t*)scratch(ctx, "lbvh.v2", 4 * nn, &es);
+  const int n_tiles = (int)((nn + kSortTile - 1) / kSortTile);
+  uint32_t* counts = (uint32_t*)scratch(ctx, "lbvh.counts", 4 * (size_t)kRadix * n_tiles, &es);
+  uint32_t* totals = (uint32_t*)scratch(ctx, "lbvh.totals", 4 * kRadix, &es);
+  int2* child = (int2*)scratch(ctx, "lbvh.child", 8 * n_nodes, &es);
+  int2* range = (int2*)scratch(ctx, "lbvh.range", 8 * n_nodes, &es);
+  int* parent = (int*)scratch(ctx, "lbvh.parent", 4 * (2 * nn), &es);
+  int* arrive = (int*)scratch(ctx, "lbvh.arrive", 4 * n_nodes, &es);
+  float4* blo = (float4*)scratch(ctx, "lbvh.blo", 16 * (2 * nn), &es);
+  float4* bhi = (float4*)scratch(ctx, "lbvh.bhi", 16 * (2 * nn), &es);
+  if (es != EOS_OK) return es;
+
+  uint32_t* keys = (uint32_t*)sc->d_codes;
+  uint32_t* vals = (uint32_t*)sc->d_order;
+  EOS_CUDA(cudaEventRecord(ctx->ev0, st));
+  if (n > 0) {
+    uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    EOS_CUDA(cudaMemcpyAsync(bounds, init, sizeof init, cudaMemcpyHostToDevice, st));
+    int g = std::min(grid_for(nn, 256), ctx->num_sms * 8);
+    k_centroids<<<g, 256, 0, st>>>(d_verts, n_verts, d_tris, n, cent, bounds, ctx->d_err);
+    k_morton<<<grid_for(nn, 256), 256, 0, st>>>(cent, n, bounds, keys, vals);
+    uint32_t *ki = keys, *vi = vals, *ko = k2, *vo = v2;
+    for (int shift = 0; shift < 30; shift += kRadixBits) {
+      k_sort_hist<<<n_tiles, kSortThreads, 0, st>>>(ki, n, shift, counts, n_tiles);
+      k_sort_scan_rows<<<kRadix, kSortThreads, 0, st>>>(counts, n_tiles, totals);
+      k_sort_scan_digits<<<1, kRadix, 0, st>>>(totals);
+      k_sort_scatter<<<n_tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n, shift, counts, n_tiles, totals);
+      std::swap(ki, ko);
+      std::swap(vi, vo);
+    }
+    // 4 passes: the sorted result is back in (keys, vals)
+    k_records<<<grid_for(nn, 256), 256, 0, st>>>(d_verts, d_normals, n_verts, d_tris, d_obj, vals, n,
+                                                 (uint32_t)sc->dev.n_obj, (float4*)sc->d_tris, (float4*)sc->d_shade,
+                                                 (int32_t*)sc->d_pos_of_id, blo, bhi, ctx->d_err);
+  }
+  if (n >= 2) {
+    EOS_CUDA(cudaMemsetAsync(parent, 0xff, 4 * (2 * nn), st));
+    EOS_CUDA(cudaMemsetAsync(arrive, 0, 4 * n_nodes, st));
+    k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys, n, child, range, parent);
+    k_refit<<<grid_for(nn, 256), 256, 0, st>>>(n, child, range, parent, blo, bhi, arrive,
+                                              (float4*)sc->d_nodes, sc->leaf_size, ctx->d_err);
+  } else {
+    k_small_root<<<1, 1, 0, st>>>(n, blo, bhi, (float4*)sc->d_nodes);
+  }
+  EOS_CUDA(cudaGetLastError());
+  EOS_CUDA(cudaEventRecord(ctx->ev1, st));
+  EOS_CUDA(cudaEventSynchronize(ctx->ev1));
+  EOS_CUDA(cudaEventElapsedTime(&sc->build_ms, ctx->ev0, ctx->ev1));
+  return EOS_OK;
+}
+
+}  // namespace eos

@@ -1,0 +1,288 @@
+// BVH traversal and shading device functions (header-only; included by the kernel TUs).
+//
+// Nearest hit = the smallest t >= 0 over all triangles, exact ties resolved to the larger
+// triangle id.  This is the reference's result (src/BVH.cpp:609-659 keeps t <= best
+// through Triangle::hit, src/Triangle.cpp:37-38) without its dependence on one particular
+// tree: the reference keeps the later of two equal hits in its own traversal order.
+// Shadow rays = any triangle hit at t >= 0 (src/BVH.cpp:661-716 with the uninitialised
+// distance at :703 read as FLT_MAX).
+//
+// Box tests are conservative so that culling never removes the exact answer:
+//  * slab far distances are widened by 1 + 2*gamma(3) (rounding of (b - o) * (1/d));
+//  * a box is culled against the current best t only beyond best * (1 + 2^-12), a margin
+//    for the rounding of the triangle test's own t;
+//  * a direction component with |d| < 1e-30 is treated as parallel: its slab is the whole
+//    line when the origin lies inside the closed slab and empty otherwise (the
+//    reference's (b - o) * inf turns into NaN there, src/Box.cu:234-255).
+#pragma once
+#include "eos_internal.cuh"
+
+namespace eos {
+
+constexpr float kSlack = 1.0000004f;           // 1 + 2*gamma(3)
+constexpr float kCull = 1.000244140625f;       // 1 + 2^-12
+constexpr float kParallelEps = 1e-30f;
+constexpr float kRayEps = 1e-3f;               // shadow / mirror ray offset, src/RayTracer.cpp:305
+
+struct SlabRay {
+  float ox, oy, oz, ix, iy, iz;
+  bool par;
+};
+
+__device__ __forceinline__ SlabRay make_slab(f3 o, f3 d) {
+  SlabRay r;
+  r.ox = o.x; r.oy = o.y; r.oz = o.z;
+  bool px = fabsf(d.x) < kParallelEps, py = fabsf(d.y) < kParallelEps, pz = fabsf(d.z) < kParallelEps;
+  r.ix = px ? 0.0f : 1.0f / d.x;
+  r.iy = py ? 0.0f : 1.0f / d.y;
+  r.iz = pz ? 0.0f : 1.0f / d.z;
+  r.par = px || py || pz;
+  return r;
+}
+
+// Entry distance of a box, or kInf when the box is missed or starts beyond `limit`.
+template <bool PAR>
+__device__ __forceinline__ float slab(const SlabRay& r, float lx, float ly, float lz, float hx, float hy,
+                                      float hz, float limit) {
+  float t0x = (lx - r.ox) * r.ix, t1x = (hx - r.ox) * r.ix;
+  float t0y = (ly - r.oy) * r.iy, t1y = (hy - r.oy) * r.iy;
+  float t0z = (lz - r.oz) * r.iz, t1z = (hz - r.oz) * r.iz;
+  float nx = fminf(t0x, t1x), fx = fmaxf(t0x, t1x);
+  float ny = fminf(t0y, t1y), fy = fmaxf(t0y, t1y);
+  float nz = fminf(t0z, t1z), fz = fmaxf(t0z, t1z);
+  if (PAR) {
+    if (r.ix == 0.0f) { nx = -kInf; fx = (r.ox >= lx && r.ox <= hx) ? kInf : -kInf; }
+    if (r.iy == 0.0f) { ny = -kInf; fy = (r.oy >= ly && r.oy <= hy) ? kInf : -kInf; }
+    if (r.iz == 0.0f) { nz = -kInf; fz = (r.oz >= lz && r.oz <= hz) ? kInf : -kInf; }
+  }
+  float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, 0.0f));
+  float tf = fminf(fminf(fminf(fx, fy), fz) * kSlack, limit);
+  return tn <= tf ? tn : kInf;
+}
+
+struct Hit {
+  float t, u, v;
+  int pos;  // sorted position, -1 on a miss
+  int id;   // triangle id
+  unsigned nodes, tests;  // interior nodes fetched, triangles tested
+};
+
+struct AnyResult {
+  int hit;
+  unsigned nodes, tests;
+};
+
+// Per-thread traversal stack: the first SH entries live in shared memory (column
+// threadIdx.x of a [SH][blockDim] array), deeper entries spill to local memory.
+template <int SH>
+struct TraversalStack {
+  uint2* sh;
+  int stride;
+  int sp;
+  uint2 spill[kStackMax - SH];
+  __device__ __forceinline__ TraversalStack(uint2* base, int str) : sh(base), stride(str), sp(0) {}
+  __device__ __forceinline__ bool push(int node, float t) {
+    uint2 v = make_uint2((uint32_t)node, __float_as_uint(t));
+    if (sp < SH) sh[sp * stride] = v;
+    else if (sp < kStackMax) spill[sp - SH] = v;
+    else return false;
+    ++sp;
+    return true;
+  }
+  __device__ __forceinline__ uint2 pop() {
+    --sp;
+    return sp < SH ? sh[sp * stride] : spill[sp - SH];
+  }
+};
+
+__device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p, f3& v1, f3& e1, f3& e2, int& id) {
+  float4 a = __ldg(tris + 3 * (size_t)p);
+  float4 b = __ldg(tris + 3 * (size_t)p + 1);
+  float4 c = __ldg(tris + 3 * (size_t)p + 2);
+  v1 = mk3(a.x, a.y, a.z);
+  e1 = mk3(a.w, b.x, b.y);
+  e2 = mk3(b.z, b.w, c.x);
+  id = __float_as_int(c.y);
+}
+
+template <bool PAR, int SH>
+__device__ __noinline__ Hit closest_hit_t(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  Hit h;
+  h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
+  SlabRay r = make_slab(o, d);
+  TraversalStack<SH> st(shs, stride);
+  int node = 0;
+  for (;;) {
+    const float4* nd = s.nodes + 4 * (size_t)node;
+    float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
+    int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+    ++h.nodes;
+    float lim = h.t * kCull;
+    float tn0 = slab<PAR>(r, a.x, a.y, a.z, a.w, b.x, b.y, lim);
+    float tn1 = slab<PAR>(r, b.z, b.w, c.x, c.y, c.z, c.w, lim);
+    bool h0 = tn0 != kInf && ref.z >= 0;
+    bool h1 = tn1 != kInf && ref.w >= 0;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      bool hit = side == 0 ? h0 : h1;
+      int cnt = side == 0 ? ref.z : ref.w;
+      int first = side == 0 ? ref.x : ref.y;
+      if (hit && cnt > 0) {
+        h.tests += cnt;
+        for (int p = first; p < first + cnt; ++p) {
+          f3 v1, e1, e2;
+          int id;
+          load_tri(s.tris, p, v1, e1, e2, id);
+          float t, u, v;
+          if (mt_intersect(o, d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
+            h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
+          }
+        }
+        if (side == 0) h0 = false; else h1 = false;
+      }
+    }
+    if (h0 && h1) {
+      bool sw = tn1 < tn0;
+      if (!st.push(sw ? ref.x : ref.y, sw ? tn0 : tn1)) {
+        atomicOr(err, kErrStack);
+        return h;
+      }
+      node = sw ? ref.y : ref.x;
+      continue;
+    }
+    if (h0) { node = ref.x; continue; }
+    if (h1) { node = ref.y; continue; }
+    bool found = false;
+    while (st.sp > 0) {
+      uint2 e = st.pop();
+      if (__uint_as_float(e.y) <= h.t * kCull) {
+        node = (int)e.x;
+        found = true;
+        break;
+      }
+    }
+    if (!found) return h;
+  }
+}
+
+template <bool PAR, int SH>
+__device__ __noinline__ AnyResult any_hit_t(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  AnyResult res{0, 0u, 0u};
+  SlabRay r = make_slab(o, d);
+  TraversalStack<SH> st(shs, stride);
+  int node = 0;
+  for (;;) {
+    const float4* nd = s.nodes + 4 * (size_t)node;
+    float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
+    int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+    ++res.nodes;
+    float tn0 = slab<PAR>(r, a.x, a.y, a.z, a.w, b.x, b.y, kInf);
+    float tn1 = slab<PAR>(r, b.z, b.w, c.x, c.y, c.z, c.w, kInf);
+    bool h0 = tn0 != kInf && ref.z >= 0;
+    bool h1 = tn1 != kInf && ref.w >= 0;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      bool hit = side == 0 ? h0 : h1;
+      int cnt = side == 0 ? ref.z : ref.w;
+      int first = side == 0 ? ref.x : ref.y;
+      if (hit && cnt > 0) {
+        for (int p = first; p < first + cnt; ++p) {
+          f3 v1, e1, e2;
+          int id;
+          load_tri(s.tris, p, v1, e1, e2, id);
+          float t, u, v;
+          ++res.tests;
+          if (mt_intersect(o, d, v1, e1, e2, t, u, v)) {
+            res.hit = 1;
+            return res;
+          }
+        }
+        if (side == 0) h0 = false; else h1 = false;
+      }
+    }
+    if (h0 && h1) {
+      bool sw = tn1 < tn0;
+      if (!st.push(sw ? ref.x : ref.y, 0.0f)) {
+        atomicOr(err, kErrStack);
+        return res;
+      }
+      node = sw ? ref.y : ref.x;
+      continue;
+    }
+    if (h0) { node = ref.x; continue; }
+    if (h1) { node = ref.y; continue; }
+    if (st.sp == 0) return res;
+    node = (int)st.pop().x;
+  }
+}
+
+template <int SH>
+__device__ __forceinline__ Hit closest_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  if (fabsf(d.x) < kParallelEps || fabsf(d.y) < kParallelEps || fabsf(d.z) < kParallelEps)
+    return closest_hit_t<true, SH>(s, o, d, shs, stride, err);
+  return closest_hit_t<false, SH>(s, o, d, shs, stride, err);
+}
+
+template <int SH>
+__device__ __forceinline__ AnyResult any_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  if (fabsf(d.x) < kParallelEps || fabsf(d.y) < kParallelEps || fabsf(d.z) < kParallelEps)
+    return any_hit_t<true, SH>(s, o, d, shs, stride, err);
+  return any_hit_t<false, SH>(s, o, d, shs, stride, err);
+}
+
+// Traversal work counters, reduced per warp into the context's counter block:
+// [3] interior nodes fetched by nearest-hit rays, [4] their triangle tests,
+// [5] nodes fetched by shadow rays, [6] their triangle tests, [7] shaded hits.
+enum { kCntPrimary = 0, kCntShadow = 1, kCntSecondary = 2, kCntNodesC = 3, kCntTestsC = 4, kCntNodesA = 5,
+       kCntTestsA = 6, kCntHits = 7, kNumCounts = 8 };
+
+__device__ __forceinline__ void warp_add_count(unsigned long long* dst, unsigned long long v) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// ------------------------------------------------------------------ shading
+// Hit point o + t*d and the shading normal normalize(n1(1-u-v) + n2 u + n3 v), normalised
+// once more as the reference does after its (identity) world transform
+// (src/Triangle.cpp:41-46, src/BVH.cpp:373-380).
+__device__ __forceinline__ void hit_geometry(const DevScene& s, f3 o, f3 d, const Hit& h, f3& P, f3& N, int& obj) {
+  P = add3(o, scale3(h.t, d));
+  const float4* sr = s.shade + 3 * (size_t)h.pos;
+  float4 a = __ldg(sr), b = __ldg(sr + 1), c = __ldg(sr + 2);
+  f3 n1 = mk3(a.x, a.y, a.z), n2 = mk3(a.w, b.x, b.y), n3 = mk3(b.z, b.w, c.x);
+  obj = __float_as_int(c.y);
+  float w = (1.0f - h.u) - h.v;
+  f3 n = norm3(add3(add3(scale3(w, n1), scale3(h.u, n2)), scale3(h.v, n3)));
+  N = norm3(n);
+}
+
+// RayTracer::calcPhong + findDiffuseColor for one light (src/RayTracer.cpp:418-458):
+// diffuse max(0, L.N) kd Lc, specular [V.R > 0] pow(V.R, shininess) Lc ks with
+// R = normalize(2 (N.L) N - L) and V towards the camera position.
+__device__ __forceinline__ f3 phong_light(const float* m, const float* l, f3 P, f3 N, f3 cam) {
+  f3 L = norm3(sub3(mk3(l[0], l[1], l[2]), P));
+  f3 V = norm3(sub3(cam, P));
+  float ndl = dot3(N, L);
+  float two = 2.0f * ndl;
+  f3 R = norm3(sub3(scale3(two, N), L));
+  float dd = dot3(L, N);
+  dd = dd > 0.0f ? dd : 0.0f;
+  f3 diff = mk3((dd * m[0]) * l[3], (dd * m[1]) * l[4], (dd * m[2]) * l[5]);
+  float vr = dot3(V, R);
+  if (vr > 0.0f) {
+    float st = powf(vr, m[6]);
+    return add3(diff, mk3((st * l[3]) * m[3], (st * l[4]) * m[4], (st * l[5]) * m[5]));
+  }
+  return diff;
+}
+
+// 8-bit quantisation of src/RayTracer.cpp:150-153: floor(c == 1 ? 255 : min(256 c, 255)).
+// 256*c, the min and the floor are exact in float, so the float form matches the
+// reference's double arithmetic bit for bit.
+__device__ __forceinline__ uint8_t quantize(float c) {
+  float q = c == 1.0f ? 255.0f : fminf(c * 256.0f, 255.0f);
+  q = floorf(q);
+  return (uint8_t)(q > 0.0f ? q : 0.0f);
+}
+
+}  // namespace eos

@@ -1,0 +1,218 @@
+/*
+ * eos_c.h -- C ABI of the B200-native Eos render path (sm_100a).
+ *
+ * Plain C: pointers, sizes and POD structs only.  Every function returns an eos_status
+ * and never calls exit() or traps; the reference reports errors by printing and exit()
+ * (src/cudaQualifiers.h:35-45).
+ *
+ * Each entry point replaces a reference interface:
+ *   eos_ctx_create / destroy     cudaSetDevice + per-renderer setup
+ *                                (src/MultiDeviceRenderer.cu:31-110; single GPU here)
+ *   eos_scene_create             Scene::flush + createCudaScene
+ *                                (src/Scene.cpp:204-209, src/cudaStructures.cu:483-543):
+ *                                uploads the triangles once and builds a Morton-code LBVH
+ *                                on the GPU instead of the CPU top-down BVH
+ *                                (src/BVH.cpp:97-111)
+ *   eos_scene_set_materials      Scene::addMaterial + copyMaterials (src/Scene.cpp:85-91,
+ *                                src/cudaStructures.cu:407-481)
+ *   eos_scene_set_lights         Scene::addLightSource + copyLights (src/Scene.cpp:77-83,
+ *                                src/cudaStructures.cu:177-218)
+ *   eos_render                   DeviceRenderer::renderCudaSceneToHostBufferMegaKernel and
+ *                                the C wrapper rayTrace_MegaKernel (src/DeviceRenderer.cu:61-109,
+ *                                src/kernelWrapper.h:30), with the CPU RayTracer's full
+ *                                Whitted semantics (src/RayTracer.cpp:85-458)
+ *   eos_render_batch             (no reference counterpart: many views / scenes per launch)
+ *   eos_render_backward          (no reference counterpart: adjoint of the shading)
+ *   eos_trace_closest / any      Scene::findMinDistanceIntersectionBVH /
+ *                                shadowRayVisibilityBVH (src/Scene.cpp:145-158)
+ *
+ * Buffers are owned by the caller.  A pointer argument may be host or device memory; the
+ * library tells them apart with cudaPointerGetAttributes and stages host buffers through
+ * its own device memory.  Calls on one context are serialised on its stream.
+ */
+#ifndef EOS_C_H
+#define EOS_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EOS_ABI_VERSION 1
+#define EOS_MAX_BOUNCES 8   /* trace_depth <= EOS_MAX_BOUNCES - 1 */
+#define EOS_MAX_LIGHTS 32
+#define EOS_HIT_NONE (-1)     /* ray traced, nothing hit */
+#define EOS_HIT_UNTRACED (-2) /* bounce not reached */
+
+typedef enum eos_status {
+  EOS_OK = 0,
+  EOS_ERR_INVALID_ARG = 1,
+  EOS_ERR_OOM = 2,
+  EOS_ERR_CUDA = 3,
+  EOS_ERR_TIMEOUT = 4,        /* a bounded device loop ran out of iterations */
+  EOS_ERR_STACK_OVERFLOW = 5, /* traversal stack exhausted (tree deeper than supported) */
+  EOS_ERR_QUEUE_OVERFLOW = 6,
+  EOS_ERR_UNSUPPORTED = 7,
+  EOS_ERR_NO_DEVICE = 8
+} eos_status;
+
+typedef struct eos_ctx eos_ctx;
+typedef struct eos_scene eos_scene;
+
+/* Material of one object (src/Material.h:46-78).  The reference's diffuse/specular are
+ * vec4 with an unused alpha and its shininess is an int; reflective = reflectivity > 0.
+ * The ambient term is unused by the reference renderer (src/RayTracer.cpp:412-413). */
+typedef struct eos_material {
+  float kd[3];
+  float ks[3];
+  float shininess;
+  float reflectivity;
+} eos_material;
+
+/* Point light (src/LightSource.h:27-39); the position's w is 1. */
+typedef struct eos_light {
+  float position[3];
+  float color[3];
+} eos_light;
+
+/* Pinhole camera, the reference's POD Camera (src/Camera.h:30-64): no fov, the lengths of
+ * right and up set it.  Primary ray of pixel (x, y):
+ *   d = normalize(aa*right + bb*up + view),  aa = ((x + ox) - W/2) * (1/(W/2)),
+ *   bb = ((y + oy) - H/2) * (1/(H/2)),  row 0 = bottom  (src/RayTracer.cpp:119-145). */
+typedef struct eos_camera {
+  float position[3];
+  float view[3];
+  float right[3];
+  float up[3];
+  int32_t width;
+  int32_t height;
+} eos_camera;
+
+enum { EOS_MODE_PLAIN = 0, EOS_MODE_WAVEFRONT = 1 };
+
+typedef struct eos_render_params {
+  int32_t trace_depth;  /* RayTracer::setTracedDepth: deepest bounce index (depth 2 -> 1) */
+  float pixel_offset;   /* sub-pixel sample position: 0 = reference corners, 0.5 = centres */
+  int32_t spp;          /* samples per pixel: 1, or >1 with hashed jitter */
+  uint32_t jitter_seed;
+  int32_t mode;         /* EOS_MODE_PLAIN (one launch per frame) or EOS_MODE_WAVEFRONT */
+  int32_t block_size;   /* 0 = autotuned / default */
+  int32_t queue_chunk;  /* rays taken per queue grab in the persistent kernels; 0 = default */
+  int32_t stack_depth;  /* shared-memory part of the traversal stack; 0 = default */
+  int32_t flags;        /* EOS_FLAG_* */
+} eos_render_params;
+
+/* Wavefront only: run the stages eagerly (no graph) with CUDA events between them and
+ * report per-stage device time in eos_stats.stage_ms. */
+#define EOS_FLAG_STAGE_TIMING 1
+
+typedef struct eos_build_params {
+  int32_t leaf_size;    /* subtrees with <= leaf_size triangles become one leaf; 0 = 4 */
+} eos_build_params;
+
+/* Per-path record of the bounce path: hit triangle id per bounce and, per bounce, the
+ * bit mask of lights whose shadow ray was blocked.  It is also the forward record that
+ * eos_render_backward replays (visibility frozen). */
+typedef struct eos_path_record {
+  int32_t hit[EOS_MAX_BOUNCES];
+  uint32_t shadow[EOS_MAX_BOUNCES];
+} eos_path_record;
+
+typedef struct eos_stats {
+  uint64_t primary_rays;
+  uint64_t shadow_rays;
+  uint64_t secondary_rays;
+  uint64_t nodes_closest;  /* BVH nodes fetched by nearest-hit (primary + mirror) rays */
+  uint64_t tests_closest;  /* ray-triangle tests of nearest-hit rays */
+  uint64_t nodes_shadow;   /* BVH nodes fetched by shadow rays */
+  uint64_t tests_shadow;   /* ray-triangle tests of shadow rays */
+  uint64_t shaded_hits;    /* hits shaded (each fetches normals + material) */
+  float gpu_ms;            /* device time of the render, CUDA events on the context stream */
+  int32_t error_flags;     /* device-side error bits raised during the call */
+  uint32_t kernel_launches;/* kernels launched by the call (graph kernel nodes included) */
+  float stage_ms[3];       /* with EOS_FLAG_STAGE_TIMING: nearest-hit, shadow, other stages */
+} eos_stats;
+
+typedef struct eos_scene_info {
+  uint32_t n_tris;
+  uint32_t n_nodes;       /* interior nodes of the LBVH (n_tris - 1) */
+  uint32_t leaf_size;
+  uint32_t n_objects;
+  uint32_t n_lights;
+  float build_ms;         /* device time of the LBVH build */
+  uint64_t device_bytes;  /* device memory held by the scene */
+} eos_scene_info;
+
+/* One view of one scene for eos_render_batch.  Outputs follow eos_render. */
+typedef struct eos_job {
+  const eos_scene* scene;
+  eos_camera camera;
+  int32_t trace_depth;
+  float pixel_offset;
+  int32_t spp;
+  uint32_t jitter_seed;
+  float* rgb_out;              /* [H*W*3] device, nullable */
+  uint8_t* rgba8_out;          /* [H*W*4] device, nullable */
+  eos_path_record* paths_out;  /* [H*W*spp] device, nullable */
+} eos_job;
+
+/* Gradients of an image loss L; d_rgb = dL/drgb per pixel. */
+typedef struct eos_grads {
+  float* materials;  /* [n_objects * 7]: dL/dkd rgb, dL/dks rgb, dL/dlog(shininess) */
+  float* lights;     /* [n_lights * 6]:  dL/dcolor rgb, dL/dposition xyz */
+} eos_grads;
+
+/* ---------------------------------------------------------------------------- context */
+int32_t eos_abi_version(void);
+const char* eos_status_string(eos_status s);
+eos_status eos_ctx_create(int32_t device, eos_ctx** out);
+eos_status eos_ctx_destroy(eos_ctx* ctx);
+/* Use a caller stream (a cudaStream_t) instead of the context's own; NULL restores it. */
+eos_status eos_ctx_set_stream(eos_ctx* ctx, void* stream);
+eos_status eos_ctx_synchronize(eos_ctx* ctx);
+
+/* ---------------------------------------------------------------------------- scenes */
+eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* normals, uint32_t n_verts,
+                            const uint32_t* tris, const uint32_t* tri_obj, uint32_t n_tris,
+                            const eos_material* materials, uint32_t n_materials,
+                            const eos_light* lights, uint32_t n_lights,
+                            const eos_build_params* build, eos_scene** out);
+eos_status eos_scene_destroy(eos_scene* scene);
+eos_status eos_scene_set_materials(eos_scene* scene, const eos_material* materials, uint32_t n);
+eos_status eos_scene_set_lights(eos_scene* scene, const eos_light* lights, uint32_t n);
+eos_status eos_scene_get_info(const eos_scene* scene, eos_scene_info* info);
+/* Test hook: Morton codes of the triangles in sorted order and the sorted triangle ids. */
+eos_status eos_scene_get_morton(const eos_scene* scene, uint32_t* codes, uint32_t* order);
+
+/* ---------------------------------------------------------------------------- render */
+/* rgb_out [H*W*3] float, rgba8_out [H*W*4] (src/RayTracer.cpp:150-153 quantisation),
+ * hit_out [H*W*spp] primary hit triangle id, paths_out [H*W*spp]; all nullable. */
+eos_status eos_render(eos_ctx* ctx, const eos_scene* scene, const eos_camera* camera,
+                      const eos_render_params* params, float* rgb_out, uint8_t* rgba8_out,
+                      int32_t* hit_out, eos_path_record* paths_out, eos_stats* stats);
+
+/* Many views of one or several resident scenes through one wavefront pass (persistent
+ * kernels over a global ray queue, replayed as a CUDA graph when the batch repeats). */
+eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs,
+                            const eos_render_params* params, eos_stats* stats);
+
+/* Adjoint of the shading with visibility frozen from the forward records.  Views are
+ * n_views cameras of equal size rendered with spp 1; paths / d_rgb are [n_views*H*W]. */
+eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* scene, const eos_camera* cameras,
+                               uint32_t n_views, const eos_render_params* params,
+                               const eos_path_record* paths, const float* d_rgb, eos_grads* grads);
+
+/* ---------------------------------------------------------------------------- queries */
+/* rays [n*6] (origin, direction).  Nearest hit: ids (EOS_HIT_NONE on a miss), t (may be
+ * NULL).  Any hit: occluded[i] = 1 when some triangle is hit at t >= 0. */
+eos_status eos_trace_closest(eos_ctx* ctx, const eos_scene* scene, const float* rays, uint32_t n,
+                             int32_t* ids, float* t);
+eos_status eos_trace_any(eos_ctx* ctx, const eos_scene* scene, const float* rays, uint32_t n,
+                         uint8_t* occluded);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EOS_C_H */

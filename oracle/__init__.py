@@ -1,0 +1,290 @@
+"""CPU checkers for the render path -- TEST INFRASTRUCTURE.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+import this package.  The product (``eos_b200``) never does: it fails loudly when its
+CUDA library is missing instead of falling back here.
+
+Two checkers live here:
+
+* :class:`Oracle` -- ``liboracle.so``, our C restatement of the reference render path
+  (``eos_oracle.c``; every function cites the reference lines it follows), with
+  tree-independent nearest-hit semantics, near-tie flags and an FP64 frozen-visibility
+  forward + adjoint.
+* :class:`RefRenderer` -- ``_ref/libeosref.so``, the reference's own CPU renderer
+  (src/RayTracer.cpp, src/Scene.cpp, src/BVH.cpp, ...) compiled from its sources by
+  ``oracle/Makefile`` with the one-line shadow fix documented there.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_longlong, c_uint32, c_uint8, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libeosref.so")
+REF_SRC = "/root/reference/src"
+MAXB = 8
+HIT_NONE = -1
+HIT_UNTRACED = -2
+FLAG_TIE, FLAG_NEAR_ORIGIN, FLAG_OUT_OF_RANGE, FLAG_AXIS_PARALLEL = 1, 2, 4, 8
+
+
+def build(ref: bool = True) -> None:
+    """Compile the restatement and, when the reference tree is present, the reference."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if ref and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(POINTER(ct)) if a is not None else None
+
+
+_lib_oracle = None
+_lib_ref = None
+
+
+def lib_oracle():
+    global _lib_oracle
+    if _lib_oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        L = ctypes.CDLL(ORACLE_SO)
+        L.oracle_scene_create.restype = c_void_p
+        L.oracle_scene_create.argtypes = [POINTER(c_float), POINTER(c_float), c_int, POINTER(c_uint32),
+                                          POINTER(c_uint32), c_int, POINTER(c_float), c_int,
+                                          POINTER(c_float), c_int]
+        L.oracle_scene_destroy.argtypes = [c_void_p]
+        L.oracle_render.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
+                                    c_uint32, POINTER(c_int32), c_int, c_int, POINTER(c_float),
+                                    POINTER(c_int32), POINTER(c_uint32), POINTER(c_uint32),
+                                    POINTER(c_longlong)]
+        L.oracle_closest.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_float),
+                                     POINTER(c_uint8)]
+        L.oracle_any.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_uint8)]
+        L.oracle_closest_brute.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_int32),
+                                           POINTER(c_float)]
+        L.oracle_morton.argtypes = [POINTER(c_float), POINTER(c_uint32), c_int, POINTER(c_uint32),
+                                    POINTER(c_int32)]
+        L.oracle_frozen_f64.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_float, c_int,
+                                        POINTER(c_int32), POINTER(c_uint32), POINTER(c_double),
+                                        POINTER(c_double), POINTER(c_double), POINTER(c_double),
+                                        POINTER(c_double), POINTER(c_double), c_int]
+        _lib_oracle = L
+    return _lib_oracle
+
+
+def lib_ref():
+    global _lib_ref
+    if _lib_ref is None:
+        if not os.path.exists(REF_SO):
+            build(ref=True)
+        if not os.path.exists(REF_SO):
+            raise RuntimeError("reference CPU build unavailable (oracle/_ref/libeosref.so missing)")
+        L = ctypes.CDLL(REF_SO)
+        L.eosref_scene_create.restype = c_void_p
+        L.eosref_scene_create.argtypes = [POINTER(c_float), POINTER(c_float), c_int, POINTER(c_uint32),
+                                          POINTER(c_uint32), c_int, POINTER(c_float), c_int,
+                                          POINTER(c_float), c_int, c_int, POINTER(c_double)]
+        L.eosref_scene_destroy.argtypes = [c_void_p]
+        L.eosref_scene_stats.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int)]
+        L.eosref_render.restype = c_int
+        L.eosref_render.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
+                                    POINTER(c_int32), c_int, POINTER(c_float), POINTER(c_int32),
+                                    POINTER(c_uint32), POINTER(c_longlong), POINTER(c_double)]
+        L.eosref_render_rgba8.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_int,
+                                          POINTER(c_uint8), POINTER(c_double)]
+        L.eosref_closest_hit.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_float)]
+        L.eosref_any_hit.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_uint8)]
+        L.eosref_morton3.argtypes = [POINTER(c_uint32), c_int, POINTER(c_uint32)]
+        _lib_ref = L
+    return _lib_ref
+
+
+def ref_available() -> bool:
+    try:
+        lib_ref()
+        return True
+    except (RuntimeError, OSError, subprocess.CalledProcessError):
+        return False
+
+
+def _scene_args(sc):
+    return (_p(sc.verts, c_float), _p(sc.normals, c_float), int(sc.verts.shape[0]), _p(sc.tris, c_uint32),
+            _p(sc.tri_obj, c_uint32), sc.n_tris, _p(sc.materials, c_float), sc.n_objects,
+            _p(sc.lights, c_float), sc.n_lights)
+
+
+def _pix(pixels):
+    if pixels is None:
+        return None, 0
+    px = np.ascontiguousarray(pixels, dtype=np.int32)
+    return px, int(px.size)
+
+
+def _rays(rays):
+    return np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+
+
+def morton(verts: np.ndarray, tris: np.ndarray):
+    """30-bit Morton codes of triangle centroids and the stable (code, id) sorted order."""
+    L = lib_oracle()
+    v = np.ascontiguousarray(verts, np.float32)
+    t = np.ascontiguousarray(tris, np.uint32)
+    n = t.shape[0]
+    codes = np.zeros(n, np.uint32)
+    order = np.zeros(n, np.int32)
+    L.oracle_morton(_p(v, c_float), _p(t, c_uint32), n, _p(codes, c_uint32), _p(order, c_int32))
+    return codes, order
+
+
+class Oracle:
+    """The C restatement, over one scene."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self._keep = scene
+        self.h = lib_oracle().oracle_scene_create(*_scene_args(scene))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib_oracle is not None:
+            _lib_oracle.oracle_scene_destroy(self.h)
+            self.h = None
+
+    def render(self, cam, trace_depth: int, pixel_offset: float = 0.5, spp: int = 1, jitter_seed: int = 0,
+               pixels=None, nthreads: int | None = None):
+        L = lib_oracle()
+        px, npix = _pix(pixels)
+        n = npix if px is not None else cam.width * cam.height
+        rgb = np.zeros((n, 3), np.float32)
+        hits = np.zeros((n * spp, MAXB), np.int32)
+        shadows = np.zeros((n * spp, MAXB), np.uint32)
+        flags = np.zeros(n * spp, np.uint32)
+        counts = np.zeros(3, np.int64)
+        c12 = cam.as_array()
+        L.oracle_render(self.h, _p(c12, c_float), cam.width, cam.height, pixel_offset, trace_depth, spp,
+                        jitter_seed, _p(px, c_int32), npix, nthreads or os.cpu_count(), _p(rgb, c_float),
+                        _p(hits, c_int32), _p(shadows, c_uint32), _p(flags, c_uint32), _p(counts, c_longlong))
+        return dict(rgb=rgb, hits=hits, shadows=shadows, flags=flags, counts=counts)
+
+    def closest(self, rays):
+        r = _rays(rays)
+        n = r.shape[0]
+        ids = np.zeros(n, np.int32)
+        ts = np.zeros(n, np.float32)
+        tie = np.zeros(n, np.uint8)
+        lib_oracle().oracle_closest(self.h, _p(r, c_float), n, _p(ids, c_int32), _p(ts, c_float), _p(tie, c_uint8))
+        return ids, ts, tie
+
+    def closest_brute(self, rays):
+        r = _rays(rays)
+        n = r.shape[0]
+        ids = np.zeros(n, np.int32)
+        ts = np.zeros(n, np.float32)
+        lib_oracle().oracle_closest_brute(self.h, _p(r, c_float), n, _p(ids, c_int32), _p(ts, c_float))
+        return ids, ts
+
+    def any(self, rays):
+        r = _rays(rays)
+        occ = np.zeros(r.shape[0], np.uint8)
+        lib_oracle().oracle_any(self.h, _p(r, c_float), r.shape[0], _p(occ, c_uint8))
+        return occ
+
+    def frozen_f64(self, cams, width, height, pixel_offset, trace_depth, hits, shadows, mat_params,
+                   light_params, g=None, nthreads=None):
+        """FP64 re-render with frozen visibility; with g, also the adjoint of <g, rgb>.
+
+        mat_params: [K, 8] kd rgb, ks rgb, log shininess, reflectivity (float64)
+        light_params: [L, 6] position xyz, colour rgb (float64)
+        Returns rgb [V*H*W, 3] and, with g, (grad_mat [K, 7], grad_light [L, 6]).
+        """
+        L = lib_oracle()
+        cams_a = np.ascontiguousarray(np.stack([c.as_array() for c in cams]), np.float32)
+        nv = len(cams)
+        npx = nv * width * height
+        h = np.ascontiguousarray(hits, np.int32).reshape(npx, MAXB)
+        s = np.ascontiguousarray(shadows, np.uint32).reshape(npx, MAXB)
+        mp = np.ascontiguousarray(mat_params, np.float64)
+        lp = np.ascontiguousarray(light_params, np.float64)
+        rgb = np.zeros((npx, 3), np.float64)
+        gm = np.zeros((mp.shape[0], 7), np.float64)
+        gl = np.zeros((lp.shape[0], 6), np.float64)
+        ga = None if g is None else np.ascontiguousarray(g, np.float64).reshape(npx, 3)
+        L.oracle_frozen_f64(self.h, _p(cams_a, c_float), nv, width, height, pixel_offset, trace_depth,
+                            _p(h, c_int32), _p(s, c_uint32), _p(mp, c_double), _p(lp, c_double),
+                            _p(rgb, c_double), _p(ga, c_double), _p(gm, c_double), _p(gl, c_double),
+                            nthreads or os.cpu_count())
+        if g is None:
+            return rgb
+        return rgb, gm, gl
+
+
+class RefRenderer:
+    """The reference's own CPU renderer, compiled from its sources, over one scene."""
+
+    def __init__(self, scene, build_threads: int = 1):
+        L = lib_ref()
+        self.scene = scene
+        secs = c_double(0.0)
+        self.h = L.eosref_scene_create(*_scene_args(scene), build_threads, ctypes.byref(secs))
+        self.build_seconds = secs.value
+        nn, ml = c_int(0), c_int(0)
+        L.eosref_scene_stats(self.h, ctypes.byref(nn), ctypes.byref(ml))
+        self.n_nodes, self.max_leaf = nn.value, ml.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib_ref is not None:
+            _lib_ref.eosref_scene_destroy(self.h)
+            self.h = None
+
+    def render(self, cam, trace_depth: int, pixel_offset: float = 0.0, pixels=None, nthreads=None,
+               paths: bool = True):
+        L = lib_ref()
+        px, npix = _pix(pixels)
+        n = npix if px is not None else cam.width * cam.height
+        rgb = np.zeros((n, 3), np.float32)
+        hits = np.zeros((n, MAXB), np.int32) if paths else None
+        shadows = np.zeros((n, MAXB), np.uint32) if paths else None
+        counts = np.zeros(3, np.int64)
+        secs = c_double(0.0)
+        c12 = cam.as_array()
+        rc = L.eosref_render(self.h, _p(c12, c_float), cam.width, cam.height, pixel_offset, trace_depth,
+                             nthreads or os.cpu_count(), _p(px, c_int32), npix, _p(rgb, c_float),
+                             _p(hits, c_int32), _p(shadows, c_uint32), _p(counts, c_longlong), ctypes.byref(secs))
+        if rc != 0:
+            raise ValueError("reference renderer rejected trace_depth (it cannot be set below 1)")
+        return dict(rgb=rgb, hits=hits, shadows=shadows, counts=counts, seconds=secs.value)
+
+    def render_rgba8(self, cam, trace_depth: int, nthreads=None):
+        L = lib_ref()
+        out = np.zeros((cam.height, cam.width, 4), np.uint8)
+        secs = c_double(0.0)
+        c12 = cam.as_array()
+        L.eosref_render_rgba8(self.h, _p(c12, c_float), cam.width, cam.height, trace_depth,
+                              nthreads or os.cpu_count(), _p(out, c_uint8), ctypes.byref(secs))
+        return out, secs.value
+
+    def closest(self, rays):
+        r = _rays(rays)
+        ids = np.zeros(r.shape[0], np.int32)
+        pts = np.zeros((r.shape[0], 3), np.float32)
+        lib_ref().eosref_closest_hit(self.h, _p(r, c_float), r.shape[0], _p(ids, c_int32), _p(pts, c_float))
+        return ids, pts
+
+    def any(self, rays):
+        r = _rays(rays)
+        occ = np.zeros(r.shape[0], np.uint8)
+        lib_ref().eosref_any_hit(self.h, _p(r, c_float), r.shape[0], _p(occ, c_uint8))
+        return occ
+
+
+def ref_morton3(xyz: np.ndarray) -> np.ndarray:
+    """The reference's EncodeMorton3 (src/morton.h:45-48), compiled, on [n, 3] uint32."""
+    a = np.ascontiguousarray(xyz, np.uint32).reshape(-1, 3)
+    out = np.zeros(a.shape[0], np.uint32)
+    lib_ref().eosref_morton3(_p(a, c_uint32), a.shape[0], _p(out, c_uint32))
+    return out

@@ -1,0 +1,670 @@
+/*
+ * eos_oracle.c -- CPU restatement of the Eos render path.  TEST INFRASTRUCTURE ONLY:
+ * loaded by tests/, by the smoke check and by the CPU-baseline leg of bench.py as the
+ * checker; the product never links or calls it.
+ *
+ * What is restated, with the reference lines each part follows:
+ *   - Moller-Trumbore with the |det| < 1e-5 rejection and t < 0 / u / v bounds, in the
+ *     reference's operation order                        src/Triangle.cpp:57-91
+ *   - hit point o + t*d and the normal normalize(n1(1-u-v) + n2 u + n3 v), normalised a
+ *     second time after the identity world transform    src/Triangle.cpp:26-55,
+ *                                                        src/BVH.cpp:369-381
+ *   - primary rays  normalize(aa*right + bb*up + view)   src/RayTracer.cpp:119-145
+ *   - per-light shadow ray P + 1e-3*L, Phong diffuse + specular with V from the camera,
+ *     mirror ray normalize(reflect(d, N)) from P + 1e-3*r, colour fold
+ *     phong + reflectivity * trace(next), depth rule     src/RayTracer.cpp:268-458
+ *   - glm 0.9.6 arithmetic: dot = (x0y0 + x1y1) + x2y2, normalize = v * (1/sqrt(dot)),
+ *     reflect = I - (N*dot(N,I))*2                        glm/detail/func_geometric.inl:65-72,
+ *                                                        :154-173; func_exponential.inl:150-153
+ *   - 30-bit Morton codes: EncodeMorton3 / Part1By2      src/morton.h:30-48
+ *
+ * Semantics that differ on purpose from the reference's traversal, so that the result
+ * does not depend on a particular tree:
+ *   - nearest hit = the smallest t >= 0 over ALL triangles (exact ties: the larger
+ *     triangle id wins).  The reference walks its own tree and keeps the later of equal
+ *     hits; its interior boxes are tested against [0.001, 999] (src/BVH.cpp:609-659).
+ *   - shadow ray = any triangle with t >= 0 (the reference, with its uninitialised
+ *     distance at src/BVH.cpp:703 fixed to FLT_MAX, accepts every t >= 0 in the leaves
+ *     its box tests reach, src/BVH.cpp:661-716).
+ * Paths where these differences can matter are flagged per path (near ties within
+ * 2 ulp; hits closer than 1e-3 to a ray origin), so parity tests can count them.
+ *
+ * The FP64 section re-renders with frozen visibility (given hit ids and shadow masks)
+ * and evaluates the analytic adjoint of an image loss with respect to per-object
+ * kd / ks / log-shininess and per-light colour / position.
+ *
+ * Built with -ffp-contract=off and without -ffast-math (oracle/Makefile).
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#define MAXB 8
+#define HIT_NONE (-1)
+#define HIT_UNTRACED (-2)
+#define FLAG_TIE 1u
+#define FLAG_NEAR_ORIGIN 2u
+#define FLAG_OUT_OF_RANGE 4u
+#define FLAG_AXIS_PARALLEL 8u
+#define LEAF_MAX 4
+
+typedef struct { float x, y, z; } v3f;
+
+static inline v3f V3(float x, float y, float z) { v3f r = {x, y, z}; return r; }
+static inline v3f vadd(v3f a, v3f b) { return V3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3f vsub(v3f a, v3f b) { return V3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3f vscale(float s, v3f a) { return V3(s * a.x, s * a.y, s * a.z); }
+static inline float vdot(v3f a, v3f b) { float x = a.x * b.x, y = a.y * b.y, z = a.z * b.z; return (x + y) + z; }
+static inline v3f vcross(v3f a, v3f b) {
+  return V3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+static inline v3f vnorm(v3f a) { float s = 1.0f / sqrtf(vdot(a, a)); return V3(a.x * s, a.y * s, a.z * s); }
+static inline float fget(v3f a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+
+typedef struct {
+  float lo[3], hi[3];
+  int left, right;   /* children (interior) */
+  int start, count;  /* triangle range in sorted order (leaf when count > 0) */
+} onode;
+
+typedef struct {
+  int nt, nobj, nl;
+  v3f *v1, *v2, *v3, *e1, *e2, *n1, *n2, *n3; /* sorted (Morton) order */
+  int32_t *id;                                 /* sorted position -> triangle id */
+  uint32_t *obj;                               /* sorted position -> object */
+  float *mats;                                 /* nobj x 8 */
+  float *lights;                               /* nl x 6 */
+  onode *nodes;
+  int nnodes;
+  /* by triangle id, for the frozen-visibility FP64 path */
+  int32_t *pos_of_id;
+} oscene;
+
+/* ---------------------------------------------------------------- Morton codes */
+static inline uint32_t part1by2(uint32_t x) {
+  x &= 0x000003ffu;
+  x = (x ^ (x << 16)) & 0xff0000ffu;
+  x = (x ^ (x << 8)) & 0x0300f00fu;
+  x = (x ^ (x << 4)) & 0x030c30c3u;
+  x = (x ^ (x << 2)) & 0x09249249u;
+  return x;
+}
+static inline uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return (part1by2(z) << 2) + (part1by2(y) << 1) + part1by2(x);
+}
+
+typedef struct { uint32_t code; int32_t idx; } keyidx;
+static int cmp_keyidx(const void* a, const void* b) {
+  const keyidx* x = (const keyidx*)a; const keyidx* y = (const keyidx*)b;
+  if (x->code != y->code) return x->code < y->code ? -1 : 1;
+  return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
+static inline v3f load3(const float* p, uint32_t i) { return V3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+/* Centroid ((v1 + v2) + v3) / 3 (src/Triangle.h:37), quantised per axis over the
+ * centroid bounds: q = min(1023, (uint)((1024 * (c - lo)) / (hi - lo))), 0 for a flat axis. */
+void oracle_morton(const float* verts, const uint32_t* tris, int nt, uint32_t* codes,
+                   int32_t* order) {
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  v3f* c = (v3f*)malloc(sizeof(v3f) * (size_t)(nt > 0 ? nt : 1));
+  for (int i = 0; i < nt; ++i) {
+    v3f a = load3(verts, tris[3 * i]), b = load3(verts, tris[3 * i + 1]), d = load3(verts, tris[3 * i + 2]);
+    v3f s = vadd(vadd(a, b), d);
+    c[i] = V3(s.x / 3.0f, s.y / 3.0f, s.z / 3.0f);
+    for (int k = 0; k < 3; ++k) {
+      float v = fget(c[i], k);
+      if (v < lo[k]) lo[k] = v;
+      if (v > hi[k]) hi[k] = v;
+    }
+  }
+  keyidx* ki = (keyidx*)malloc(sizeof(keyidx) * (size_t)(nt > 0 ? nt : 1));
+  for (int i = 0; i < nt; ++i) {
+    uint32_t q[3];
+    for (int k = 0; k < 3; ++k) {
+      float ext = hi[k] - lo[k];
+      if (ext > 0.0f) {
+        float f = (1024.0f * (fget(c[i], k) - lo[k])) / ext;
+        uint32_t u = (uint32_t)f;
+        q[k] = u > 1023u ? 1023u : u;
+      } else {
+        q[k] = 0;
+      }
+    }
+    codes[i] = morton3(q[0], q[1], q[2]);
+    ki[i].code = codes[i];
+    ki[i].idx = i;
+  }
+  qsort(ki, (size_t)nt, sizeof(keyidx), cmp_keyidx);
+  for (int i = 0; i < nt; ++i) order[i] = ki[i].idx;
+  free(ki);
+  free(c);
+}
+
+/* ---------------------------------------------------------------- scene + BVH */
+static void box_of_range(const oscene* s, int a, int b, float lo[3], float hi[3]) {
+  for (int k = 0; k < 3; ++k) { lo[k] = FLT_MAX; hi[k] = -FLT_MAX; }
+  for (int i = a; i < b; ++i) {
+    v3f p[3] = {s->v1[i], s->v2[i], s->v3[i]};
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) {
+        float v = fget(p[j], k);
+        if (v < lo[k]) lo[k] = v;
+        if (v > hi[k]) hi[k] = v;
+      }
+  }
+}
+
+static int build_rec(oscene* s, int a, int b) {
+  int me = s->nnodes++;
+  onode* n = &s->nodes[me];
+  box_of_range(s, a, b, n->lo, n->hi);
+  if (b - a <= LEAF_MAX) {
+    n->start = a; n->count = b - a; n->left = n->right = -1;
+    return me;
+  }
+  int mid = a + (b - a) / 2;
+  n->count = 0; n->start = a;
+  int l = build_rec(s, a, mid);
+  int r = build_rec(s, mid, b);
+  s->nodes[me].left = l;
+  s->nodes[me].right = r;
+  return me;
+}
+
+void* oracle_scene_create(const float* verts, const float* normals, int nv, const uint32_t* tris,
+                          const uint32_t* tri_obj, int nt, const float* mats, int nobj,
+                          const float* lights, int nl) {
+  (void)nv;
+  oscene* s = (oscene*)calloc(1, sizeof(oscene));
+  s->nt = nt; s->nobj = nobj; s->nl = nl;
+  size_t n = (size_t)(nt > 0 ? nt : 1);
+  s->v1 = malloc(sizeof(v3f) * n); s->v2 = malloc(sizeof(v3f) * n); s->v3 = malloc(sizeof(v3f) * n);
+  s->e1 = malloc(sizeof(v3f) * n); s->e2 = malloc(sizeof(v3f) * n);
+  s->n1 = malloc(sizeof(v3f) * n); s->n2 = malloc(sizeof(v3f) * n); s->n3 = malloc(sizeof(v3f) * n);
+  s->id = malloc(sizeof(int32_t) * n); s->obj = malloc(sizeof(uint32_t) * n);
+  s->pos_of_id = malloc(sizeof(int32_t) * n);
+  uint32_t* codes = malloc(sizeof(uint32_t) * n);
+  int32_t* order = malloc(sizeof(int32_t) * n);
+  oracle_morton(verts, tris, nt, codes, order);
+  for (int p = 0; p < nt; ++p) {
+    int i = order[p];
+    const uint32_t* t = tris + 3 * i;
+    s->v1[p] = load3(verts, t[0]); s->v2[p] = load3(verts, t[1]); s->v3[p] = load3(verts, t[2]);
+    s->n1[p] = load3(normals, t[0]); s->n2[p] = load3(normals, t[1]); s->n3[p] = load3(normals, t[2]);
+    s->e1[p] = vsub(s->v2[p], s->v1[p]);
+    s->e2[p] = vsub(s->v3[p], s->v1[p]);
+    s->id[p] = i;
+    s->obj[p] = tri_obj[i];
+    s->pos_of_id[i] = p;
+  }
+  free(codes); free(order);
+  s->mats = malloc(sizeof(float) * 8 * (size_t)(nobj > 0 ? nobj : 1));
+  memcpy(s->mats, mats, sizeof(float) * 8 * (size_t)nobj);
+  s->lights = malloc(sizeof(float) * 6 * (size_t)(nl > 0 ? nl : 1));
+  memcpy(s->lights, lights, sizeof(float) * 6 * (size_t)nl);
+  s->nodes = malloc(sizeof(onode) * (2 * n + 1));
+  s->nnodes = 0;
+  if (nt > 0) build_rec(s, 0, nt);
+  return s;
+}
+
+void oracle_scene_destroy(void* h) {
+  oscene* s = (oscene*)h;
+  if (!s) return;
+  free(s->v1); free(s->v2); free(s->v3); free(s->e1); free(s->e2);
+  free(s->n1); free(s->n2); free(s->n3); free(s->id); free(s->obj); free(s->pos_of_id);
+  free(s->mats); free(s->lights); free(s->nodes); free(s);
+}
+
+/* ---------------------------------------------------------------- intersection */
+/* Triangle::RayTriangleIntersection, src/Triangle.cpp:57-91 (e1, e2 precomputed with the
+ * same subtraction). Returns 1 and t,u,v on a hit. */
+static inline int mt_hit(v3f o, v3f d, v3f v1, v3f e1, v3f e2, float* t, float* u, float* v) {
+  v3f P = vcross(d, e2);
+  float det = vdot(e1, P);
+  if (det > -0.00001f && det < 0.00001f) return 0;
+  float inv_det = 1.0f / det;
+  v3f T = vsub(o, v1);
+  v3f Q = vcross(T, e1);
+  float tt = vdot(e2, Q) * inv_det;
+  if (tt < 0.0f) return 0;
+  float uu = vdot(T, P) * inv_det;
+  if (uu < 0.0f || uu > 1.0f) return 0;
+  float vv = vdot(d, Q) * inv_det;
+  if (vv < 0.0f || uu + vv > 1.0f) return 0;
+  *t = tt; *u = uu; *v = vv;
+  return 1;
+}
+
+/* Conservative slab test: the float interval is widened by 1 + 2*gamma(3) so that no box
+ * that contains a hit with t in [0, tlimit] is rejected by rounding. */
+static const float kSlack = 1.0000004f;          /* 1 + 2 * gamma(3), gamma(n) = n u / (1 - n u) */
+static const float kCullSlack = 1.000244140625f; /* 1 + 2^-12: margin against MT's own t error */
+
+/* A direction component that is exactly zero makes the slab of that axis either the
+ * whole line (origin inside the closed slab) or empty; it is tested by containment
+ * instead of by 0 * inf products (the reference's test yields NaN there,
+ * src/Box.cu:234-255). */
+typedef struct { v3f o, inv; int par[3]; } bray;
+
+static inline bray make_bray(v3f o, v3f d) {
+  bray r; r.o = o;
+  float dd[3] = {d.x, d.y, d.z}, iv[3];
+  for (int k = 0; k < 3; ++k) { r.par[k] = fabsf(dd[k]) < 1e-30f; iv[k] = r.par[k] ? 0.0f : 1.0f / dd[k]; }
+  r.inv = V3(iv[0], iv[1], iv[2]);
+  return r;
+}
+
+static inline int box_test(const onode* n, const bray* r, float tlimit) {
+  float tmin = -FLT_MAX, tmax = FLT_MAX;
+  float oo[3] = {r->o.x, r->o.y, r->o.z}, ii[3] = {r->inv.x, r->inv.y, r->inv.z};
+  for (int k = 0; k < 3; ++k) {
+    if (r->par[k]) {
+      if (oo[k] < n->lo[k] || oo[k] > n->hi[k]) return 0;
+      continue;
+    }
+    float a = (n->lo[k] - oo[k]) * ii[k];
+    float b = (n->hi[k] - oo[k]) * ii[k];
+    float lo = a < b ? a : b, hi = a < b ? b : a;
+    if (lo > tmin) tmin = lo;
+    if (hi < tmax) tmax = hi;
+  }
+  tmax *= kSlack;
+  return tmin <= tmax && tmax >= 0.0f && tmin <= tlimit;
+}
+
+static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+typedef struct { int pos; float t, u, v; float t2; } chit;
+
+/* Nearest hit with the larger-id tie rule; also tracks the second-nearest distinct hit
+ * (culling by it) so near ties can be flagged. */
+static chit closest(const oscene* s, v3f o, v3f d) {
+  chit h; h.pos = -1; h.t = FLT_MAX; h.u = h.v = 0; h.t2 = FLT_MAX;
+  if (s->nt == 0) return h;
+  bray br = make_bray(o, d);
+  int stack[128]; int sp = 0;
+  stack[sp++] = 0;
+  while (sp) {
+    const onode* n = &s->nodes[stack[--sp]];
+    float lim = h.t2 < FLT_MAX ? h.t2 * kCullSlack : FLT_MAX;
+    if (!box_test(n, &br, lim)) continue;
+    if (n->count) {
+      for (int p = n->start; p < n->start + n->count; ++p) {
+        float t, u, v;
+        if (!mt_hit(o, d, s->v1[p], s->e1[p], s->e2[p], &t, &u, &v)) continue;
+        int better = h.pos < 0 || t < h.t || (t == h.t && s->id[p] > s->id[h.pos]);
+        if (better) {
+          if (h.pos >= 0 && h.t < h.t2) h.t2 = h.t;
+          h.pos = p; h.t = t; h.u = u; h.v = v;
+        } else if (t < h.t2) {
+          h.t2 = t;
+        }
+      }
+    } else {
+      stack[sp++] = n->left;
+      stack[sp++] = n->right;
+    }
+  }
+  return h;
+}
+
+static int any_hit(const oscene* s, v3f o, v3f d) {
+  if (s->nt == 0) return 0;
+  bray br = make_bray(o, d);
+  int stack[128]; int sp = 0;
+  stack[sp++] = 0;
+  while (sp) {
+    const onode* n = &s->nodes[stack[--sp]];
+    if (!box_test(n, &br, FLT_MAX)) continue;
+    if (n->count) {
+      for (int p = n->start; p < n->start + n->count; ++p) {
+        float t, u, v;
+        if (mt_hit(o, d, s->v1[p], s->e1[p], s->e2[p], &t, &u, &v)) return 1;
+      }
+    } else {
+      stack[sp++] = n->left;
+      stack[sp++] = n->right;
+    }
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------- FP32 render */
+static inline uint32_t hash32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+  return x;
+}
+
+/* Sub-pixel offsets of sample `s` of pixel `p`: the pixel offset for spp == 1, else a
+ * hashed jitter in [0, 1). */
+static inline void sample_offset(uint32_t p, int smp, int spp, uint32_t seed, float off,
+                                 float* ox, float* oy) {
+  if (spp <= 1) { *ox = off; *oy = off; return; }
+  uint32_t h1 = hash32(p * 0x9E3779B9u ^ hash32((uint32_t)smp * 0x85EBCA6Bu + seed));
+  uint32_t h2 = hash32(h1 ^ 0x68E31DA4u);
+  *ox = (float)(h1 >> 8) * (1.0f / 16777216.0f);
+  *oy = (float)(h2 >> 8) * (1.0f / 16777216.0f);
+}
+
+static inline v3f primary_dir(const float* cam, int w, int hgt, int x, int y, float ox, float oy) {
+  float nw = w / 2.0f, nh = hgt / 2.0f;
+  float inw = 1.0f / nw, inh = 1.0f / nh;
+  float bb = (((float)y + oy) - nh) * inh;
+  float aa = (((float)x + ox) - nw) * inw;
+  v3f right = V3(cam[6], cam[7], cam[8]), up = V3(cam[9], cam[10], cam[11]), view = V3(cam[3], cam[4], cam[5]);
+  v3f d = vadd(vadd(vscale(aa, right), vscale(bb, up)), view);
+  return vnorm(d);
+}
+
+/* Hit point and shading normal (src/Triangle.cpp:41-46, src/BVH.cpp:379-380). */
+static inline void hit_geometry(const oscene* s, int p, v3f o, v3f d, float t, float u, float v,
+                                v3f* P, v3f* N) {
+  *P = vadd(o, vscale(t, d));
+  float w = (1.0f - u) - v;
+  v3f a = vscale(w, s->n1[p]), b = vscale(u, s->n2[p]), c = vscale(v, s->n3[p]);
+  v3f n = vnorm(vadd(vadd(a, b), c));
+  *N = vnorm(n);
+}
+
+/* RayTracer::calcPhong for one light (src/RayTracer.cpp:418-458). */
+static inline v3f phong_one(const float* m, const float* l, v3f P, v3f N, v3f cam) {
+  v3f L = vnorm(vsub(V3(l[0], l[1], l[2]), P));
+  v3f Vv = vnorm(vsub(cam, P));
+  float ndl = vdot(N, L);
+  float two = 2.0f * ndl;
+  v3f R = vnorm(vsub(vscale(two, N), L));
+  float dd = vdot(L, N);
+  dd = dd > 0.0f ? dd : 0.0f;
+  v3f diff = V3((dd * m[0]) * l[3], (dd * m[1]) * l[4], (dd * m[2]) * l[5]);
+  float vr = vdot(Vv, R);
+  if (vr > 0.0f) {
+    float st = powf(vr, m[6]);
+    v3f sp = V3((st * l[3]) * m[3], (st * l[4]) * m[4], (st * l[5]) * m[5]);
+    return vadd(diff, sp);
+  }
+  return diff;
+}
+
+typedef struct { long long prim, shadow, second; } counts_t;
+
+static v3f trace_path(const oscene* s, const float* cam, v3f o, v3f d, int trace_depth, int32_t* hits,
+                      uint32_t* shadows, uint32_t* flags, counts_t* cnt) {
+  v3f phong[MAXB];
+  float refl[MAXB];
+  int nb = 0;
+  v3f campos = V3(cam[0], cam[1], cam[2]);
+  const float eps = 1e-3f;
+  for (int k = 0; k < MAXB; ++k) {
+    if (k > trace_depth) break;
+    if (k == 0) cnt->prim++; else cnt->second++;
+    if (d.x == 0.0f || d.y == 0.0f || d.z == 0.0f) *flags |= FLAG_AXIS_PARALLEL;
+    chit h = closest(s, o, d);
+    if (h.pos < 0) { hits[k] = HIT_NONE; break; }
+    hits[k] = s->id[h.pos];
+    if (h.t2 < FLT_MAX && fbits(h.t2) - fbits(h.t) <= 2u) *flags |= FLAG_TIE;
+    if (h.t < 1e-3f || h.t > 999.0f) *flags |= FLAG_OUT_OF_RANGE;
+    v3f P, N;
+    hit_geometry(s, h.pos, o, d, h.t, h.u, h.v, &P, &N);
+    const float* m = s->mats + 8 * s->obj[h.pos];
+    v3f acc = V3(0, 0, 0);
+    uint32_t mask = 0;
+    for (int li = 0; li < s->nl; ++li) {
+      const float* l = s->lights + 6 * li;
+      v3f sd = vnorm(vsub(V3(l[0], l[1], l[2]), P));
+      v3f so = vadd(P, vscale(eps, sd));
+      cnt->shadow++;
+      if (sd.x == 0.0f || sd.y == 0.0f || sd.z == 0.0f) *flags |= FLAG_AXIS_PARALLEL;
+      int occ = any_hit(s, so, sd);
+      if (occ) {
+        mask |= 1u << li;
+        chit sh = closest(s, so, sd);
+        if (sh.pos >= 0 && sh.t < 1e-3f) *flags |= FLAG_NEAR_ORIGIN;
+      } else {
+        acc = vadd(acc, phong_one(m, l, P, N, campos));
+      }
+    }
+    shadows[k] = mask;
+    phong[k] = acc;
+    refl[k] = 0.0f;
+    nb = k + 1;
+    if (!(m[7] > 0.0f)) break;
+    refl[k] = m[7];
+    float dn = vdot(N, d);
+    v3f r = V3(d.x - ((N.x * dn) * 2.0f), d.y - ((N.y * dn) * 2.0f), d.z - ((N.z * dn) * 2.0f));
+    v3f rd = vnorm(r);
+    o = vadd(P, vscale(eps, rd));
+    d = rd;
+  }
+  /* c_k = phong_k + refl_k * c_{k+1} (src/RayTracer.cpp:356-357,410) */
+  v3f c = V3(0, 0, 0);
+  for (int k = nb - 1; k >= 0; --k) c = vadd(phong[k], vscale(refl[k], c));
+  return c;
+}
+
+/* rgb [npix,3]; hits/shadows [npix*spp, 8]; flags [npix*spp]; counts [3]. */
+int oracle_render(void* h, const float* cam, int w, int hgt, float pixel_offset, int trace_depth,
+                  int spp, uint32_t jitter_seed, const int32_t* pix, int npix, int nthreads,
+                  float* rgb, int32_t* hits, uint32_t* shadows, uint32_t* flags, long long* counts) {
+  const oscene* s = (const oscene*)h;
+  int n = pix ? npix : w * hgt;
+  if (spp < 1) spp = 1;
+  long long c0 = 0, c1 = 0, c2 = 0;
+#pragma omp parallel for schedule(dynamic, 32) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : c0, c1, c2)
+  for (int i = 0; i < n; ++i) {
+    int p = pix ? pix[i] : i;
+    int x = p % w, y = p / w;
+    v3f sum = V3(0, 0, 0);
+    counts_t cnt = {0, 0, 0};
+    for (int smp = 0; smp < spp; ++smp) {
+      size_t r = (size_t)i * spp + smp;
+      int32_t hh[MAXB]; uint32_t ss[MAXB]; uint32_t fl = 0;
+      for (int k = 0; k < MAXB; ++k) { hh[k] = HIT_UNTRACED; ss[k] = 0; }
+      float ox, oy;
+      sample_offset((uint32_t)p, smp, spp, jitter_seed, pixel_offset, &ox, &oy);
+      v3f d = primary_dir(cam, w, hgt, x, y, ox, oy);
+      v3f c = trace_path(s, cam, V3(cam[0], cam[1], cam[2]), d, trace_depth, hh, ss, &fl, &cnt);
+      sum = vadd(sum, c);
+      if (hits) memcpy(hits + r * MAXB, hh, sizeof hh);
+      if (shadows) memcpy(shadows + r * MAXB, ss, sizeof ss);
+      if (flags) flags[r] = fl;
+    }
+    if (spp > 1) sum = vscale(1.0f / (float)spp, sum);
+    rgb[3 * (size_t)i] = sum.x; rgb[3 * (size_t)i + 1] = sum.y; rgb[3 * (size_t)i + 2] = sum.z;
+    c0 += cnt.prim; c1 += cnt.shadow; c2 += cnt.second;
+  }
+  if (counts) { counts[0] = c0; counts[1] = c1; counts[2] = c2; }
+  return 0;
+}
+
+/* Nearest / any hit of arbitrary rays [n,6]: ids (-1 = miss), t, near-tie flag. */
+void oracle_closest(void* h, const float* rays, int n, int32_t* ids, float* ts, uint8_t* tie) {
+  const oscene* s = (const oscene*)h;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    const float* r = rays + 6 * (size_t)i;
+    chit c = closest(s, V3(r[0], r[1], r[2]), V3(r[3], r[4], r[5]));
+    ids[i] = c.pos < 0 ? HIT_NONE : s->id[c.pos];
+    if (ts) ts[i] = c.pos < 0 ? FLT_MAX : c.t;
+    if (tie) tie[i] = (c.pos >= 0 && c.t2 < FLT_MAX && fbits(c.t2) - fbits(c.t) <= 2u) ? 1 : 0;
+  }
+}
+
+void oracle_any(void* h, const float* rays, int n, uint8_t* occ) {
+  const oscene* s = (const oscene*)h;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    const float* r = rays + 6 * (size_t)i;
+    occ[i] = (uint8_t)any_hit(s, V3(r[0], r[1], r[2]), V3(r[3], r[4], r[5]));
+  }
+}
+
+/* Brute force over every triangle (validates the BVH culling above on small scenes). */
+void oracle_closest_brute(void* h, const float* rays, int n, int32_t* ids, float* ts) {
+  const oscene* s = (const oscene*)h;
+  for (int i = 0; i < n; ++i) {
+    const float* r = rays + 6 * (size_t)i;
+    v3f o = V3(r[0], r[1], r[2]), d = V3(r[3], r[4], r[5]);
+    int best = -1; float bt = FLT_MAX;
+    for (int p = 0; p < s->nt; ++p) {
+      float t, u, v;
+      if (!mt_hit(o, d, s->v1[p], s->e1[p], s->e2[p], &t, &u, &v)) continue;
+      if (best < 0 || t < bt || (t == bt && s->id[p] > s->id[best])) { best = p; bt = t; }
+    }
+    ids[i] = best < 0 ? HIT_NONE : s->id[best];
+    if (ts) ts[i] = bt;
+  }
+}
+
+/* ---------------------------------------------------------------- FP64 adjoint */
+typedef struct { double x, y, z; } v3d;
+static inline v3d D3(double x, double y, double z) { v3d r = {x, y, z}; return r; }
+static inline v3d dadd(v3d a, v3d b) { return D3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3d dsub(v3d a, v3d b) { return D3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3d dsc(double s, v3d a) { return D3(s * a.x, s * a.y, s * a.z); }
+static inline double ddot(v3d a, v3d b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3d dcross(v3d a, v3d b) { return D3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
+static inline double dlen(v3d a) { return sqrt(ddot(a, a)); }
+static inline v3d dnorm(v3d a) { return dsc(1.0 / dlen(a), a); }
+static inline v3d f2d(v3f a) { return D3(a.x, a.y, a.z); }
+
+/* Parameters: per object [kd r,g,b, ks r,g,b, log shininess, reflectivity] (8 doubles),
+ * per light [position xyz, colour rgb] (6 doubles).  Gradients: per object
+ * [kd rgb, ks rgb, log shininess] (7), per light [colour rgb, position xyz] (6). */
+typedef struct {
+  const oscene* s;
+  const double* mp;  /* nobj x 8 */
+  const double* lp;  /* nl x 6 */
+} f64ctx;
+
+/* One frozen path in FP64: re-derive each bounce's hit from the stored triangle id and
+ * shade it; when g != NULL accumulate the adjoint of <g, colour>. */
+static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, int y, float ox,
+                    float oy, const int32_t* hits, const uint32_t* shadows, int trace_depth,
+                    const double* g, double* gm, double* gl) {
+  const oscene* s = c->s;
+  double nw = w / 2.0, nh = hgt / 2.0;
+  double aa = ((x + (double)ox) - nw) / nw, bb = ((y + (double)oy) - nh) / nh;
+  v3d campos = D3(cam[0], cam[1], cam[2]);
+  v3d d = dnorm(dadd(dadd(dsc(aa, D3(cam[6], cam[7], cam[8])), dsc(bb, D3(cam[9], cam[10], cam[11]))),
+                     D3(cam[3], cam[4], cam[5])));
+  v3d o = campos;
+  v3d col = D3(0, 0, 0);
+  double T = 1.0;
+  for (int k = 0; k <= trace_depth && k < MAXB; ++k) {
+    int id = hits[k];
+    if (id < 0) break;
+    int p = s->pos_of_id[id];
+    v3d v1 = f2d(s->v1[p]), e1 = f2d(s->e1[p]), e2 = f2d(s->e2[p]);
+    v3d Pm = dcross(d, e2);
+    double det = ddot(e1, Pm);
+    v3d Tv = dsub(o, v1);
+    v3d Q = dcross(Tv, e1);
+    double t = ddot(e2, Q) / det, u = ddot(Tv, Pm) / det, v = ddot(d, Q) / det;
+    v3d P = dadd(o, dsc(t, d));
+    v3d N = dnorm(dadd(dadd(dsc(1.0 - u - v, f2d(s->n1[p])), dsc(u, f2d(s->n2[p]))), dsc(v, f2d(s->n3[p]))));
+    int ob = (int)s->obj[p];
+    const double* m = c->mp + 8 * ob;
+    double shin = exp(m[6]);
+    v3d V = dnorm(dsub(campos, P));
+    for (int li = 0; li < s->nl; ++li) {
+      if (shadows[k] & (1u << li)) continue;
+      const double* l = c->lp + 6 * li;
+      v3d uvec = dsub(D3(l[0], l[1], l[2]), P);
+      double ul = dlen(uvec);
+      v3d L = dsc(1.0 / ul, uvec);
+      double ndl = ddot(N, L);
+      v3d wv = dsub(dsc(2.0 * ndl, N), L);
+      double wl = dlen(wv);
+      v3d R = dsc(1.0 / wl, wv);
+      double fd = ndl > 0.0 ? ndl : 0.0;
+      double vr = ddot(V, R);
+      double fs = vr > 0.0 ? pow(vr, shin) : 0.0;
+      double C[3] = {l[3], l[4], l[5]};
+      col.x += T * (fd * m[0] * C[0] + fs * C[0] * m[3]);
+      col.y += T * (fd * m[1] * C[1] + fs * C[1] * m[4]);
+      col.z += T * (fd * m[2] * C[2] + fs * C[2] * m[5]);
+      if (!g) continue;
+      double* gmo = gm + 7 * ob;
+      double* glo = gl + 6 * li;
+      double a = 0.0, b = 0.0, sl = 0.0;
+      for (int ch = 0; ch < 3; ++ch) {
+        double gc = g[ch] * T;
+        gmo[ch] += gc * fd * C[ch];
+        gmo[3 + ch] += gc * fs * C[ch];
+        glo[ch] += gc * (fd * m[ch] + fs * m[3 + ch]);
+        a += gc * C[ch] * m[ch];
+        b += gc * C[ch] * m[3 + ch];
+      }
+      if (vr > 0.0) {
+        sl = b * fs * log(vr) * shin;
+        gmo[6] += sl;
+      }
+      v3d gp = D3(0, 0, 0);
+      if (ndl > 0.0) {
+        v3d gd = dsc(1.0 / ul, dsub(N, dsc(ndl, L)));
+        gp = dadd(gp, dsc(a, gd));
+      }
+      if (vr > 0.0) {
+        v3d q = dsc(1.0 / wl, dsub(V, dsc(vr, R)));
+        v3d q2 = dsub(dsc(2.0 * ddot(N, q), N), q);
+        v3d gs = dsc(1.0 / ul, dsub(q2, dsc(ddot(L, q2), L)));
+        double dfs = shin * pow(vr, shin - 1.0);
+        gp = dadd(gp, dsc(b * dfs, gs));
+      }
+      glo[3] += gp.x; glo[4] += gp.y; glo[5] += gp.z;
+    }
+    double refl = m[7];
+    if (!(refl > 0.0) || k + 1 > trace_depth) break;
+    T *= refl;
+    v3d r = dsub(d, dsc(2.0 * ddot(N, d), N));
+    v3d rd = dnorm(r);
+    o = dadd(P, dsc(1e-3, rd));
+    d = rd;
+  }
+  return col;
+}
+
+/* Frozen-visibility FP64 render of n_views cameras (cams: n_views x 12; every view has
+ * w x hgt pixels and spp == 1 at pixel_offset).  hits / shadows: [n_views*w*hgt, 8].
+ * rgb_out: [n_views*w*hgt, 3].  If g is non-NULL, also writes gradients of <g, rgb>. */
+int oracle_frozen_f64(void* h, const float* cams, int n_views, int w, int hgt, float pixel_offset,
+                      int trace_depth, const int32_t* hits, const uint32_t* shadows,
+                      const double* mat_params, const double* light_params, double* rgb_out,
+                      const double* g, double* grad_mat, double* grad_light, int nthreads) {
+  const oscene* s = (const oscene*)h;
+  f64ctx c = {s, mat_params, light_params};
+  size_t npx = (size_t)w * hgt;
+  int nth = nthreads > 0 ? nthreads : 1;
+  size_t gms = (size_t)7 * s->nobj, gls = (size_t)6 * s->nl;
+  double* gmt = g ? calloc((size_t)nth * gms + 1, sizeof(double)) : NULL;
+  double* glt = g ? calloc((size_t)nth * gls + 1, sizeof(double)) : NULL;
+#pragma omp parallel num_threads(nth)
+  {
+    int tid = omp_get_thread_num();
+#pragma omp for schedule(dynamic, 64)
+    for (long long i = 0; i < (long long)(n_views * npx); ++i) {
+      int view = (int)(i / (long long)npx);
+      int p = (int)(i % (long long)npx);
+      const float* cam = cams + 12 * view;
+      v3d col = f64_path(&c, cam, w, hgt, p % w, p / w, pixel_offset, pixel_offset, hits + MAXB * i,
+                         shadows + MAXB * i, trace_depth, g ? g + 3 * i : NULL,
+                         g ? gmt + gms * tid : NULL, g ? glt + gls * tid : NULL);
+      if (rgb_out) { rgb_out[3 * i] = col.x; rgb_out[3 * i + 1] = col.y; rgb_out[3 * i + 2] = col.z; }
+    }
+  }
+  if (g) {
+    memset(grad_mat, 0, sizeof(double) * gms);
+    memset(grad_light, 0, sizeof(double) * gls);
+    for (int t = 0; t < nth; ++t) {
+      for (size_t k = 0; k < gms; ++k) grad_mat[k] += gmt[gms * t + k];
+      for (size_t k = 0; k < gls; ++k) grad_light[k] += glt[gls * t + k];
+    }
+    free(gmt); free(glt);
+  }
+  return 0;
+}

@@ -1,0 +1,308 @@
+// Test-only harness around the reference's own CPU renderer.
+//
+// This file is test infrastructure: it is linked with the reference's CPU sources
+// (src/Scene.cpp, src/RayTracer.cpp, src/BVH.cpp, src/Triangle.cpp, src/Box.cu,
+// src/Material.cpp, src/RayIntersection.cpp, src/LightSource.cpp, src/getTime.cpp)
+// into oracle/_ref/libeosref.so by oracle/Makefile.  Only the tests, the smoke check
+// and the CPU-baseline leg of the benchmark load it.  It never ships with the product.
+//
+// What it adds on top of the reference:
+//  * builds a Scene of Triangle surfaces from flat float32 arrays with identity
+//    transforms (src/Scene.cpp:47-106, src/Triangle.h:35-41);
+//  * gives every triangle its own material index (a per-triangle copy of its object's
+//    Material) so the hit triangle id can be read back from
+//    RayIntersection::getMaterialIndex (src/RayIntersection.h:51-55, src/Triangle.cpp:50-51);
+//  * evaluates the reference's private RayTracer::rayTrace per pixel to get the FP32
+//    colour before the 8-bit quantisation of src/RayTracer.cpp:150-153;
+//  * replays the bounce path (closest hit, per-light shadow ray, mirror ray) through the
+//    public Scene queries with the ray construction of src/RayTracer.cpp:119-145,326-359.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <stack>
+#include <vector>
+#include <omp.h>
+#include <glm/glm.hpp>
+#include <glm/gtx/type_aligned.hpp>
+
+// RayTracer::rayTrace is private in the reference; the harness needs it to read the
+// FP32 colour of one primary ray.  Standard headers are included above, so the macro
+// only reaches the reference's own class definitions.
+#define private public
+#include "RayTracer.h"
+#include "Scene.h"
+#include "Triangle.h"
+#include "morton.h"
+#undef private
+
+double getRealTime();
+
+namespace {
+
+constexpr int kMaxBounces = 8;
+constexpr int32_t kHitNone = -1;      // ray traced, nothing hit
+constexpr int32_t kHitUntraced = -2;  // bounce not reached
+
+struct RefScene {
+  Scene scene;
+  glm::mat4 identity{1.0f};
+  glm::mat4 identity_inv{1.0f};
+  glm::mat4 identity_inv_t{1.0f};
+  std::vector<Material> object_materials;
+  std::vector<Triangle*> triangles;
+  std::vector<LightSource*> lights;
+  int max_leaf = 0;
+  int n_nodes = 0;
+};
+
+Camera make_camera(const float* c, int w, int h) {
+  Camera cam;
+  cam.setPosition(glm::vec3(c[0], c[1], c[2]));
+  cam.setViewingDirection(glm::vec3(c[3], c[4], c[5]));
+  cam.setRightVector(glm::vec3(c[6], c[7], c[8]));
+  cam.setUpVector(glm::vec3(c[9], c[10], c[11]));
+  cam.setWidth(w);
+  cam.setHeight(h);
+  return cam;
+}
+
+// Primary ray of pixel (x, y), src/RayTracer.cpp:119-145; pixel_offset 0 is the
+// reference's own integer-corner convention, 0.5 samples pixel centres.
+Ray primary_ray(const Camera& camera, int x, int y, float ox, float oy) {
+  float norm_width = camera.getWidth() / 2.0f;
+  float norm_height = camera.getHeight() / 2.0f;
+  float inv_norm_width = 1.0f / norm_width;
+  float inv_norm_height = 1.0f / norm_height;
+  float bb = (((float)y + oy) - norm_height) * inv_norm_height;
+  float aa = (((float)x + ox) - norm_width) * inv_norm_width;
+  glm::vec3 d = (aa * camera.getRightVector()) + (bb * camera.getUpVector()) + camera.getViewingDirection();
+  d = glm::normalize(d);
+  Ray ray;
+  ray.setOrigin(camera.getPosition());
+  ray.setDirection(d);
+  return ray;
+}
+
+// Bounce path of one primary ray: the same queries and ray construction as
+// RayTracer::rayTrace / shadeIntersection (src/RayTracer.cpp:268-359).
+void replay_path(const RefScene& rs, Ray ray, int trace_depth, int32_t* hits,
+                 uint32_t* shadows, long long* cnt) {
+  const float epsilon = 1e-3f;
+  const Scene& scene = rs.scene;
+  for (int depth = 0; depth < kMaxBounces; ++depth) {
+    if (depth > trace_depth) return;
+    RayIntersection isect;
+    cnt[depth == 0 ? 0 : 2]++;
+    bool hit = scene.findMinDistanceIntersectionBVH(ray, isect);
+    if (!hit) {
+      hits[depth] = kHitNone;
+      return;
+    }
+    int id = isect.getMaterialIndex();
+    hits[depth] = id;
+    const glm::vec3& P = isect.getPoint();
+    uint32_t mask = 0;
+    int nl = scene.getNumLightSources();
+    for (int i = 0; i < nl; ++i) {
+      const LightSource* light = scene.getLightSource(i);
+      glm::vec3 sd = glm::normalize(glm::vec3(light->getPosition()) - P);
+      glm::vec3 so = P + epsilon * sd;
+      Ray sray;
+      sray.setOrigin(so);
+      sray.setDirection(sd);
+      cnt[1]++;
+      if (scene.shadowRayVisibilityBVH(sray)) mask |= 1u << i;
+    }
+    shadows[depth] = mask;
+    const Material& m = scene.getMaterialAtIndex(id);
+    if (!m.isReflective()) return;
+    glm::vec3 rd = glm::normalize(glm::reflect(ray.getDirection(), isect.getNormal()));
+    glm::vec3 ro = P + epsilon * rd;
+    ray.setOrigin(ro);
+    ray.setDirection(rd);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Builds the reference Scene and its BVH (Scene::flush, src/Scene.cpp:204-209).
+// build_threads = 1 gives a deterministic tree: the SAH sweep's OpenMP loop races on
+// shared temporaries otherwise (src/BVH.cpp:454-480).
+void* eosref_scene_create(const float* verts, const float* normals, int nv, const uint32_t* tris,
+                          const uint32_t* tri_obj, int nt, const float* mats, int nobj,
+                          const float* lights, int nl, int build_threads, double* build_seconds) {
+  (void)nv;
+  RefScene* rs = new RefScene();
+  rs->object_materials.resize(nobj);
+  for (int k = 0; k < nobj; ++k) {
+    const float* m = mats + 8 * k;
+    Material mat(0.0f, glm::vec4(m[0], m[1], m[2], 1.0f), glm::vec4(m[3], m[4], m[5], 1.0f),
+                 (int)m[6]);
+    mat.setReflective(m[7] > 0.0f);
+    mat.setReflectionIntensity(m[7]);
+    mat.setTransparent(false);
+    mat.setRefractiveIndex(1.0f);
+    rs->object_materials[k] = mat;
+  }
+  rs->scene.setMaxTracedDepth(8);
+  rs->scene.setAmbientRefractiveIndex(1.0f);
+  rs->scene.useBvh(true);
+  rs->scene.setAASamples(1);
+  rs->triangles.resize(nt);
+  for (int i = 0; i < nt; ++i) {
+    const uint32_t* t = tris + 3 * i;
+    glm::vec3 v[3], n[3];
+    for (int j = 0; j < 3; ++j) {
+      v[j] = glm::vec3(verts[3 * t[j]], verts[3 * t[j] + 1], verts[3 * t[j] + 2]);
+      n[j] = glm::vec3(normals[3 * t[j]], normals[3 * t[j] + 1], normals[3 * t[j] + 2]);
+    }
+    Triangle* tri = new Triangle(v[0], v[1], v[2], n[0], n[1], n[2]);
+    tri->setTransformation(rs->identity);
+    tri->setInverseTransformation(rs->identity_inv);
+    tri->setInverseTransposeTransformation(rs->identity_inv_t);
+    tri->setMaterial(rs->object_materials[tri_obj[i]]);
+    tri->setMaterialIndex(i);
+    tri->setTransformationIndex(0);
+    rs->scene.addMaterial(rs->object_materials[tri_obj[i]]);
+    rs->scene.addSurface(tri);
+    rs->triangles[i] = tri;
+  }
+  for (int i = 0; i < nl; ++i) {
+    const float* l = lights + 6 * i;
+    LightSource* ls = new LightSource(glm::vec4(l[0], l[1], l[2], 1.0f), glm::vec4(l[3], l[4], l[5], 1.0f));
+    rs->lights.push_back(ls);
+    rs->scene.addLightSource(ls);
+  }
+  int prev = omp_get_max_threads();
+  omp_set_num_threads(build_threads > 0 ? build_threads : 1);
+  double t0 = getRealTime();
+  rs->scene.flush();
+  double t1 = getRealTime();
+  omp_set_num_threads(prev);
+  if (build_seconds) *build_seconds = t1 - t0;
+  const BVH& bvh = rs->scene.getBVH();
+  BvhNode* nodes = bvh.getNodesBuffer();
+  rs->n_nodes = bvh.getNodesBufferSize();
+  for (int i = 0; i < rs->n_nodes; ++i)
+    if (nodes[i].type == BVH_LEAF) rs->max_leaf = std::max(rs->max_leaf, nodes[i].numSurfacesEncapulated);
+  return rs;
+}
+
+void eosref_scene_stats(void* h, int* n_nodes, int* max_leaf) {
+  RefScene* rs = (RefScene*)h;
+  *n_nodes = rs->n_nodes;
+  *max_leaf = rs->max_leaf;
+}
+
+void eosref_scene_destroy(void* h) {
+  RefScene* rs = (RefScene*)h;
+  for (Triangle* t : rs->triangles) delete t;
+  for (LightSource* l : rs->lights) delete l;
+  delete rs;
+}
+
+// FP32 colour and bounce path per pixel.  pix == NULL renders every pixel in row-major
+// order (row 0 = bottom, as the reference); otherwise npix listed pixel indices.
+// hits / shadows are [npix, 8]; counts gets primary, shadow and secondary ray counts.
+int eosref_render(void* h, const float* cam12, int w, int hgt, float pixel_offset, int trace_depth,
+                  int nthreads, const int32_t* pix, int npix, float* rgb, int32_t* hits,
+                  uint32_t* shadows, long long* counts, double* seconds) {
+  RefScene* rs = (RefScene*)h;
+  Camera cam = make_camera(cam12, w, hgt);
+  RayTracer rt;
+  rt.setAASamples(RAYTRACER_NO_AA);
+  rt.setTracedDepth(trace_depth);
+  if (rt.getTracedDepth() != trace_depth) return -1;  // the reference cannot set depth 0
+  int n = pix ? npix : w * hgt;
+  long long c0 = 0, c1 = 0, c2 = 0;
+  double t0 = getRealTime();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : c0, c1, c2)
+  for (int i = 0; i < n; ++i) {
+    int p = pix ? pix[i] : i;
+    int x = p % w, y = p / w;
+    Ray ray = primary_ray(cam, x, y, pixel_offset, pixel_offset);
+    glm::vec4 c = rt.rayTrace(rs->scene, cam, ray, 0);
+    rgb[3 * i] = c.x;
+    rgb[3 * i + 1] = c.y;
+    rgb[3 * i + 2] = c.z;
+    if (hits) {
+      int32_t* hh = hits + kMaxBounces * i;
+      uint32_t* ss = shadows + kMaxBounces * i;
+      for (int k = 0; k < kMaxBounces; ++k) { hh[k] = kHitUntraced; ss[k] = 0; }
+      long long cnt[3] = {0, 0, 0};
+      replay_path(*rs, ray, trace_depth, hh, ss, cnt);
+      c0 += cnt[0];
+      c1 += cnt[1];
+      c2 += cnt[2];
+    }
+  }
+  double t1 = getRealTime();
+  if (counts) { counts[0] = c0; counts[1] = c1; counts[2] = c2; }
+  if (seconds) *seconds = t1 - t0;
+  return 0;
+}
+
+// The reference's own frame call, RayTracer::render (src/RayTracer.cpp:85-174), into a
+// caller-owned RGBA8 buffer.  This is what the CPU baseline times.
+int eosref_render_rgba8(void* h, const float* cam12, int w, int hgt, int trace_depth, int nthreads,
+                        unsigned char* out, double* seconds) {
+  RefScene* rs = (RefScene*)h;
+  Camera cam = make_camera(cam12, w, hgt);
+  RayTracer rt;
+  rt.setAASamples(RAYTRACER_NO_AA);
+  rt.setTracedDepth(trace_depth);
+  int prev = omp_get_max_threads();
+  omp_set_num_threads(nthreads > 0 ? nthreads : 1);
+  double t0 = getRealTime();
+  rt.render(rs->scene, cam, out);
+  double t1 = getRealTime();
+  omp_set_num_threads(prev);
+  if (seconds) *seconds = t1 - t0;
+  return 0;
+}
+
+// Nearest hit / shadow visibility of arbitrary rays through the public Scene queries
+// (src/Scene.cpp:145-158).  rays: [n, 6] origin, direction.
+void eosref_closest_hit(void* h, const float* rays, int n, int32_t* ids, float* pts) {
+  RefScene* rs = (RefScene*)h;
+  for (int i = 0; i < n; ++i) {
+    const float* r = rays + 6 * i;
+    Ray ray;
+    ray.setOrigin(glm::vec3(r[0], r[1], r[2]));
+    ray.setDirection(glm::vec3(r[3], r[4], r[5]));
+    RayIntersection isect;
+    bool hit = rs->scene.findMinDistanceIntersectionBVH(ray, isect);
+    ids[i] = hit ? isect.getMaterialIndex() : kHitNone;
+    if (pts) {
+      glm::vec3 p = isect.getPoint();
+      pts[3 * i] = hit ? p.x : 0.0f;
+      pts[3 * i + 1] = hit ? p.y : 0.0f;
+      pts[3 * i + 2] = hit ? p.z : 0.0f;
+    }
+  }
+}
+
+void eosref_any_hit(void* h, const float* rays, int n, uint8_t* occluded) {
+  RefScene* rs = (RefScene*)h;
+  for (int i = 0; i < n; ++i) {
+    const float* r = rays + 6 * i;
+    Ray ray;
+    ray.setOrigin(glm::vec3(r[0], r[1], r[2]));
+    ray.setDirection(glm::vec3(r[3], r[4], r[5]));
+    occluded[i] = rs->scene.shadowRayVisibilityBVH(ray) ? 1 : 0;
+  }
+}
+
+// The reference's 30-bit 3-D Morton encoder (src/morton.h:30-48), for golden vectors.
+void eosref_morton3(const uint32_t* xyz, int n, uint32_t* out) {
+  for (int i = 0; i < n; ++i) out[i] = EncodeMorton3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+}
+
+}  // extern "C"

@@ -1,0 +1,60 @@
+"""Generates the golden fixtures in this directory from the reference's own CPU code.
+
+Runs the reference renderer compiled from its sources (oracle/_ref/libeosref.so, built by
+oracle/Makefile from the reference tree) and its EncodeMorton3 on seeded inputs and
+stores the outputs as small .npz files.  The GPU box has no reference tree, so the
+tests read these files there.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from eos_b200 import scenes  # noqa: E402
+
+
+def render_case(name, scene, cam, trace_depth):
+    ref = oracle.RefRenderer(scene, build_threads=1)
+    r = ref.render(cam, trace_depth, pixel_offset=0.0, nthreads=os.cpu_count())
+    nb = trace_depth + 1
+    rgba8, _ = ref.render_rgba8(cam, trace_depth, nthreads=os.cpu_count())
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), rgb=r["rgb"], hits=r["hits"][:, :nb],
+                        shadows=r["shadows"][:, :nb].astype(np.uint8 if scene.n_lights <= 8 else np.uint32),
+                        counts=r["counts"], rgba8=rgba8, cam=cam.as_array(),
+                        size=np.array([cam.width, cam.height, trace_depth]),
+                        ref_nodes=np.array([ref.n_nodes, ref.max_leaf]))
+    print(name, r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
+
+
+def morton_case():
+    rng = np.random.default_rng(7)
+    xyz = rng.integers(0, 1024, size=(4096, 3), dtype=np.uint32)
+    edge = np.array([[0, 0, 0], [1023, 1023, 1023], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1023, 0, 0],
+                     [0, 1023, 0], [0, 0, 1023], [512, 256, 128], [2047, 4095, 1024]], np.uint32)
+    xyz = np.concatenate([edge, xyz])
+    codes = oracle.ref_morton3(xyz)
+    np.savez_compressed(os.path.join(HERE, "morton3.npz"), xyz=xyz, codes=codes)
+    print("morton3", codes[:10])
+
+
+def main():
+    oracle.build(ref=True)
+    morton_case()
+    render_case("config1_128", scenes.config1_scene(), scenes.config1_camera(128, 128), 1)
+    for seed in (11, 12):
+        sc = scenes.small_random_scene(seed, n_spheres=5, level=2, lights=3, refl=0.6)
+        cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 96, 72)
+        render_case(f"small{seed}", sc, cam, 3)
+
+
+if __name__ == "__main__":
+    main()

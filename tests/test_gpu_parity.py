@@ -1,0 +1,232 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle, the compiled reference
+and the golden fixtures recorded from the reference."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from eos_b200 import api, scenes
+from tests.parity import RGB_TOL, classify, path_mismatch, primary_rays
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def paths_split(p):
+    p = p.cpu().numpy() if hasattr(p, "cpu") else p
+    return p[:, :8], p[:, 8:].view(np.uint32)
+
+
+def gpu_render(ctx, dsc, cam, td, off, spp=1, mode="plain", outputs=("rgb", "paths"), **kw):
+    r = api.render(ctx, dsc, cam, td, pixel_offset=off, spp=spp, mode=mode, outputs=outputs, device=False, **kw)
+    return r
+
+
+@pytest.fixture(scope="module")
+def c1(ctx):
+    sc = scenes.config1_scene()
+    return sc, api.DeviceScene(ctx, sc)
+
+
+def test_morton_codes_and_order_bit_exact(ctx, c1):
+    sc, dsc = c1
+    codes, order = dsc.morton()
+    oc, oo = oracle.morton(sc.verts, sc.tris)
+    assert np.array_equal(order, oo.astype(np.uint32))
+    assert np.array_equal(codes, oc[oo])
+
+
+def test_morton_config2_bit_exact(ctx):
+    sc = scenes.config2_scene()
+    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
+    codes, order = dsc.morton()
+    oc, oo = oracle.morton(sc.verts, sc.tris)
+    assert np.array_equal(order, oo.astype(np.uint32))
+    assert np.array_equal(codes, oc[oo])
+    info = dsc.info()
+    assert info["n_tris"] == sc.n_tris == 1_056_768
+
+
+def test_plain_matches_oracle_exactly_config1(ctx, c1):
+    sc, dsc = c1
+    cam = scenes.config1_camera()
+    g = gpu_render(ctx, dsc, cam, 1, 0.5)
+    o = oracle.Oracle(sc).render(cam, 1, pixel_offset=0.5)
+    gh, gs = paths_split(g["paths"])
+    assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+    d = np.abs(g["rgb"] - o["rgb"]).max(1)
+    assert d.max() <= RGB_TOL
+    assert (d == 0).mean() > 0.99
+    st = g["stats"]
+    assert (st["primary_rays"], st["shadow_rays"], st["secondary_rays"]) == tuple(int(v) for v in o["counts"])
+
+
+def test_plain_matches_compiled_reference_config1(ctx, c1):
+    """512x512, reference pixel convention: hit ids + paths bit-exact except flagged paths."""
+    if not oracle.ref_available():
+        pytest.skip("reference CPU build unavailable")
+    sc, dsc = c1
+    cam = scenes.config1_camera()
+    g = gpu_render(ctx, dsc, cam, 1, 0.0, outputs=("rgb", "paths", "rgba8"))
+    refr = oracle.RefRenderer(sc)
+    ref = refr.render(cam, 1, pixel_offset=0.0)
+    o = oracle.Oracle(sc).render(cam, 1, pixel_offset=0.0)
+    gh, gs = paths_split(g["paths"])
+    mm = path_mismatch(gh, gs, ref["hits"], ref["shadows"], 2)
+    c = classify(mm, o["flags"])
+    print("config1 512^2 vs reference:", c)
+    assert c["unexplained"] == 0, c
+    d = np.abs(g["rgb"] - ref["rgb"]).max(1)
+    assert d[~mm].max() <= RGB_TOL
+    rgba, _ = refr.render_rgba8(cam, 1)
+    q_mm = (g["rgba8"].reshape(-1, 4) != rgba.reshape(-1, 4)).any(1)
+    assert (q_mm & ~mm).sum() <= 0.001 * mm.size  # 8-bit output equal outside flagged paths
+
+
+@pytest.mark.parametrize("name,scene_fn", [
+    ("config1_128", lambda: scenes.config1_scene()),
+    ("small11", lambda: scenes.small_random_scene(11, n_spheres=5, level=2, lights=3, refl=0.6)),
+    ("small12", lambda: scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)),
+])
+def test_plain_matches_reference_golden(ctx, name, scene_fn):
+    gd = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    W, H, td = (int(v) for v in gd["size"])
+    cam = scenes.CameraData(*[gd["cam"][3 * i:3 * i + 3] for i in range(4)], W, H)
+    sc = scene_fn()
+    dsc = api.DeviceScene(ctx, sc)
+    g = gpu_render(ctx, dsc, cam, td, 0.0, outputs=("rgb", "paths", "rgba8"))
+    o = oracle.Oracle(sc).render(cam, td, pixel_offset=0.0)
+    gh, gs = paths_split(g["paths"])
+    nb = td + 1
+    mm = path_mismatch(gh, gs, gd["hits"], gd["shadows"], nb)
+    c = classify(mm, o["flags"])
+    assert c["unexplained"] == 0, c
+    assert np.abs(g["rgb"] - gd["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    # and bit-exact against the oracle everywhere
+    assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+
+
+@pytest.mark.parametrize("spp,td", [(1, 1), (2, 3)])
+def test_wavefront_equals_plain(ctx, spp, td):
+    sc = scenes.small_random_scene(31, n_spheres=6, level=3, lights=3, refl=0.7)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 161, 97)  # ragged tiles
+    a = gpu_render(ctx, dsc, cam, td, 0.5, spp=spp, jitter_seed=5)
+    b = gpu_render(ctx, dsc, cam, td, 0.5, spp=spp, jitter_seed=5, mode="wavefront")
+    assert np.array_equal(a["paths"], b["paths"])
+    assert np.array_equal(a["rgb"], b["rgb"])
+    for k in ("primary_rays", "shadow_rays", "secondary_rays"):
+        assert a["stats"][k] == b["stats"][k]
+    if spp == 2:
+        o = oracle.Oracle(sc).render(cam, td, pixel_offset=0.5, spp=2, jitter_seed=5)
+        gh, gs = paths_split(a["paths"])
+        assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+        assert np.abs(a["rgb"] - o["rgb"]).max() <= RGB_TOL
+
+
+def test_batch_matches_single_renders(ctx):
+    import torch
+    s1 = scenes.config1_scene()
+    s2 = scenes.small_random_scene(41, n_spheres=8, level=3, lights=2, refl=0.5)
+    d1, d2 = api.DeviceScene(ctx, s1), api.DeviceScene(ctx, s2)
+    jobs = [api.BatchJob(d1, scenes.look_at((0, 1.5, 4), (0, 0, 0), 60, 256, 256), 1),
+            api.BatchJob(d2, scenes.look_at((1, 3, 9), (0, 0, 0), 50, 320, 180), 2),
+            api.BatchJob(d1, scenes.look_at((3, 2, -3), (0, 0, 0), 40, 96, 128), 2, spp=2, jitter_seed=3)]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    for rep in range(2):  # second call replays the captured graph
+        st = api.render_batch(ctx, jobs, outs)
+        torch.cuda.synchronize()
+        for j, o in zip(jobs, outs):
+            ref = gpu_render(ctx, j.scene, j.camera, j.trace_depth, j.pixel_offset, spp=j.spp,
+                             jitter_seed=j.jitter_seed)
+            assert np.array_equal(o["rgb"].cpu().numpy(), ref["rgb"])
+            assert np.array_equal(o["paths"].cpu().numpy(), ref["paths"])
+        assert st["primary_rays"] == sum(j.camera.width * j.camera.height * j.spp for j in jobs)
+
+
+def _random_rays(n, seed, lo=-3, hi=3):
+    rng = np.random.default_rng(seed)
+    r = np.concatenate([rng.uniform(lo, hi, (n, 3)), rng.normal(size=(n, 3))], 1).astype(np.float32)
+    r[:, 3:] /= np.linalg.norm(r[:, 3:], axis=1, keepdims=True)
+    ax = np.zeros((n // 4, 6), np.float32)
+    ax[:, :3] = rng.uniform(lo, hi, (n // 4, 3))
+    ax[np.arange(n // 4), 3 + rng.integers(0, 3, n // 4)] = rng.choice([-1.0, 1.0], n // 4)
+    return np.concatenate([r, ax])
+
+
+@pytest.mark.parametrize("leaf", [1, 4, 8])
+def test_queries_match_oracle(ctx, leaf):
+    sc = scenes.small_random_scene(51, n_spheres=8, level=3, lights=2)
+    dsc = api.DeviceScene(ctx, sc, leaf_size=leaf)
+    orc = oracle.Oracle(sc)
+    rays = _random_rays(20000, 9)
+    ids, t = api.trace_closest(ctx, dsc, rays)
+    oid, ot, _ = orc.closest(rays)
+    assert np.array_equal(ids, oid)
+    assert np.array_equal(t[ids >= 0], ot[oid >= 0])
+    occ = api.trace_any(ctx, dsc, rays)
+    assert np.array_equal(occ, orc.any(rays))
+
+
+def test_edge_scenes(ctx):
+    cam = scenes.look_at((0, 0, 5), (0, 0, 0), 60, 33, 17)
+    mat = np.array([[0.5, 0.5, 0.5, 0.2, 0.2, 0.2, 16, 0.3]], np.float32)
+    light = np.array([[2, 2, 2, 1, 1, 1]], np.float32)
+    # empty scene: every ray misses
+    empty = scenes.SceneData(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0), mat, light)
+    d0 = api.DeviceScene(ctx, empty)
+    r = gpu_render(ctx, d0, cam, 2, 0.5)
+    assert np.all(r["rgb"] == 0)
+    gh, _ = paths_split(r["paths"])
+    assert np.all(gh[:, 0] == -1) and np.all(gh[:, 1:] == -2)
+    # one triangle, facing the camera; plus a degenerate (zero-area) one
+    V = np.array([[-1, -1, 0], [1, -1, 0], [0, 1, 0], [0, 0, 1], [0, 0, 1], [0, 0, 1]], np.float32)
+    N = np.tile([[0, 0, 1]], (6, 1)).astype(np.float32)
+    for tris in (np.array([[0, 1, 2]]), np.array([[0, 1, 2], [3, 4, 5]])):
+        s1 = scenes.SceneData(V, N, tris, np.zeros(len(tris)), mat, light)
+        d1 = api.DeviceScene(ctx, s1)
+        g = gpu_render(ctx, d1, cam, 2, 0.5)
+        o = oracle.Oracle(s1).render(cam, 2, pixel_offset=0.5)
+        gh, gs = paths_split(g["paths"])
+        assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+        assert np.abs(g["rgb"] - o["rgb"]).max() <= RGB_TOL
+        assert (gh[:, 0] == 0).sum() > 50
+
+
+def test_invalid_arguments_report_status(ctx):
+    from eos_b200._lib import EosError
+    mat = np.array([[0.5, 0.5, 0.5, 0.2, 0.2, 0.2, 16, 0.0]], np.float32)
+    V = np.zeros((3, 3), np.float32)
+    bad = scenes.SceneData(V, V, np.array([[0, 1, 7]]), np.zeros(1), mat, np.zeros((0, 6)))
+    with pytest.raises(EosError) as e:
+        api.DeviceScene(ctx, bad)
+    assert e.value.code == 1
+    sc = scenes.small_random_scene(3)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0, 0, 5), (0, 0, 0), 60, 8, 8)
+    with pytest.raises(EosError):
+        api.render(ctx, dsc, cam, 8, device=False)  # trace_depth beyond EOS_MAX_BOUNCES - 1
+    with pytest.raises(EosError):
+        api.render(ctx, dsc, cam, 1, spp=0, device=False)
+    # the context stays usable after rejected calls
+    r = api.render(ctx, dsc, cam, 1, device=False)
+    assert r["rgb"].shape == (64, 3)
+
+
+def test_config2_sampled_pixels_match_oracle(ctx):
+    """1920x1080, ~1.06M triangles, depth 3, 4 lights: 30k sampled paths vs the oracle."""
+    sc = scenes.config2_scene()
+    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
+    cam = scenes.config2_camera()
+    g = api.render(ctx, dsc, cam, 2, pixel_offset=0.5, outputs=("rgb", "paths"), device=True)
+    rng = np.random.default_rng(0)
+    pix = np.sort(rng.choice(cam.width * cam.height, 30000, replace=False)).astype(np.int32)
+    o = oracle.Oracle(sc).render(cam, 2, pixel_offset=0.5, pixels=pix)
+    gp = g["paths"].cpu().numpy()[pix]
+    gh, gs = paths_split(gp)
+    assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+    assert np.abs(g["rgb"].cpu().numpy()[pix] - o["rgb"]).max() <= RGB_TOL
+    st = g["stats"]
+    assert st["primary_rays"] == cam.width * cam.height
+    assert st["shadow_rays"] > st["primary_rays"]

@@ -1,0 +1,157 @@
+"""CPU tests: the oracle pinned against the reference's golden vectors and, where the
+reference tree is present, against the compiled reference itself."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from eos_b200 import scenes
+from tests.parity import RGB_TOL, classify, path_mismatch, primary_rays
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, f"{name}.npz"))
+
+
+def test_morton_golden_vectors():
+    """EncodeMorton3 (src/morton.h:45-48) outputs recorded from the compiled reference."""
+    g = load("morton3")
+    xyz = g["xyz"].astype(np.uint64)
+
+    def spread(x):
+        x = x & 0x3FF
+        out = np.zeros_like(x)
+        for b in range(10):
+            out |= ((x >> b) & 1) << (3 * b)
+        return out
+
+    codes = (spread(xyz[:, 2]) << 2) + (spread(xyz[:, 1]) << 1) + spread(xyz[:, 0])
+    assert np.array_equal(codes.astype(np.uint32), g["codes"])
+
+
+def test_oracle_morton_order_is_stable_sort():
+    sc = scenes.small_random_scene(3)
+    codes, order = oracle.morton(sc.verts, sc.tris)
+    keys = codes[order].astype(np.uint64) << 32 | order.astype(np.uint64)
+    assert np.all(np.diff(keys.astype(np.int64)) > 0)
+    # duplicate centroids: identical triangles keep id order
+    v = np.zeros((3, 3), np.float32)
+    v[1, 0] = 1
+    v[2, 1] = 1
+    tris = np.array([[0, 1, 2]] * 5, np.uint32)
+    c, o = oracle.morton(v, tris)
+    assert list(o) == [0, 1, 2, 3, 4] and len(set(c.tolist())) == 1
+
+
+@pytest.mark.parametrize("name,scene_fn", [
+    ("config1_128", lambda: scenes.config1_scene()),
+    ("small11", lambda: scenes.small_random_scene(11, n_spheres=5, level=2, lights=3, refl=0.6)),
+    ("small12", lambda: scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)),
+])
+def test_oracle_matches_reference_golden(name, scene_fn):
+    """Oracle paths and colours vs the reference's own renderer output (golden file)."""
+    g = load(name)
+    W, H, td = (int(v) for v in g["size"])
+    cam = scenes.CameraData(*[g["cam"][3 * i:3 * i + 3] for i in range(4)], W, H)
+    sc = scene_fn()
+    r = oracle.Oracle(sc).render(cam, td, pixel_offset=0.0)
+    nb = td + 1
+    mm = path_mismatch(r["hits"], r["shadows"], g["hits"], g["shadows"], nb)
+    c = classify(mm, r["flags"])
+    assert c["unexplained"] == 0, c
+    assert c["mismatch"] <= 0.002 * c["paths"], c
+    d = np.abs(r["rgb"] - g["rgb"]).max(1)
+    assert d[~mm].max() <= RGB_TOL
+    # the restatement reproduces the reference's float colours exactly on matching paths
+    assert (d[~mm] == 0).mean() > 0.999
+    assert np.array_equal(r["counts"][0], g["counts"][0])
+
+
+def test_oracle_bvh_equals_brute_force():
+    sc = scenes.small_random_scene(5, n_spheres=6, level=2)
+    orc = oracle.Oracle(sc)
+    cam = scenes.look_at((1, 2.5, 8), (0, 0, 0), 60, 48, 40)
+    rays = primary_rays(cam, 0.5)
+    rng = np.random.default_rng(1)
+    rnd = np.concatenate([rng.uniform(-3, 3, (2000, 3)), rng.normal(size=(2000, 3))], 1).astype(np.float32)
+    rnd[:, 3:] /= np.linalg.norm(rnd[:, 3:], axis=1, keepdims=True)
+    # axis-parallel rays: exact zero direction components
+    ax = np.zeros((300, 6), np.float32)
+    ax[:, :3] = rng.uniform(-3, 3, (300, 3))
+    ax[np.arange(300), 3 + rng.integers(0, 3, 300)] = rng.choice([-1.0, 1.0], 300)
+    for R in (rays, rnd, ax):
+        a, ta, _ = orc.closest(R)
+        b, tb = orc.closest_brute(R)
+        assert np.array_equal(a, b)
+        assert np.array_equal(ta[a >= 0], tb[b >= 0])
+
+
+def test_oracle_any_hit_semantics():
+    sc = scenes.small_random_scene(6)
+    orc = oracle.Oracle(sc)
+    rng = np.random.default_rng(2)
+    r = np.concatenate([rng.uniform(-3, 3, (3000, 3)), rng.normal(size=(3000, 3))], 1).astype(np.float32)
+    r[:, 3:] /= np.linalg.norm(r[:, 3:], axis=1, keepdims=True)
+    occ = orc.any(r)
+    ids, _ = orc.closest_brute(r)
+    assert np.array_equal(occ.astype(bool), ids >= 0)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference CPU build unavailable")
+def test_oracle_matches_compiled_reference_config1_full():
+    """Full 512x512 config-1 frame: oracle vs the compiled reference renderer."""
+    sc = scenes.config1_scene()
+    cam = scenes.config1_camera()
+    ref = oracle.RefRenderer(sc).render(cam, 1, pixel_offset=0.0)
+    r = oracle.Oracle(sc).render(cam, 1, pixel_offset=0.0)
+    mm = path_mismatch(r["hits"], r["shadows"], ref["hits"], ref["shadows"], 2)
+    c = classify(mm, r["flags"])
+    assert c["unexplained"] == 0, c
+    d = np.abs(r["rgb"] - ref["rgb"]).max(1)
+    assert d[~mm].max() <= RGB_TOL
+
+
+def test_frozen_f64_adjoint_matches_central_differences():
+    """FP64 analytic adjoint vs central differences (step 1e-3) of the FP64 frozen render."""
+    sc = scenes.small_random_scene(21, n_spheres=4, level=2, lights=2, refl=0.4)
+    cams = [scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 24, 20),
+            scenes.look_at((-6.0, 4.0, 6.0), (0, -0.5, 0), 55.0, 24, 20)]
+    orc = oracle.Oracle(sc)
+    td = 2
+    hits, shadows = [], []
+    for c in cams:
+        r = orc.render(c, td, pixel_offset=0.5)
+        hits.append(r["hits"])
+        shadows.append(r["shadows"])
+    hits = np.concatenate(hits)
+    shadows = np.concatenate(shadows)
+    mp = sc.materials.astype(np.float64).copy()
+    mp[:, 6] = np.log(mp[:, 6])
+    lp = sc.lights.astype(np.float64).copy()
+    rng = np.random.default_rng(3)
+    target = rng.uniform(0, 0.5, (len(cams) * 24 * 20, 3))
+
+    def loss(m, l):
+        rgb = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, m, l)
+        return float(((rgb - target) ** 2).sum()), rgb
+
+    L0, rgb = loss(mp, lp)
+    g = 2.0 * (rgb - target)
+    _, gm, gl = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, mp, lp, g=g)
+    h = 1e-3
+    checks = [("m", 0, 0), ("m", 1, 4), ("m", 2, 6), ("m", 4, 2), ("l", 0, 0), ("l", 1, 4), ("l", 0, 3), ("l", 1, 5)]
+    for kind, i, j in checks:
+        m2, l2 = mp.copy(), lp.copy()
+        arr = m2 if kind == "m" else l2
+        orig = arr[i, 3 + j if kind == "l" and j < 3 else (j - 3 if kind == "l" else j)]
+        col = (3 + j) if (kind == "l" and j < 3) else ((j - 3) if kind == "l" else (j if j < 6 else 6))
+        arr[i, col] = orig + h
+        Lp, _ = loss(m2 if kind == "m" else mp, l2 if kind == "l" else lp)
+        arr[i, col] = orig - h
+        Lm, _ = loss(m2 if kind == "m" else mp, l2 if kind == "l" else lp)
+        fd = (Lp - Lm) / (2 * h)
+        an = gm[i, j] if kind == "m" else gl[i, j]
+        assert abs(fd - an) <= 1e-3 * max(1.0, abs(fd)), (kind, i, j, fd, an)
