@@ -1,0 +1,478 @@
+// eos.hpp -- header-only C++ drop-in for the reference's render-frame API, over eos_c.h.
+//
+// Mirrors the classes a caller of the reference uses to render a frame:
+//   Material, LightSource, Triangle (Surface), Scene   src/Material.h, src/LightSource.h,
+//                                                      src/Triangle.h, src/Scene.h
+//   Camera                                              src/Camera.h
+//   createCudaScene / cudaScene_t                       src/cudaStructures.h:86-98
+//   DeviceCameraHandler                                 src/DeviceCameraHandler.h
+//   DeviceRenderer::renderCudaSceneToHostBufferMegaKernel
+//                                                       src/DeviceRenderer.h:33-55
+//   MultiDeviceRenderer::renderSceneToHostBuffer        src/MultiDeviceRenderer.h:31-45
+//   RayTracer::render (same call, run on the GPU)       src/RayTracer.h:38-68
+// with the same names, argument meaning and output layout (RGBA8, row 0 = bottom).
+//
+// Differences a caller sees:
+//  * the frame has the CPU RayTracer's full semantics (shadow rays, mirror bounces up to
+//    the traced depth, its 8-bit quantisation) instead of the reference GPU kernel's
+//    primary-only shading;
+//  * errors throw eos::Error (with the eos_status) instead of exit();
+//  * vectors are any type with .x/.y/.z(/.w) members (glm types work unchanged);
+//  * per-surface transforms are applied to the vertices (M) and normals (M^-T) once in
+//    createCudaScene; with identity transforms the frame equals the reference bit for
+//    bit on hit ids and paths;
+//  * the scene must be triangles only, as the reference GPU upload requires
+//    (src/cudaStructures.cu:342-348); one GPU (the reference's split-frame multi-GPU mode
+//    is not part of this path).
+#ifndef EOS_EOS_HPP
+#define EOS_EOS_HPP
+
+#include <cmath>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../eos_c.h"
+
+namespace eos {
+
+struct Error : std::runtime_error {
+  eos_status status;
+  Error(eos_status s, const char* where)
+      : std::runtime_error(std::string(where) + ": " + eos_status_string(s)), status(s) {}
+};
+
+inline void check(eos_status s, const char* where) {
+  if (s != EOS_OK) throw Error(s, where);
+}
+
+struct vec3 {
+  float x = 0, y = 0, z = 0;
+  vec3() = default;
+  vec3(float a, float b, float c) : x(a), y(b), z(c) {}
+  template <class V>
+  vec3(const V& v) : x(v.x), y(v.y), z(v.z) {}
+};
+
+struct vec4 {
+  float x = 0, y = 0, z = 0, w = 0;
+  vec4() = default;
+  explicit vec4(float s) : x(s), y(s), z(s), w(s) {}
+  vec4(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+  template <class V>
+  vec4(const V& v) : x(v.x), y(v.y), z(v.z), w(v.w) {}
+};
+
+// Column-major 4x4 (m[col][row]), the layout of glm::mat4.
+struct mat4 {
+  float m[4][4];
+  mat4() : mat4(1.0f) {}
+  explicit mat4(float d) {
+    for (int c = 0; c < 4; ++c)
+      for (int r = 0; r < 4; ++r) m[c][r] = c == r ? d : 0.0f;
+  }
+  template <class M>
+  static mat4 from(const M& g) {
+    mat4 o;
+    for (int c = 0; c < 4; ++c)
+      for (int r = 0; r < 4; ++r) o.m[c][r] = g[c][r];
+    return o;
+  }
+  bool identity() const {
+    for (int c = 0; c < 4; ++c)
+      for (int r = 0; r < 4; ++r)
+        if (m[c][r] != (c == r ? 1.0f : 0.0f)) return false;
+    return true;
+  }
+};
+
+inline vec3 transform_point(const mat4& M, const vec3& p) {
+  return vec3(M.m[0][0] * p.x + M.m[1][0] * p.y + M.m[2][0] * p.z + M.m[3][0],
+              M.m[0][1] * p.x + M.m[1][1] * p.y + M.m[2][1] * p.z + M.m[3][1],
+              M.m[0][2] * p.x + M.m[1][2] * p.y + M.m[2][2] * p.z + M.m[3][2]);
+}
+
+// Normal transform by the inverse transpose of the upper 3x3 of M.
+inline vec3 transform_normal(const mat4& M, const vec3& n) {
+  double a[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) a[r][c] = M.m[c][r];
+  double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+               a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+  double inv[3][3];
+  inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+  inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+  inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+  inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+  inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+  inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+  inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+  inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+  inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+  // (M^-1)^T n
+  return vec3((float)(inv[0][0] * n.x + inv[1][0] * n.y + inv[2][0] * n.z),
+              (float)(inv[0][1] * n.x + inv[1][1] * n.y + inv[2][1] * n.z),
+              (float)(inv[0][2] * n.x + inv[1][2] * n.y + inv[2][2] * n.z));
+}
+
+// src/Material.h:46-78 (ambient stored, unused by the renderer as in the reference).
+class Material {
+ public:
+  Material() : m_Ambient(0.2f), m_Diffuse(1.0f), m_Specular(1.0f), m_Shininess(128) {}
+  Material(float ambient, vec4 diffuse, vec4 specular, int shininess)
+      : m_Ambient(ambient), m_Diffuse(diffuse), m_Specular(specular), m_Shininess(shininess) {}
+  void setAmbientIntensity(float a) { m_Ambient = a; }
+  void setDiffuseColor(vec4 c) { m_Diffuse = c; }
+  void setSpecularColor(vec4 c) { m_Specular = c; }
+  void setReflective(bool r) { m_Reflective = r; }
+  void setReflectionIntensity(float i) { m_ReflectionIntensity = i; }
+  void setTransparent(bool t) { m_Transparent = t; }
+  void setRefractiveIndex(float n) { m_RefractiveIndex = n; }
+  float getAmbientIntensity() const { return m_Ambient; }
+  const vec4& getDiffuseColor() const { return m_Diffuse; }
+  const vec4& getSpecularColor() const { return m_Specular; }
+  int getShininess() const { return m_Shininess; }
+  bool isReflective() const { return m_Reflective; }
+  float getReflectiveIntensity() const { return m_ReflectionIntensity; }
+  bool isTransparent() const { return m_Transparent; }
+  float getRefractiveIndex() const { return m_RefractiveIndex; }
+
+  eos_material to_c() const {
+    eos_material m;
+    m.kd[0] = m_Diffuse.x; m.kd[1] = m_Diffuse.y; m.kd[2] = m_Diffuse.z;
+    m.ks[0] = m_Specular.x; m.ks[1] = m_Specular.y; m.ks[2] = m_Specular.z;
+    m.shininess = (float)m_Shininess;
+    m.reflectivity = m_Reflective ? m_ReflectionIntensity : 0.0f;
+    return m;
+  }
+
+ private:
+  float m_Ambient;
+  vec4 m_Diffuse, m_Specular;
+  int m_Shininess;
+  bool m_Reflective = false;
+  float m_ReflectionIntensity = 0.0f;
+  bool m_Transparent = false;
+  float m_RefractiveIndex = 1.0f;
+};
+
+// src/LightSource.h:27-39
+class LightSource {
+ public:
+  LightSource() : m_Position(0.0f), m_Color(1.0f) {}
+  LightSource(const vec4& position, const vec4& color) : m_Position(position), m_Color(color) {}
+  const vec4& getPosition() const { return m_Position; }
+  const vec4& getLightColor() const { return m_Color; }
+
+ private:
+  vec4 m_Position, m_Color;
+};
+
+// src/surface.h + src/Triangle.h:32-99, triangles only.
+class Surface {
+ public:
+  virtual ~Surface() = default;
+};
+
+class Triangle : public Surface {
+ public:
+  Triangle(const vec3& v1, const vec3& v2, const vec3& v3, const vec3& n1, const vec3& n2, const vec3& n3)
+      : m_V{v1, v2, v3}, m_N{n1, n2, n3} {}
+  void setTransformation(const mat4& M) { m_M = M; }
+  template <class M>
+  void setTransformation(M& g) { m_M = mat4::from(g); }
+  void setMaterial(Material& m) { m_Material = &m; }
+  Material& getMaterial() { return *m_Material; }
+  void setMaterialIndex(int i) { m_MaterialIndex = i; }
+  int getMaterialIndex() const { return m_MaterialIndex; }
+  void setTransformationIndex(int i) { m_TransformationIndex = i; }
+  int getTransformationIndex() const { return m_TransformationIndex; }
+  const vec3& getV1() const { return m_V[0]; }
+  const vec3& getV2() const { return m_V[1]; }
+  const vec3& getV3() const { return m_V[2]; }
+  const vec3& getN1() const { return m_N[0]; }
+  const vec3& getN2() const { return m_N[1]; }
+  const vec3& getN3() const { return m_N[2]; }
+  const mat4& transformation() const { return m_M; }
+
+ private:
+  vec3 m_V[3], m_N[3];
+  mat4 m_M;
+  Material* m_Material = nullptr;
+  int m_MaterialIndex = 0;
+  int m_TransformationIndex = 0;
+};
+
+// src/Camera.h:30-64
+class Camera {
+ public:
+  template <class V> void setPosition(const V& p) { m_Position = vec3(p); }
+  template <class V> void setViewingDirection(const V& d) { m_View = vec3(d); }
+  template <class V> void setRightVector(const V& r) { m_Right = vec3(r); }
+  template <class V> void setUpVector(const V& u) { m_Up = vec3(u); }
+  void setWidth(int w) { m_Width = w; }
+  void setHeight(int h) { m_Height = h; }
+  const vec3& getPosition() const { return m_Position; }
+  const vec3& getViewingDirection() const { return m_View; }
+  const vec3& getRightVector() const { return m_Right; }
+  const vec3& getUpVector() const { return m_Up; }
+  int getWidth() const { return m_Width; }
+  int getHeight() const { return m_Height; }
+
+  eos_camera to_c() const {
+    eos_camera c;
+    const vec3* v[4] = {&m_Position, &m_View, &m_Right, &m_Up};
+    float* o[4] = {c.position, c.view, c.right, c.up};
+    for (int i = 0; i < 4; ++i) {
+      o[i][0] = v[i]->x;
+      o[i][1] = v[i]->y;
+      o[i][2] = v[i]->z;
+    }
+    c.width = m_Width;
+    c.height = m_Height;
+    return c;
+  }
+
+ private:
+  vec3 m_Position, m_View, m_Right, m_Up;
+  int m_Width = 0, m_Height = 0;
+};
+
+// One library context per process and device (the reference keeps one CUDA context
+// per GPU).  Created on first use on device 0.
+inline eos_ctx* default_context(int device = 0) {
+  struct Holder {
+    eos_ctx* ctx = nullptr;
+    ~Holder() {
+      if (ctx) eos_ctx_destroy(ctx);
+    }
+  };
+  static Holder h;
+  if (!h.ctx) check(eos_ctx_create(device, &h.ctx), "eos_ctx_create");
+  return h.ctx;
+}
+
+// src/Scene.h:42-118
+class Scene {
+ public:
+  bool addSurface(Surface* s) {
+    Triangle* t = dynamic_cast<Triangle*>(s);
+    if (!t) return false;  // triangles only (src/cudaStructures.cu:342-348)
+    m_Surfaces.push_back(t);
+    return true;
+  }
+  bool addLightSource(LightSource* l) {
+    if (!l) return false;
+    m_Lights.push_back(l);
+    return true;
+  }
+  int addMaterial(Material m) {
+    m_Materials.push_back(m);
+    return (int)m_Materials.size() - 1;
+  }
+  int addTransformation(const mat4& M) {
+    m_Transforms.push_back(M);
+    return (int)m_Transforms.size() - 1;
+  }
+  const Material& getMaterialAtIndex(int i) const { return m_Materials[i]; }
+  int getNumMaterials() const { return (int)m_Materials.size(); }
+  int getNumSurfaces() const { return (int)m_Surfaces.size(); }
+  int getNumLightSources() const { return (int)m_Lights.size(); }
+  const LightSource* getLightSource(int i) const { return i < (int)m_Lights.size() ? m_Lights[i] : nullptr; }
+  Triangle* getSurface(int i) const { return i < (int)m_Surfaces.size() ? m_Surfaces[i] : nullptr; }
+  void setAmbientRefractiveIndex(float n) { m_AmbientIndex = n; }
+  float getAmbientRefractiveIndex() const { return m_AmbientIndex; }
+  void setMaxTracedDepth(int d) { m_MaxTracedDepth = d; }
+  int getMaxTracedDepth() const { return m_MaxTracedDepth; }
+  void useBvh(bool u) { m_UseBvh = u; }
+  bool isUsingBvh() const { return m_UseBvh; }
+  void setAASamples(int s) { m_AASamples = s; }
+  int getAASamples() const { return m_AASamples; }
+  // The reference builds its CPU BVH here (src/Scene.cpp:204-209); the LBVH is built on the
+  // GPU by createCudaScene, so flush only freezes the surface list.
+  void flush() { m_Flushed = true; }
+
+ private:
+  std::vector<Triangle*> m_Surfaces;
+  std::vector<LightSource*> m_Lights;
+  std::vector<Material> m_Materials;
+  std::vector<mat4> m_Transforms;
+  float m_AmbientIndex = 1.0f;
+  int m_MaxTracedDepth = 0;
+  bool m_UseBvh = true;
+  bool m_Flushed = false;
+  int m_AASamples = 1;
+};
+
+// The device scene (src/cudaStructures.h:86-92): here the library's resident scene.
+struct cudaScene_t {
+  eos_scene* scene = nullptr;
+  eos_ctx* ctx = nullptr;
+  ~cudaScene_t() {
+    if (scene) eos_scene_destroy(scene);
+  }
+};
+
+// src/cudaStructures.cu:483-543: flattens the surfaces (one vertex triple per triangle,
+// one material per triangle, as the reference's per-triangle material index) and builds
+// the LBVH on the device.  The returned object owns the device scene.
+inline cudaScene_t* createCudaScene(Scene* scene, eos_ctx* ctx = nullptr) {
+  if (!scene) throw Error(EOS_ERR_INVALID_ARG, "createCudaScene");
+  if (!ctx) ctx = default_context();
+  const int n = scene->getNumSurfaces();
+  std::vector<float> v(9 * (size_t)n), nrm(9 * (size_t)n);
+  std::vector<uint32_t> tris(3 * (size_t)n), obj(n);
+  std::vector<eos_material> mats;
+  std::vector<const Material*> seen;
+  for (int i = 0; i < n; ++i) {
+    Triangle* t = scene->getSurface(i);
+    const mat4& M = t->transformation();
+    const bool ident = M.identity();
+    const vec3 V[3] = {t->getV1(), t->getV2(), t->getV3()};
+    const vec3 N[3] = {t->getN1(), t->getN2(), t->getN3()};
+    for (int j = 0; j < 3; ++j) {
+      vec3 p = ident ? V[j] : transform_point(M, V[j]);
+      vec3 q = ident ? N[j] : transform_normal(M, N[j]);
+      v[9 * i + 3 * j] = p.x; v[9 * i + 3 * j + 1] = p.y; v[9 * i + 3 * j + 2] = p.z;
+      nrm[9 * i + 3 * j] = q.x; nrm[9 * i + 3 * j + 1] = q.y; nrm[9 * i + 3 * j + 2] = q.z;
+      tris[3 * i + j] = (uint32_t)(3 * i + j);
+    }
+    // material per triangle: its scene material index, as the reference shades through
+    // Scene::getMaterialAtIndex(intersection.getMaterialIndex()) (src/RayTracer.cpp:317,430)
+    int mi = t->getMaterialIndex();
+    if (mi < 0 || mi >= scene->getNumMaterials()) throw Error(EOS_ERR_INVALID_ARG, "createCudaScene: material index");
+    obj[i] = (uint32_t)mi;
+  }
+  for (int k = 0; k < scene->getNumMaterials(); ++k) mats.push_back(scene->getMaterialAtIndex(k).to_c());
+  if (mats.empty()) mats.push_back(Material().to_c());
+  std::vector<eos_light> lights;
+  for (int k = 0; k < scene->getNumLightSources(); ++k) {
+    const LightSource* l = scene->getLightSource(k);
+    eos_light c;
+    c.position[0] = l->getPosition().x; c.position[1] = l->getPosition().y; c.position[2] = l->getPosition().z;
+    c.color[0] = l->getLightColor().x; c.color[1] = l->getLightColor().y; c.color[2] = l->getLightColor().z;
+    lights.push_back(c);
+  }
+  std::unique_ptr<cudaScene_t> cs(new cudaScene_t());
+  cs->ctx = ctx;
+  check(eos_scene_create(ctx, v.data(), nrm.data(), (uint32_t)(3 * n), tris.data(), obj.data(), (uint32_t)n,
+                         mats.data(), (uint32_t)mats.size(), lights.data(), (uint32_t)lights.size(), nullptr,
+                         &cs->scene),
+        "createCudaScene");
+  return cs.release();
+}
+
+// src/DeviceCameraHandler.h: the camera travels as kernel arguments, so the "device"
+// camera is a host copy that the renderer reads at each frame.
+class DeviceCameraHandler {
+ public:
+  Camera* setDeviceCamera(const Camera* host) {
+    m_Camera = *host;
+    return &m_Camera;
+  }
+  void updateDeviceCamera(const Camera* host) { m_Camera = *host; }
+  Camera* getDeviceCamera() { return &m_Camera; }
+
+ private:
+  Camera m_Camera;
+};
+
+constexpr int kDefaultTraceDepth = 4;  // RAYTRACER_DEFAULT_TRACE_DEPTH, src/RayTracer.h:36
+
+inline void render_rgba8(eos_ctx* ctx, const eos_scene* sc, const Camera& cam, int trace_depth, void* image,
+                         int mode = EOS_MODE_PLAIN) {
+  eos_camera c = cam.to_c();
+  eos_render_params p{};
+  p.trace_depth = trace_depth;
+  p.pixel_offset = 0.0f;  // the reference's integer pixel positions
+  p.spp = 1;
+  p.mode = mode;
+  check(eos_render(ctx, sc, &c, &p, nullptr, (uint8_t*)image, nullptr, nullptr, nullptr), "eos_render");
+}
+
+// src/DeviceRenderer.h:33-55
+class DeviceRenderer {
+ public:
+  DeviceRenderer(Camera* camera, int width, int height) : m_Camera(camera), m_Width(width), m_Height(height) {}
+  // Renders one frame into a caller-owned RGBA8 buffer of width*height*4 bytes.
+  void renderCudaSceneToHostBufferMegaKernel(cudaScene_t* deviceScene, void* imageBuffer) {
+    Camera c = *m_Camera;
+    c.setWidth(m_Width);
+    c.setHeight(m_Height);
+    render_rgba8(deviceScene->ctx, deviceScene->scene, c, m_TraceDepth, imageBuffer, EOS_MODE_PLAIN);
+  }
+  void renderCudaSceneToHostBufferWarpShuffleMegaKernel(cudaScene_t* deviceScene, void* imageBuffer) {
+    Camera c = *m_Camera;
+    c.setWidth(m_Width);
+    c.setHeight(m_Height);
+    render_rgba8(deviceScene->ctx, deviceScene->scene, c, m_TraceDepth, imageBuffer, EOS_MODE_WAVEFRONT);
+  }
+  void setCamera(Camera* c) { m_Camera = c; }
+  int getWidth() const { return m_Width; }
+  int getHeight() const { return m_Height; }
+  Camera* getDeviceCamera() const { return m_Camera; }
+  void setTracedDepth(int d) {
+    if (d > 0) m_TraceDepth = d;
+  }
+
+ private:
+  Camera* m_Camera;
+  int m_Width, m_Height;
+  int m_TraceDepth = kDefaultTraceDepth;
+};
+
+// src/MultiDeviceRenderer.h:31-45, on one GPU.
+class MultiDeviceRenderer {
+ public:
+  MultiDeviceRenderer(Scene* scene, Camera* camera, int width, int height)
+      : m_Scene(createCudaScene(scene)), m_Width(width), m_Height(height) {
+    (void)camera;
+  }
+  void renderSceneToHostBuffer(void* imageBuffer, Camera* hostCamera) {
+    Camera c = *hostCamera;
+    c.setWidth(m_Width);
+    c.setHeight(m_Height);
+    render_rgba8(m_Scene->ctx, m_Scene->scene, c, m_TraceDepth, imageBuffer);
+  }
+  void setTracedDepth(int d) {
+    if (d > 0) m_TraceDepth = d;
+  }
+
+ private:
+  std::unique_ptr<cudaScene_t> m_Scene;
+  int m_Width, m_Height;
+  int m_TraceDepth = kDefaultTraceDepth;
+};
+
+// src/RayTracer.h:38-68: the CPU renderer's call, run on the GPU.  A scene is uploaded
+// on the first render and reused while the same Scene object is rendered.
+class RayTracer {
+ public:
+  void render(const Scene& scene, const Camera& camera, unsigned char* outputImage) {
+    if (m_Source != &scene) {
+      m_Device.reset(createCudaScene(const_cast<Scene*>(&scene)));
+      m_Source = &scene;
+    }
+    render_rgba8(m_Device->ctx, m_Device->scene, camera, m_TraceDepth, outputImage);
+  }
+  int getAASamples() const { return m_AASamples; }
+  void setAASamples(int s) {
+    if (s > 0) m_AASamples = s;
+  }
+  int getTracedDepth() const { return m_TraceDepth; }
+  void setTracedDepth(int d) {
+    if (d > 0) m_TraceDepth = d;
+  }
+
+ private:
+  int m_AASamples = 0;
+  int m_TraceDepth = kDefaultTraceDepth;
+  const Scene* m_Source = nullptr;
+  std::unique_ptr<cudaScene_t> m_Device;
+};
+
+}  // namespace eos
+
+#endif  // EOS_EOS_HPP
