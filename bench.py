@@ -48,7 +48,12 @@ def parse():
     ap.add_argument("--views", type=int, default=4)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling case for ncu: one 1080p view, batched and plain steps only")
+    a = ap.parse_args()
+    if a.profile:
+        a.views, a.no_adjoint, a.no_cpu_baseline = 1, True, True
+    return a
 
 
 def dist_env():
@@ -278,6 +283,11 @@ def run_ours(args, rank, world, local):
     clocks = clk.summary()
     mrays_b = rays_b / (ms_b * 1e-3) / 1e6
     mrays_p = rays_p / (ms_p * 1e-3) / 1e6
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_case": True, "batched_mrays": round(mrays_b, 1),
+                              "plain_mrays": round(mrays_p, 1)}), flush=True)
+        return
 
     # e2e: reference-facing call with pinned host output, camera in / image out per view
     host_imgs = [torch.empty((c.height, c.width, 4), dtype=torch.uint8).pin_memory() for c in cams]

@@ -42,9 +42,10 @@ def test_backward_matches_fp64_adjoint(ctx, td):
     p = paths.cpu().numpy()
     rgb64, om, ol = orc.frozen_f64(cams, 64, 64, 0.5, td, p[:, :8], p[:, 8:].view(np.uint32), mp, lp,
                                    g=g.cpu().numpy().astype(np.float64))
-    # FP32 forward vs the FP64 re-render of the same frozen paths (colours up to ~4)
+    # FP32 forward vs the FP64 re-render of the same frozen paths: colours up to ~4 with
+    # shininess up to e^5, so pow() turns ~1e-7 direction rounding into ~1e-4 relative
     r32 = rgb.cpu().numpy()
-    assert (np.abs(rgb64 - r32) / np.maximum(1.0, np.abs(rgb64))).max() < 1e-4
+    assert (np.abs(rgb64 - r32) / np.maximum(1.0, np.abs(rgb64))).max() < 1e-3
     gm = gm.cpu().numpy()
     gl = gl.cpu().numpy()
     for name, a, b in [("kd", gm[:, 0:3], om[:, 0:3]), ("ks", gm[:, 3:6], om[:, 3:6]),
