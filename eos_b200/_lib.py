@@ -105,7 +105,12 @@ SIGNATURES = [
                                       c_void_p, c_void_p, POINTER(Grads)]),
     ("eos_trace_closest", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
     ("eos_trace_any", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+    ("eos_render_noalloc", c_int32, [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
+                                     c_void_p, POINTER(Stats)]),
 ]
+
+NOALLOC_MAX_PATHS = 16384
+NOALLOC_MAX_LIGHTS = 8
 
 _lib = None
 

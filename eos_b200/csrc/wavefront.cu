@@ -19,6 +19,7 @@
 // CUDA graph and replayed; the job table is uploaded before each replay.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "trace.cuh"
@@ -358,16 +359,18 @@ namespace {
 // Device time per stage when the caller asks for it (eager launches only): events around
 // each kernel, waited for right away.
 struct StageTimer {
-  eos_ctx* ctx;
   bool on;
-  eos_status begin() { return on ? (cudaEventRecord(ctx->ev0, ctx->stream) == cudaSuccess ? EOS_OK : EOS_ERR_CUDA) : EOS_OK; }
+  cudaStream_t st;
+  cudaEvent_t e0, e1;
+  float* acc;  // [3] milliseconds per stage
+  eos_status begin() { return on ? (cudaEventRecord(e0, st) == cudaSuccess ? EOS_OK : EOS_ERR_CUDA) : EOS_OK; }
   eos_status end(int stage) {
     if (!on) return EOS_OK;
-    EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
-    EOS_CUDA(cudaEventSynchronize(ctx->ev1));
+    EOS_CUDA(cudaEventRecord(e1, st));
+    EOS_CUDA(cudaEventSynchronize(e1));
     float ms = 0.0f;
-    EOS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    ctx->stage_ms[stage] += ms;
+    EOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    acc[stage] += ms;
     return EOS_OK;
   }
 };
@@ -379,12 +382,12 @@ struct StageTimer {
   } while (0)
 
 template <int SH>
-eos_status launch_sequence(eos_ctx* ctx, const WfArgs& base, const std::vector<Chunk>& chunks, int depth,
-                           int block, int grid_closest, int grid_any, int* ctr, size_t smem, StageTimer tm,
+eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, const Chunk* chunks, int n_chunks,
+                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem, StageTimer tm,
                            uint32_t& launches) {
-  cudaStream_t st = ctx->stream;
-  const int grid_lin = ctx->num_sms * 8;
-  for (const Chunk& c : chunks) {
+  const int grid_lin = num_sms * 8;
+  for (int ci = 0; ci < n_chunks; ++ci) {
+    const Chunk& c = chunks[ci];
     WfArgs A = base;
     A.c0 = c.c0;
     A.n_chunk = c.n;
@@ -423,6 +426,70 @@ eos_status launch_sequence(eos_ctx* ctx, const WfArgs& base, const std::vector<C
   return EOS_OK;
 }
 
+// Device job record of one view (tiled, padded path count).
+void fill_job(const eos_job& J, long long path_off, DevJob& d) {
+  memset(&d, 0, sizeof d);
+  d.s = J.scene->dev;
+  for (int k = 0; k < 3; ++k) {
+    d.cam[k] = J.camera.position[k];
+    d.cam[3 + k] = J.camera.view[k];
+    d.cam[6 + k] = J.camera.right[k];
+    d.cam[9 + k] = J.camera.up[k];
+  }
+  d.w = J.camera.width;
+  d.h = J.camera.height;
+  d.trace_depth = J.trace_depth;
+  d.spp = J.spp;
+  d.off = J.pixel_offset;
+  d.seed = J.jitter_seed;
+  d.rgb = J.rgb_out;
+  d.rgba8 = J.rgba8_out;
+  d.paths = J.paths_out;
+  d.tiles_x = (d.w + kTileW - 1) / kTileW;
+  long long tiles_y = (d.h + kTileH - 1) / kTileH;
+  d.n_paths = (long long)d.tiles_x * tiles_y * 32 * d.spp;
+  d.path_off = path_off;
+}
+
+struct LaunchConfig {
+  int block, sh, qchunk, grid_c, grid_a;
+  size_t smem;
+};
+
+LaunchConfig launch_config(const eos_render_params& p, int num_sms) {
+  LaunchConfig c;
+  c.block = p.block_size > 0 ? std::min(512, std::max(32, (p.block_size / 32) * 32)) : 128;
+  c.sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
+  c.qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
+  c.smem = (size_t)c.sh * c.block * sizeof(uint2);
+  int occ_c = 0, occ_a = 0;
+  if (c.sh == 8) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 8>, c.block, c.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<8>, c.block, c.smem);
+  } else if (c.sh == 16) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 16>, c.block, c.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<16>, c.block, c.smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 32>, c.block, c.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<32>, c.block, c.smem);
+  }
+  c.grid_c = num_sms * std::max(1, occ_c);
+  c.grid_a = num_sms * std::max(1, occ_a);
+  return c;
+}
+
+eos_status run_sequence(cudaStream_t st, int num_sms, const LaunchConfig& lc, const WfArgs& A, const Chunk* chunks,
+                        int n_chunks, int depth, StageTimer tm, uint32_t& launches) {
+  if (lc.sh == 8)
+    return launch_sequence<8>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
+                              tm, launches);
+  if (lc.sh == 16)
+    return launch_sequence<16>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr,
+                               lc.smem, tm, launches);
+  return launch_sequence<32>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
+                             tm, launches);
+}
+
 }  // namespace
 
 eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, const eos_render_params& p,
@@ -435,27 +502,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   for (uint32_t j = 0; j < n_jobs; ++j) {
     const eos_job& J = jobs[j];
     DevJob& d = dj[j];
-    memset(&d, 0, sizeof d);
-    d.s = J.scene->dev;
-    for (int k = 0; k < 3; ++k) {
-      d.cam[k] = J.camera.position[k];
-      d.cam[3 + k] = J.camera.view[k];
-      d.cam[6 + k] = J.camera.right[k];
-      d.cam[9 + k] = J.camera.up[k];
-    }
-    d.w = J.camera.width;
-    d.h = J.camera.height;
-    d.trace_depth = J.trace_depth;
-    d.spp = J.spp;
-    d.off = J.pixel_offset;
-    d.seed = J.jitter_seed;
-    d.rgb = J.rgb_out;
-    d.rgba8 = J.rgba8_out;
-    d.paths = J.paths_out;
-    d.tiles_x = (d.w + kTileW - 1) / kTileW;
-    long long tiles_y = (d.h + kTileH - 1) / kTileH;
-    d.n_paths = (long long)d.tiles_x * tiles_y * 32 * d.spp;
-    d.path_off = total;
+    fill_job(J, total, d);
     // chunks aligned to whole pixels of this job
     long long unit = 32ll * d.spp;
     long long per = std::max(unit, (kChunkPaths / unit) * unit);
@@ -488,10 +535,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   if (es != EOS_OK) return es;
   EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
 
-  const int block = p.block_size > 0 ? std::min(512, std::max(32, (p.block_size / 32) * 32)) : 128;
-  const int sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
-  const int qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
-  const size_t smem = (size_t)sh * block * sizeof(uint2);
+  const LaunchConfig lc = launch_config(p, ctx->num_sms);
+  const int block = lc.block, sh = lc.sh, qchunk = lc.qchunk;
 
   WfArgs A;
   memset(&A, 0, sizeof A);
@@ -511,26 +556,10 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   A.err = ctx->d_err;
   A.counts = ctx->d_counts;
 
-  int occ_c = 0, occ_a = 0;
-  if (sh == 8) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 8>, block, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<8>, block, smem);
-  } else if (sh == 16) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 16>, block, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<16>, block, smem);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 32>, block, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<32>, block, smem);
-  }
-  const int grid_c = ctx->num_sms * std::max(1, occ_c);
-  const int grid_a = ctx->num_sms * std::max(1, occ_a);
-
   uint32_t launches = 0;
-  StageTimer tm{ctx, !use_graph && (p.flags & EOS_FLAG_STAGE_TIMING) != 0};
+  StageTimer tm{!use_graph && (p.flags & EOS_FLAG_STAGE_TIMING) != 0, ctx->stream, ctx->ev0, ctx->ev1, ctx->stage_ms};
   auto run = [&]() -> eos_status {
-    if (sh == 8) return launch_sequence<8>(ctx, A, merged, depth, block, grid_c, grid_a, ctr, smem, tm, launches);
-    if (sh == 16) return launch_sequence<16>(ctx, A, merged, depth, block, grid_c, grid_a, ctr, smem, tm, launches);
-    return launch_sequence<32>(ctx, A, merged, depth, block, grid_c, grid_a, ctr, smem, tm, launches);
+    return run_sequence(ctx->stream, ctx->num_sms, lc, A, merged.data(), (int)merged.size(), depth, tm, launches);
   };
   if (!use_graph) {
     eos_status rs = run();
@@ -575,3 +604,164 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
 }
 
 }  // namespace eos
+
+// ---------------------------------------------------------------------------------
+// Allocation-free render (eos_render_noalloc).
+//
+// For callers that must not allocate device memory at render time: code running inside
+// another framework's memory pool or allocator, real-time loops that forbid allocation
+// after start-up, or processes that hand all device memory to another owner.  The
+// wavefront's queues live in one fixed, file-scope device array instead of context
+// scratch; the caller passes the scene, the camera and device output buffers.
+//
+// Capacity: kNoAllocMaxPaths padded paths (8x4-pixel tiles x spp; 16,384 = 128x128 at
+// 1 spp) and kNoAllocMaxLights lights.  The array (about 7.6 MB) is held on every GPU that
+// loads this library until the process exits.  Every call shares it and it keeps the last
+// call's contents, so calls that overlap on the GPU (two streams, two threads) race; the
+// counters, error word and colour accumulators are cleared at the start of each call.
+// ---------------------------------------------------------------------------------
+namespace eos {
+namespace {
+
+constexpr int kNoAllocMaxPaths = EOS_NOALLOC_MAX_PATHS;
+constexpr int kNoAllocMaxLights = EOS_NOALLOC_MAX_LIGHTS;
+constexpr size_t kNaJob = 0;
+constexpr size_t kNaCtr = 256;
+constexpr size_t kNaErr = 512;
+constexpr size_t kNaCounts = 768;
+constexpr size_t kNaR0 = 1024;
+constexpr size_t kNaR1 = kNaR0 + sizeof(RayQ) * (size_t)kNoAllocMaxPaths;
+constexpr size_t kNaHits = kNaR1 + sizeof(RayQ) * (size_t)kNoAllocMaxPaths;
+constexpr size_t kNaMasks = kNaHits + sizeof(HitQ) * (size_t)kNoAllocMaxPaths;
+constexpr size_t kNaSq = kNaMasks + 4 * (size_t)kNoAllocMaxPaths;
+constexpr size_t kNaAcc = kNaSq + sizeof(ShadowQ) * (size_t)kNoAllocMaxPaths * kNoAllocMaxLights;
+constexpr size_t kNaBytes = kNaAcc + sizeof(float4) * (size_t)kNoAllocMaxPaths * kMaxBounces;
+static_assert(sizeof(DevJob) <= kNaCtr - kNaJob, "job record does not fit its slot");
+static_assert(sizeof(int) * kCtr * kMaxBounces <= kNaErr - kNaCtr, "counters do not fit their slot");
+static_assert(sizeof(unsigned long long) * kCounters <= kNaR0 - kNaCounts, "ray counters do not fit their slot");
+static_assert(kNaSq % 256 == 0 && kNaAcc % 256 == 0, "queues must stay 256-byte aligned");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+// The job record travels as a kernel argument, so no host staging buffer is involved.
+__global__ void k_na_put_job(DevJob j, DevJob* dst) { *dst = j; }
+
+// Device address of g_noalloc_scratch per device.  In host code the symbol names a host
+// stand-in, not device memory, so the address is looked up once per device, with that
+// device current, and cached.
+std::mutex g_na_mutex;
+unsigned char* g_na_base[64] = {};
+
+eos_status noalloc_base(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= 64) return EOS_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (!g_na_base[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return EOS_ERR_CUDA;
+    }
+    g_na_base[dev] = (unsigned char*)p;
+  }
+  *out = g_na_base[dev];
+  return EOS_OK;
+}
+
+eos_status na_error_status(int e) {
+  if (e & (kErrStack | kErrDepth)) return EOS_ERR_STACK_OVERFLOW;
+  if (e & kErrQueue) return EOS_ERR_QUEUE_OVERFLOW;
+  if (e & kErrIndex) return EOS_ERR_INVALID_ARG;
+  if (e & kErrTimeout) return EOS_ERR_TIMEOUT;
+  return EOS_OK;
+}
+
+}  // namespace
+}  // namespace eos
+
+extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camera* camera,
+                                         const eos_render_params* params, void* stream, float* rgb_out,
+                                         eos_path_record* paths_out, eos_stats* stats) {
+  using namespace eos;
+  if (!scene || !camera || !params || !scene->ctx) return EOS_ERR_INVALID_ARG;
+  if (camera->width <= 0 || camera->height <= 0 || camera->width > kNoAllocMaxPaths ||
+      camera->height > kNoAllocMaxPaths)
+    return EOS_ERR_INVALID_ARG;
+  if (params->trace_depth < 0 || params->trace_depth >= EOS_MAX_BOUNCES || params->spp < 1 ||
+      params->spp > kNoAllocMaxPaths)
+    return EOS_ERR_INVALID_ARG;
+  if (scene->dev.n_lights > kNoAllocMaxLights) return EOS_ERR_INVALID_ARG;
+  if ((rgb_out && !is_device_ptr(rgb_out)) || (paths_out && !is_device_ptr(paths_out))) return EOS_ERR_INVALID_ARG;
+  const int dev = scene->ctx->device;
+  EOS_CUDA(cudaSetDevice(dev));
+  unsigned char* base = nullptr;
+  eos_status st = noalloc_base(dev, &base);
+  if (st != EOS_OK) return st;
+  int num_sms = 0;
+  EOS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+
+  eos_job J;
+  memset(&J, 0, sizeof J);
+  J.scene = scene;
+  J.camera = *camera;
+  J.trace_depth = params->trace_depth;
+  J.pixel_offset = params->pixel_offset;
+  J.spp = params->spp;
+  J.jitter_seed = params->jitter_seed;
+  J.rgb_out = rgb_out;
+  J.paths_out = paths_out;
+  DevJob job;
+  fill_job(J, 0, job);
+  if (job.n_paths > kNoAllocMaxPaths) return EOS_ERR_INVALID_ARG;  // beyond the fixed scratch capacity
+
+  cudaStream_t s = (cudaStream_t)stream;
+  k_na_put_job<<<1, 1, 0, s>>>(job, (DevJob*)(base + kNaJob));
+  EOS_CUDA(cudaMemsetAsync(base + kNaErr, 0, sizeof(int), s));
+  EOS_CUDA(cudaMemsetAsync(base + kNaCounts, 0, sizeof(unsigned long long) * kCounters, s));
+
+  WfArgs A;
+  memset(&A, 0, sizeof A);
+  A.jobs = (const DevJob*)(base + kNaJob);
+  A.n_jobs = 1;
+  A.depth = params->trace_depth;
+  A.rin = (const RayQ*)(base + kNaR1);
+  A.rout = (RayQ*)(base + kNaR0);
+  A.hits = (HitQ*)(base + kNaHits);
+  A.masks = (uint32_t*)(base + kNaMasks);
+  A.sq = (ShadowQ*)(base + kNaSq);
+  A.acc = (float4*)(base + kNaAcc);
+  A.ctr = (int*)(base + kNaCtr);
+  A.cap_r = kNoAllocMaxPaths;
+  A.cap_s = kNoAllocMaxPaths * kNoAllocMaxLights;
+  const LaunchConfig lc = launch_config(*params, num_sms);
+  A.qchunk = lc.qchunk;
+  A.err = (int*)(base + kNaErr);
+  A.counts = (unsigned long long*)(base + kNaCounts);
+  Chunk ch{0, (int)job.n_paths};
+  StageTimer tm{false, s, nullptr, nullptr, nullptr};
+  uint32_t launches = 1;
+  st = run_sequence(s, num_sms, lc, A, &ch, 1, A.depth, tm, launches);
+  if (st != EOS_OK) return st;
+
+  struct {
+    unsigned long long c[kCounters];
+    int err;
+  } h;
+  EOS_CUDA(cudaMemcpyAsync(h.c, base + kNaCounts, sizeof h.c, cudaMemcpyDeviceToHost, s));
+  EOS_CUDA(cudaMemcpyAsync(&h.err, base + kNaErr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  EOS_CUDA(cudaStreamSynchronize(s));
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->primary_rays = h.c[kCntPrimary];
+    stats->shadow_rays = h.c[kCntShadow];
+    stats->secondary_rays = h.c[kCntSecondary];
+    stats->nodes_closest = h.c[kCntNodesC];
+    stats->tests_closest = h.c[kCntTestsC];
+    stats->nodes_shadow = h.c[kCntNodesA];
+    stats->tests_shadow = h.c[kCntTestsA];
+    stats->shaded_hits = h.c[kCntHits];
+    stats->error_flags = h.err;
+    stats->kernel_launches = launches;
+  }
+  return na_error_status(h.err);
+}

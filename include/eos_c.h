@@ -212,6 +212,28 @@ eos_status eos_trace_closest(eos_ctx* ctx, const eos_scene* scene, const float* 
 eos_status eos_trace_any(eos_ctx* ctx, const eos_scene* scene, const float* rays, uint32_t n,
                          uint8_t* occluded);
 
+/* ---------------------------------------------------------------------------- no-alloc */
+/* Renders one view without allocating any device memory.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc while rendering -- code
+ * that runs under another framework's allocator or memory pool, real-time loops that
+ * forbid allocation after start-up, processes whose device memory belongs to another
+ * owner.  The wavefront renderer's queues live in one fixed device array inside the
+ * library (about 7.6 MB, held on every GPU that loads the library until the process
+ * exits); scene, camera, stream and device output buffers come from the caller.
+ *
+ * Limits: at most EOS_NOALLOC_MAX_PATHS paths counted in 8x4-pixel tiles times spp
+ * (128x128 at 1 spp) and at most EOS_NOALLOC_MAX_LIGHTS lights; larger requests return
+ * EOS_ERR_INVALID_ARG without touching the GPU.  rgb_out [H*W*3] and paths_out [H*W*spp]
+ * must be device memory (either may be NULL); stats may be NULL.  The call waits for its
+ * stream.  The first call on a device looks up the array's device address (make that
+ * first call before any stream capture).  All calls share the one array: calls that
+ * overlap on the GPU race, so serialise them. */
+#define EOS_NOALLOC_MAX_PATHS 16384
+#define EOS_NOALLOC_MAX_LIGHTS 8
+eos_status eos_render_noalloc(const eos_scene* scene, const eos_camera* camera,
+                              const eos_render_params* params, void* stream, float* rgb_out,
+                              eos_path_record* paths_out, eos_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif
