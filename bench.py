@@ -37,6 +37,23 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Mrays/s @1080p 1M tris, batched vs plain GPU; fwd+adjoint ms/view"
+TUNING = os.path.join(ROOT, "eos_b200", "tuning_b200.json")
+
+
+def run_autotune():
+    """Tunes one representative workload per scene-size bucket and writes the table."""
+    import numpy as np
+    from eos_b200 import api, autotune, scenes
+    ctx = api.Context(0)
+    rng = scenes.rng_for(4242)
+    work = [(scenes.config1_scene(), [scenes.config1_camera()]),
+            (scenes.mixed_scene(rng, 60_000, "mixed60k"), [scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 512, 512)]),
+            (scenes.mixed_scene(rng, 300_000, "mixed300k"), [scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 512, 512)]),
+            (scenes.config2_scene(), views_for(0, 4))]
+    table = autotune.tune(ctx, work, path=TUNING, trace_depth=2)
+    print(json.dumps({str(k): {"setting": v["setting"], "mrays": round(v["mrays"], 1),
+                               "default_mrays": round(v["default_mrays"], 1)} for k, v in table.items()}))
+    del np
 
 
 def parse():
@@ -50,6 +67,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: one 1080p view, batched and plain steps only")
+    ap.add_argument("--autotune", action="store_true",
+                    help=f"tune block / queue chunk / stack depth / leaf size per scene-size bucket and "
+                         f"write {os.path.relpath(TUNING, ROOT)}")
+    ap.add_argument("--no-tuning", action="store_true", help="ignore the committed tuning table")
     a = ap.parse_args()
     if a.profile:
         a.views, a.no_adjoint, a.no_cpu_baseline = 1, True, True
@@ -203,6 +224,10 @@ def main():
         import torch
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    if args.autotune:
+        if rank == 0:
+            run_autotune()
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         if world > 1:
@@ -221,6 +246,11 @@ def run_ours(args, rank, world, local):
     dev = local
     torch.cuda.set_device(dev)
     ctx = api.Context(dev)
+    tuned = False
+    if not args.no_tuning and os.path.exists(TUNING):
+        from eos_b200 import autotune
+        autotune.apply_table(ctx, autotune.load_table(TUNING))
+        tuned = True
     sc = scenes.config2_scene()
     dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
     info = dsc.info()
@@ -356,7 +386,8 @@ def run_ours(args, rank, world, local):
         "config": {"workload": f"{len(cams)} views/GPU at 1920x1080 of the 1,056,768-tri scene "
                                "(height field 128^2 + 200 level-4 icospheres), depth 3, 4 lights, 1 spp",
                    "mode": "batched persistent wavefront, CUDA graph", "l2": "inputs larger than L2 (scene records "
-                   f"{info['device_bytes'] / 1e6:.0f} MB)", "leaf_size": info["leaf_size"]},
+                   f"{info['device_bytes'] / 1e6:.0f} MB)", "leaf_size": info["leaf_size"],
+                   "tuning": "eos_b200/tuning_b200.json" if tuned else "defaults"},
         "plain": {"value": round(mrays_p, 2), "unit": "Mrays/s", "ms_per_step": round(ms_p / args.steps, 3)},
         "batched_over_plain": round(mrays_b / mrays_p, 3),
         "rays_per_step": {"total": rays_b / args.steps / world},

@@ -53,6 +53,10 @@ class RenderParams(Structure):
 FLAG_STAGE_TIMING = 1
 
 
+class Tuning(Structure):
+    _fields_ = [("block_size", c_int32), ("queue_chunk", c_int32), ("stack_depth", c_int32), ("leaf_size", c_int32)]
+
+
 class BuildParams(Structure):
     _fields_ = [("leaf_size", c_int32)]
 
@@ -91,6 +95,8 @@ SIGNATURES = [
     ("eos_ctx_destroy", c_int32, [c_void_p]),
     ("eos_ctx_set_stream", c_int32, [c_void_p, c_void_p]),
     ("eos_ctx_synchronize", c_int32, [c_void_p]),
+    ("eos_ctx_set_tuning", c_int32, [c_void_p, c_uint32, POINTER(Tuning)]),
+    ("eos_ctx_clear_tuning", c_int32, [c_void_p]),
     ("eos_scene_create", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_uint32,
                                    c_void_p, c_uint32, c_void_p, c_uint32, POINTER(BuildParams), POINTER(c_void_p)]),
     ("eos_scene_destroy", c_int32, [c_void_p]),

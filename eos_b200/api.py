@@ -90,7 +90,8 @@ def materials_array(mats: np.ndarray) -> np.ndarray:
 class DeviceScene:
     """A scene resident in HBM with its LBVH (eos_scene_create)."""
 
-    def __init__(self, ctx: Context, scene: SceneData, leaf_size: int = 4, inputs_on_device: bool = False):
+    def __init__(self, ctx: Context, scene: SceneData, leaf_size: int = 0, inputs_on_device: bool = False):
+        """leaf_size 0 takes the context's tuned value for this scene size (4 without a table)."""
         self.ctx = ctx
         self.scene = scene
         self.lib = ctx.lib

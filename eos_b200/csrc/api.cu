@@ -155,6 +155,24 @@ eos_status set_device(eos_ctx* ctx) {
   return EOS_OK;
 }
 
+// Tuned entry for a scene of n triangles (zeros when the table has none).
+eos_tuning tuned_for(const eos_ctx* ctx, uint32_t n) {
+  eos_tuning t{0, 0, 0, 0};
+  auto it = ctx->tuning.upper_bound(n);
+  if (it != ctx->tuning.begin()) t = std::prev(it)->second;
+  return t;
+}
+
+// Parameters left at 0 take the tuned value.
+eos_render_params with_tuning(const eos_ctx* ctx, const eos_render_params& p, uint32_t n_tris) {
+  eos_render_params q = p;
+  eos_tuning t = tuned_for(ctx, n_tris);
+  if (q.block_size <= 0) q.block_size = t.block_size;
+  if (q.queue_chunk <= 0) q.queue_chunk = t.queue_chunk;
+  if (q.stack_depth <= 0) q.stack_depth = t.stack_depth;
+  return q;
+}
+
 }  // namespace
 
 extern "C" {
@@ -228,6 +246,21 @@ eos_status eos_ctx_synchronize(eos_ctx* ctx) {
   return EOS_OK;
 }
 
+eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning* t) {
+  if (!ctx || !t) return EOS_ERR_INVALID_ARG;
+  if (t->block_size < 0 || t->block_size > 1024 || t->queue_chunk < 0 || t->stack_depth < 0 || t->leaf_size < 0 ||
+      t->leaf_size > 32)
+    return EOS_ERR_INVALID_ARG;
+  ctx->tuning[min_tris] = *t;
+  return EOS_OK;
+}
+
+eos_status eos_ctx_clear_tuning(eos_ctx* ctx) {
+  if (!ctx) return EOS_ERR_INVALID_ARG;
+  ctx->tuning.clear();
+  return EOS_OK;
+}
+
 eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* normals, uint32_t n_verts,
                             const uint32_t* tris, const uint32_t* tri_obj, uint32_t n_tris,
                             const eos_material* materials, uint32_t n_materials, const eos_light* lights,
@@ -235,11 +268,12 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   if (!ctx || !out) return EOS_ERR_INVALID_ARG;
   *out = nullptr;
   if (n_tris > 0 && (!verts || !normals || !tris || !tri_obj || n_verts == 0)) return EOS_ERR_INVALID_ARG;
-  if (n_tris > (1u << 28) || n_materials == 0 || !materials || n_lights > EOS_MAX_LIGHTS ||
+  if (n_tris >= (1u << 25) || n_materials == 0 || !materials || n_lights > EOS_MAX_LIGHTS ||
       (n_lights > 0 && !lights))
     return EOS_ERR_INVALID_ARG;
-  int leaf = build && build->leaf_size > 0 ? build->leaf_size : 4;
-  if (leaf > 64) return EOS_ERR_INVALID_ARG;
+  int leaf = build && build->leaf_size > 0 ? build->leaf_size : tuned_for(ctx, n_tris).leaf_size;
+  if (leaf <= 0) leaf = 4;
+  if (leaf > 32) return EOS_ERR_INVALID_ARG;  // leaf refs hold counts up to 32
   eos_status st = set_device(ctx);
   if (st != EOS_OK) return st;
   eos_scene* sc = new eos_scene();
@@ -354,7 +388,8 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, 
   if ((st = begin_call(ctx)) != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   if (p->mode == EOS_MODE_PLAIN) {
-    st = render_plain(ctx, sc, *cam, *p, (float*)o_rgb.dev, (uint8_t*)o_q.dev, (int32_t*)o_hit.dev,
+    st = render_plain(ctx, sc, *cam, with_tuning(ctx, *p, (uint32_t)sc->dev.n_tris), (float*)o_rgb.dev,
+                      (uint8_t*)o_q.dev, (int32_t*)o_hit.dev,
                       (eos_path_record*)o_paths.dev);
   } else {
     if (hit_out) return EOS_ERR_UNSUPPORTED;  // per-path hits come from paths_out in this mode
@@ -368,7 +403,7 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, 
     job.rgb_out = (float*)o_rgb.dev;
     job.rgba8_out = (uint8_t*)o_q.dev;
     job.paths_out = (eos_path_record*)o_paths.dev;
-    st = render_wavefront(ctx, &job, 1, *p, false);
+    st = render_wavefront(ctx, &job, 1, with_tuning(ctx, *p, (uint32_t)sc->dev.n_tris), false);
   }
   if (st != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -398,7 +433,9 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   if ((st = set_device(ctx)) != EOS_OK) return st;
   if ((st = begin_call(ctx)) != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-  st = render_wavefront(ctx, jobs, n_jobs, *p, (p->flags & EOS_FLAG_STAGE_TIMING) == 0);
+  uint32_t largest = 0;
+  for (uint32_t j = 0; j < n_jobs; ++j) largest = std::max(largest, (uint32_t)jobs[j].scene->dev.n_tris);
+  st = render_wavefront(ctx, jobs, n_jobs, with_tuning(ctx, *p, largest), (p->flags & EOS_FLAG_STAGE_TIMING) == 0);
   if (st != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   st = end_call(ctx, stats);

@@ -36,7 +36,8 @@ enum : int {
 //    [1] c0.hi.y c0.hi.z c1.lo.x c1.lo.y
 //    [2] c1.lo.z c1.hi.x c1.hi.y c1.hi.z
 //    [3] ref0 ref1 count0 count1          (int)
-//  count > 0: leaf, triangles [ref, ref + count) in sorted order
+//  count > 0: leaf of `count` triangles, ref = 0x80000000 | (count-1) << 25 | first
+//             (sorted positions [first, first + count); count <= 32, first < 2^25)
 //  count == 0: interior node `ref`;  count < 0: empty child
 //
 //  Triangle record (intersection), 48 B = 3 x float4, sorted (Morton) order:
@@ -75,6 +76,8 @@ struct eos_ctx {
   std::map<std::string, eos::DevBuffer> scratch;
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
+  // autotuner table: min triangle count -> tuned parameters
+  std::map<uint32_t, eos_tuning> tuning;
   // per-call bookkeeping reported in eos_stats
   uint32_t launches = 0;
   float stage_ms[3] = {0, 0, 0};

@@ -272,18 +272,23 @@ __global__ void k_records(const float* __restrict__ verts, const float* __restri
                           fmaxf(fmaxf(v1.z, v2.z), v3.z), 0.0f);
 }
 
+// Leaf reference: 0x80000000 | (count - 1) << 25 | first  (count <= 32, first < 2^25).
+__host__ __device__ __forceinline__ int pack_leaf(int first, int count) {
+  return (int)(0x80000000u | ((uint32_t)(count - 1) << 25) | (uint32_t)first);
+}
+
 __device__ __forceinline__ void child_ref(int c, int n, const int2* __restrict__ range, int leaf_size, int& ref,
                                           int& cnt) {
   if (c >= n - 1) {
-    ref = c - (n - 1);
     cnt = 1;
+    ref = pack_leaf(c - (n - 1), 1);
     return;
   }
   int2 r = range[c];
   int size = r.y - r.x + 1;
   if (size <= leaf_size) {
-    ref = r.x;
     cnt = size;
+    ref = pack_leaf(r.x, size);
   } else {
     ref = c;
     cnt = 0;
@@ -332,7 +337,8 @@ __global__ void k_small_root(int n, const float4* __restrict__ blo, const float4
   nodes[0] = make_float4(l.x, l.y, l.z, h.x);
   nodes[1] = make_float4(h.y, h.z, 0.0f, 0.0f);
   nodes[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  nodes[3] = make_float4(__int_as_float(0), __int_as_float(0), __int_as_float(n == 1 ? 1 : -1), __int_as_float(-1));
+  nodes[3] = make_float4(__int_as_float(pack_leaf(0, 1)), __int_as_float(-1), __int_as_float(n == 1 ? 1 : -1),
+                         __int_as_float(-1));
 }
 
 inline int grid_for(size_t n, int block) { return (int)std::max<size_t>(1, (n + block - 1) / block); }

@@ -86,11 +86,15 @@ __global__ void k_render_plain(PlainParams P) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;
-  const int n_pix = P.width * P.height;
   unsigned cnt[kNumCounts] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix < n_pix) {
-    int x = pix % P.width, y = pix / P.width;
+  // one warp = one 8x4 pixel tile (coherent primary rays)
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tiles_x = (P.width + 7) >> 3;
+  const int tile = g >> 5, lane = g & 31;
+  const int x = (tile % tiles_x) * 8 + (lane & 7);
+  const int y = (tile / tiles_x) * 4 + (lane >> 3);
+  const int pix = y * P.width + x;
+  if (x < P.width && y < P.height) {
     f3 sum = mk3(0.0f, 0.0f, 0.0f);
     for (int smp = 0; smp < P.spp; ++smp) {
       int32_t hits[kMaxBounces];
@@ -184,10 +188,15 @@ eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam
   P.counts = ctx->d_counts;
   const int block = clamp_block(p.block_size);
   const int sh = pick_stack(p.stack_depth);
-  const int n_pix = cam.width * cam.height;
-  const int grid = std::max(1, (n_pix + block - 1) / block);
+  const long long n_threads = (long long)((cam.width + 7) / 8) * ((cam.height + 3) / 4) * 32;
+  const int grid = (int)std::max<long long>(1, (n_threads + block - 1) / block);
   const size_t smem = (size_t)sh * block * sizeof(uint2);
   cudaStream_t st = ctx->stream;
+  if (smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
+    if (sh == 8) cudaFuncSetAttribute(k_render_plain<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else if (sh == 16) cudaFuncSetAttribute(k_render_plain<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else cudaFuncSetAttribute(k_render_plain<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
   if (sh == 8) k_render_plain<8><<<grid, block, smem, st>>>(P);
   else if (sh == 16) k_render_plain<16><<<grid, block, smem, st>>>(P);
   else k_render_plain<32><<<grid, block, smem, st>>>(P);

@@ -41,16 +41,17 @@ __device__ __forceinline__ SlabRay make_slab(f3 o, f3 d) {
 }
 
 // Entry distance of a box, or kInf when the box is missed or starts beyond `limit`.
-template <bool PAR>
-__device__ __forceinline__ float slab(const SlabRay& r, float lx, float ly, float lz, float hx, float hy,
-                                      float hz, float limit) {
+// Rays with a (near-)zero direction component take the containment branch; it is
+// warp-uniform in practice (whole pixel columns share it).
+__device__ __forceinline__ float slab(const SlabRay& r, float lx, float ly, float lz, float hx, float hy, float hz,
+                                      float limit) {
   float t0x = (lx - r.ox) * r.ix, t1x = (hx - r.ox) * r.ix;
   float t0y = (ly - r.oy) * r.iy, t1y = (hy - r.oy) * r.iy;
   float t0z = (lz - r.oz) * r.iz, t1z = (hz - r.oz) * r.iz;
   float nx = fminf(t0x, t1x), fx = fmaxf(t0x, t1x);
   float ny = fminf(t0y, t1y), fy = fmaxf(t0y, t1y);
   float nz = fminf(t0z, t1z), fz = fmaxf(t0z, t1z);
-  if (PAR) {
+  if (r.par) {
     if (r.ix == 0.0f) { nx = -kInf; fx = (r.ox >= lx && r.ox <= hx) ? kInf : -kInf; }
     if (r.iy == 0.0f) { ny = -kInf; fy = (r.oy >= ly && r.oy <= hy) ? kInf : -kInf; }
     if (r.iz == 0.0f) { nz = -kInf; fz = (r.oz >= lz && r.oz <= hz) ? kInf : -kInf; }
@@ -72,8 +73,18 @@ struct AnyResult {
   unsigned nodes, tests;
 };
 
-// Per-thread traversal stack: the first SH entries live in shared memory (column
-// threadIdx.x of a [SH][blockDim] array), deeper entries spill to local memory.
+// Child references in a node record (written by the LBVH build):
+//   >= 0          interior node index
+//   leaf          0x80000000 | (count - 1) << 25 | first   (count <= 32, first < 2^25)
+//   kDone (-1)    end of traversal (never stored in a node; bit 30 distinguishes it)
+constexpr int kDone = -1;
+__device__ __forceinline__ bool is_leaf_ref(int r) { return (r & 0xC0000000) == (int)0x80000000; }
+__device__ __forceinline__ int leaf_first(int r) { return r & 0x01ffffff; }
+__device__ __forceinline__ int leaf_count(int r) { return ((r >> 25) & 31) + 1; }
+
+// Per-thread traversal stack of (child ref, entry distance): the first SH entries live in
+// shared memory (column threadIdx.x of a [SH][blockDim] array), deeper entries spill to
+// local memory, kStackMax in total.
 template <int SH>
 struct TraversalStack {
   uint2* sh;
@@ -81,8 +92,8 @@ struct TraversalStack {
   int sp;
   uint2 spill[kStackMax - SH];
   __device__ __forceinline__ TraversalStack(uint2* base, int str) : sh(base), stride(str), sp(0) {}
-  __device__ __forceinline__ bool push(int node, float t) {
-    uint2 v = make_uint2((uint32_t)node, __float_as_uint(t));
+  __device__ __forceinline__ bool push(int ref, float t) {
+    uint2 v = make_uint2((uint32_t)ref, __float_as_uint(t));
     if (sp < SH) sh[sp * stride] = v;
     else if (sp < kStackMax) spill[sp - SH] = v;
     else return false;
@@ -92,6 +103,14 @@ struct TraversalStack {
   __device__ __forceinline__ uint2 pop() {
     --sp;
     return sp < SH ? sh[sp * stride] : spill[sp - SH];
+  }
+  // Next entry whose box starts no later than `limit`, or kDone.
+  __device__ __forceinline__ int next(float limit) {
+    while (sp > 0) {
+      uint2 e = pop();
+      if (__uint_as_float(e.y) <= limit) return (int)e.x;
+    }
+    return kDone;
   }
 };
 
@@ -105,129 +124,143 @@ __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p,
   id = __float_as_int(c.y);
 }
 
-template <bool PAR, int SH>
-__device__ __noinline__ Hit closest_hit_t(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+// One node fetch: both child boxes tested, the nearer hit child becomes `cur`, the farther
+// one is pushed; no hit pops the stack.  Returns false on stack overflow.
+template <int SH>
+__device__ __forceinline__ bool visit_node(const DevScene& s, const SlabRay& r, int& cur, float limit,
+                                           TraversalStack<SH>& st, unsigned& nodes) {
+  const float4* nd = s.nodes + 4 * (size_t)cur;
+  float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
+  int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+  ++nodes;
+  float tn0 = slab(r, a.x, a.y, a.z, a.w, b.x, b.y, limit);
+  float tn1 = slab(r, b.z, b.w, c.x, c.y, c.z, c.w, limit);
+  bool h0 = tn0 != kInf && ref.z >= 0;
+  bool h1 = tn1 != kInf && ref.w >= 0;
+  if (h0 && h1) {
+    bool sw = tn1 < tn0;
+    if (!st.push(sw ? ref.x : ref.y, sw ? tn0 : tn1)) return false;
+    cur = sw ? ref.y : ref.x;
+  } else if (h0) {
+    cur = ref.x;
+  } else if (h1) {
+    cur = ref.y;
+  } else {
+    cur = st.next(limit);
+  }
+  return true;
+}
+
+// Nearest hit.  Traversal in the two-loop form of Aila & Laine ("Understanding the
+// efficiency of ray traversal on GPUs", HPG 2009): a lane that reaches a leaf parks it and
+// keeps descending until every lane of the warp holds a leaf, then the lanes intersect
+// their leaves together, so triangle tests run with full warps.
+template <int SH>
+__device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
   Hit h;
   h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
   SlabRay r = make_slab(o, d);
   TraversalStack<SH> st(shs, stride);
-  int node = 0;
+  int cur = 0;   // interior node, leaf ref or kDone
+  int leaf = 0;  // parked leaf (0 = none)
   for (;;) {
-    const float4* nd = s.nodes + 4 * (size_t)node;
-    float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
-    int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 3);
-    ++h.nodes;
-    float lim = h.t * kCull;
-    float tn0 = slab<PAR>(r, a.x, a.y, a.z, a.w, b.x, b.y, lim);
-    float tn1 = slab<PAR>(r, b.z, b.w, c.x, c.y, c.z, c.w, lim);
-    bool h0 = tn0 != kInf && ref.z >= 0;
-    bool h1 = tn1 != kInf && ref.w >= 0;
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      bool hit = side == 0 ? h0 : h1;
-      int cnt = side == 0 ? ref.z : ref.w;
-      int first = side == 0 ? ref.x : ref.y;
-      if (hit && cnt > 0) {
-        h.tests += cnt;
-        for (int p = first; p < first + cnt; ++p) {
-          f3 v1, e1, e2;
-          int id;
-          load_tri(s.tris, p, v1, e1, e2, id);
-          float t, u, v;
-          if (mt_intersect(o, d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
-            h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
-          }
-        }
-        if (side == 0) h0 = false; else h1 = false;
-      }
-    }
-    if (h0 && h1) {
-      bool sw = tn1 < tn0;
-      if (!st.push(sw ? ref.x : ref.y, sw ? tn0 : tn1)) {
+    while (cur >= 0) {
+      if (!visit_node<SH>(s, r, cur, h.t * kCull, st, h.nodes)) {
         atomicOr(err, kErrStack);
         return h;
       }
-      node = sw ? ref.y : ref.x;
-      continue;
+      if (cur != kDone && cur < 0 && leaf == 0) {
+        leaf = cur;
+        cur = st.next(h.t * kCull);
+      }
+      if (!__any_sync(__activemask(), leaf == 0)) break;
     }
-    if (h0) { node = ref.x; continue; }
-    if (h1) { node = ref.y; continue; }
-    bool found = false;
-    while (st.sp > 0) {
-      uint2 e = st.pop();
-      if (__uint_as_float(e.y) <= h.t * kCull) {
-        node = (int)e.x;
-        found = true;
-        break;
+    while (leaf != 0) {
+      const int first = leaf_first(leaf), cnt = leaf_count(leaf);
+      h.tests += cnt;
+      for (int p = first; p < first + cnt; ++p) {
+        f3 v1, e1, e2;
+        int id;
+        load_tri(s.tris, p, v1, e1, e2, id);
+        float t, u, v;
+        if (mt_intersect(o, d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
+          h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
+        }
+      }
+      leaf = 0;
+      if (cur != kDone && cur < 0) {
+        leaf = cur;
+        cur = st.next(h.t * kCull);
       }
     }
-    if (!found) return h;
+    if (cur == kDone) return h;
   }
 }
 
-template <bool PAR, int SH>
-__device__ __noinline__ AnyResult any_hit_t(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+// Any hit at t >= 0 (shadow rays), same two-loop form; returns at the first hit.
+template <int SH>
+__device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
   AnyResult res{0, 0u, 0u};
   SlabRay r = make_slab(o, d);
   TraversalStack<SH> st(shs, stride);
-  int node = 0;
+  int cur = 0;
+  int leaf = 0;
   for (;;) {
-    const float4* nd = s.nodes + 4 * (size_t)node;
-    float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
-    int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 3);
-    ++res.nodes;
-    float tn0 = slab<PAR>(r, a.x, a.y, a.z, a.w, b.x, b.y, kInf);
-    float tn1 = slab<PAR>(r, b.z, b.w, c.x, c.y, c.z, c.w, kInf);
-    bool h0 = tn0 != kInf && ref.z >= 0;
-    bool h1 = tn1 != kInf && ref.w >= 0;
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      bool hit = side == 0 ? h0 : h1;
-      int cnt = side == 0 ? ref.z : ref.w;
-      int first = side == 0 ? ref.x : ref.y;
-      if (hit && cnt > 0) {
-        for (int p = first; p < first + cnt; ++p) {
-          f3 v1, e1, e2;
-          int id;
-          load_tri(s.tris, p, v1, e1, e2, id);
-          float t, u, v;
-          ++res.tests;
-          if (mt_intersect(o, d, v1, e1, e2, t, u, v)) {
-            res.hit = 1;
-            return res;
-          }
-        }
-        if (side == 0) h0 = false; else h1 = false;
-      }
-    }
-    if (h0 && h1) {
-      bool sw = tn1 < tn0;
-      if (!st.push(sw ? ref.x : ref.y, 0.0f)) {
+    while (cur >= 0) {
+      if (!visit_node<SH>(s, r, cur, kInf, st, res.nodes)) {
         atomicOr(err, kErrStack);
         return res;
       }
-      node = sw ? ref.y : ref.x;
-      continue;
+      if (cur != kDone && cur < 0 && leaf == 0) {
+        leaf = cur;
+        cur = st.next(kInf);
+      }
+      if (!__any_sync(__activemask(), leaf == 0)) break;
     }
-    if (h0) { node = ref.x; continue; }
-    if (h1) { node = ref.y; continue; }
-    if (st.sp == 0) return res;
-    node = (int)st.pop().x;
+    while (leaf != 0) {
+      const int first = leaf_first(leaf), cnt = leaf_count(leaf);
+      for (int p = first; p < first + cnt; ++p) {
+        f3 v1, e1, e2;
+        int id;
+        load_tri(s.tris, p, v1, e1, e2, id);
+        float t, u, v;
+        ++res.tests;
+        if (mt_intersect(o, d, v1, e1, e2, t, u, v)) {
+          res.hit = 1;
+          return res;
+        }
+      }
+      leaf = 0;
+      if (cur != kDone && cur < 0) {
+        leaf = cur;
+        cur = st.next(kInf);
+      }
+    }
+    if (cur == kDone) return res;
   }
 }
 
+// Out-of-line copies for the plain megakernel, which calls both traversals: keeping them
+// out of line bounds its register allocation.  The specialised wavefront kernels inline.
 template <int SH>
-__device__ __forceinline__ Hit closest_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
-  if (fabsf(d.x) < kParallelEps || fabsf(d.y) < kParallelEps || fabsf(d.z) < kParallelEps)
-    return closest_hit_t<true, SH>(s, o, d, shs, stride, err);
-  return closest_hit_t<false, SH>(s, o, d, shs, stride, err);
+__device__ __noinline__ Hit closest_hit_call(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  return closest_hit_body<SH>(s, o, d, shs, stride, err);
+}
+template <int SH>
+__device__ __noinline__ AnyResult any_hit_call(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  return any_hit_body<SH>(s, o, d, shs, stride, err);
 }
 
-template <int SH>
+template <int SH, bool INLINE = false>
+__device__ __forceinline__ Hit closest_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  if (INLINE) return closest_hit_body<SH>(s, o, d, shs, stride, err);
+  return closest_hit_call<SH>(s, o, d, shs, stride, err);
+}
+
+template <int SH, bool INLINE = false>
 __device__ __forceinline__ AnyResult any_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
-  if (fabsf(d.x) < kParallelEps || fabsf(d.y) < kParallelEps || fabsf(d.z) < kParallelEps)
-    return any_hit_t<true, SH>(s, o, d, shs, stride, err);
-  return any_hit_t<false, SH>(s, o, d, shs, stride, err);
+  if (INLINE) return any_hit_body<SH>(s, o, d, shs, stride, err);
+  return any_hit_call<SH>(s, o, d, shs, stride, err);
 }
 
 // Traversal work counters, reduced per warp into the context's counter block:

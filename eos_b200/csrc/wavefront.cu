@@ -162,7 +162,7 @@ __global__ void k_wf_closest(WfArgs A) {
       const DevJob& J = A.jobs[jb];
       if (valid) {
         ++nrays;
-        Hit h = closest_hit<SH>(J.s, o, d, shs, stride, A.err);
+        Hit h = closest_hit<SH, true>(J.s, o, d, shs, stride, A.err);
         nodes += h.nodes;
         tests += h.tests;
         hit = h.pos >= 0;
@@ -258,7 +258,7 @@ __global__ void k_wf_any(WfArgs A) {
       int hi = __float_as_int(s.a.w);
       int key = __float_as_int(s.b.w);
       const DevJob& J = A.jobs[key >> 5];
-      AnyResult ar = any_hit<SH>(J.s, mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z), shs, stride, A.err);
+      AnyResult ar = any_hit<SH, true>(J.s, mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z), shs, stride, A.err);
       nodes += ar.nodes;
       tests += ar.tests;
       if (ar.hit) atomicOr(&A.masks[hi], 1u << (key & 31));
@@ -462,6 +462,22 @@ LaunchConfig launch_config(const eos_render_params& p, int num_sms) {
   c.sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
   c.qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
   c.smem = (size_t)c.sh * c.block * sizeof(uint2);
+  if (c.smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
+    const int b = (int)c.smem;
+    if (c.sh == 8) {
+      cudaFuncSetAttribute(k_wf_closest<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+      cudaFuncSetAttribute(k_wf_closest<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+      cudaFuncSetAttribute(k_wf_any<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    } else if (c.sh == 16) {
+      cudaFuncSetAttribute(k_wf_closest<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+      cudaFuncSetAttribute(k_wf_closest<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+      cudaFuncSetAttribute(k_wf_any<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    } else {
+      cudaFuncSetAttribute(k_wf_closest<true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+      cudaFuncSetAttribute(k_wf_closest<false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+      cudaFuncSetAttribute(k_wf_any<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    }
+  }
   int occ_c = 0, occ_a = 0;
   if (c.sh == 8) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 8>, c.block, c.smem);

@@ -108,8 +108,16 @@ typedef struct eos_render_params {
  * report per-stage device time in eos_stats.stage_ms. */
 #define EOS_FLAG_STAGE_TIMING 1
 
+/* Tuned launch / layout parameters of one scene-size bucket (see eos_ctx_set_tuning). */
+typedef struct eos_tuning {
+  int32_t block_size;
+  int32_t queue_chunk;
+  int32_t stack_depth;
+  int32_t leaf_size;
+} eos_tuning;
+
 typedef struct eos_build_params {
-  int32_t leaf_size;    /* subtrees with <= leaf_size triangles become one leaf; 0 = 4 */
+  int32_t leaf_size;    /* subtrees with <= leaf_size (1..32) triangles become one leaf; 0 = 4 */
 } eos_build_params;
 
 /* Per-path record of the bounce path: hit triangle id per bounce and, per bounce, the
@@ -172,6 +180,11 @@ eos_status eos_ctx_destroy(eos_ctx* ctx);
 /* Use a caller stream (a cudaStream_t) instead of the context's own; NULL restores it. */
 eos_status eos_ctx_set_stream(eos_ctx* ctx, void* stream);
 eos_status eos_ctx_synchronize(eos_ctx* ctx);
+/* Autotuner table (no reference counterpart): parameters for scenes of at least min_tris
+ * triangles.  A render / scene-create parameter left at 0 takes the entry with the largest
+ * min_tris not above the scene's triangle count (for a batch: its largest scene). */
+eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning* tuning);
+eos_status eos_ctx_clear_tuning(eos_ctx* ctx);
 
 /* ---------------------------------------------------------------------------- scenes */
 eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* normals, uint32_t n_verts,

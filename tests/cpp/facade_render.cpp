@@ -1,0 +1,99 @@
+// Renders a scene through the C++ drop-in facade (include/eos/eos.hpp) the way a caller
+// of the reference does (src/main.cpp:340-480): Material / Triangle / LightSource /
+// Scene / Camera, createCudaScene, DeviceRenderer and RayTracer.
+//
+//   facade_render <scene.bin> <out_device_renderer.rgba> <out_raytracer.rgba>
+//
+// scene.bin: int32 n_verts, n_tris, n_mats, n_lights, width, height, trace_depth;
+// float32 verts[3n], normals[3n]; uint32 tris[3m], tri_obj[m]; float32 mats[8k],
+// lights[6l], camera[12].
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+#include <vector>
+
+#include "eos/eos.hpp"
+
+template <class T>
+static bool read_n(FILE* f, std::vector<T>& v, size_t n) {
+  v.resize(n);
+  return fread(v.data(), sizeof(T), n, f) == n;
+}
+
+int main(int argc, char** argv) {
+  if (argc != 4) {
+    fprintf(stderr, "usage: %s scene.bin out_dr.rgba out_rt.rgba\n", argv[0]);
+    return 2;
+  }
+  FILE* f = fopen(argv[1], "rb");
+  if (!f) return 2;
+  int32_t hdr[7];
+  if (fread(hdr, sizeof(int32_t), 7, f) != 7) return 2;
+  const int nv = hdr[0], nt = hdr[1], nm = hdr[2], nl = hdr[3], W = hdr[4], H = hdr[5], td = hdr[6];
+  std::vector<float> verts, normals, mats, lights, cam;
+  std::vector<uint32_t> tris, obj;
+  bool ok = read_n(f, verts, 3 * nv) && read_n(f, normals, 3 * nv) && read_n(f, tris, 3 * nt) && read_n(f, obj, nt) &&
+            read_n(f, mats, 8 * nm) && read_n(f, lights, 6 * nl) && read_n(f, cam, 12);
+  fclose(f);
+  if (!ok) return 2;
+
+  try {
+    eos::Scene scene;
+    scene.useBvh(true);
+    scene.setAmbientRefractiveIndex(1.0f);
+    for (int k = 0; k < nm; ++k) {
+      const float* m = &mats[8 * k];
+      eos::Material mat(0.0f, eos::vec4(m[0], m[1], m[2], 1.0f), eos::vec4(m[3], m[4], m[5], 1.0f), (int)m[6]);
+      mat.setReflective(m[7] > 0.0f);
+      mat.setReflectionIntensity(m[7]);
+      mat.setTransparent(false);
+      scene.addMaterial(mat);
+    }
+    std::vector<std::unique_ptr<eos::Triangle>> owned;
+    auto V = [&](const std::vector<float>& a, uint32_t i) { return eos::vec3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); };
+    for (int i = 0; i < nt; ++i) {
+      const uint32_t* t = &tris[3 * i];
+      owned.emplace_back(new eos::Triangle(V(verts, t[0]), V(verts, t[1]), V(verts, t[2]), V(normals, t[0]),
+                                           V(normals, t[1]), V(normals, t[2])));
+      owned.back()->setMaterialIndex((int)obj[i]);
+      scene.addSurface(owned.back().get());
+    }
+    std::vector<std::unique_ptr<eos::LightSource>> ls;
+    for (int i = 0; i < nl; ++i) {
+      const float* l = &lights[6 * i];
+      ls.emplace_back(new eos::LightSource(eos::vec4(l[0], l[1], l[2], 1.0f), eos::vec4(l[3], l[4], l[5], 1.0f)));
+      scene.addLightSource(ls.back().get());
+    }
+    scene.flush();
+
+    eos::Camera camera;
+    camera.setPosition(eos::vec3(cam[0], cam[1], cam[2]));
+    camera.setViewingDirection(eos::vec3(cam[3], cam[4], cam[5]));
+    camera.setRightVector(eos::vec3(cam[6], cam[7], cam[8]));
+    camera.setUpVector(eos::vec3(cam[9], cam[10], cam[11]));
+    camera.setWidth(W);
+    camera.setHeight(H);
+
+    std::unique_ptr<eos::cudaScene_t> dscene(eos::createCudaScene(&scene));
+    eos::DeviceRenderer renderer(&camera, W, H);
+    renderer.setTracedDepth(td);
+    std::vector<unsigned char> img(4 * (size_t)W * H, 0);
+    renderer.renderCudaSceneToHostBufferMegaKernel(dscene.get(), img.data());
+
+    eos::RayTracer rt;
+    rt.setTracedDepth(td);
+    std::vector<unsigned char> img2(4 * (size_t)W * H, 0);
+    rt.render(scene, camera, img2.data());
+
+    FILE* o = fopen(argv[2], "wb");
+    fwrite(img.data(), 1, img.size(), o);
+    fclose(o);
+    o = fopen(argv[3], "wb");
+    fwrite(img2.data(), 1, img2.size(), o);
+    fclose(o);
+  } catch (const eos::Error& e) {
+    fprintf(stderr, "eos error: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}
