@@ -397,6 +397,14 @@ def run_ours(args, rank, world, local):
         "roofline": roof,
         "clocks": clocks,
         "lbvh_build_ms": round(info["build_ms"], 3),
+        "bvh": {"layout": {1: "sah", 2: "fixed"}.get(info["layout"], "?"), "leaf_size": info["leaf_size"],
+                "sah_cost": round(info["sah_cost"], 2)},
+        "traversal_per_ray": {
+            "nearest_nodes": round(st["nodes_closest"] / max(1, st["primary_rays"] + st["secondary_rays"]), 2),
+            "nearest_tests": round(st["tests_closest"] / max(1, st["primary_rays"] + st["secondary_rays"]), 2),
+            "shadow_nodes": round(st["nodes_shadow"] / max(1, st["shadow_rays"]), 2),
+            "shadow_tests": round(st["tests_shadow"] / max(1, st["shadow_rays"]), 2),
+            "rays": {"primary": st["primary_rays"], "shadow": st["shadow_rays"], "secondary": st["secondary_rays"]}},
     }
     if adj:
         line["adjoint"] = adj

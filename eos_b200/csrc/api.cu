@@ -249,7 +249,7 @@ eos_status eos_ctx_synchronize(eos_ctx* ctx) {
 eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning* t) {
   if (!ctx || !t) return EOS_ERR_INVALID_ARG;
   if (t->block_size < 0 || t->block_size > 1024 || t->queue_chunk < 0 || t->stack_depth < 0 || t->leaf_size < 0 ||
-      t->leaf_size > 32)
+      t->leaf_size > 32 || t->layout < EOS_LAYOUT_DEFAULT || t->layout > EOS_LAYOUT_FIXED)
     return EOS_ERR_INVALID_ARG;
   ctx->tuning[min_tris] = *t;
   return EOS_OK;
@@ -271,14 +271,19 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   if (n_tris >= (1u << 25) || n_materials == 0 || !materials || n_lights > EOS_MAX_LIGHTS ||
       (n_lights > 0 && !lights))
     return EOS_ERR_INVALID_ARG;
-  int leaf = build && build->leaf_size > 0 ? build->leaf_size : tuned_for(ctx, n_tris).leaf_size;
-  if (leaf <= 0) leaf = 4;
+  const eos_tuning tuned = tuned_for(ctx, n_tris);
+  int leaf = build && build->leaf_size > 0 ? build->leaf_size : tuned.leaf_size;
+  if (leaf <= 0) leaf = 8;
   if (leaf > 32) return EOS_ERR_INVALID_ARG;  // leaf refs hold counts up to 32
+  int layout = build && build->layout != EOS_LAYOUT_DEFAULT ? build->layout : tuned.layout;
+  if (layout == EOS_LAYOUT_DEFAULT) layout = EOS_LAYOUT_SAH;
+  if (layout != EOS_LAYOUT_SAH && layout != EOS_LAYOUT_FIXED) return EOS_ERR_INVALID_ARG;
   eos_status st = set_device(ctx);
   if (st != EOS_OK) return st;
   eos_scene* sc = new eos_scene();
   sc->ctx = ctx;
   sc->leaf_size = leaf;
+  sc->layout = layout;
   auto fail = [&](eos_status s) {
     eos_scene_destroy(sc);
     return s;
@@ -353,6 +358,8 @@ eos_status eos_scene_get_info(const eos_scene* sc, eos_scene_info* info) {
   info->n_tris = (uint32_t)sc->dev.n_tris;
   info->n_nodes = sc->n_nodes;
   info->leaf_size = (uint32_t)sc->leaf_size;
+  info->layout = (uint32_t)sc->layout;
+  info->sah_cost = sc->sah_cost;
   info->n_objects = (uint32_t)sc->dev.n_obj;
   info->n_lights = (uint32_t)sc->dev.n_lights;
   info->build_ms = sc->build_ms;

@@ -106,7 +106,9 @@ struct eos_scene {
   void* d_codes = nullptr;  // sorted Morton codes (kept for the test hook)
   void* d_order = nullptr;  // sorted triangle ids
   uint32_t n_nodes = 0;
-  int leaf_size = 4;
+  int leaf_size = 8;
+  int layout = EOS_LAYOUT_SAH;
+  float sah_cost = 0.0f;
   float build_ms = 0.0f;
   size_t device_bytes = 0;
 };

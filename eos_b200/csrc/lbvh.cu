@@ -265,11 +265,11 @@ __global__ void k_records(const float* __restrict__ verts, const float* __restri
   }
   srec[3 * (size_t)p + 2] = make_float4(n3.z, __int_as_float((int)ob), 0.0f, 0.0f);
   pos_of_id[id] = p;
-  size_t leaf = (size_t)(n - 1) + p;
+  size_t leaf = (size_t)(n - 1) + p;  // .w: SAH cost of one triangle, leaf flag
   blo[leaf] = make_float4(fminf(fminf(v1.x, v2.x), v3.x), fminf(fminf(v1.y, v2.y), v3.y),
-                          fminf(fminf(v1.z, v2.z), v3.z), 0.0f);
+                          fminf(fminf(v1.z, v2.z), v3.z), 1.0f);
   bhi[leaf] = make_float4(fmaxf(fmaxf(v1.x, v2.x), v3.x), fmaxf(fmaxf(v1.y, v2.y), v3.y),
-                          fmaxf(fmaxf(v1.z, v2.z), v3.z), 0.0f);
+                          fmaxf(fmaxf(v1.z, v2.z), v3.z), 1.0f);
 }
 
 // Leaf reference: 0x80000000 | (count - 1) << 25 | first  (count <= 32, first < 2^25).
@@ -277,30 +277,42 @@ __host__ __device__ __forceinline__ int pack_leaf(int first, int count) {
   return (int)(0x80000000u | ((uint32_t)(count - 1) << 25) | (uint32_t)first);
 }
 
-__device__ __forceinline__ void child_ref(int c, int n, const int2* __restrict__ range, int leaf_size, int& ref,
+// Reference to child c: a one-triangle leaf, a collapsed subtree (leaf of its whole
+// range) or an interior node.  `collapsed` is the child's own decision from the refit.
+__device__ __forceinline__ void child_ref(int c, int n, const int2* __restrict__ range, bool collapsed, int& ref,
                                           int& cnt) {
   if (c >= n - 1) {
     cnt = 1;
     ref = pack_leaf(c - (n - 1), 1);
     return;
   }
-  int2 r = range[c];
-  int size = r.y - r.x + 1;
-  if (size <= leaf_size) {
-    cnt = size;
-    ref = pack_leaf(r.x, size);
+  if (collapsed) {
+    int2 r = range[c];
+    cnt = r.y - r.x + 1;
+    ref = pack_leaf(r.x, cnt);
   } else {
     ref = c;
     cnt = 0;
   }
 }
 
+constexpr float kCostNode = 1.0f;  // SAH cost of visiting one node (two box tests)
+constexpr float kCostTri = 1.0f;   // SAH cost of one triangle test
+
+__device__ __forceinline__ float half_area(float4 l, float4 h) {
+  float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
+  return dx * dy + dy * dz + dz * dx;
+}
+
 // Bottom-up refit: one thread per leaf walks to the root; the second thread to reach an
-// interior node merges the two child boxes and writes the node record.  Bounded walk:
-// the tree depth is at most kStackMax.
+// interior node merges the two child boxes, decides whether the subtree becomes one leaf
+// and writes the node record.  Leaf decision: fixed layout -> the range has at most
+// max_leaf triangles; SAH layout -> additionally the leaf's cost kCostTri * n is not above
+// kCostNode + (A_l cost_l + A_r cost_r) / A.  Box .w carries the subtree cost (lo) and the
+// leaf decision (hi).  Bounded walk: the tree depth is at most kStackMax.
 __global__ void k_refit(int n, const int2* __restrict__ child, const int2* __restrict__ range,
                         const int* __restrict__ parent, float4* blo, float4* bhi, int* __restrict__ arrive,
-                        float4* __restrict__ nodes, int leaf_size, int* err) {
+                        float4* __restrict__ nodes, int max_leaf, int sah, int* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int node = parent[n - 1 + p];
@@ -315,11 +327,21 @@ __global__ void k_refit(int n, const int2* __restrict__ child, const int2* __res
     int2 c = child[node];
     float4 l0 = __ldcg(&blo[c.x]), h0 = __ldcg(&bhi[c.x]);
     float4 l1 = __ldcg(&blo[c.y]), h1 = __ldcg(&bhi[c.y]);
-    blo[node] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
-    bhi[node] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+    float4 lo = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+    float4 hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+    int2 rg = range[node];
+    int size = rg.y - rg.x + 1;
+    float a = half_area(lo, hi);
+    float inner = kCostNode + (a > 0.0f ? (half_area(l0, h0) * l0.w + half_area(l1, h1) * l1.w) / a : l0.w + l1.w);
+    float as_leaf = size <= max_leaf ? kCostTri * (float)size : kInf;
+    bool collapse = sah ? (as_leaf <= inner) : (size <= max_leaf);
+    lo.w = collapse ? as_leaf : inner;
+    hi.w = collapse ? 1.0f : 0.0f;
+    blo[node] = lo;
+    bhi[node] = hi;
     int r0, n0, r1, n1;
-    child_ref(c.x, n, range, leaf_size, r0, n0);
-    child_ref(c.y, n, range, leaf_size, r1, n1);
+    child_ref(c.x, n, range, h0.w != 0.0f, r0, n0);
+    child_ref(c.y, n, range, h1.w != 0.0f, r1, n1);
     float4* o = nodes + 4 * (size_t)node;
     o[0] = make_float4(l0.x, l0.y, l0.z, h0.x);
     o[1] = make_float4(h0.y, h0.z, l1.x, l1.y);
@@ -405,7 +427,10 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
     EOS_CUDA(cudaMemsetAsync(arrive, 0, 4 * n_nodes, st));
     k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys, n, child, range, parent);
     k_refit<<<grid_for(nn, 256), 256, 0, st>>>(n, child, range, parent, blo, bhi, arrive,
-                                              (float4*)sc->d_nodes, sc->leaf_size, ctx->d_err);
+                                              (float4*)sc->d_nodes, sc->leaf_size, sc->layout == EOS_LAYOUT_SAH,
+                                              ctx->d_err);
+    // SAH cost of the tree (subtree cost of the root, in triangle-test units)
+    EOS_CUDA(cudaMemcpyAsync(&sc->sah_cost, &blo[0].w, sizeof(float), cudaMemcpyDeviceToHost, st));
   } else {
     k_small_root<<<1, 1, 0, st>>>(n, blo, bhi, (float4*)sc->d_nodes);
   }

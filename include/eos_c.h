@@ -114,10 +114,19 @@ typedef struct eos_tuning {
   int32_t queue_chunk;
   int32_t stack_depth;
   int32_t leaf_size;
+  int32_t layout;
 } eos_tuning;
 
+/* Node layout of the LBVH: which subtrees become leaves. */
+enum {
+  EOS_LAYOUT_DEFAULT = 0, /* tuned value, else SAH */
+  EOS_LAYOUT_SAH = 1,     /* leaf when n <= leaf_size and its SAH cost is not above the split's */
+  EOS_LAYOUT_FIXED = 2    /* leaf whenever n <= leaf_size */
+};
+
 typedef struct eos_build_params {
-  int32_t leaf_size;    /* subtrees with <= leaf_size (1..32) triangles become one leaf; 0 = 4 */
+  int32_t leaf_size;    /* largest leaf, 1..32 triangles; 0 = tuned value, else 8 */
+  int32_t layout;       /* EOS_LAYOUT_* */
 } eos_build_params;
 
 /* Per-path record of the bounce path: hit triangle id per bounce and, per bounce, the
@@ -147,6 +156,8 @@ typedef struct eos_scene_info {
   uint32_t n_tris;
   uint32_t n_nodes;       /* interior nodes of the LBVH (n_tris - 1) */
   uint32_t leaf_size;
+  uint32_t layout;        /* EOS_LAYOUT_SAH or EOS_LAYOUT_FIXED */
+  float sah_cost;         /* SAH cost of the tree, in triangle-test units */
   uint32_t n_objects;
   uint32_t n_lights;
   float build_ms;         /* device time of the LBVH build */

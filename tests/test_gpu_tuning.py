@@ -14,9 +14,10 @@ def test_results_invariant_under_tuning(ctx):
     sc = scenes.small_random_scene(81, n_spheres=10, level=3, lights=3, refl=0.5)
     cam = scenes.look_at((1.0, 3.0, 9.0), (0, -0.5, 0), 55.0, 200, 150)
     ref = None
-    for leaf in (1, 3, 8, 32):
-        dsc = api.DeviceScene(ctx, sc, leaf_size=leaf)
+    for layout, leaf in (("fixed", 1), ("fixed", 3), ("sah", 8), ("sah", 32), ("fixed", 32)):
+        dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, layout=layout)
         assert dsc.info()["leaf_size"] == leaf
+        assert dsc.info()["sah_cost"] > 0
         for mode in ("plain", "wavefront"):
             for block, stack, chunk in ((64, 8, 32), (128, 16, 64), (256, 32, 256)):
                 r = api.render(ctx, dsc, cam, 2, pixel_offset=0.5, mode=mode, outputs=("rgb", "paths"),
@@ -29,8 +30,9 @@ def test_results_invariant_under_tuning(ctx):
 
 
 def test_autotuner_writes_and_applies_table(ctx, tmp_path, monkeypatch):
-    monkeypatch.setattr(autotune, "CANDIDATES", {"leaf_size": [2, 4], "block_size": [64, 128],
-                                                 "stack_depth": [8, 16], "queue_chunk": [64, 128]})
+    monkeypatch.setattr(autotune, "CANDIDATES", {"layout": ["sah", "fixed"], "leaf_size": [2, 4],
+                                                 "block_size": [64, 128], "stack_depth": [8, 16],
+                                                 "queue_chunk": [64, 128]})
     sc = scenes.small_random_scene(82, n_spheres=12, level=3, lights=2)
     cams = [scenes.look_at((1.0, 3.0, 9.0), (0, -0.5, 0), 55.0, 160, 120)]
     path = tmp_path / "tuning.json"
@@ -43,4 +45,5 @@ def test_autotuner_writes_and_applies_table(ctx, tmp_path, monkeypatch):
     dsc = api.DeviceScene(ctx, sc, leaf_size=0)
     assert dsc.info()["leaf_size"] == table[b]["setting"]["leaf_size"]
     ctx.lib.eos_ctx_clear_tuning(ctx.h)
-    assert api.DeviceScene(ctx, sc, leaf_size=0).info()["leaf_size"] == 4
+    info = api.DeviceScene(ctx, sc, leaf_size=0).info()
+    assert info["leaf_size"] == 8 and info["layout"] == 1
