@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--views", type=int, default=4)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-config3", action="store_true", help="skip the 80-job batching workload")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: one 1080p view, batched and plain steps only")
     ap.add_argument("--autotune", action="store_true",
@@ -73,7 +74,7 @@ def parse():
     ap.add_argument("--no-tuning", action="store_true", help="ignore the committed tuning table")
     a = ap.parse_args()
     if a.profile:
-        a.views, a.no_adjoint, a.no_cpu_baseline = 1, True, True
+        a.views, a.no_adjoint, a.no_cpu_baseline, a.no_config3 = 1, True, True, True
     return a
 
 
@@ -304,14 +305,20 @@ def run_ours(args, rank, world, local):
             rays = float(r)
         return ms, rays, launches
 
+    def step_refill():
+        return api.render_batch(ctx, jobs, outs, refill=True)
+
     for _ in range(args.warmup):
         step_batched()
+        step_refill()
         step_plain()
     with ClockSampler(dev) as clk:
         ms_b, rays_b, launches_b = timed(step_batched, args.steps)
+        ms_c, rays_c, _ = timed(step_refill, args.steps)
         ms_p, rays_p, launches_p = timed(step_plain, args.steps)
     clocks = clk.summary()
     mrays_b = rays_b / (ms_b * 1e-3) / 1e6
+    mrays_c = rays_c / (ms_c * 1e-3) / 1e6
     mrays_p = rays_p / (ms_p * 1e-3) / 1e6
     if args.profile:
         if rank == 0:
@@ -372,7 +379,11 @@ def run_ours(args, rank, world, local):
     # adjoint: forward (with path records) + backward per view, config-4 style parameters
     adj = None
     if not args.no_adjoint:
-        adj = adjoint_timing(ctx, dsc, cams[:1], td, stream)
+        adj = adjoint_timing(ctx, stream)
+
+    batch3 = None
+    if not args.no_config3:
+        batch3 = config3_timing(ctx, stream, max(2, args.steps // 2), max(1, args.warmup))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -390,6 +401,8 @@ def run_ours(args, rank, world, local):
                    "tuning": "eos_b200/tuning_b200.json" if tuned else "defaults"},
         "plain": {"value": round(mrays_p, 2), "unit": "Mrays/s", "ms_per_step": round(ms_p / args.steps, 3)},
         "batched_over_plain": round(mrays_b / mrays_p, 3),
+        "batched_refill": {"value": round(mrays_c, 2), "unit": "Mrays/s",
+                           "note": "same batch, persistent kernels with lane refill (EOS_FLAG_REFILL)"},
         "rays_per_step": {"total": rays_b / args.steps / world},
         "e2e": {"value": round(e2e, 2), "unit": "Mrays/s", "mode": e2e_mode,
                 "h2d_bytes_per_step": len(cams) * (56 + 36), "d2h_bytes_per_step": 4 * npx_step},
@@ -408,6 +421,8 @@ def run_ours(args, rank, world, local):
     }
     if adj:
         line["adjoint"] = adj
+    if batch3:
+        line["config3_batch"] = batch3
     if cpu:
         line["cpu_baseline"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items()
                                 if k in ("value", "unit", "cores", "kind", "sample")}
@@ -419,37 +434,95 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
-def adjoint_timing(ctx, dsc, cams, td, stream, reps=5):
-    """fwd (plain render with path records) vs fwd + render_backward, ms per view."""
+def config3_timing(ctx, stream, steps, warmup):
+    """Batching workload: 64 views of the config-1 scene at mixed resolutions plus 16 mixed
+    scenes (10k-500k tris) at 512^2, depth 3, as one eos_render_batch call (graph replay)
+    against one eos_render call per view."""
     import torch
-    from eos_b200 import api
-    cam = cams[0]
-    npx = cam.width * cam.height
-    out = {"rgb": torch.empty((npx, 3), device="cuda"), "paths": torch.empty((npx, 16), dtype=torch.int32,
-                                                                                device="cuda")}
-    g = torch.full((npx, 3), 0.01, device="cuda")
+    from eos_b200 import api, scenes
+    spec = scenes.config3_jobs()
+    dev = {}
+    jobs = []
+    for j in spec:
+        if id(j.scene) not in dev:
+            dev[id(j.scene)] = api.DeviceScene(ctx, j.scene, inputs_on_device=True)
+        jobs.append(api.BatchJob(dev[id(j.scene)], j.camera, j.trace_depth, j.pixel_offset))
+    outs = api.make_batch_outputs(jobs, ("rgba8",))
 
-    def fwd():
-        api.render(ctx, dsc, cam, td, pixel_offset=0.5, outputs=(), out=dict(out))
+    def batched():
+        return [api.render_batch(ctx, jobs, outs)]
 
-    def fwdbwd():
-        fwd()
-        api.render_backward(ctx, dsc, [cam], td, out["paths"], g, pixel_offset=0.5)
+    def plain():
+        return [api.render(ctx, j.scene, j.camera, j.trace_depth, j.pixel_offset, outputs=(), out=dict(o))["stats"]
+                for j, o in zip(jobs, outs)]
 
     res = {}
-    for name, fn in (("fwd", fwd), ("fwd_adj", fwdbwd)):
-        fn()
+    for name, fn in (("batched", batched), ("plain", plain)):
+        for _ in range(warmup):
+            fn()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(reps):
-            fn()
+        rays = 0
+        for _ in range(steps):
+            rays += sum(s["primary_rays"] + s["shadow_rays"] + s["secondary_rays"] for s in fn())
         e1.record(stream)
         torch.cuda.synchronize()
-        res[name] = e0.elapsed_time(e1) / reps
-    return {"fwd_ms_per_view": round(res["fwd"], 3), "fwd_adj_ms_per_view": round(res["fwd_adj"], 3),
-            "ratio": round(res["fwd_adj"] / res["fwd"], 3), "view": f"{cam.width}x{cam.height}"}
+        ms = e0.elapsed_time(e1)
+        res[name] = {"mrays": round(rays / (ms * 1e-3) / 1e6, 1), "ms_per_step": round(ms / steps, 3)}
+    n_tris = sorted({j.scene.n_tris for j in spec})
+    return {"jobs": len(jobs), "scenes": len(dev), "tris_range": [n_tris[0], n_tris[-1]],
+            "pixels": sum(j.camera.width * j.camera.height for j in spec), **res,
+            "batched_over_plain": round(res["batched"]["mrays"] / res["plain"]["mrays"], 3)}
+
+
+def adjoint_timing(ctx, stream, reps=5):
+    """Differentiation workload (config 4): 8 views at 256^2 of 50 level-3 icospheres on a
+    ground quad, 3 lights, depth 2.  fwd = plain render of the views with path records;
+    fwd+adj adds eos_render_backward of an image L2 loss; ms per view.  Also the same on one
+    1080p view of the 1M-triangle scene."""
+    import torch
+    from eos_b200 import api, scenes
+
+    def measure(dsc, cams, td):
+        outs = []
+        for c in cams:
+            npx = c.width * c.height
+            outs.append({"rgb": torch.empty((npx, 3), device="cuda"),
+                         "paths": torch.empty((npx, 16), dtype=torch.int32, device="cuda")})
+        g = [torch.full((c.width * c.height, 3), 0.01, device="cuda") for c in cams]
+
+        def fwd():
+            for c, o in zip(cams, outs):
+                api.render(ctx, dsc, c, td, pixel_offset=0.5, outputs=(), out=dict(o))
+
+        def fwdbwd():
+            fwd()
+            for c, o, gg in zip(cams, outs, g):
+                api.render_backward(ctx, dsc, [c], td, o["paths"], gg, pixel_offset=0.5)
+
+        res = {}
+        for name, fn in (("fwd", fwd), ("fwd_adj", fwdbwd)):
+            fn()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            res[name] = e0.elapsed_time(e1) / reps / len(cams)
+        return {"fwd_ms_per_view": round(res["fwd"], 4), "fwd_adj_ms_per_view": round(res["fwd_adj"], 4),
+                "ratio": round(res["fwd_adj"] / res["fwd"], 3),
+                "views": f"{len(cams)} x {cams[0].width}x{cams[0].height}"}
+
+    sc4 = scenes.config4_scene()
+    d4 = api.DeviceScene(ctx, sc4, inputs_on_device=True)
+    out = measure(d4, scenes.config4_cameras(8, 256), 1)
+    out["workload"] = "config 4: 50 ico3 + quad, 3 lights, depth 2"
+    return out
 
 
 if __name__ == "__main__":

@@ -51,6 +51,7 @@ class RenderParams(Structure):
 
 
 FLAG_STAGE_TIMING = 1
+FLAG_REFILL = 2
 
 
 class Tuning(Structure):

@@ -127,9 +127,9 @@ __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p,
 // One node fetch: both child boxes tested, the nearer hit child becomes `cur`, the farther
 // one is pushed; no hit pops the stack.  Returns false on stack overflow.
 template <int SH>
-__device__ __forceinline__ bool visit_node(const DevScene& s, const SlabRay& r, int& cur, float limit,
-                                           TraversalStack<SH>& st, unsigned& nodes) {
-  const float4* nd = s.nodes + 4 * (size_t)cur;
+__device__ __forceinline__ bool visit_node(const float4* __restrict__ node_base, const SlabRay& r, int& cur,
+                                           float limit, TraversalStack<SH>& st, unsigned& nodes) {
+  const float4* nd = node_base + 4 * (size_t)cur;
   float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
   int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 3);
   ++nodes;
@@ -165,7 +165,7 @@ __device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, u
   int leaf = 0;  // parked leaf (0 = none)
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node<SH>(s, r, cur, h.t * kCull, st, h.nodes)) {
+      if (!visit_node<SH>(s.nodes, r, cur, h.t * kCull, st, h.nodes)) {
         atomicOr(err, kErrStack);
         return h;
       }
@@ -207,7 +207,7 @@ __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d,
   int leaf = 0;
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node<SH>(s, r, cur, kInf, st, res.nodes)) {
+      if (!visit_node<SH>(s.nodes, r, cur, kInf, st, res.nodes)) {
         atomicOr(err, kErrStack);
         return res;
       }
@@ -238,6 +238,111 @@ __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d,
     }
     if (cur == kDone) return res;
   }
+}
+
+// ------------------------------------------------------------------ resumable traversal
+// Per-lane traversal state for persistent kernels that refill lanes: a lane whose ray
+// ends takes the next ray from the queue while the other lanes of its warp continue, so
+// no lane idles until the slowest ray of its group ends.  One step = one round of the
+// two-loop traversal above (descend until the warp holds leaves, then intersect them).
+struct TravScene {
+  const float4* nodes;
+  const float4* tris;
+};
+
+template <int SH>
+struct RayTraversal {
+  SlabRay r;
+  f3 o, d;
+  TraversalStack<SH> st;
+  int cur, leaf;
+  __device__ __forceinline__ RayTraversal(uint2* base, int stride) : st(base, stride), cur(kDone), leaf(0) {}
+  __device__ __forceinline__ void start(f3 o_, f3 d_) {
+    o = o_;
+    d = d_;
+    r = make_slab(o_, d_);
+    st.sp = 0;
+    cur = 0;
+    leaf = 0;
+  }
+  __device__ __forceinline__ bool done() const { return cur == kDone && leaf == 0; }
+  __device__ __forceinline__ void finish() {
+    cur = kDone;
+    leaf = 0;
+  }
+};
+
+// One step of a nearest-hit traversal; h accumulates across steps.
+template <int SH>
+__device__ __forceinline__ void closest_step(const TravScene& s, RayTraversal<SH>& T, Hit& h, int* err) {
+  while (T.cur >= 0) {
+    if (!visit_node<SH>(s.nodes, T.r, T.cur, h.t * kCull, T.st, h.nodes)) {
+      atomicOr(err, kErrStack);
+      T.finish();
+      return;
+    }
+    if (T.cur != kDone && T.cur < 0 && T.leaf == 0) {
+      T.leaf = T.cur;
+      T.cur = T.st.next(h.t * kCull);
+    }
+    if (!__any_sync(__activemask(), T.leaf == 0)) break;
+  }
+  while (T.leaf != 0) {
+    const int first = leaf_first(T.leaf), cnt = leaf_count(T.leaf);
+    h.tests += cnt;
+    for (int p = first; p < first + cnt; ++p) {
+      f3 v1, e1, e2;
+      int id;
+      load_tri(s.tris, p, v1, e1, e2, id);
+      float t, u, v;
+      if (mt_intersect(T.o, T.d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
+        h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
+      }
+    }
+    T.leaf = 0;
+    if (T.cur != kDone && T.cur < 0) {
+      T.leaf = T.cur;
+      T.cur = T.st.next(h.t * kCull);
+    }
+  }
+}
+
+// One step of a shadow-ray traversal; returns true when the ray is blocked (it ends).
+template <int SH>
+__device__ __forceinline__ bool any_step(const TravScene& s, RayTraversal<SH>& T, unsigned& nodes, unsigned& tests,
+                                         int* err) {
+  while (T.cur >= 0) {
+    if (!visit_node<SH>(s.nodes, T.r, T.cur, kInf, T.st, nodes)) {
+      atomicOr(err, kErrStack);
+      T.finish();
+      return false;
+    }
+    if (T.cur != kDone && T.cur < 0 && T.leaf == 0) {
+      T.leaf = T.cur;
+      T.cur = T.st.next(kInf);
+    }
+    if (!__any_sync(__activemask(), T.leaf == 0)) break;
+  }
+  while (T.leaf != 0) {
+    const int first = leaf_first(T.leaf), cnt = leaf_count(T.leaf);
+    for (int p = first; p < first + cnt; ++p) {
+      f3 v1, e1, e2;
+      int id;
+      load_tri(s.tris, p, v1, e1, e2, id);
+      float t, u, v;
+      ++tests;
+      if (mt_intersect(T.o, T.d, v1, e1, e2, t, u, v)) {
+        T.finish();
+        return true;
+      }
+    }
+    T.leaf = 0;
+    if (T.cur != kDone && T.cur < 0) {
+      T.leaf = T.cur;
+      T.cur = T.st.next(kInf);
+    }
+  }
+  return false;
 }
 
 // Out-of-line copies for the plain megakernel, which calls both traversals: keeping them

@@ -240,6 +240,224 @@ __global__ void k_wf_closest(WfArgs A) {
   warp_add_count(&A.counts[kCntTestsC], tests);
 }
 
+// Emits the results of lanes whose nearest-hit ray has ended (`pending`): path record, hit
+// record, one shadow ray per light (compacted light-major inside the warp's block of the
+// queue, so a warp of the any-hit kernel mostly traces towards one light) and the mirror
+// ray (ballot / popc compaction, one atomic per warp).  Warp-uniform: every lane calls it.
+__device__ __forceinline__ void emit_results(const WfArgs& A, int* ctr, bool pending, int i, int path, int jb,
+                                             const Hit& h, f3 o, f3 d, unsigned& nshadow, unsigned& nhits) {
+  const int lane = threadIdx.x & 31;
+  const DevJob& J = A.jobs[jb];
+  bool hit = pending && h.pos >= 0;
+  bool refl = false;
+  f3 P = mk3(0, 0, 0), N = P;
+  int obj = -1;
+  if (pending) {
+    nhits += hit;
+    if (J.paths) {
+      int x, y, smp;
+      path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
+      J.paths[((size_t)y * J.w + x) * J.spp + smp].hit[A.k] = hit ? h.id : EOS_HIT_NONE;
+    }
+    if (hit) {
+      hit_geometry(J.s, o, d, h, P, N, obj);
+      refl = J.s.mats[8 * obj + 7] > 0.0f && A.k < J.trace_depth;
+    }
+    HitQ hq;
+    hq.a = make_float4(P.x, P.y, P.z, __int_as_float(path));
+    hq.b = make_float4(N.x, N.y, N.z, __int_as_float(hit ? obj : -1));
+    A.hits[i] = hq;
+    A.masks[i] = 0u;
+  }
+  int nl = hit ? J.s.n_lights : 0;
+  int maxl = nl;
+  for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(0xffffffffu, maxl, off));
+  if (maxl > 0) {
+    int total = nl;
+    for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
+    int wbase = 0;
+    if (lane == 0) wbase = atomicAdd(&ctr[2], total);
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    bool fits = wbase + total <= A.cap_s;
+    if (!fits && lane == 0) atomicOr(A.err, kErrQueue);
+    int prefix = 0;
+    for (int l = 0; l < maxl; ++l) {
+      uint32_t bl = __ballot_sync(0xffffffffu, l < nl);
+      if (l < nl && fits) {
+        const float* lp = J.s.lights + 6 * l;
+        f3 sd = norm3(sub3(mk3(lp[0], lp[1], lp[2]), P));
+        f3 so = add3(P, scale3(kRayEps, sd));
+        ShadowQ s;
+        s.a = make_float4(so.x, so.y, so.z, __int_as_float(i));
+        s.b = make_float4(sd.x, sd.y, sd.z, __int_as_float((jb << 5) | l));
+        A.sq[wbase + prefix + __popc(bl & lanemask_lt())] = s;
+      }
+      prefix += __popc(bl);
+    }
+    nshadow += nl;
+  }
+  uint32_t rb = __ballot_sync(0xffffffffu, refl);
+  if (rb) {
+    int rbase = 0;
+    if (lane == 0) rbase = atomicAdd(&ctr[1], __popc(rb));
+    rbase = __shfl_sync(0xffffffffu, rbase, 0);
+    if (refl) {
+      int pos = rbase + __popc(rb & lanemask_lt());
+      if (pos >= A.cap_r) {
+        atomicOr(A.err, kErrQueue);
+      } else {
+        f3 rd = norm3(reflect3(d, N));
+        f3 ro = add3(P, scale3(kRayEps, rd));
+        RayQ r;
+        r.a = make_float4(ro.x, ro.y, ro.z, __int_as_float(path));
+        r.b = make_float4(rd.x, rd.y, rd.z, 0.0f);
+        A.rout[pos] = r;
+      }
+    }
+  }
+}
+
+// Nearest-hit stage with lane refill: each iteration (1) emits the results of lanes whose
+// ray ended, (2) gives idle lanes new rays from the queue (one atomic per warp for all of
+// them), (3) advances every active lane by one traversal step.
+template <bool PRIMARY, int SH>
+__global__ void k_wf_closest_refill(WfArgs A) {
+  extern __shared__ uint2 shstack[];
+  int* ctr = A.ctr + A.k * kCtr;
+  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // mirror rays of bounce k-1
+  const int lane = threadIdx.x & 31;
+  RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
+  TravScene ts{nullptr, nullptr};
+  Hit h;
+  h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
+  int i = -1, path = -1, jb = 0;
+  bool pending = false;
+  bool more = true;  // warp-uniform: the queue still has rays
+  unsigned nrays = 0, nshadow = 0, nhits = 0;
+  unsigned long long nodes = 0, tests = 0;
+  for (;;) {
+    if (__any_sync(0xffffffffu, pending)) {
+      emit_results(A, ctr, pending, i, path, jb, h, T.o, T.d, nshadow, nhits);
+      if (pending) {
+        nodes += h.nodes;
+        tests += h.tests;
+        pending = false;
+        i = -1;
+      }
+    }
+    const uint32_t idle = __ballot_sync(0xffffffffu, i < 0);
+    if (idle && more) {
+      const int want = __popc(idle);
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&ctr[3], want);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base + want >= n_in) more = false;
+      if (i < 0) {
+        const int k = base + __popc(idle & lanemask_lt());
+        if (k < n_in) {
+          f3 o, d;
+          bool ok = true;
+          if (PRIMARY) {
+            long long gp = A.c0 + k;
+            jb = find_job(A.jobs, A.n_jobs, gp);
+            const DevJob& J = A.jobs[jb];
+            int x, y, smp;
+            ok = path_pixel(J, gp - J.path_off, x, y, smp);
+            if (ok) {
+              float ox, oy;
+              sample_offset((uint32_t)(y * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
+              d = primary_direction(J.cam, J.w, J.h, x, y, ox, oy);
+              o = mk3(J.cam[0], J.cam[1], J.cam[2]);
+              path = k;
+            }
+          } else {
+            RayQ r = A.rin[k];
+            o = mk3(r.a.x, r.a.y, r.a.z);
+            d = mk3(r.b.x, r.b.y, r.b.z);
+            path = __float_as_int(r.a.w);
+            jb = find_job(A.jobs, A.n_jobs, A.c0 + path);
+          }
+          if (ok) {
+            i = k;
+            ++nrays;
+            ts.nodes = A.jobs[jb].s.nodes;
+            ts.tris = A.jobs[jb].s.tris;
+            T.start(o, d);
+            h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
+          }
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, i >= 0) == 0) {
+      if (!more) break;
+      continue;
+    }
+    if (i >= 0) {
+      closest_step<SH>(ts, T, h, A.err);
+      if (T.done()) pending = true;
+    }
+  }
+  warp_add_count(&A.counts[A.k == 0 ? kCntPrimary : kCntSecondary], nrays);
+  warp_add_count(&A.counts[kCntShadow], nshadow);
+  warp_add_count(&A.counts[kCntHits], nhits);
+  warp_add_count(&A.counts[kCntNodesC], nodes);
+  warp_add_count(&A.counts[kCntTestsC], tests);
+}
+
+// Shadow stage with lane refill (see k_wf_closest_refill).
+template <int SH>
+__global__ void k_wf_any_refill(WfArgs A) {
+  extern __shared__ uint2 shstack[];
+  int* ctr = A.ctr + A.k * kCtr;
+  const int n = min(ctr[2], A.cap_s);
+  const int lane = threadIdx.x & 31;
+  RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
+  TravScene ts{nullptr, nullptr};
+  int i = -1, hi = 0, key = 0;
+  bool more = true;
+  unsigned nn = 0, nt = 0;
+  unsigned long long nodes = 0, tests = 0;
+  for (;;) {
+    const uint32_t idle = __ballot_sync(0xffffffffu, i < 0);
+    if (idle && more) {
+      const int want = __popc(idle);
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&ctr[4], want);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base + want >= n) more = false;
+      if (i < 0) {
+        const int k = base + __popc(idle & lanemask_lt());
+        if (k < n) {
+          ShadowQ s = A.sq[k];
+          i = k;
+          hi = __float_as_int(s.a.w);
+          key = __float_as_int(s.b.w);
+          const DevScene& S = A.jobs[key >> 5].s;
+          ts.nodes = S.nodes;
+          ts.tris = S.tris;
+          T.start(mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z));
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, i >= 0) == 0) {
+      if (!more) break;
+      continue;
+    }
+    if (i >= 0) {
+      if (any_step<SH>(ts, T, nn, nt, A.err)) {
+        atomicOr(&A.masks[hi], 1u << (key & 31));
+        i = -1;
+      } else if (T.done()) {
+        i = -1;
+      }
+    }
+  }
+  nodes += nn;
+  tests += nt;
+  warp_add_count(&A.counts[kCntNodesA], nodes);
+  warp_add_count(&A.counts[kCntTestsA], tests);
+}
+
 template <int SH>
 __global__ void k_wf_any(WfArgs A) {
   extern __shared__ uint2 shstack[];
@@ -381,11 +599,25 @@ struct StageTimer {
     if (s_ != EOS_OK) return s_;    \
   } while (0)
 
+// The nearest-hit / shadow kernels of one configuration: the chunked form (default; a
+// warp takes `queue_chunk` rays and finishes all before taking more) or lane refill.
+template <int SH>
+struct StageKernels {
+  void (*closest_primary)(WfArgs);
+  void (*closest)(WfArgs);
+  void (*any)(WfArgs);
+  static StageKernels get(bool refill) {
+    if (refill) return {k_wf_closest_refill<true, SH>, k_wf_closest_refill<false, SH>, k_wf_any_refill<SH>};
+    return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any<SH>};
+  }
+};
+
 template <int SH>
 eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, const Chunk* chunks, int n_chunks,
-                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem, StageTimer tm,
-                           uint32_t& launches) {
+                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem, bool refill,
+                           StageTimer tm, uint32_t& launches) {
   const int grid_lin = num_sms * 8;
+  const StageKernels<SH> K = StageKernels<SH>::get(refill);
   for (int ci = 0; ci < n_chunks; ++ci) {
     const Chunk& c = chunks[ci];
     WfArgs A = base;
@@ -403,13 +635,10 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
       A.rin = rin;
       A.rout = bufs[k & 1];
       EOS_TRY(tm.begin());
-      if (k == 0)
-        k_wf_closest<true, SH><<<grid_closest, block, smem, st>>>(A);
-      else
-        k_wf_closest<false, SH><<<grid_closest, block, smem, st>>>(A);
+      (k == 0 ? K.closest_primary : K.closest)<<<grid_closest, block, smem, st>>>(A);
       EOS_TRY(tm.end(0));
       EOS_TRY(tm.begin());
-      k_wf_any<SH><<<grid_any, block, smem, st>>>(A);
+      K.any<<<grid_any, block, smem, st>>>(A);
       EOS_TRY(tm.end(1));
       EOS_TRY(tm.begin());
       k_wf_shade<<<grid_lin, 256, 0, st>>>(A);
@@ -453,44 +682,35 @@ void fill_job(const eos_job& J, long long path_off, DevJob& d) {
 
 struct LaunchConfig {
   int block, sh, qchunk, grid_c, grid_a;
+  bool refill;
   size_t smem;
 };
+
+template <int SH>
+void configure(LaunchConfig& c, int num_sms) {
+  const StageKernels<SH> K = StageKernels<SH>::get(c.refill);
+  if (c.smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
+    cudaFuncSetAttribute(K.closest_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+    cudaFuncSetAttribute(K.closest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+    cudaFuncSetAttribute(K.any, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+  }
+  int occ_c = 0, occ_a = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, K.closest, c.block, c.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, K.any, c.block, c.smem);
+  c.grid_c = num_sms * std::max(1, occ_c);
+  c.grid_a = num_sms * std::max(1, occ_a);
+}
 
 LaunchConfig launch_config(const eos_render_params& p, int num_sms) {
   LaunchConfig c;
   c.block = p.block_size > 0 ? std::min(512, std::max(32, (p.block_size / 32) * 32)) : 128;
   c.sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
   c.qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
+  c.refill = (p.flags & EOS_FLAG_REFILL) != 0;
   c.smem = (size_t)c.sh * c.block * sizeof(uint2);
-  if (c.smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
-    const int b = (int)c.smem;
-    if (c.sh == 8) {
-      cudaFuncSetAttribute(k_wf_closest<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-      cudaFuncSetAttribute(k_wf_closest<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-      cudaFuncSetAttribute(k_wf_any<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    } else if (c.sh == 16) {
-      cudaFuncSetAttribute(k_wf_closest<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-      cudaFuncSetAttribute(k_wf_closest<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-      cudaFuncSetAttribute(k_wf_any<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    } else {
-      cudaFuncSetAttribute(k_wf_closest<true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-      cudaFuncSetAttribute(k_wf_closest<false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-      cudaFuncSetAttribute(k_wf_any<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    }
-  }
-  int occ_c = 0, occ_a = 0;
-  if (c.sh == 8) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 8>, c.block, c.smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<8>, c.block, c.smem);
-  } else if (c.sh == 16) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 16>, c.block, c.smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<16>, c.block, c.smem);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_wf_closest<false, 32>, c.block, c.smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_wf_any<32>, c.block, c.smem);
-  }
-  c.grid_c = num_sms * std::max(1, occ_c);
-  c.grid_a = num_sms * std::max(1, occ_a);
+  if (c.sh == 8) configure<8>(c, num_sms);
+  else if (c.sh == 16) configure<16>(c, num_sms);
+  else configure<32>(c, num_sms);
   return c;
 }
 
@@ -498,12 +718,12 @@ eos_status run_sequence(cudaStream_t st, int num_sms, const LaunchConfig& lc, co
                         int n_chunks, int depth, StageTimer tm, uint32_t& launches) {
   if (lc.sh == 8)
     return launch_sequence<8>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                              tm, launches);
+                              lc.refill, tm, launches);
   if (lc.sh == 16)
     return launch_sequence<16>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr,
-                               lc.smem, tm, launches);
+                               lc.smem, lc.refill, tm, launches);
   return launch_sequence<32>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                             tm, launches);
+                             lc.refill, tm, launches);
 }
 
 }  // namespace
@@ -584,7 +804,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   }
 
   // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
-  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)(size_t)d_jobs,
+  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.refill,
+                                (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
                                 (long long)(size_t)acc};
   for (const Chunk& c : merged) {

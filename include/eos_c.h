@@ -107,6 +107,11 @@ typedef struct eos_render_params {
 /* Wavefront only: run the stages eagerly (no graph) with CUDA events between them and
  * report per-stage device time in eos_stats.stage_ms. */
 #define EOS_FLAG_STAGE_TIMING 1
+/* Wavefront only: lane refill (a lane whose ray ends takes the next ray from the queue at
+ * once) instead of the default chunked persistent kernels (a warp takes queue_chunk rays
+ * and finishes them all before taking more).  Measured slower on B200 for the 1080p
+ * 1M-triangle workload: refilled lanes break the warps' ray coherence. */
+#define EOS_FLAG_REFILL 2
 
 /* Tuned launch / layout parameters of one scene-size bucket (see eos_ctx_set_tuning). */
 typedef struct eos_tuning {

@@ -18,10 +18,11 @@ def test_results_invariant_under_tuning(ctx):
         dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, layout=layout)
         assert dsc.info()["leaf_size"] == leaf
         assert dsc.info()["sah_cost"] > 0
-        for mode in ("plain", "wavefront"):
+        for mode, refill in (("plain", False), ("wavefront", False), ("wavefront", True)):
             for block, stack, chunk in ((64, 8, 32), (128, 16, 64), (256, 32, 256)):
                 r = api.render(ctx, dsc, cam, 2, pixel_offset=0.5, mode=mode, outputs=("rgb", "paths"),
-                               device=False, block_size=block, stack_depth=stack, queue_chunk=chunk)
+                               device=False, block_size=block, stack_depth=stack, queue_chunk=chunk,
+                               refill=refill)
                 if ref is None:
                     ref = r
                     continue
