@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-config3", action="store_true", help="skip the 80-job batching workload")
+    ap.add_argument("--no-config5", action="store_true", help="skip the 4.5M-triangle 4K stress workload")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: one 1080p view, batched and plain steps only")
     ap.add_argument("--autotune", action="store_true",
@@ -74,7 +75,7 @@ def parse():
     ap.add_argument("--no-tuning", action="store_true", help="ignore the committed tuning table")
     a = ap.parse_args()
     if a.profile:
-        a.views, a.no_adjoint, a.no_cpu_baseline, a.no_config3 = 1, True, True, True
+        a.views, a.no_adjoint, a.no_cpu_baseline, a.no_config3, a.no_config5 = 1, True, True, True, True
     return a
 
 
@@ -384,6 +385,9 @@ def run_ours(args, rank, world, local):
     batch3 = None
     if not args.no_config3:
         batch3 = config3_timing(ctx, stream, max(2, args.steps // 2), max(1, args.warmup))
+    stress5 = None
+    if not args.no_config5:
+        stress5 = config5_timing(ctx, stream, 2, 1)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -423,6 +427,8 @@ def run_ours(args, rank, world, local):
         line["adjoint"] = adj
     if batch3:
         line["config3_batch"] = batch3
+    if stress5:
+        line["config5_stress"] = stress5
     if cpu:
         line["cpu_baseline"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items()
                                 if k in ("value", "unit", "cores", "kind", "sample")}
@@ -475,6 +481,46 @@ def config3_timing(ctx, stream, steps, warmup):
     return {"jobs": len(jobs), "scenes": len(dev), "tris_range": [n_tris[0], n_tris[-1]],
             "pixels": sum(j.camera.width * j.camera.height for j in spec), **res,
             "batched_over_plain": round(res["batched"]["mrays"] / res["plain"]["mrays"], 3)}
+
+
+def config5_timing(ctx, stream, steps, warmup):
+    """Stress workload: 3840x2160, 2 spp with jitter, depth 4, 8 lights, 4,524,288 thin
+    triangles; one frame per step, batched wavefront vs plain."""
+    import torch
+    from eos_b200 import api, scenes
+    sc = scenes.config5_scene()
+    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
+    cam = scenes.config5_camera()
+    job = [api.BatchJob(dsc, cam, 3, 0.5, spp=2, jitter_seed=7)]
+    outs = api.make_batch_outputs(job, ("rgba8",))
+
+    def batched():
+        return [api.render_batch(ctx, job, outs)]
+
+    def plain():
+        return [api.render(ctx, dsc, cam, 3, pixel_offset=0.5, spp=2, jitter_seed=7, outputs=(),
+                           out=dict(outs[0]))["stats"]]
+
+    res = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rays = 0
+        for _ in range(steps):
+            rays += sum(s["primary_rays"] + s["shadow_rays"] + s["secondary_rays"] for s in fn())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name] = {"mrays": round(rays / (ms * 1e-3) / 1e6, 1), "ms_per_frame": round(ms / steps, 2),
+                     "rays_per_frame": rays // steps}
+    info = dsc.info()
+    return {"tris": sc.n_tris, "resolution": "3840x2160", "spp": 2, "depth": 4, "lights": 8, **res,
+            "batched_over_plain": round(res["batched"]["mrays"] / res["plain"]["mrays"], 3),
+            "lbvh_build_ms": round(info["build_ms"], 2)}
 
 
 def adjoint_timing(ctx, stream, reps=5):

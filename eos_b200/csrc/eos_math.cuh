@@ -61,6 +61,42 @@ EOS_HD bool mt_intersect(f3 o, f3 d, f3 v1, f3 e1, f3 e2, float& t, float& u, fl
   return true;
 }
 
+// The same test with the rejections evaluated cheapest first; the result (accept and the
+// bits of t, u, v) is identical to mt_intersect because acceptance is the conjunction of
+// the same five conditions on the same values:
+//   u = (T.P) * (1/det), v = (d.Q) * (1/det), t = (e2.Q) * (1/det)
+// A product of two floats rounds to a value of the product's sign (or to zero), so when
+// a numerator's sign is opposite to det's and its magnitude is far from the underflow
+// range, u (v, t) < 0 is decided without the division; misses mostly end there.
+__device__ __forceinline__ bool opposite_sign_reject(float num, float det) {
+  return (num < 0.0f) != (det < 0.0f) && fabsf(num) > 1e-30f;
+}
+
+__device__ __forceinline__ bool mt_intersect_fast(f3 o, f3 d, f3 v1, f3 e1, f3 e2, float& t, float& u, float& v) {
+  f3 P = cross3(d, e2);
+  float det = dot3(e1, P);
+  if (det > -0.00001f && det < 0.00001f) return false;
+  f3 T = sub3(o, v1);
+  float nu = dot3(T, P);
+  if (opposite_sign_reject(nu, det)) return false;  // u < 0
+  f3 Q = cross3(T, e1);
+  float nv = dot3(d, Q);
+  if (opposite_sign_reject(nv, det)) return false;  // v < 0
+  float nt = dot3(e2, Q);
+  if (opposite_sign_reject(nt, det)) return false;  // t < 0
+  float inv_det = 1.0f / det;
+  float uu = nu * inv_det;
+  if (uu < 0.0f || uu > 1.0f) return false;
+  float vv = nv * inv_det;
+  if (vv < 0.0f || uu + vv > 1.0f) return false;
+  float tt = nt * inv_det;
+  if (tt < 0.0f) return false;
+  t = tt;
+  u = uu;
+  v = vv;
+  return true;
+}
+
 // Primary ray direction of pixel (x, y) with sub-pixel offset (ox, oy)
 // (src/RayTracer.cpp:119-145; offset 0 reproduces the reference's integer corners).
 EOS_HD f3 primary_direction(const float* cam, int w, int h, int x, int y, float ox, float oy) {

@@ -183,7 +183,7 @@ __device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, u
         int id;
         load_tri(s.tris, p, v1, e1, e2, id);
         float t, u, v;
-        if (mt_intersect(o, d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
+        if (mt_intersect_fast(o, d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
           h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
         }
       }
@@ -225,7 +225,7 @@ __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d,
         load_tri(s.tris, p, v1, e1, e2, id);
         float t, u, v;
         ++res.tests;
-        if (mt_intersect(o, d, v1, e1, e2, t, u, v)) {
+        if (mt_intersect_fast(o, d, v1, e1, e2, t, u, v)) {
           res.hit = 1;
           return res;
         }
@@ -295,7 +295,7 @@ __device__ __forceinline__ void closest_step(const TravScene& s, RayTraversal<SH
       int id;
       load_tri(s.tris, p, v1, e1, e2, id);
       float t, u, v;
-      if (mt_intersect(T.o, T.d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
+      if (mt_intersect_fast(T.o, T.d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
         h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
       }
     }
@@ -331,7 +331,7 @@ __device__ __forceinline__ bool any_step(const TravScene& s, RayTraversal<SH>& T
       load_tri(s.tris, p, v1, e1, e2, id);
       float t, u, v;
       ++tests;
-      if (mt_intersect(T.o, T.d, v1, e1, e2, t, u, v)) {
+      if (mt_intersect_fast(T.o, T.d, v1, e1, e2, t, u, v)) {
         T.finish();
         return true;
       }
