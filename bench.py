@@ -161,6 +161,20 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+def algorithmic_bytes(st, width):
+    """Algorithmic bytes of the shadow (any-hit) and nearest-hit stages from the traversal
+    counters: 32 B per ray in; 4 B out per shadow ray, 16 B per nearest hit; 28 B per child
+    box visited (an AABB and a reference; a node visit reads `width` of them); 40 B per
+    triangle test (three vertices and an id); 84 B per shaded hit (normals 36 B, material
+    32 B, colour read-modify-write 16 B).  Layout-independent floor: what a node or
+    triangle record holds beyond this (padding, counts) is not counted."""
+    node = 28 * width
+    shadow = (32 + 4) * st["shadow_rays"] + node * st["nodes_shadow"] + 40 * st["tests_shadow"]
+    closest = ((32 + 16) * (st["primary_rays"] + st["secondary_rays"]) + node * st["nodes_closest"]
+               + 40 * st["tests_closest"] + 84 * st["shaded_hits"])
+    return shadow, closest
+
+
 def profile_traffic():
     """Per-ray DRAM traffic of the top kernels from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
@@ -309,22 +323,32 @@ def run_ours(args, rank, world, local):
     def step_refill():
         return api.render_batch(ctx, jobs, outs, refill=True)
 
+    b0 = None
+    if args.profile:
+        # bounce 0 of view 0 alone, before anything else: the launches that an ncu capture with
+        # -s 0 -c 1 of k_wf_closest / k_wf_any sees, so its DRAM bytes divide by known ray counts
+        b0 = api.render_batch(ctx, [api.BatchJob(dsc, cams[0], 0, 0.5)], outs[:1])
+
+    # clocks are sampled every 200 ms from the warm-up to the end of the GPU measurements
+    clk = ClockSampler(dev).__enter__()
     for _ in range(args.warmup):
         step_batched()
         step_refill()
         step_plain()
-    with ClockSampler(dev) as clk:
-        ms_b, rays_b, launches_b = timed(step_batched, args.steps)
-        ms_c, rays_c, _ = timed(step_refill, args.steps)
-        ms_p, rays_p, launches_p = timed(step_plain, args.steps)
-    clocks = clk.summary()
+    ms_b, rays_b, launches_b = timed(step_batched, args.steps)
+    ms_c, rays_c, _ = timed(step_refill, args.steps)
+    ms_p, rays_p, launches_p = timed(step_plain, args.steps)
     mrays_b = rays_b / (ms_b * 1e-3) / 1e6
     mrays_c = rays_c / (ms_c * 1e-3) / 1e6
     mrays_p = rays_p / (ms_p * 1e-3) / 1e6
     if args.profile:
+        clk.__exit__(None, None, None)
         if rank == 0:
             print(json.dumps({"profile_case": True, "batched_mrays": round(mrays_b, 1),
-                              "plain_mrays": round(mrays_p, 1)}), flush=True)
+                              "plain_mrays": round(mrays_p, 1),
+                              "bounce0": {k: b0[k] for k in ("primary_rays", "shadow_rays", "nodes_closest",
+                                                             "tests_closest", "nodes_shadow", "tests_shadow",
+                                                             "shaded_hits")}}), flush=True)
         return
 
     # e2e: reference-facing call with pinned host output, camera in / image out per view
@@ -359,23 +383,23 @@ def run_ours(args, rank, world, local):
     # roofline of the dominant kernel: per-stage device time of the wavefront (eager, one step)
     st = api.render_batch(ctx, jobs, outs, stage_timing=True)
     peak, peak_kind = measured_peak()
-    shadow_bytes = 36 * st["shadow_rays"] + 64 * st["nodes_shadow"] + 48 * st["tests_shadow"]
-    closest_bytes = (48 * (st["primary_rays"] + st["secondary_rays"]) + 64 * st["nodes_closest"]
-                     + 48 * st["tests_closest"] + 96 * st["shaded_hits"])
+    shadow_bytes, closest_bytes = algorithmic_bytes(st, info["width"])
     stage = st["stage_ms"]
     alg = {"closest": (closest_bytes, stage[0]), "shadow": (shadow_bytes, stage[1])}
     top = max(alg, key=lambda k: alg[k][1])
     bytes_top, ms_top = alg[top]
-    launches_top = (td + 1) * max(1, int(np.ceil(sum(1 for _ in cams))))
+    # one launch per bounce per chunk of <= 2^21 paths (8x4-pixel tiles)
+    paths = sum(((c.width + 7) // 8) * ((c.height + 3) // 4) * 32 for c in cams)
+    launches_top = (td + 1) * int(np.ceil(paths / float(1 << 21)))
     achieved = bytes_top / (ms_top * 1e-3) / 1e9
     traffic = profile_traffic().get(top)
     rays_top = (st["shadow_rays"] if top == "shadow" else st["primary_rays"] + st["secondary_rays"])
     roof = {"bound": "hbm", "kernel": "k_wf_any" if top == "shadow" else "k_wf_closest",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "peak_kind": peak_kind,
-            "traffic": (round(traffic["dram_bytes_per_ray"] * rays_top / ((td + 1)), 0) if traffic else None),
-            "algorithmic_bytes_per_step": bytes_top, "stage_ms": [round(x, 3) for x in stage],
-            "stage_launches_per_step": launches_top}
+            "traffic": (round(traffic["dram_bytes_per_ray"] * rays_top / launches_top) if traffic else None),
+            "algorithmic_bytes_per_launch": round(bytes_top / launches_top), "launches": launches_top,
+            "ms_per_launch": round(ms_top / launches_top, 4), "stage_ms": [round(x, 3) for x in stage]}
 
     # adjoint: forward (with path records) + backward per view, config-4 style parameters
     adj = None
@@ -388,6 +412,8 @@ def run_ours(args, rank, world, local):
     stress5 = None
     if not args.no_config5:
         stress5 = config5_timing(ctx, stream, 2, 1)
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -20,13 +20,14 @@ from . import _lib as L
 from . import api
 
 CANDIDATES = {
+    "width": [2, 4],
     "layout": ["sah", "fixed"],
     "leaf_size": [2, 4, 8, 16],
     "block_size": [64, 128, 256],
     "stack_depth": [8, 16, 32],
     "queue_chunk": [32, 64, 128],
 }
-DEFAULT = {"layout": "sah", "leaf_size": 8, "block_size": 128, "stack_depth": 16, "queue_chunk": 32}
+DEFAULT = {"width": 4, "layout": "fixed", "leaf_size": 4, "block_size": 128, "stack_depth": 16, "queue_chunk": 32}
 LAYOUT_CODE = {"sah": L.LAYOUT_SAH, "fixed": L.LAYOUT_FIXED}
 
 
@@ -56,14 +57,15 @@ def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log
     best = dict(DEFAULT)
     scenes_by_leaf = {}
 
-    def scene_for(layout, leaf):
-        if (layout, leaf) not in scenes_by_leaf:
-            scenes_by_leaf[(layout, leaf)] = api.DeviceScene(ctx, scene_data, leaf_size=leaf, inputs_on_device=True,
-                                                             layout=layout)
-        return scenes_by_leaf[(layout, leaf)]
+    def scene_for(width, layout, leaf):
+        key = (width, layout, leaf)
+        if key not in scenes_by_leaf:
+            scenes_by_leaf[key] = api.DeviceScene(ctx, scene_data, leaf_size=leaf, inputs_on_device=True,
+                                                  layout=layout, width=width)
+        return scenes_by_leaf[key]
 
     def measure(setting):
-        dsc = scene_for(setting["layout"], setting["leaf_size"])
+        dsc = scene_for(setting["width"], setting["layout"], setting["leaf_size"])
         jobs = [api.BatchJob(dsc, c, trace_depth, 0.5) for c in cameras]
         outs = api.make_batch_outputs(jobs, ("rgba8",))
         p = {k: setting[k] for k in ("block_size", "stack_depth", "queue_chunk")}
@@ -71,7 +73,7 @@ def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log
 
     best_v = measure(best)
     trials = [(dict(best), best_v)]
-    for key in ("layout", "leaf_size", "block_size", "stack_depth", "queue_chunk"):
+    for key in ("width", "layout", "leaf_size", "block_size", "stack_depth", "queue_chunk"):
         for v in CANDIDATES[key]:
             if v == best[key]:
                 continue
@@ -100,6 +102,7 @@ def apply_table(ctx, table: dict) -> None:
         t.stack_depth = int(s["stack_depth"])
         t.leaf_size = int(s["leaf_size"])
         t.layout = LAYOUT_CODE.get(s.get("layout", "sah"), L.LAYOUT_SAH)
+        t.width = int(s.get("width", 2))
         L.check(ctx.lib.eos_ctx_set_tuning(ctx.h, int(bucket), byref(t)), "eos_ctx_set_tuning")
 
 

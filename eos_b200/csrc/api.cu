@@ -249,7 +249,8 @@ eos_status eos_ctx_synchronize(eos_ctx* ctx) {
 eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning* t) {
   if (!ctx || !t) return EOS_ERR_INVALID_ARG;
   if (t->block_size < 0 || t->block_size > 1024 || t->queue_chunk < 0 || t->stack_depth < 0 || t->leaf_size < 0 ||
-      t->leaf_size > 32 || t->layout < EOS_LAYOUT_DEFAULT || t->layout > EOS_LAYOUT_FIXED)
+      t->leaf_size > 32 || t->layout < EOS_LAYOUT_DEFAULT || t->layout > EOS_LAYOUT_FIXED ||
+      (t->width != 0 && t->width != 2 && t->width != 4))
     return EOS_ERR_INVALID_ARG;
   ctx->tuning[min_tris] = *t;
   return EOS_OK;
@@ -278,12 +279,16 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   int layout = build && build->layout != EOS_LAYOUT_DEFAULT ? build->layout : tuned.layout;
   if (layout == EOS_LAYOUT_DEFAULT) layout = EOS_LAYOUT_SAH;
   if (layout != EOS_LAYOUT_SAH && layout != EOS_LAYOUT_FIXED) return EOS_ERR_INVALID_ARG;
+  int width = build && build->width != 0 ? build->width : tuned.width;
+  if (width == 0) width = 4;
+  if (width != 2 && width != 4) return EOS_ERR_INVALID_ARG;
   eos_status st = set_device(ctx);
   if (st != EOS_OK) return st;
   eos_scene* sc = new eos_scene();
   sc->ctx = ctx;
   sc->leaf_size = leaf;
   sc->layout = layout;
+  sc->width = width;
   auto fail = [&](eos_status s) {
     eos_scene_destroy(sc);
     return s;
@@ -310,6 +315,7 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   sc->dev.pos_of_id = (const int32_t*)sc->d_pos_of_id;
   sc->dev.mats = (const float*)sc->d_mats;
   sc->dev.lights = (const float*)sc->d_lights;
+  sc->dev.width = sc->width;
   if ((st = end_call(ctx, nullptr)) != EOS_OK) return fail(st);
   // object ids must index the material table: checked on the device copy
   {
@@ -360,6 +366,7 @@ eos_status eos_scene_get_info(const eos_scene* sc, eos_scene_info* info) {
   info->leaf_size = (uint32_t)sc->leaf_size;
   info->layout = (uint32_t)sc->layout;
   info->sah_cost = sc->sah_cost;
+  info->width = (uint32_t)sc->width;
   info->n_objects = (uint32_t)sc->dev.n_obj;
   info->n_lights = (uint32_t)sc->dev.n_lights;
   info->build_ms = sc->build_ms;

@@ -15,7 +15,9 @@ namespace eos {
 
 constexpr int kMaxBounces = EOS_MAX_BOUNCES;
 constexpr int kMaxLights = EOS_MAX_LIGHTS;
-constexpr int kStackMax = 64;  // >= LBVH depth bound: 30 code bits + 32 index bits + 2
+// Traversal stack entries: >= the binary LBVH depth bound (30 code bits + 32 index bits + 2)
+// and >= 3 per level of the 4-wide layout (which is used only when its depth allows).
+constexpr int kStackMax = 96;
 constexpr float kInf = __builtin_huge_valf();
 constexpr int kCounters = 8;  // ray / traversal counters per call (see trace.cuh)
 
@@ -55,7 +57,7 @@ struct DevScene {
   int32_t n_tris;
   int32_t n_obj;
   int32_t n_lights;
-  int32_t pad;
+  int32_t width;  // node layout: 2 (binary) or 4 (4-wide)
 };
 
 struct DevBuffer {
@@ -108,6 +110,8 @@ struct eos_scene {
   uint32_t n_nodes = 0;
   int leaf_size = 8;
   int layout = EOS_LAYOUT_SAH;
+  int width = 2;        // 2: binary 64-B nodes, 4: 4-wide 128-B nodes
+  int wide_levels = 0;  // depth of the 4-wide tree
   float sah_cost = 0.0f;
   float build_ms = 0.0f;
   size_t device_bytes = 0;

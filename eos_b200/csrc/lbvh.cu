@@ -351,6 +351,86 @@ __global__ void k_refit(int n, const int2* __restrict__ child, const int2* __res
   }
 }
 
+// ------------------------------------------------------------------ 4-wide layout
+// Each 4-wide node is made from one binary node by replacing its interior child of largest
+// surface area by that child's two children until it has four children or only leaves
+// (one-triangle leaves and collapsed subtrees stay leaves).  Top-down, one launch per
+// level; frontier entries are (binary node, 4-wide node) pairs.
+//
+// 4-wide node, 128 B = 8 x float4 (structure of arrays over the four children):
+//   [0] lo.x[4] [1] lo.y[4] [2] lo.z[4] [3] hi.x[4] [4] hi.y[4] [5] hi.z[4]
+//   [6] ref[4] (as the binary layout; kEmptyRef for a missing child)  [7] count[4]
+constexpr int kEmptyRef = (int)0xC0000000;
+
+__global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* __restrict__ range,
+                             const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                             const int2* __restrict__ frontier_in, int n_in, int2* __restrict__ frontier_out,
+                             int* __restrict__ n_out, int* __restrict__ w_count, float4* __restrict__ wnodes,
+                             int max_nodes, int* err) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_in) return;
+  const int2 item = frontier_in[t];
+  int c[4];
+  int2 ch = child[item.x];
+  c[0] = ch.x;
+  c[1] = ch.y;
+  int k = 2;
+  while (k < 4) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (int i = 0; i < k; ++i) {
+      const int ci = c[i];
+      if (ci >= n - 1 || bhi[ci].w != 0.0f) continue;  // triangle or collapsed subtree: a leaf
+      const float a = half_area(blo[ci], bhi[ci]);
+      if (a > best_area) {
+        best_area = a;
+        best = i;
+      }
+    }
+    if (best < 0) break;
+    const int2 g = child[c[best]];
+    c[best] = g.x;
+    c[k++] = g.y;
+  }
+  float v[6][4];
+  int ref[4], cnt[4];
+  for (int i = 0; i < 4; ++i) {
+    if (i >= k) {
+      for (int a = 0; a < 6; ++a) v[a][i] = 0.0f;
+      ref[i] = kEmptyRef;
+      cnt[i] = -1;
+      continue;
+    }
+    const int ci = c[i];
+    const float4 l = blo[ci], h = bhi[ci];
+    v[0][i] = l.x; v[1][i] = l.y; v[2][i] = l.z;
+    v[3][i] = h.x; v[4][i] = h.y; v[5][i] = h.z;
+    if (ci >= n - 1) {
+      cnt[i] = 1;
+      ref[i] = pack_leaf(ci - (n - 1), 1);
+    } else if (h.w != 0.0f) {
+      const int2 r = range[ci];
+      cnt[i] = r.y - r.x + 1;
+      ref[i] = pack_leaf(r.x, cnt[i]);
+    } else {
+      const int w = atomicAdd(w_count, 1);
+      if (w >= max_nodes) {  // cannot happen: a 4-wide tree has fewer nodes than the binary one
+        atomicOr(err, kErrQueue);
+        ref[i] = kEmptyRef;
+        cnt[i] = -1;
+        continue;
+      }
+      frontier_out[atomicAdd(n_out, 1)] = make_int2(ci, w);
+      ref[i] = w;
+      cnt[i] = 0;
+    }
+  }
+  float4* o = wnodes + 8 * (size_t)item.y;
+  for (int a = 0; a < 6; ++a) o[a] = make_float4(v[a][0], v[a][1], v[a][2], v[a][3]);
+  o[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+  o[7] = make_float4(__int_as_float(cnt[0]), __int_as_float(cnt[1]), __int_as_float(cnt[2]), __int_as_float(cnt[3]));
+}
+
 // Root record for scenes of 0 or 1 triangle (no interior node exists).
 __global__ void k_small_root(int n, const float4* __restrict__ blo, const float4* __restrict__ bhi,
                              float4* __restrict__ nodes) {
@@ -364,6 +444,51 @@ __global__ void k_small_root(int n, const float4* __restrict__ blo, const float4
 }
 
 inline int grid_for(size_t n, int block) { return (int)std::max<size_t>(1, (n + block - 1) / block); }
+
+// Converts the binary tree (node records already written) into the 4-wide layout.  The
+// traversal stack needs at most 3 entries per 4-wide level; when the 4-wide tree is deeper
+// than kStackMax / 3 levels the scene keeps the binary layout.
+eos_status build_wide(eos_ctx* ctx, eos_scene* sc, int n, const int2* child, const int2* range, const float4* blo,
+                      const float4* bhi) {
+  cudaStream_t st = ctx->stream;
+  eos_status es = EOS_OK;
+  const int max_nodes = n - 1;
+  int2* fa = (int2*)scratch(ctx, "lbvh.wide.fa", 8 * (size_t)n, &es);
+  int2* fb = (int2*)scratch(ctx, "lbvh.wide.fb", 8 * (size_t)n, &es);
+  int* cnt = (int*)scratch(ctx, "lbvh.wide.cnt", 8, &es);
+  if (es != EOS_OK) return es;
+  void* wide = nullptr;
+  EOS_CUDA(cudaMalloc(&wide, 128 * (size_t)max_nodes));
+  int h_init[2] = {1, 0};  // w_count, n_out
+  int2 root = make_int2(0, 0);
+  cudaError_t ce = cudaMemcpyAsync(cnt, h_init, sizeof h_init, cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(fa, &root, sizeof root, cudaMemcpyHostToDevice, st);
+  int n_in = 1, levels = 0;
+  while (ce == cudaSuccess && n_in > 0) {
+    ce = cudaMemsetAsync(cnt + 1, 0, sizeof(int), st);
+    if (ce != cudaSuccess) break;
+    k_wide_level<<<grid_for(n_in, 128), 128, 0, st>>>(n, child, range, blo, bhi, fa, n_in, fb, cnt + 1, cnt,
+                                                       (float4*)wide, max_nodes, ctx->d_err);
+    ++levels;
+    ce = cudaMemcpyAsync(&n_in, cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    std::swap(fa, fb);
+    if (levels > 4 * kStackMax) break;  // bounded: depth <= the binary depth
+  }
+  int w_count = 0;
+  if (ce == cudaSuccess) ce = cudaMemcpy(&w_count, cnt, sizeof(int), cudaMemcpyDeviceToHost);
+  if (ce != cudaSuccess || n_in > 0 || 3 * levels > kStackMax) {
+    cudaFree(wide);
+    sc->width = 2;
+    return ce == cudaSuccess ? EOS_OK : EOS_ERR_CUDA;
+  }
+  cudaFree(sc->d_nodes);
+  sc->d_nodes = wide;
+  sc->device_bytes += 128 * (size_t)max_nodes - 64 * (size_t)sc->n_nodes;
+  sc->n_nodes = (uint32_t)w_count;
+  sc->wide_levels = levels;
+  return EOS_OK;
+}
 
 }  // namespace
 
@@ -431,8 +556,13 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
                                               ctx->d_err);
     // SAH cost of the tree (subtree cost of the root, in triangle-test units)
     EOS_CUDA(cudaMemcpyAsync(&sc->sah_cost, &blo[0].w, sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (sc->width == 4) {
+      eos_status ws = build_wide(ctx, sc, n, child, range, blo, bhi);
+      if (ws != EOS_OK) return ws;
+    }
   } else {
     k_small_root<<<1, 1, 0, st>>>(n, blo, bhi, (float4*)sc->d_nodes);
+    sc->width = 2;
   }
   EOS_CUDA(cudaGetLastError());
   EOS_CUDA(cudaEventRecord(ctx->ev1, st));

@@ -78,7 +78,7 @@ struct AnyResult {
 //   leaf          0x80000000 | (count - 1) << 25 | first   (count <= 32, first < 2^25)
 //   kDone (-1)    end of traversal (never stored in a node; bit 30 distinguishes it)
 constexpr int kDone = -1;
-__device__ __forceinline__ bool is_leaf_ref(int r) { return (r & 0xC0000000) == (int)0x80000000; }
+__device__ __forceinline__ bool is_leaf_ref(int r) { return ((uint32_t)r & 0xC0000000u) == 0x80000000u; }
 __device__ __forceinline__ int leaf_first(int r) { return r & 0x01ffffff; }
 __device__ __forceinline__ int leaf_count(int r) { return ((r >> 25) & 31) + 1; }
 
@@ -151,6 +151,61 @@ __device__ __forceinline__ bool visit_node(const float4* __restrict__ node_base,
   return true;
 }
 
+// One fetch of a 4-wide node (128 B): four child boxes tested; with SORT the hit children
+// are ordered by entry distance (five compare-exchanges), the nearest becomes `cur` and the
+// others are pushed farthest first; without SORT (shadow rays) the first hit is taken.
+constexpr int kEmptyRef = (int)0xC0000000;
+
+template <int SH, bool SORT>
+__device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const SlabRay& r, int& cur,
+                                            float limit, TraversalStack<SH>& st, unsigned& nodes) {
+  const float4* nd = node_base + 8 * (size_t)cur;
+  const float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+  const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+  const int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 6);
+  ++nodes;
+  float t[4];
+  int c[4] = {ref.x, ref.y, ref.z, ref.w};
+  t[0] = ref.x != kEmptyRef ? slab(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, limit) : kInf;
+  t[1] = ref.y != kEmptyRef ? slab(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, limit) : kInf;
+  t[2] = ref.z != kEmptyRef ? slab(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, limit) : kInf;
+  t[3] = ref.w != kEmptyRef ? slab(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, limit) : kInf;
+  if (SORT) {
+#define EOS_CX(a, b)                 \
+  if (t[b] < t[a]) {                 \
+    float tt = t[a]; t[a] = t[b]; t[b] = tt; \
+    int cc = c[a]; c[a] = c[b]; c[b] = cc;   \
+  }
+    EOS_CX(0, 1) EOS_CX(2, 3) EOS_CX(0, 2) EOS_CX(1, 3) EOS_CX(1, 2)
+#undef EOS_CX
+    if (t[0] == kInf) {
+      cur = st.next(limit);
+      return true;
+    }
+#pragma unroll
+    for (int i = 3; i >= 1; --i)
+      if (t[i] != kInf && !st.push(c[i], t[i])) return false;
+    cur = c[0];
+    return true;
+  }
+  int first = -1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (t[i] == kInf) continue;
+    if (first < 0) first = i;
+    else if (!st.push(c[i], t[i])) return false;
+  }
+  cur = first < 0 ? st.next(limit) : c[first];
+  return true;
+}
+
+template <int SH, bool SORT>
+__device__ __forceinline__ bool visit_any_width(int width, const float4* __restrict__ node_base, const SlabRay& r,
+                                                int& cur, float limit, TraversalStack<SH>& st, unsigned& nodes) {
+  if (width == 4) return visit_node4<SH, SORT>(node_base, r, cur, limit, st, nodes);
+  return visit_node<SH>(node_base, r, cur, limit, st, nodes);
+}
+
 // Nearest hit.  Traversal in the two-loop form of Aila & Laine ("Understanding the
 // efficiency of ray traversal on GPUs", HPG 2009): a lane that reaches a leaf parks it and
 // keeps descending until every lane of the warp holds a leaf, then the lanes intersect
@@ -165,7 +220,7 @@ __device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, u
   int leaf = 0;  // parked leaf (0 = none)
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node<SH>(s.nodes, r, cur, h.t * kCull, st, h.nodes)) {
+      if (!visit_any_width<SH, true>(s.width, s.nodes, r, cur, h.t * kCull, st, h.nodes)) {
         atomicOr(err, kErrStack);
         return h;
       }
@@ -207,7 +262,7 @@ __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d,
   int leaf = 0;
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node<SH>(s.nodes, r, cur, kInf, st, res.nodes)) {
+      if (!visit_any_width<SH, false>(s.width, s.nodes, r, cur, kInf, st, res.nodes)) {
         atomicOr(err, kErrStack);
         return res;
       }
@@ -248,6 +303,7 @@ __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d,
 struct TravScene {
   const float4* nodes;
   const float4* tris;
+  int width;
 };
 
 template <int SH>
@@ -276,7 +332,7 @@ struct RayTraversal {
 template <int SH>
 __device__ __forceinline__ void closest_step(const TravScene& s, RayTraversal<SH>& T, Hit& h, int* err) {
   while (T.cur >= 0) {
-    if (!visit_node<SH>(s.nodes, T.r, T.cur, h.t * kCull, T.st, h.nodes)) {
+    if (!visit_any_width<SH, true>(s.width, s.nodes, T.r, T.cur, h.t * kCull, T.st, h.nodes)) {
       atomicOr(err, kErrStack);
       T.finish();
       return;
@@ -312,7 +368,7 @@ template <int SH>
 __device__ __forceinline__ bool any_step(const TravScene& s, RayTraversal<SH>& T, unsigned& nodes, unsigned& tests,
                                          int* err) {
   while (T.cur >= 0) {
-    if (!visit_node<SH>(s.nodes, T.r, T.cur, kInf, T.st, nodes)) {
+    if (!visit_any_width<SH, false>(s.width, s.nodes, T.r, T.cur, kInf, T.st, nodes)) {
       atomicOr(err, kErrStack);
       T.finish();
       return false;

@@ -327,7 +327,7 @@ __global__ void k_wf_closest_refill(WfArgs A) {
   const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // mirror rays of bounce k-1
   const int lane = threadIdx.x & 31;
   RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
-  TravScene ts{nullptr, nullptr};
+  TravScene ts{nullptr, nullptr, 2};
   Hit h;
   h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
   int i = -1, path = -1, jb = 0;
@@ -382,6 +382,7 @@ __global__ void k_wf_closest_refill(WfArgs A) {
             ++nrays;
             ts.nodes = A.jobs[jb].s.nodes;
             ts.tris = A.jobs[jb].s.tris;
+            ts.width = A.jobs[jb].s.width;
             T.start(o, d);
             h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
           }
@@ -412,7 +413,7 @@ __global__ void k_wf_any_refill(WfArgs A) {
   const int n = min(ctr[2], A.cap_s);
   const int lane = threadIdx.x & 31;
   RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
-  TravScene ts{nullptr, nullptr};
+  TravScene ts{nullptr, nullptr, 2};
   int i = -1, hi = 0, key = 0;
   bool more = true;
   unsigned nn = 0, nt = 0;
@@ -435,6 +436,7 @@ __global__ void k_wf_any_refill(WfArgs A) {
           const DevScene& S = A.jobs[key >> 5].s;
           ts.nodes = S.nodes;
           ts.tris = S.tris;
+          ts.width = S.width;
           T.start(mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z));
         }
       }

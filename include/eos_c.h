@@ -120,6 +120,7 @@ typedef struct eos_tuning {
   int32_t stack_depth;
   int32_t leaf_size;
   int32_t layout;
+  int32_t width;
 } eos_tuning;
 
 /* Node layout of the LBVH: which subtrees become leaves. */
@@ -132,6 +133,8 @@ enum {
 typedef struct eos_build_params {
   int32_t leaf_size;    /* largest leaf, 1..32 triangles; 0 = tuned value, else 8 */
   int32_t layout;       /* EOS_LAYOUT_* */
+  int32_t width;        /* node width: 2 (64-B binary nodes) or 4 (128-B 4-child nodes);
+                           0 = tuned value, else 4 */
 } eos_build_params;
 
 /* Per-path record of the bounce path: hit triangle id per bounce and, per bounce, the
@@ -162,6 +165,7 @@ typedef struct eos_scene_info {
   uint32_t n_nodes;       /* interior nodes of the LBVH (n_tris - 1) */
   uint32_t leaf_size;
   uint32_t layout;        /* EOS_LAYOUT_SAH or EOS_LAYOUT_FIXED */
+  uint32_t width;         /* 2 or 4 (a 4-wide request too deep for the stack stays 2) */
   float sah_cost;         /* SAH cost of the tree, in triangle-test units */
   uint32_t n_objects;
   uint32_t n_lights;

@@ -155,10 +155,11 @@ def _random_rays(n, seed, lo=-3, hi=3):
     return np.concatenate([r, ax])
 
 
-@pytest.mark.parametrize("leaf", [1, 4, 8])
-def test_queries_match_oracle(ctx, leaf):
+@pytest.mark.parametrize("leaf,width", [(1, 2), (4, 2), (8, 2), (1, 4), (4, 4), (16, 4)])
+def test_queries_match_oracle(ctx, leaf, width):
     sc = scenes.small_random_scene(51, n_spheres=8, level=3, lights=2)
-    dsc = api.DeviceScene(ctx, sc, leaf_size=leaf)
+    dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, width=width)
+    assert dsc.info()["width"] == width
     orc = oracle.Oracle(sc)
     rays = _random_rays(20000, 9)
     ids, t = api.trace_closest(ctx, dsc, rays)
@@ -214,10 +215,12 @@ def test_invalid_arguments_report_status(ctx):
     assert r["rgb"].shape == (64, 3)
 
 
-def test_config2_sampled_pixels_match_oracle(ctx):
+@pytest.mark.parametrize("width", [2, 4])
+def test_config2_sampled_pixels_match_oracle(ctx, width):
     """1920x1080, ~1.06M triangles, depth 3, 4 lights: 30k sampled paths vs the oracle."""
     sc = scenes.config2_scene()
-    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
+    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True, width=width)
+    assert dsc.info()["width"] == width
     cam = scenes.config2_camera()
     g = api.render(ctx, dsc, cam, 2, pixel_offset=0.5, outputs=("rgb", "paths"), device=True)
     rng = np.random.default_rng(0)
