@@ -398,6 +398,8 @@ def run_ours(args, rank, world, local):
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "peak_kind": peak_kind,
             "traffic": (round(traffic["dram_bytes_per_ray"] * rays_top / launches_top) if traffic else None),
+            "traffic_source": ("ncu capture of the same kernel, cold caches, DRAM bytes per ray x rays per launch"
+                               if traffic else None),
             "algorithmic_bytes_per_launch": round(bytes_top / launches_top), "launches": launches_top,
             "ms_per_launch": round(ms_top / launches_top, 4), "stage_ms": [round(x, 3) for x in stage]}
 

@@ -315,7 +315,6 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   sc->dev.pos_of_id = (const int32_t*)sc->d_pos_of_id;
   sc->dev.mats = (const float*)sc->d_mats;
   sc->dev.lights = (const float*)sc->d_lights;
-  sc->dev.width = sc->width;
   if ((st = end_call(ctx, nullptr)) != EOS_OK) return fail(st);
   // object ids must index the material table: checked on the device copy
   {

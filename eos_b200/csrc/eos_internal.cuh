@@ -57,7 +57,6 @@ struct DevScene {
   int32_t n_tris;
   int32_t n_obj;
   int32_t n_lights;
-  int32_t width;  // node layout: 2 (binary) or 4 (4-wide)
 };
 
 struct DevBuffer {
@@ -110,8 +109,8 @@ struct eos_scene {
   uint32_t n_nodes = 0;
   int leaf_size = 8;
   int layout = EOS_LAYOUT_SAH;
-  int width = 2;        // 2: binary 64-B nodes, 4: 4-wide 128-B nodes
-  int wide_levels = 0;  // depth of the 4-wide tree
+  int width = 4;   // children per 128-B node record: 4, or 2 (binary tree)
+  int levels = 0;  // depth of the tree of records
   float sah_cost = 0.0f;
   float build_ms = 0.0f;
   size_t device_bytes = 0;

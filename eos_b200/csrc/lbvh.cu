@@ -1,5 +1,5 @@
 // GPU LBVH build: Morton codes -> stable radix sort -> Karras hierarchy -> atomic refit
-// -> 64-byte node / 48-byte triangle records.
+// -> 128-byte node records (4-wide, or 2 children per record) / 48-byte triangle records.
 //
 // Replaces the reference's CPU top-down median/SAH build (src/BVH.cpp:97-111,549-606) and
 // its SoA upload (src/cudaStructures.cu:36-174,274-405).  The Morton encoder is the
@@ -277,25 +277,6 @@ __host__ __device__ __forceinline__ int pack_leaf(int first, int count) {
   return (int)(0x80000000u | ((uint32_t)(count - 1) << 25) | (uint32_t)first);
 }
 
-// Reference to child c: a one-triangle leaf, a collapsed subtree (leaf of its whole
-// range) or an interior node.  `collapsed` is the child's own decision from the refit.
-__device__ __forceinline__ void child_ref(int c, int n, const int2* __restrict__ range, bool collapsed, int& ref,
-                                          int& cnt) {
-  if (c >= n - 1) {
-    cnt = 1;
-    ref = pack_leaf(c - (n - 1), 1);
-    return;
-  }
-  if (collapsed) {
-    int2 r = range[c];
-    cnt = r.y - r.x + 1;
-    ref = pack_leaf(r.x, cnt);
-  } else {
-    ref = c;
-    cnt = 0;
-  }
-}
-
 constexpr float kCostNode = 1.0f;  // SAH cost of visiting one node (two box tests)
 constexpr float kCostTri = 1.0f;   // SAH cost of one triangle test
 
@@ -305,14 +286,14 @@ __device__ __forceinline__ float half_area(float4 l, float4 h) {
 }
 
 // Bottom-up refit: one thread per leaf walks to the root; the second thread to reach an
-// interior node merges the two child boxes, decides whether the subtree becomes one leaf
-// and writes the node record.  Leaf decision: fixed layout -> the range has at most
+// interior node merges the two child boxes and decides whether the subtree becomes one
+// leaf (node records are written afterwards by the wide conversion).  Leaf decision: fixed layout -> the range has at most
 // max_leaf triangles; SAH layout -> additionally the leaf's cost kCostTri * n is not above
 // kCostNode + (A_l cost_l + A_r cost_r) / A.  Box .w carries the subtree cost (lo) and the
 // leaf decision (hi).  Bounded walk: the tree depth is at most kStackMax.
 __global__ void k_refit(int n, const int2* __restrict__ child, const int2* __restrict__ range,
                         const int* __restrict__ parent, float4* blo, float4* bhi, int* __restrict__ arrive,
-                        float4* __restrict__ nodes, int max_leaf, int sah, int* err) {
+                        int max_leaf, int sah, int* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int node = parent[n - 1 + p];
@@ -339,34 +320,37 @@ __global__ void k_refit(int n, const int2* __restrict__ child, const int2* __res
     hi.w = collapse ? 1.0f : 0.0f;
     blo[node] = lo;
     bhi[node] = hi;
-    int r0, n0, r1, n1;
-    child_ref(c.x, n, range, h0.w != 0.0f, r0, n0);
-    child_ref(c.y, n, range, h1.w != 0.0f, r1, n1);
-    float4* o = nodes + 4 * (size_t)node;
-    o[0] = make_float4(l0.x, l0.y, l0.z, h0.x);
-    o[1] = make_float4(h0.y, h0.z, l1.x, l1.y);
-    o[2] = make_float4(l1.z, h1.x, h1.y, h1.z);
-    o[3] = make_float4(__int_as_float(r0), __int_as_float(r1), __int_as_float(n0), __int_as_float(n1));
     node = parent[node];
   }
 }
 
-// ------------------------------------------------------------------ 4-wide layout
-// Each 4-wide node is made from one binary node by replacing its interior child of largest
-// surface area by that child's two children until it has four children or only leaves
-// (one-triangle leaves and collapsed subtrees stay leaves).  Top-down, one launch per
-// level; frontier entries are (binary node, 4-wide node) pairs.
+// ------------------------------------------------------------------ node records
+// Every node record has four child slots.  A node is made from one binary node by
+// replacing its interior child of largest surface area by that child's two children until
+// it has `max_children` children (4 for the 4-wide layout, 2 for the binary one) or only
+// leaves (one-triangle leaves and collapsed subtrees stay leaves).  Top-down, one launch
+// per level; frontier entries are (binary node, record) pairs.
 //
-// 4-wide node, 128 B = 8 x float4 (structure of arrays over the four children):
+// Record, 128 B = 8 x float4 (structure of arrays over the four slots):
 //   [0] lo.x[4] [1] lo.y[4] [2] lo.z[4] [3] hi.x[4] [4] hi.y[4] [5] hi.z[4]
-//   [6] ref[4] (as the binary layout; kEmptyRef for a missing child)  [7] count[4]
+//   [6] ref[4]: interior record index, packed leaf, or kEmptyRef for an unused slot
+//       (whose box is lo = hi = +inf: every slab test misses it, so the traversal needs
+//       no per-slot check)
+//   [7] count[4]: triangles of a leaf, 0 for an interior child, -1 for an unused slot
 constexpr int kEmptyRef = (int)0xC0000000;
+
+__device__ __forceinline__ void write_record(float4* o, const float (&v)[6][4], const int (&ref)[4],
+                                             const int (&cnt)[4]) {
+  for (int a = 0; a < 6; ++a) o[a] = make_float4(v[a][0], v[a][1], v[a][2], v[a][3]);
+  o[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+  o[7] = make_float4(__int_as_float(cnt[0]), __int_as_float(cnt[1]), __int_as_float(cnt[2]), __int_as_float(cnt[3]));
+}
 
 __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* __restrict__ range,
                              const float4* __restrict__ blo, const float4* __restrict__ bhi,
                              const int2* __restrict__ frontier_in, int n_in, int2* __restrict__ frontier_out,
                              int* __restrict__ n_out, int* __restrict__ w_count, float4* __restrict__ wnodes,
-                             int max_nodes, int* err) {
+                             int max_nodes, int max_children, int* err) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_in) return;
   const int2 item = frontier_in[t];
@@ -375,7 +359,7 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
   c[0] = ch.x;
   c[1] = ch.y;
   int k = 2;
-  while (k < 4) {
+  while (k < max_children) {
     int best = -1;
     float best_area = -1.0f;
     for (int i = 0; i < k; ++i) {
@@ -396,7 +380,7 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
   int ref[4], cnt[4];
   for (int i = 0; i < 4; ++i) {
     if (i >= k) {
-      for (int a = 0; a < 6; ++a) v[a][i] = 0.0f;
+      for (int a = 0; a < 6; ++a) v[a][i] = kInf;  // a box no ray enters
       ref[i] = kEmptyRef;
       cnt[i] = -1;
       continue;
@@ -414,8 +398,9 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
       ref[i] = pack_leaf(r.x, cnt[i]);
     } else {
       const int w = atomicAdd(w_count, 1);
-      if (w >= max_nodes) {  // cannot happen: a 4-wide tree has fewer nodes than the binary one
+      if (w >= max_nodes) {  // cannot happen: the tree has at most n - 1 records
         atomicOr(err, kErrQueue);
+        for (int a = 0; a < 6; ++a) v[a][i] = kInf;
         ref[i] = kEmptyRef;
         cnt[i] = -1;
         continue;
@@ -425,68 +410,79 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
       cnt[i] = 0;
     }
   }
-  float4* o = wnodes + 8 * (size_t)item.y;
-  for (int a = 0; a < 6; ++a) o[a] = make_float4(v[a][0], v[a][1], v[a][2], v[a][3]);
-  o[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
-  o[7] = make_float4(__int_as_float(cnt[0]), __int_as_float(cnt[1]), __int_as_float(cnt[2]), __int_as_float(cnt[3]));
+  write_record(wnodes + 8 * (size_t)item.y, v, ref, cnt);
 }
 
-// Root record for scenes of 0 or 1 triangle (no interior node exists).
+// Root record of a scene with 0 or 1 triangle (no binary interior node exists).
 __global__ void k_small_root(int n, const float4* __restrict__ blo, const float4* __restrict__ bhi,
                              float4* __restrict__ nodes) {
-  float4 l = n == 1 ? blo[0] : make_float4(0, 0, 0, 0);
-  float4 h = n == 1 ? bhi[0] : make_float4(0, 0, 0, 0);
-  nodes[0] = make_float4(l.x, l.y, l.z, h.x);
-  nodes[1] = make_float4(h.y, h.z, 0.0f, 0.0f);
-  nodes[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  nodes[3] = make_float4(__int_as_float(pack_leaf(0, 1)), __int_as_float(-1), __int_as_float(n == 1 ? 1 : -1),
-                         __int_as_float(-1));
+  float v[6][4];
+  for (int a = 0; a < 6; ++a)
+    for (int i = 0; i < 4; ++i) v[a][i] = kInf;
+  int ref[4] = {kEmptyRef, kEmptyRef, kEmptyRef, kEmptyRef};
+  int cnt[4] = {-1, -1, -1, -1};
+  if (n == 1) {
+    const float4 l = blo[0], h = bhi[0];
+    v[0][0] = l.x; v[1][0] = l.y; v[2][0] = l.z;
+    v[3][0] = h.x; v[4][0] = h.y; v[5][0] = h.z;
+    ref[0] = pack_leaf(0, 1);
+    cnt[0] = 1;
+  }
+  write_record(nodes, v, ref, cnt);
 }
 
 inline int grid_for(size_t n, int block) { return (int)std::max<size_t>(1, (n + block - 1) / block); }
 
-// Converts the binary tree (node records already written) into the 4-wide layout.  The
-// traversal stack needs at most 3 entries per 4-wide level; when the 4-wide tree is deeper
-// than kStackMax / 3 levels the scene keeps the binary layout.
-eos_status build_wide(eos_ctx* ctx, eos_scene* sc, int n, const int2* child, const int2* range, const float4* blo,
-                      const float4* bhi) {
+// Writes the node records of the binary tree in the given width (top-down, one launch per
+// level).  Returns the number of levels through *levels (kStackMax * 4 + 1 when the walk
+// did not end, which cannot happen for a tree of depth <= kStackMax).
+eos_status write_records(eos_ctx* ctx, int n, const int2* child, const int2* range, const float4* blo,
+                         const float4* bhi, int width, float4* out, int max_nodes, int* levels, int* n_records) {
   cudaStream_t st = ctx->stream;
   eos_status es = EOS_OK;
-  const int max_nodes = n - 1;
   int2* fa = (int2*)scratch(ctx, "lbvh.wide.fa", 8 * (size_t)n, &es);
   int2* fb = (int2*)scratch(ctx, "lbvh.wide.fb", 8 * (size_t)n, &es);
   int* cnt = (int*)scratch(ctx, "lbvh.wide.cnt", 8, &es);
   if (es != EOS_OK) return es;
-  void* wide = nullptr;
-  EOS_CUDA(cudaMalloc(&wide, 128 * (size_t)max_nodes));
-  int h_init[2] = {1, 0};  // w_count, n_out
+  int h_init[2] = {1, 0};  // record count (the root is record 0), frontier size
   int2 root = make_int2(0, 0);
-  cudaError_t ce = cudaMemcpyAsync(cnt, h_init, sizeof h_init, cudaMemcpyHostToDevice, st);
-  if (ce == cudaSuccess) ce = cudaMemcpyAsync(fa, &root, sizeof root, cudaMemcpyHostToDevice, st);
-  int n_in = 1, levels = 0;
-  while (ce == cudaSuccess && n_in > 0) {
-    ce = cudaMemsetAsync(cnt + 1, 0, sizeof(int), st);
-    if (ce != cudaSuccess) break;
-    k_wide_level<<<grid_for(n_in, 128), 128, 0, st>>>(n, child, range, blo, bhi, fa, n_in, fb, cnt + 1, cnt,
-                                                       (float4*)wide, max_nodes, ctx->d_err);
-    ++levels;
-    ce = cudaMemcpyAsync(&n_in, cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  EOS_CUDA(cudaMemcpyAsync(cnt, h_init, sizeof h_init, cudaMemcpyHostToDevice, st));
+  EOS_CUDA(cudaMemcpyAsync(fa, &root, sizeof root, cudaMemcpyHostToDevice, st));
+  int n_in = 1, lv = 0;
+  while (n_in > 0 && lv <= 4 * kStackMax) {  // bounded: the depth is at most the binary depth
+    EOS_CUDA(cudaMemsetAsync(cnt + 1, 0, sizeof(int), st));
+    k_wide_level<<<grid_for(n_in, 128), 128, 0, st>>>(n, child, range, blo, bhi, fa, n_in, fb, cnt + 1, cnt, out,
+                                                       max_nodes, width, ctx->d_err);
+    ++lv;
+    EOS_CUDA(cudaMemcpyAsync(&n_in, cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EOS_CUDA(cudaStreamSynchronize(st));
     std::swap(fa, fb);
-    if (levels > 4 * kStackMax) break;  // bounded: depth <= the binary depth
   }
-  int w_count = 0;
-  if (ce == cudaSuccess) ce = cudaMemcpy(&w_count, cnt, sizeof(int), cudaMemcpyDeviceToHost);
-  if (ce != cudaSuccess || n_in > 0 || 3 * levels > kStackMax) {
-    cudaFree(wide);
+  EOS_CUDA(cudaMemcpy(n_records, cnt, sizeof(int), cudaMemcpyDeviceToHost));
+  *levels = n_in > 0 ? 4 * kStackMax + 1 : lv;
+  return EOS_OK;
+}
+
+// Node records of the scene.  The traversal stack holds at most width - 1 entries per
+// level, so a 4-wide tree deeper than kStackMax / 3 levels (degenerate geometry) is written
+// with two children per record instead; a binary tree's depth is at most 62 <= kStackMax.
+eos_status build_records(eos_ctx* ctx, eos_scene* sc, int n, const int2* child, const int2* range,
+                         const float4* blo, const float4* bhi) {
+  const int max_nodes = n - 1;
+  EOS_CUDA(cudaMalloc(&sc->d_nodes, 128 * (size_t)max_nodes));
+  sc->device_bytes += 128 * (size_t)max_nodes;
+  int levels = 0, records = 0;
+  eos_status es = write_records(ctx, n, child, range, blo, bhi, sc->width, (float4*)sc->d_nodes, max_nodes, &levels,
+                                &records);
+  if (es != EOS_OK) return es;
+  if (sc->width == 4 && 3 * levels > kStackMax) {
     sc->width = 2;
-    return ce == cudaSuccess ? EOS_OK : EOS_ERR_CUDA;
+    es = write_records(ctx, n, child, range, blo, bhi, 2, (float4*)sc->d_nodes, max_nodes, &levels, &records);
+    if (es != EOS_OK) return es;
   }
-  cudaFree(sc->d_nodes);
-  sc->d_nodes = wide;
-  sc->device_bytes += 128 * (size_t)max_nodes - 64 * (size_t)sc->n_nodes;
-  sc->n_nodes = (uint32_t)w_count;
-  sc->wide_levels = levels;
+  if ((sc->width - 1) * levels > kStackMax) return EOS_ERR_STACK_OVERFLOW;
+  sc->n_nodes = (uint32_t)records;
+  sc->levels = levels;
   return EOS_OK;
 }
 
@@ -499,15 +495,13 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
   const size_t nn = std::max<size_t>(1, n);
   eos_status es = EOS_OK;
   const size_t n_nodes = std::max<size_t>(1, nn - 1);
-  // persistent scene buffers
-  EOS_CUDA(cudaMalloc(&sc->d_nodes, 64 * n_nodes));
+  // persistent scene buffers (node records: build_records, or one root record below)
   EOS_CUDA(cudaMalloc(&sc->d_tris, 48 * nn));
   EOS_CUDA(cudaMalloc(&sc->d_shade, 48 * nn));
   EOS_CUDA(cudaMalloc(&sc->d_pos_of_id, 4 * nn));
   EOS_CUDA(cudaMalloc(&sc->d_codes, 4 * nn));
   EOS_CUDA(cudaMalloc(&sc->d_order, 4 * nn));
-  sc->device_bytes += 64 * n_nodes + 48 * nn * 2 + 4 * nn * 3;
-  sc->n_nodes = (uint32_t)n_nodes;
+  sc->device_bytes += 48 * nn * 2 + 4 * nn * 3;
   // temporaries
   float4* cent = (float4*)scratch(ctx, "lbvh.cent", 16 * nn, &es);
   uint32_t* bounds = (uint32_t*)scratch(ctx, "lbvh.bounds", 64, &es);
@@ -551,18 +545,18 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
     EOS_CUDA(cudaMemsetAsync(parent, 0xff, 4 * (2 * nn), st));
     EOS_CUDA(cudaMemsetAsync(arrive, 0, 4 * n_nodes, st));
     k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys, n, child, range, parent);
-    k_refit<<<grid_for(nn, 256), 256, 0, st>>>(n, child, range, parent, blo, bhi, arrive,
-                                              (float4*)sc->d_nodes, sc->leaf_size, sc->layout == EOS_LAYOUT_SAH,
-                                              ctx->d_err);
+    k_refit<<<grid_for(nn, 256), 256, 0, st>>>(n, child, range, parent, blo, bhi, arrive, sc->leaf_size,
+                                              sc->layout == EOS_LAYOUT_SAH, ctx->d_err);
     // SAH cost of the tree (subtree cost of the root, in triangle-test units)
     EOS_CUDA(cudaMemcpyAsync(&sc->sah_cost, &blo[0].w, sizeof(float), cudaMemcpyDeviceToHost, st));
-    if (sc->width == 4) {
-      eos_status ws = build_wide(ctx, sc, n, child, range, blo, bhi);
-      if (ws != EOS_OK) return ws;
-    }
+    eos_status ws = build_records(ctx, sc, n, child, range, blo, bhi);
+    if (ws != EOS_OK) return ws;
   } else {
+    EOS_CUDA(cudaMalloc(&sc->d_nodes, 128));
+    sc->device_bytes += 128;
     k_small_root<<<1, 1, 0, st>>>(n, blo, bhi, (float4*)sc->d_nodes);
-    sc->width = 2;
+    sc->n_nodes = 1;
+    sc->levels = 1;
   }
   EOS_CUDA(cudaGetLastError());
   EOS_CUDA(cudaEventRecord(ctx->ev1, st));

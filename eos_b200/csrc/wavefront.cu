@@ -117,7 +117,7 @@ __device__ __forceinline__ int grab(int* ctr, int qchunk) {
 }
 
 template <bool PRIMARY, int SH>
-__global__ void k_wf_closest(WfArgs A) {
+__global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;
@@ -317,9 +317,25 @@ __device__ __forceinline__ void emit_results(const WfArgs& A, int* ctr, bool pen
   }
 }
 
+// Warp-level pool of queue entries for the refill kernels: when the pool is empty, lane 0
+// takes the next `chunk` entries with one atomic.  Returns true when the pool holds
+// entries.  pool, pool_end and more stay warp-uniform.
+__device__ __forceinline__ bool refill_pool(int* counter, int chunk, int n, int lane, int& pool, int& pool_end,
+                                            bool& more) {
+  if (pool >= pool_end && more) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(counter, chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    pool = base;
+    pool_end = min(base + chunk, n);
+    if (pool_end >= n) more = false;
+  }
+  return pool < pool_end;
+}
+
 // Nearest-hit stage with lane refill: each iteration (1) emits the results of lanes whose
-// ray ended, (2) gives idle lanes new rays from the queue (one atomic per warp for all of
-// them), (3) advances every active lane by one traversal step.
+// ray ended, (2) gives idle lanes new rays from the warp's pool of queue entries (refilled
+// `queue_chunk` entries at a time), (3) advances every active lane by one traversal step.
 template <bool PRIMARY, int SH>
 __global__ void k_wf_closest_refill(WfArgs A) {
   extern __shared__ uint2 shstack[];
@@ -327,12 +343,13 @@ __global__ void k_wf_closest_refill(WfArgs A) {
   const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // mirror rays of bounce k-1
   const int lane = threadIdx.x & 31;
   RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
-  TravScene ts{nullptr, nullptr, 2};
+  TravScene ts{nullptr, nullptr};
   Hit h;
   h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
   int i = -1, path = -1, jb = 0;
   bool pending = false;
-  bool more = true;  // warp-uniform: the queue still has rays
+  bool more = true;              // warp-uniform: the queue may still have rays
+  int pool = 0, pool_end = 0;    // warp-uniform: queue entries taken by this warp, not yet started
   unsigned nrays = 0, nshadow = 0, nhits = 0;
   unsigned long long nodes = 0, tests = 0;
   for (;;) {
@@ -346,51 +363,46 @@ __global__ void k_wf_closest_refill(WfArgs A) {
       }
     }
     const uint32_t idle = __ballot_sync(0xffffffffu, i < 0);
-    if (idle && more) {
-      const int want = __popc(idle);
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&ctr[3], want);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (base + want >= n_in) more = false;
-      if (i < 0) {
-        const int k = base + __popc(idle & lanemask_lt());
-        if (k < n_in) {
-          f3 o, d;
-          bool ok = true;
-          if (PRIMARY) {
-            long long gp = A.c0 + k;
-            jb = find_job(A.jobs, A.n_jobs, gp);
-            const DevJob& J = A.jobs[jb];
-            int x, y, smp;
-            ok = path_pixel(J, gp - J.path_off, x, y, smp);
-            if (ok) {
-              float ox, oy;
-              sample_offset((uint32_t)(y * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
-              d = primary_direction(J.cam, J.w, J.h, x, y, ox, oy);
-              o = mk3(J.cam[0], J.cam[1], J.cam[2]);
-              path = k;
-            }
-          } else {
-            RayQ r = A.rin[k];
-            o = mk3(r.a.x, r.a.y, r.a.z);
-            d = mk3(r.b.x, r.b.y, r.b.z);
-            path = __float_as_int(r.a.w);
-            jb = find_job(A.jobs, A.n_jobs, A.c0 + path);
-          }
+    if (idle && refill_pool(&ctr[3], A.qchunk, n_in, lane, pool, pool_end, more)) {
+      const int rank = __popc(idle & lanemask_lt());
+      const int avail = pool_end - pool;
+      const int k = pool + rank;
+      pool += min(__popc(idle), avail);
+      if (i < 0 && rank < avail) {
+        f3 o, d;
+        bool ok = true;
+        if (PRIMARY) {
+          long long gp = A.c0 + k;
+          jb = find_job(A.jobs, A.n_jobs, gp);
+          const DevJob& J = A.jobs[jb];
+          int x, y, smp;
+          ok = path_pixel(J, gp - J.path_off, x, y, smp);
           if (ok) {
-            i = k;
-            ++nrays;
-            ts.nodes = A.jobs[jb].s.nodes;
-            ts.tris = A.jobs[jb].s.tris;
-            ts.width = A.jobs[jb].s.width;
-            T.start(o, d);
-            h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
+            float ox, oy;
+            sample_offset((uint32_t)(y * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
+            d = primary_direction(J.cam, J.w, J.h, x, y, ox, oy);
+            o = mk3(J.cam[0], J.cam[1], J.cam[2]);
+            path = k;
           }
+        } else {
+          RayQ r = A.rin[k];
+          o = mk3(r.a.x, r.a.y, r.a.z);
+          d = mk3(r.b.x, r.b.y, r.b.z);
+          path = __float_as_int(r.a.w);
+          jb = find_job(A.jobs, A.n_jobs, A.c0 + path);
+        }
+        if (ok) {
+          i = k;
+          ++nrays;
+          ts.nodes = A.jobs[jb].s.nodes;
+          ts.tris = A.jobs[jb].s.tris;
+          T.start(o, d);
+          h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
         }
       }
     }
     if (__ballot_sync(0xffffffffu, i >= 0) == 0) {
-      if (!more) break;
+      if (!more && pool >= pool_end) break;
       continue;
     }
     if (i >= 0) {
@@ -413,36 +425,32 @@ __global__ void k_wf_any_refill(WfArgs A) {
   const int n = min(ctr[2], A.cap_s);
   const int lane = threadIdx.x & 31;
   RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
-  TravScene ts{nullptr, nullptr, 2};
+  TravScene ts{nullptr, nullptr};
   int i = -1, hi = 0, key = 0;
   bool more = true;
+  int pool = 0, pool_end = 0;
   unsigned nn = 0, nt = 0;
   unsigned long long nodes = 0, tests = 0;
   for (;;) {
     const uint32_t idle = __ballot_sync(0xffffffffu, i < 0);
-    if (idle && more) {
-      const int want = __popc(idle);
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&ctr[4], want);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (base + want >= n) more = false;
-      if (i < 0) {
-        const int k = base + __popc(idle & lanemask_lt());
-        if (k < n) {
-          ShadowQ s = A.sq[k];
-          i = k;
-          hi = __float_as_int(s.a.w);
-          key = __float_as_int(s.b.w);
-          const DevScene& S = A.jobs[key >> 5].s;
-          ts.nodes = S.nodes;
-          ts.tris = S.tris;
-          ts.width = S.width;
-          T.start(mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z));
-        }
+    if (idle && refill_pool(&ctr[4], A.qchunk, n, lane, pool, pool_end, more)) {
+      const int rank = __popc(idle & lanemask_lt());
+      const int avail = pool_end - pool;
+      const int k = pool + rank;
+      pool += min(__popc(idle), avail);
+      if (i < 0 && rank < avail) {
+        ShadowQ s = A.sq[k];
+        i = k;
+        hi = __float_as_int(s.a.w);
+        key = __float_as_int(s.b.w);
+        const DevScene& S = A.jobs[key >> 5].s;
+        ts.nodes = S.nodes;
+        ts.tris = S.tris;
+        T.start(mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z));
       }
     }
     if (__ballot_sync(0xffffffffu, i >= 0) == 0) {
-      if (!more) break;
+      if (!more && pool >= pool_end) break;
       continue;
     }
     if (i >= 0) {
@@ -461,7 +469,7 @@ __global__ void k_wf_any_refill(WfArgs A) {
 }
 
 template <int SH>
-__global__ void k_wf_any(WfArgs A) {
+__global__ void __launch_bounds__(256, 4) k_wf_any(WfArgs A) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;

@@ -133,7 +133,7 @@ enum {
 typedef struct eos_build_params {
   int32_t leaf_size;    /* largest leaf, 1..32 triangles; 0 = tuned value, else 8 */
   int32_t layout;       /* EOS_LAYOUT_* */
-  int32_t width;        /* node width: 2 (64-B binary nodes) or 4 (128-B 4-child nodes);
+  int32_t width;        /* children per 128-B node record: 4, or 2 (binary tree);
                            0 = tuned value, else 4 */
 } eos_build_params;
 
