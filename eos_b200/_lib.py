@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import (POINTER, Structure, c_char_p, c_float, c_int32, c_uint8, c_uint32, c_uint64,
+from ctypes import (POINTER, Structure, c_char_p, c_float, c_int32, c_size_t, c_uint8, c_uint32, c_uint64,
                     c_void_p)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -22,7 +22,8 @@ MODE_WAVEFRONT = 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error",
           4: "device loop ran out of iterations", 5: "traversal stack overflow",
-          6: "ray queue overflow", 7: "unsupported", 8: "no CUDA device"}
+          6: "ray queue overflow", 7: "unsupported", 8: "no CUDA device", 9: "file could not be read",
+          10: "malformed input file"}
 
 
 class EosError(RuntimeError):
@@ -77,6 +78,11 @@ class Stats(Structure):
                 ("kernel_launches", c_uint32), ("stage_ms", c_float * 3)]
 
 
+class MeshInfo(Structure):
+    _fields_ = [("n_verts", c_uint32), ("n_tris", c_uint32), ("normals_from_file", c_uint32), ("n_faces", c_uint32),
+                ("bounds", c_float * 6)]
+
+
 class SceneInfo(Structure):
     _fields_ = [("n_tris", c_uint32), ("n_nodes", c_uint32), ("leaf_size", c_uint32), ("layout", c_uint32),
                 ("width", c_uint32), ("sah_cost", c_float), ("n_objects", c_uint32), ("n_lights", c_uint32),
@@ -119,6 +125,11 @@ SIGNATURES = [
     ("eos_trace_any", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
     ("eos_render_noalloc", c_int32, [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
                                      c_void_p, POINTER(Stats)]),
+    ("eos_mesh_load_obj", c_int32, [c_char_p, POINTER(c_void_p)]),
+    ("eos_mesh_parse_obj", c_int32, [c_char_p, c_size_t, POINTER(c_void_p)]),
+    ("eos_mesh_get_info", c_int32, [c_void_p, POINTER(MeshInfo)]),
+    ("eos_mesh_get_data", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("eos_mesh_destroy", c_int32, [c_void_p]),
 ]
 
 NOALLOC_MAX_PATHS = 16384

@@ -205,7 +205,8 @@ def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",)):
 
 
 def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning) -> dict:
-    """All jobs through one wavefront pass (graph-captured); outputs are device tensors."""
+    """All jobs through one wavefront pass (graph-captured); outputs are device tensors or host
+    arrays (host outputs are filled when the call returns)."""
     arr = (L.Job * len(jobs))()
     for i, (j, o) in enumerate(zip(jobs, outs)):
         arr[i].scene = j.scene.h

@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libeos_b200.so")
-SOURCES = ["api.cu", "lbvh.cu", "render.cu", "wavefront.cu", "adjoint.cu"]
+SOURCES = ["api.cu", "lbvh.cu", "render.cu", "wavefront.cu", "adjoint.cu", "mesh.cpp"]
 HEADERS = ["eos_math.cuh", "eos_internal.cuh", "trace.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -34,7 +34,7 @@ def nvcc() -> str:
 
 
 def _flags(verbose_ptxas: bool) -> list[str]:
-    f = ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
+    f = ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
                 "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
     if verbose_ptxas:
         f += ["-Xptxas", "-v"]
@@ -52,7 +52,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     objs, jobs = [], []
     for s in SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(OUT_DIR, s.replace(".cu", ".o"))
+        obj = os.path.join(OUT_DIR, os.path.splitext(s)[0] + ".o")
         objs.append(obj)
         if force or verbose_ptxas or _mtime(obj) < max(_mtime(src), newest_dep):
             jobs.append([nvcc(), "-c", src, "-o", obj] + _flags(verbose_ptxas))

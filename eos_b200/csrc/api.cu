@@ -3,6 +3,8 @@
 // wavefront.cu and adjoint.cu.
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
+#include <vector>
 
 #include "eos_internal.cuh"
 
@@ -190,6 +192,8 @@ const char* eos_status_string(eos_status s) {
     case EOS_ERR_QUEUE_OVERFLOW: return "ray queue overflow";
     case EOS_ERR_UNSUPPORTED: return "unsupported";
     case EOS_ERR_NO_DEVICE: return "no CUDA device";
+    case EOS_ERR_IO: return "file could not be read";
+    case EOS_ERR_PARSE: return "malformed input file";
   }
   return "unknown status";
 }
@@ -439,18 +443,52 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     if (!jb.scene || !valid_camera(&jb.camera) || jb.trace_depth < 0 || jb.trace_depth >= EOS_MAX_BOUNCES ||
         jb.spp < 1 || jb.spp > 1024)
       return EOS_ERR_INVALID_ARG;
-    if ((jb.rgb_out && !is_device_ptr(jb.rgb_out)) || (jb.rgba8_out && !is_device_ptr(jb.rgba8_out)) ||
-        (jb.paths_out && !is_device_ptr(jb.paths_out)))
-      return EOS_ERR_INVALID_ARG;
   }
   if ((st = set_device(ctx)) != EOS_OK) return st;
+  // host output buffers are staged through one device buffer and copied back at the end
+  struct HostOut {
+    void* user;
+    size_t off, bytes;
+  };
+  std::vector<HostOut> host_outs;
+  std::vector<eos_job> dj(jobs, jobs + n_jobs);
+  size_t staged = 0;
+  auto plan = [&](void* user, size_t bytes) {
+    if (!user || is_device_ptr(user)) return;
+    host_outs.push_back({user, staged, bytes});
+    staged += (bytes + 255) & ~size_t(255);
+  };
+  for (const eos_job& jb : dj) {
+    const size_t npx = (size_t)jb.camera.width * jb.camera.height;
+    plan(jb.rgb_out, 12 * npx);
+    plan(jb.rgba8_out, 4 * npx);
+    plan(jb.paths_out, sizeof(eos_path_record) * npx * jb.spp);
+  }
+  char* stage = nullptr;
+  if (staged) {
+    stage = (char*)scratch(ctx, "batch.host_out", staged, &st);
+    if (st != EOS_OK) return st;
+    size_t k = 0;
+    auto swap_in = [&](auto*& ptr) {
+      if (k < host_outs.size() && ptr && (void*)ptr == host_outs[k].user)
+        ptr = reinterpret_cast<std::remove_reference_t<decltype(ptr)>>(stage + host_outs[k++].off);
+    };
+    for (eos_job& jb : dj) {
+      swap_in(jb.rgb_out);
+      swap_in(jb.rgba8_out);
+      swap_in(jb.paths_out);
+    }
+  }
   if ((st = begin_call(ctx)) != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   uint32_t largest = 0;
   for (uint32_t j = 0; j < n_jobs; ++j) largest = std::max(largest, (uint32_t)jobs[j].scene->dev.n_tris);
-  st = render_wavefront(ctx, jobs, n_jobs, with_tuning(ctx, *p, largest), (p->flags & EOS_FLAG_STAGE_TIMING) == 0);
+  st = render_wavefront(ctx, dj.data(), n_jobs, with_tuning(ctx, *p, largest),
+                        (p->flags & EOS_FLAG_STAGE_TIMING) == 0);
   if (st != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  for (const HostOut& h : host_outs)
+    EOS_CUDA(cudaMemcpyAsync(h.user, stage + h.off, h.bytes, cudaMemcpyDeviceToHost, ctx->stream));
   st = end_call(ctx, stats);
   if (stats) cudaEventElapsedTime(&stats->gpu_ms, ctx->ev0, ctx->ev1);
   return st;

@@ -3,6 +3,7 @@
 // Mirrors the classes a caller of the reference uses to render a frame:
 //   Material, LightSource, Triangle (Surface), Scene   src/Material.h, src/LightSource.h,
 //                                                      src/Triangle.h, src/Scene.h
+//   TriangleMesh (OBJ files)                            src/triangleMesh.h
 //   Camera                                              src/Camera.h
 //   createCudaScene / cudaScene_t                       src/cudaStructures.h:86-98
 //   DeviceCameraHandler                                 src/DeviceCameraHandler.h
@@ -80,6 +81,7 @@ struct mat4 {
       for (int r = 0; r < 4; ++r) o.m[c][r] = g[c][r];
     return o;
   }
+  static mat4 from(const mat4& g) { return g; }
   bool identity() const {
     for (int c = 0; c < 4; ++c)
       for (int r = 0; r < 4; ++r)
@@ -205,6 +207,65 @@ class Triangle : public Surface {
   int m_TransformationIndex = 0;
 };
 
+// src/triangleMesh.h:30-75.  loadFromFile reads a Wavefront OBJ through eos_mesh_load_obj
+// (triangulation, smooth normals when the file has none, identical vertices joined; see
+// eos_c.h) and makes one Triangle per face with the mesh's transformation, material,
+// material index and transformation index at the time of the call, as the reference does
+// (src/triangleMesh.cpp:79-160).  All faces of the file are loaded (the reference keeps
+// assimp's first mesh).
+class TriangleMesh {
+ public:
+  bool loadFromFile(const char* filename) {
+    eos_mesh* m = nullptr;
+    if (eos_mesh_load_obj(filename, &m) != EOS_OK) return false;
+    eos_mesh_info info;
+    eos_mesh_get_info(m, &info);
+    std::vector<float> v(3 * (size_t)info.n_verts), n(3 * (size_t)info.n_verts);
+    std::vector<uint32_t> t(3 * (size_t)info.n_tris);
+    eos_mesh_get_data(m, v.data(), n.data(), t.data());
+    eos_mesh_destroy(m);
+    auto V = [](const std::vector<float>& a, uint32_t i) { return vec3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); };
+    m_Triangles.clear();
+    for (uint32_t f = 0; f < info.n_tris; ++f) {
+      const uint32_t* k = &t[3 * (size_t)f];
+      m_Triangles.emplace_back(new Triangle(V(v, k[0]), V(v, k[1]), V(v, k[2]), V(n, k[0]), V(n, k[1]), V(n, k[2])));
+      Triangle* tri = m_Triangles.back().get();
+      tri->setTransformation(m_M);
+      if (m_Material) tri->setMaterial(*m_Material);
+      tri->setMaterialIndex(m_MaterialIndex);
+      tri->setTransformationIndex(m_TransformationIndex);
+    }
+    m_Valid = true;
+    return true;
+  }
+  const mat4& transformation() const { return m_M; }
+  void setTransformation(const mat4& M) { m_M = M; }
+  template <class M>
+  void setTransformation(M& g) { m_M = mat4::from(g); }
+  Material& getMaterial() { return m_OwnMaterial; }
+  void setMaterial(const Material& m) {
+    m_OwnMaterial = m;
+    m_Material = &m_OwnMaterial;
+  }
+  unsigned int getNumTriangles() const { return (unsigned int)m_Triangles.size(); }
+  Triangle* getTriangle(int i) { return m_Valid && i >= 0 && i < (int)m_Triangles.size() ? m_Triangles[i].get() : nullptr; }
+  void setSceneStartIndex(int s) { m_SceneIndexStart = s; }
+  void setSceneEndIndex(int e) { m_SceneIndexEnd = e; }
+  void setMaterialIndex(int i) { m_MaterialIndex = i; }
+  int getMaterialIndex(int) const { return m_MaterialIndex; }
+  void setTransformationIndex(int i) { m_TransformationIndex = i; }
+  int getTransformationIndex() const { return m_TransformationIndex; }
+
+ private:
+  std::vector<std::unique_ptr<Triangle>> m_Triangles;
+  mat4 m_M;
+  Material m_OwnMaterial;
+  Material* m_Material = nullptr;
+  int m_MaterialIndex = 0, m_TransformationIndex = 0;
+  int m_SceneIndexStart = 0, m_SceneIndexEnd = 0;
+  bool m_Valid = false;
+};
+
 // src/Camera.h:30-64
 class Camera {
  public:
@@ -261,6 +322,19 @@ class Scene {
     Triangle* t = dynamic_cast<Triangle*>(s);
     if (!t) return false;  // triangles only (src/cudaStructures.cu:342-348)
     m_Surfaces.push_back(t);
+    return true;
+  }
+  // src/Scene.cpp:55-75: appends the mesh's triangles and records their index range.
+  bool addTriangleMesh(TriangleMesh* mesh) {
+    if (!mesh) return false;
+    const int start = getNumSurfaces();
+    for (unsigned int i = 0; i < mesh->getNumTriangles(); ++i) {
+      Triangle* t = mesh->getTriangle((int)i);
+      if (!t) return false;
+      m_Surfaces.push_back(t);
+    }
+    mesh->setSceneStartIndex(start);
+    mesh->setSceneEndIndex(getNumSurfaces() - start);
     return true;
   }
   bool addLightSource(LightSource* l) {

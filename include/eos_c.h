@@ -25,6 +25,7 @@
  *   eos_render_backward          (no reference counterpart: adjoint of the shading)
  *   eos_trace_closest / any      Scene::findMinDistanceIntersectionBVH /
  *                                shadowRayVisibilityBVH (src/Scene.cpp:145-158)
+ *   eos_mesh_load_obj            TriangleMesh::loadFromFile (src/triangleMesh.cpp:79-160)
  *
  * Buffers are owned by the caller.  A pointer argument may be host or device memory; the
  * library tells them apart with cudaPointerGetAttributes and stages host buffers through
@@ -55,7 +56,9 @@ typedef enum eos_status {
   EOS_ERR_STACK_OVERFLOW = 5, /* traversal stack exhausted (tree deeper than supported) */
   EOS_ERR_QUEUE_OVERFLOW = 6,
   EOS_ERR_UNSUPPORTED = 7,
-  EOS_ERR_NO_DEVICE = 8
+  EOS_ERR_NO_DEVICE = 8,
+  EOS_ERR_IO = 9,             /* a file could not be read */
+  EOS_ERR_PARSE = 10          /* malformed input file */
 } eos_status;
 
 typedef struct eos_ctx eos_ctx;
@@ -181,9 +184,9 @@ typedef struct eos_job {
   float pixel_offset;
   int32_t spp;
   uint32_t jitter_seed;
-  float* rgb_out;              /* [H*W*3] device, nullable */
-  uint8_t* rgba8_out;          /* [H*W*4] device, nullable */
-  eos_path_record* paths_out;  /* [H*W*spp] device, nullable */
+  float* rgb_out;              /* [H*W*3], nullable */
+  uint8_t* rgba8_out;          /* [H*W*4], nullable */
+  eos_path_record* paths_out;  /* [H*W*spp], nullable */
 } eos_job;
 
 /* Gradients of an image loss L; d_rgb = dL/drgb per pixel. */
@@ -227,7 +230,9 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* scene, const eos_camera* ca
                       int32_t* hit_out, eos_path_record* paths_out, eos_stats* stats);
 
 /* Many views of one or several resident scenes through one wavefront pass (persistent
- * kernels over a global ray queue, replayed as a CUDA graph when the batch repeats). */
+ * kernels over a global ray queue, replayed as a CUDA graph when the batch repeats).
+ * Output buffers may be device or host memory; host buffers (pinned ones copy fastest)
+ * are filled before the call returns. */
 eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs,
                             const eos_render_params* params, eos_stats* stats);
 
@@ -244,6 +249,33 @@ eos_status eos_trace_closest(eos_ctx* ctx, const eos_scene* scene, const float* 
                              int32_t* ids, float* t);
 eos_status eos_trace_any(eos_ctx* ctx, const eos_scene* scene, const float* rays, uint32_t n,
                          uint8_t* occluded);
+
+/* ---------------------------------------------------------------------------- meshes */
+/* A triangle mesh read from a Wavefront OBJ file on the host; replaces
+ * TriangleMesh::loadFromFile (src/triangleMesh.cpp:79-160), which imports through assimp
+ * with aiProcess_Triangulate | aiProcess_GenSmoothNormals | aiProcess_JoinIdenticalVertices.
+ * The same three steps are applied: polygons triangulated (a quad from its concave corner),
+ * the file's vertex normals used when every face corner names one, otherwise smooth
+ * normals generated (normalised sum of the unit face normals of all corners within
+ * 1e-4 x the bounding-box diagonal), identical vertices joined.  Unlike the reference,
+ * which keeps assimp's first mesh only, all faces of the file are loaded.  The arrays feed
+ * eos_scene_create directly (verts, normals, tris). */
+typedef struct eos_mesh eos_mesh;
+typedef struct eos_mesh_info {
+  uint32_t n_verts;
+  uint32_t n_tris;
+  uint32_t normals_from_file; /* 1: 'vn' normals of the file, 0: generated smooth normals */
+  uint32_t n_faces;           /* 'f' statements read (before triangulation) */
+  float bounds[6];            /* min xyz, max xyz of the triangles' vertices */
+} eos_mesh_info;
+eos_status eos_mesh_load_obj(const char* path, eos_mesh** out);
+/* The same from OBJ text in memory (len bytes, need not be NUL-terminated). */
+eos_status eos_mesh_parse_obj(const char* text, size_t len, eos_mesh** out);
+eos_status eos_mesh_get_info(const eos_mesh* mesh, eos_mesh_info* info);
+/* Host arrays: verts / normals [n_verts*3] float, tris [n_tris*3] vertex indices; any may
+ * be NULL. */
+eos_status eos_mesh_get_data(const eos_mesh* mesh, float* verts, float* normals, uint32_t* tris);
+eos_status eos_mesh_destroy(eos_mesh* mesh);
 
 /* ---------------------------------------------------------------------------- no-alloc */
 /* Renders one view without allocating any device memory.  No counterpart in the

@@ -143,6 +143,13 @@ def test_batch_matches_single_renders(ctx):
             assert np.array_equal(o["rgb"].cpu().numpy(), ref["rgb"])
             assert np.array_equal(o["paths"].cpu().numpy(), ref["paths"])
         assert st["primary_rays"] == sum(j.camera.width * j.camera.height * j.spp for j in jobs)
+    # host output buffers (pageable numpy and pinned torch) are filled by the call itself
+    host = [{"rgb": np.zeros_like(o["rgb"].cpu().numpy()),
+             "paths": torch.zeros(o["paths"].shape, dtype=torch.int32).pin_memory()} for o in outs]
+    api.render_batch(ctx, jobs, host)
+    for o, h in zip(outs, host):
+        assert np.array_equal(h["rgb"], o["rgb"].cpu().numpy())
+        assert np.array_equal(h["paths"].numpy(), o["paths"].cpu().numpy())
 
 
 def _random_rays(n, seed, lo=-3, hi=3):
