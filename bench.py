@@ -457,7 +457,8 @@ def run_ours(args, rank, world, local):
         "clocks": clocks,
         "lbvh_build_ms": round(info["build_ms"], 3),
         "bvh": {"layout": {1: "sah", 2: "fixed"}.get(info["layout"], "?"), "leaf_size": info["leaf_size"],
-                "sah_cost": round(info["sah_cost"], 2)},
+                "sah_cost": round(info["sah_cost"], 2), "width": info["width"], "node_records": info["n_nodes"],
+                "scene_device_mb": round(info["device_bytes"] / 1e6, 1)},
         "traversal_per_ray": {
             "nearest_nodes": round(st["nodes_closest"] / max(1, st["primary_rays"] + st["secondary_rays"]), 2),
             "nearest_tests": round(st["tests_closest"] / max(1, st["primary_rays"] + st["secondary_rays"]), 2),

@@ -57,14 +57,15 @@ FLAG_REFILL = 2
 
 class Tuning(Structure):
     _fields_ = [("block_size", c_int32), ("queue_chunk", c_int32), ("stack_depth", c_int32), ("leaf_size", c_int32),
-                ("layout", c_int32), ("width", c_int32)]
+                ("layout", c_int32), ("width", c_int32), ("builder", c_int32)]
 
 
 LAYOUT_DEFAULT, LAYOUT_SAH, LAYOUT_FIXED = 0, 1, 2
+BUILDER_DEFAULT, BUILDER_LBVH, BUILDER_PLOC = 0, 1, 2
 
 
 class BuildParams(Structure):
-    _fields_ = [("leaf_size", c_int32), ("layout", c_int32), ("width", c_int32)]
+    _fields_ = [("leaf_size", c_int32), ("layout", c_int32), ("width", c_int32), ("builder", c_int32)]
 
 
 class PathRecord(Structure):
@@ -86,7 +87,7 @@ class MeshInfo(Structure):
 class SceneInfo(Structure):
     _fields_ = [("n_tris", c_uint32), ("n_nodes", c_uint32), ("leaf_size", c_uint32), ("layout", c_uint32),
                 ("width", c_uint32), ("sah_cost", c_float), ("n_objects", c_uint32), ("n_lights", c_uint32),
-                ("build_ms", c_float), ("device_bytes", c_uint64)]
+                ("build_ms", c_float), ("device_bytes", c_uint64), ("builder", c_uint32), ("depth", c_uint32)]
 
 
 class Job(Structure):

@@ -91,9 +91,9 @@ class DeviceScene:
     """A scene resident in HBM with its LBVH (eos_scene_create)."""
 
     def __init__(self, ctx: Context, scene: SceneData, leaf_size: int = 0, inputs_on_device: bool = False,
-                 layout: str | int = 0, width: int = 0):
-        """leaf_size / layout / width 0 take the context's tuned values for this scene size
-        (4-wide nodes, SAH collapse with leaves of up to 8 triangles without a table)."""
+                 layout: str | int = 0, width: int = 0, builder: str | int = 0):
+        """leaf_size / layout / width / builder 0 take the context's tuned values for this scene
+        size (without a table: PLOC hierarchy, 4-wide nodes, SAH collapse, leaves of <= 8)."""
         self.ctx = ctx
         self.scene = scene
         self.lib = ctx.lib
@@ -101,6 +101,7 @@ class DeviceScene:
         bp.leaf_size = leaf_size
         bp.layout = {"sah": L.LAYOUT_SAH, "fixed": L.LAYOUT_FIXED}.get(layout, layout) if layout else 0
         bp.width = int(width)
+        bp.builder = {"lbvh": L.BUILDER_LBVH, "ploc": L.BUILDER_PLOC}.get(builder, builder) if builder else 0
         arrs = [scene.verts, scene.normals, scene.tris, scene.tri_obj]
         if inputs_on_device:
             import torch

@@ -1,11 +1,11 @@
-"""Autotuner: block size, queue chunk, stack depth and node layout (leaf size) per
-scene-size bucket for the batched wavefront renderer.
+"""Autotuner: hierarchy builder, node width / layout / leaf size, block size, queue chunk
+and stack depth per scene-size bucket for the batched wavefront renderer.
 
 For each bucket (triangle count rounded down to a power of two) the tuner renders a
-representative job with coordinate descent over the candidate values: leaf size first
-(it changes the LBVH, so the scene is rebuilt), then block size, shared stack depth and
-queue chunk, keeping a value only when it is faster by more than the noise margin.  The
-table is saved as JSON and registered with the library (eos_ctx_set_tuning), so render
+representative job with coordinate descent over the candidate values: the tree parameters
+first (builder, width, layout, leaf size: each change rebuilds the scene), then block size,
+shared stack depth and queue chunk, keeping a value only when it is faster by more than the
+noise margin.  The table is saved as JSON and registered with the library (eos_ctx_set_tuning), so render
 calls that leave a parameter at 0 use the tuned value for their scene's bucket.
 """
 from __future__ import annotations
@@ -20,6 +20,7 @@ from . import _lib as L
 from . import api
 
 CANDIDATES = {
+    "builder": ["ploc", "lbvh"],
     "width": [2, 4],
     "layout": ["sah", "fixed"],
     "leaf_size": [2, 4, 8, 16],
@@ -27,8 +28,10 @@ CANDIDATES = {
     "stack_depth": [8, 16, 32],
     "queue_chunk": [32, 64, 128],
 }
-DEFAULT = {"width": 4, "layout": "fixed", "leaf_size": 4, "block_size": 128, "stack_depth": 16, "queue_chunk": 32}
+DEFAULT = {"builder": "ploc", "width": 4, "layout": "fixed", "leaf_size": 4, "block_size": 128, "stack_depth": 16,
+           "queue_chunk": 32}
 LAYOUT_CODE = {"sah": L.LAYOUT_SAH, "fixed": L.LAYOUT_FIXED}
+BUILDER_CODE = {"lbvh": L.BUILDER_LBVH, "ploc": L.BUILDER_PLOC}
 
 
 def bucket_of(n_tris: int) -> int:
@@ -57,15 +60,15 @@ def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log
     best = dict(DEFAULT)
     scenes_by_leaf = {}
 
-    def scene_for(width, layout, leaf):
-        key = (width, layout, leaf)
+    def scene_for(builder, width, layout, leaf):
+        key = (builder, width, layout, leaf)
         if key not in scenes_by_leaf:
             scenes_by_leaf[key] = api.DeviceScene(ctx, scene_data, leaf_size=leaf, inputs_on_device=True,
-                                                  layout=layout, width=width)
+                                                  layout=layout, width=width, builder=builder)
         return scenes_by_leaf[key]
 
     def measure(setting):
-        dsc = scene_for(setting["width"], setting["layout"], setting["leaf_size"])
+        dsc = scene_for(setting["builder"], setting["width"], setting["layout"], setting["leaf_size"])
         jobs = [api.BatchJob(dsc, c, trace_depth, 0.5) for c in cameras]
         outs = api.make_batch_outputs(jobs, ("rgba8",))
         p = {k: setting[k] for k in ("block_size", "stack_depth", "queue_chunk")}
@@ -73,7 +76,7 @@ def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log
 
     best_v = measure(best)
     trials = [(dict(best), best_v)]
-    for key in ("width", "layout", "leaf_size", "block_size", "stack_depth", "queue_chunk"):
+    for key in ("builder", "width", "layout", "leaf_size", "block_size", "stack_depth", "queue_chunk"):
         for v in CANDIDATES[key]:
             if v == best[key]:
                 continue
@@ -103,6 +106,7 @@ def apply_table(ctx, table: dict) -> None:
         t.leaf_size = int(s["leaf_size"])
         t.layout = LAYOUT_CODE.get(s.get("layout", "sah"), L.LAYOUT_SAH)
         t.width = int(s.get("width", 2))
+        t.builder = BUILDER_CODE.get(s.get("builder", "lbvh"), L.BUILDER_LBVH)
         L.check(ctx.lib.eos_ctx_set_tuning(ctx.h, int(bucket), byref(t)), "eos_ctx_set_tuning")
 
 

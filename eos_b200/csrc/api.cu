@@ -159,7 +159,7 @@ eos_status set_device(eos_ctx* ctx) {
 
 // Tuned entry for a scene of n triangles (zeros when the table has none).
 eos_tuning tuned_for(const eos_ctx* ctx, uint32_t n) {
-  eos_tuning t{0, 0, 0, 0};
+  eos_tuning t{0, 0, 0, 0, 0, 0, 0};
   auto it = ctx->tuning.upper_bound(n);
   if (it != ctx->tuning.begin()) t = std::prev(it)->second;
   return t;
@@ -254,7 +254,8 @@ eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning*
   if (!ctx || !t) return EOS_ERR_INVALID_ARG;
   if (t->block_size < 0 || t->block_size > 1024 || t->queue_chunk < 0 || t->stack_depth < 0 || t->leaf_size < 0 ||
       t->leaf_size > 32 || t->layout < EOS_LAYOUT_DEFAULT || t->layout > EOS_LAYOUT_FIXED ||
-      (t->width != 0 && t->width != 2 && t->width != 4))
+      (t->width != 0 && t->width != 2 && t->width != 4) || t->builder < EOS_BUILDER_DEFAULT ||
+      t->builder > EOS_BUILDER_PLOC)
     return EOS_ERR_INVALID_ARG;
   ctx->tuning[min_tris] = *t;
   return EOS_OK;
@@ -286,6 +287,9 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   int width = build && build->width != 0 ? build->width : tuned.width;
   if (width == 0) width = 4;
   if (width != 2 && width != 4) return EOS_ERR_INVALID_ARG;
+  int builder = build && build->builder != EOS_BUILDER_DEFAULT ? build->builder : tuned.builder;
+  if (builder == EOS_BUILDER_DEFAULT) builder = EOS_BUILDER_PLOC;
+  if (builder != EOS_BUILDER_LBVH && builder != EOS_BUILDER_PLOC) return EOS_ERR_INVALID_ARG;
   eos_status st = set_device(ctx);
   if (st != EOS_OK) return st;
   eos_scene* sc = new eos_scene();
@@ -293,6 +297,7 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   sc->leaf_size = leaf;
   sc->layout = layout;
   sc->width = width;
+  sc->builder = builder;
   auto fail = [&](eos_status s) {
     eos_scene_destroy(sc);
     return s;
@@ -374,6 +379,8 @@ eos_status eos_scene_get_info(const eos_scene* sc, eos_scene_info* info) {
   info->n_lights = (uint32_t)sc->dev.n_lights;
   info->build_ms = sc->build_ms;
   info->device_bytes = sc->device_bytes;
+  info->builder = (uint32_t)sc->builder;
+  info->depth = (uint32_t)sc->levels;
   return EOS_OK;
 }
 

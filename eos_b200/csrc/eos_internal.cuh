@@ -110,6 +110,7 @@ struct eos_scene {
   int leaf_size = 8;
   int layout = EOS_LAYOUT_SAH;
   int width = 4;   // children per 128-B node record: 4, or 2 (binary tree)
+  int builder = EOS_BUILDER_PLOC;
   int levels = 0;  // depth of the tree of records
   float sah_cost = 0.0f;
   float build_ms = 0.0f;
@@ -123,9 +124,15 @@ void* scratch(eos_ctx* ctx, const char* name, size_t bytes, eos_status* st);
 // Pointer classification (cudaPointerGetAttributes): true for device/managed memory.
 bool is_device_ptr(const void* p);
 
-// LBVH build (lbvh.cu).  verts/normals/tris/tri_obj are device pointers.
+// Scene build (lbvh.cu).  verts/normals/tris/tri_obj are device pointers.
 eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const float* d_normals,
                        uint32_t n_verts, const uint32_t* d_tris, const uint32_t* d_obj, uint32_t n_tris);
+
+// PLOC hierarchy over n >= 2 leaves with boxes at blo / bhi[n-1+p] in Morton order
+// (ploc.cu): child / range / parent in the refit's layout, perm[p] = record position of
+// Morton position p, *depth = tree depth (above 4 * kStackMax nothing is written).
+eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi, int2* child, int2* range,
+                      int* parent, uint32_t* perm, int* depth);
 
 // Renderers (render.cu).
 struct RenderArgs {

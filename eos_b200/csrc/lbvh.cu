@@ -1,5 +1,6 @@
-// GPU LBVH build: Morton codes -> stable radix sort -> Karras hierarchy -> atomic refit
-// -> 128-byte node records (4-wide, or 2 children per record) / 48-byte triangle records.
+// GPU BVH build: Morton codes -> stable radix sort -> hierarchy (Karras radix tree, or
+// PLOC clustering in ploc.cu) -> atomic refit -> 128-byte node records (4-wide, or 2
+// children per record) / 48-byte triangle records.
 //
 // Replaces the reference's CPU top-down median/SAH build (src/BVH.cpp:97-111,549-606) and
 // its SoA upload (src/cudaStructures.cu:36-174,274-405).  The Morton encoder is the
@@ -239,15 +240,17 @@ __global__ void k_karras(const uint32_t* __restrict__ k, int n, int2* __restrict
   parent[right] = i;
 }
 
-// Triangle records in sorted order, leaf boxes, id -> position map.
+// Triangle records, leaf boxes, id -> position map.  The triangle at Morton position m
+// goes to record position p = perm[m] (perm NULL: p = m).
 __global__ void k_records(const float* __restrict__ verts, const float* __restrict__ normals, uint32_t n_verts,
                           const uint32_t* __restrict__ tris, const uint32_t* __restrict__ obj,
-                          const uint32_t* __restrict__ order, int n, uint32_t n_obj, float4* __restrict__ trec,
-                          float4* __restrict__ srec, int32_t* __restrict__ pos_of_id, float4* __restrict__ blo,
-                          float4* __restrict__ bhi, int* err) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  uint32_t id = order[p];
+                          const uint32_t* __restrict__ order, const uint32_t* __restrict__ perm, int n, uint32_t n_obj,
+                          float4* __restrict__ trec, float4* __restrict__ srec, int32_t* __restrict__ pos_of_id,
+                          float4* __restrict__ blo, float4* __restrict__ bhi, int* err) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  uint32_t id = order[m];
+  const int p = perm ? (int)perm[m] : m;
   uint32_t a = tris[3 * (size_t)id], b = tris[3 * (size_t)id + 1], c = tris[3 * (size_t)id + 2];
   if (a >= n_verts || b >= n_verts || c >= n_verts) a = b = c = 0;  // flagged in k_centroids
   f3 v1 = load_vert(verts, a), v2 = load_vert(verts, b), v3 = load_vert(verts, c);
@@ -537,14 +540,33 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
       std::swap(vi, vo);
     }
     // 4 passes: the sorted result is back in (keys, vals)
-    k_records<<<grid_for(nn, 256), 256, 0, st>>>(d_verts, d_normals, n_verts, d_tris, d_obj, vals, n,
+    k_records<<<grid_for(nn, 256), 256, 0, st>>>(d_verts, d_normals, n_verts, d_tris, d_obj, vals, nullptr, n,
                                                  (uint32_t)sc->dev.n_obj, (float4*)sc->d_tris, (float4*)sc->d_shade,
                                                  (int32_t*)sc->d_pos_of_id, blo, bhi, ctx->d_err);
   }
   if (n >= 2) {
-    EOS_CUDA(cudaMemsetAsync(parent, 0xff, 4 * (2 * nn), st));
+    bool ploc = sc->builder == EOS_BUILDER_PLOC;
+    if (ploc) {
+      // PLOC over the leaf boxes in Morton order, then the records again in the tree's
+      // depth-first leaf order (every subtree a contiguous range)
+      uint32_t* perm = (uint32_t*)scratch(ctx, "lbvh.perm", 4 * nn, &es);
+      if (es != EOS_OK) return es;
+      int depth = 0;
+      if ((es = build_ploc(ctx, n, blo, bhi, child, range, parent, perm, &depth)) != EOS_OK) return es;
+      ploc = depth + 2 <= kStackMax;  // the refit walks at most kStackMax levels
+      if (ploc)
+        k_records<<<grid_for(nn, 256), 256, 0, st>>>(d_verts, d_normals, n_verts, d_tris, d_obj, vals, perm, n,
+                                                     (uint32_t)sc->dev.n_obj, (float4*)sc->d_tris,
+                                                     (float4*)sc->d_shade, (int32_t*)sc->d_pos_of_id, blo, bhi,
+                                                     ctx->d_err);
+      else
+        sc->builder = EOS_BUILDER_LBVH;
+    }
     EOS_CUDA(cudaMemsetAsync(arrive, 0, 4 * n_nodes, st));
-    k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys, n, child, range, parent);
+    if (!ploc) {
+      EOS_CUDA(cudaMemsetAsync(parent, 0xff, 4 * (2 * nn), st));
+      k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys, n, child, range, parent);
+    }
     k_refit<<<grid_for(nn, 256), 256, 0, st>>>(n, child, range, parent, blo, bhi, arrive, sc->leaf_size,
                                               sc->layout == EOS_LAYOUT_SAH, ctx->d_err);
     // SAH cost of the tree (subtree cost of the root, in triangle-test units)

@@ -1,0 +1,256 @@
+// PLOC hierarchy: parallel locally-ordered clustering (Meister & Bittner, "Parallel Locally-
+// Ordered Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG 2018), a second
+// builder beside the Karras LBVH.  No reference counterpart (the reference builds a CPU
+// SAH tree, src/BVH.cpp:97-111); it is a tree-quality choice only -- the traversal's
+// results do not depend on the tree.
+//
+// Input: the leaf boxes in Morton order.  Clusters start as the leaves; each iteration
+//   1. every cluster finds its nearest neighbour among the clusters within kRadius places
+//      of it (distance = surface area of the merged box; ties to the lower index);
+//   2. mutual nearest neighbours merge into a new interior node at the lower position;
+//   3. the surviving clusters are compacted in order.
+// Interior nodes are numbered in creation order (deterministic: exclusive scans, no
+// atomics), the root last.  Afterwards every node's first leaf position in depth-first
+// order (left subtree first) is found by a walk to the root, so that every subtree covers
+// a contiguous range of triangle records; the nodes are renumbered root-first into the
+// layout the refit and the node-record writer expect (interior 0..n-2 with the root 0,
+// leaf at position q -> n-1+q).
+#include <algorithm>
+#include <vector>
+
+#include <cub/device/device_scan.cuh>
+
+#include "eos_internal.cuh"
+
+namespace eos {
+namespace {
+
+constexpr int kRadius = 16;        // neighbours searched on each side
+constexpr int kNNBlock = 256;
+constexpr int kMaxWalk = 4 * kStackMax;  // bound of the walks to the root
+
+__device__ __forceinline__ float merged_area(float4 al, float4 ah, float4 bl, float4 bh) {
+  const float dx = fmaxf(ah.x, bh.x) - fminf(al.x, bl.x);
+  const float dy = fmaxf(ah.y, bh.y) - fminf(al.y, bl.y);
+  const float dz = fmaxf(ah.z, bh.z) - fminf(al.z, bl.z);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Nearest neighbour of every cluster within kRadius places (boxes staged in shared memory).
+__global__ void k_ploc_nn(int nc, const float4* __restrict__ lo, const float4* __restrict__ hi,
+                          int* __restrict__ nn) {
+  __shared__ float4 slo[kNNBlock + 2 * kRadius], shi[kNNBlock + 2 * kRadius];
+  const int b0 = blockIdx.x * kNNBlock;
+  for (int t = threadIdx.x; t < kNNBlock + 2 * kRadius; t += blockDim.x) {
+    const int g = b0 - kRadius + t;
+    if (g >= 0 && g < nc) {
+      slo[t] = lo[g];
+      shi[t] = hi[g];
+    }
+  }
+  __syncthreads();
+  const int i = b0 + threadIdx.x;
+  if (i >= nc) return;
+  const int li = threadIdx.x + kRadius;
+  const float4 al = slo[li], ah = shi[li];
+  float best = kInf;
+  int bj = i == 0 ? 1 : i - 1;
+  const int j0 = max(0, i - kRadius), j1 = min(nc - 1, i + kRadius);
+  for (int j = j0; j <= j1; ++j) {
+    if (j == i) continue;
+    const int lj = j - b0 + kRadius;
+    const float a = merged_area(al, ah, slo[lj], shi[lj]);
+    if (a < best) {
+      best = a;
+      bj = j;
+    }
+  }
+  nn[i] = bj;
+}
+
+// Cluster i survives (keep) unless it is the upper half of a mutual pair; the lower half
+// of a pair creates a node (make).  With `force` (an iteration that merged nothing) the
+// pairs (2k, 2k + 1) merge instead, which bounds the number of iterations.
+__global__ void k_ploc_flags(int nc, const int* __restrict__ nn, int force, int* __restrict__ keep,
+                             int* __restrict__ make) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  int partner;
+  if (force) {
+    partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
+  } else {
+    const int j = nn[i];
+    partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
+  }
+  keep[i] = partner < 0 || i < partner;
+  make[i] = partner >= 0 && i < partner;
+}
+
+__global__ void k_ploc_merge(int nc, const int* __restrict__ nn, int force, const int* __restrict__ keep_scan,
+                             const int* __restrict__ make_scan, int node_base, const int* __restrict__ cid,
+                             const float4* __restrict__ lo, const float4* __restrict__ hi, int* __restrict__ cid_out,
+                             float4* __restrict__ lo_out, float4* __restrict__ hi_out, int2* __restrict__ child,
+                             int* __restrict__ count, float4* __restrict__ nlo, float4* __restrict__ nhi, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  int partner;
+  if (force) {
+    partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
+  } else {
+    const int j = nn[i];
+    partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
+  }
+  if (partner >= 0 && i > partner) return;  // merged into the lower cluster
+  const int pos = keep_scan[i];
+  if (partner < 0) {
+    cid_out[pos] = cid[i];
+    lo_out[pos] = lo[i];
+    hi_out[pos] = hi[i];
+    return;
+  }
+  const int k = node_base + make_scan[i];
+  const int a = cid[i], b = cid[partner];
+  const float4 al = lo[i], ah = hi[i], bl = lo[partner], bh = hi[partner];
+  const float4 l = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
+  const float4 h = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f);
+  child[k] = make_int2(a, b);
+  count[k] = (a >= n - 1 ? 1 : count[a]) + (b >= n - 1 ? 1 : count[b]);
+  nlo[k] = l;
+  nhi[k] = h;
+  cid_out[pos] = k;
+  lo_out[pos] = l;
+  hi_out[pos] = h;
+}
+
+__global__ void k_ploc_parents(int n, const int2* __restrict__ child, int* __restrict__ parent) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n - 1) return;
+  const int2 c = child[k];
+  parent[c.x] = k;
+  parent[c.y] = k;
+}
+
+// Depth-first position of the first leaf of every node (creation-order ids: interior
+// 0..n-2, root n-2; leaf Morton position p -> n-1+p): the sum of the left siblings' leaf
+// counts along the path to the root.
+__global__ void k_ploc_positions(int n, const int2* __restrict__ child, const int* __restrict__ parent,
+                                 const int* __restrict__ count, int* __restrict__ first, int* __restrict__ depth_max) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= 2 * n - 1) return;
+  int pos = 0, node = v, steps = 0;
+  while (node != n - 2) {
+    const int p = parent[node];
+    if (p < 0 || ++steps > kMaxWalk) {  // reported as too deep: the caller falls back to the LBVH
+      atomicMax(depth_max, kMaxWalk + 1);
+      return;
+    }
+    const int2 c = child[p];
+    if (c.y == node) pos += c.x >= n - 1 ? 1 : count[c.x];
+    node = p;
+  }
+  first[v] = pos;
+  atomicMax(depth_max, steps);
+}
+
+// Root-first renumbering into the refit's layout; perm[p] = final position of the leaf at
+// Morton position p.
+__global__ void k_ploc_finalize(int n, const int2* __restrict__ child, const int* __restrict__ count,
+                                const int* __restrict__ first, int2* __restrict__ child_out,
+                                int2* __restrict__ range_out, int* __restrict__ parent_out, uint32_t* __restrict__ perm) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) perm[k] = (uint32_t)first[n - 1 + k];
+  if (k >= n - 1) return;
+  auto map = [&](int x) { return x >= n - 1 ? n - 1 + first[x] : n - 2 - x; };
+  const int f = n - 2 - k;
+  const int2 c = child[k];
+  const int a = map(c.x), b = map(c.y);
+  child_out[f] = make_int2(a, b);
+  range_out[f] = make_int2(first[k], first[k] + count[k] - 1);
+  parent_out[a] = f;
+  parent_out[b] = f;
+}
+
+inline int grid_of(long long n, int block) { return (int)std::max<long long>(1, (n + block - 1) / block); }
+
+}  // namespace
+
+// Builds the hierarchy over n >= 2 leaves whose boxes lie at blo / bhi[n-1+p] (Morton
+// position p).  Writes child / range / parent in the refit's layout and perm[p], the final
+// record position of Morton position p.  *depth = the deepest node's depth; above
+// 4 * kStackMax nothing is written and the caller must use another builder.
+eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi, int2* child, int2* range,
+                      int* parent, uint32_t* perm, int* depth) {
+  cudaStream_t st = ctx->stream;
+  eos_status es = EOS_OK;
+  const size_t nn = (size_t)n;
+  int* cid[2] = {(int*)scratch(ctx, "ploc.cid0", 4 * nn, &es), (int*)scratch(ctx, "ploc.cid1", 4 * nn, &es)};
+  float4* clo[2] = {(float4*)scratch(ctx, "ploc.lo0", 16 * nn, &es), (float4*)scratch(ctx, "ploc.lo1", 16 * nn, &es)};
+  float4* chi[2] = {(float4*)scratch(ctx, "ploc.hi0", 16 * nn, &es), (float4*)scratch(ctx, "ploc.hi1", 16 * nn, &es)};
+  int* nbr = (int*)scratch(ctx, "ploc.nn", 4 * nn, &es);
+  int* keep = (int*)scratch(ctx, "ploc.keep", 4 * (nn + 1), &es);
+  int* make = (int*)scratch(ctx, "ploc.make", 4 * (nn + 1), &es);
+  int* keep_scan = (int*)scratch(ctx, "ploc.keep_scan", 4 * (nn + 1), &es);
+  int* make_scan = (int*)scratch(ctx, "ploc.make_scan", 4 * (nn + 1), &es);
+  int2* tchild = (int2*)scratch(ctx, "ploc.child", 8 * nn, &es);
+  int* tcount = (int*)scratch(ctx, "ploc.count", 4 * nn, &es);
+  float4* tlo = (float4*)scratch(ctx, "ploc.nlo", 16 * nn, &es);
+  float4* thi = (float4*)scratch(ctx, "ploc.nhi", 16 * nn, &es);
+  int* tparent = (int*)scratch(ctx, "ploc.parent", 4 * (2 * nn), &es);
+  int* first = (int*)scratch(ctx, "ploc.first", 4 * (2 * nn), &es);
+  int* dmax = (int*)scratch(ctx, "ploc.depth", 4, &es);
+  size_t temp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, keep, keep_scan, n + 1, st);
+  void* temp = scratch(ctx, "ploc.scan_temp", std::max<size_t>(temp_bytes, 16), &es);
+  if (es != EOS_OK) return es;
+
+  // clusters = leaves in Morton order
+  EOS_CUDA(cudaMemcpyAsync(clo[0], blo + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
+  EOS_CUDA(cudaMemcpyAsync(chi[0], bhi + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
+  {
+    std::vector<int> ids(nn);
+    for (int p = 0; p < n; ++p) ids[p] = n - 1 + p;
+    EOS_CUDA(cudaMemcpyAsync(cid[0], ids.data(), 4 * nn, cudaMemcpyHostToDevice, st));
+    EOS_CUDA(cudaStreamSynchronize(st));
+  }
+  int nc = n, cur = 0, node_base = 0, iters = 0;
+  while (nc > 1) {
+    if (++iters > 4 * n + 8) return EOS_ERR_TIMEOUT;  // cannot happen: every round merges
+    k_ploc_nn<<<grid_of(nc, kNNBlock), kNNBlock, 0, st>>>(nc, clo[cur], chi[cur], nbr);
+    int force = 0;
+    for (;;) {
+      k_ploc_flags<<<grid_of(nc, 256), 256, 0, st>>>(nc, nbr, force, keep, make);
+      EOS_CUDA(cudaMemsetAsync(keep + nc, 0, 4, st));
+      EOS_CUDA(cudaMemsetAsync(make + nc, 0, 4, st));
+      EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, keep, keep_scan, nc + 1, st));
+      EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, make, make_scan, nc + 1, st));
+      int made = 0, kept = 0;
+      EOS_CUDA(cudaMemcpyAsync(&made, make_scan + nc, 4, cudaMemcpyDeviceToHost, st));
+      EOS_CUDA(cudaMemcpyAsync(&kept, keep_scan + nc, 4, cudaMemcpyDeviceToHost, st));
+      EOS_CUDA(cudaStreamSynchronize(st));
+      if (made == 0 && !force) {
+        force = 1;
+        continue;
+      }
+      k_ploc_merge<<<grid_of(nc, 256), 256, 0, st>>>(nc, nbr, force, keep_scan, make_scan, node_base, cid[cur],
+                                                     clo[cur], chi[cur], cid[cur ^ 1], clo[cur ^ 1], chi[cur ^ 1],
+                                                     tchild, tcount, tlo, thi, n);
+      node_base += made;
+      nc = kept;
+      cur ^= 1;
+      break;
+    }
+  }
+  if (node_base != n - 1) return EOS_ERR_CUDA;
+  EOS_CUDA(cudaMemsetAsync(tparent, 0xff, 4 * (2 * nn), st));
+  EOS_CUDA(cudaMemsetAsync(dmax, 0, 4, st));
+  k_ploc_parents<<<grid_of(n - 1, 256), 256, 0, st>>>(n, tchild, tparent);
+  k_ploc_positions<<<grid_of(2 * (long long)n - 1, 256), 256, 0, st>>>(n, tchild, tparent, tcount, first, dmax);
+  EOS_CUDA(cudaMemcpyAsync(depth, dmax, 4, cudaMemcpyDeviceToHost, st));
+  EOS_CUDA(cudaStreamSynchronize(st));
+  if (*depth > kMaxWalk) return EOS_OK;  // some walk did not end: outputs left unwritten
+  EOS_CUDA(cudaMemsetAsync(parent, 0xff, 4 * (2 * nn), st));
+  k_ploc_finalize<<<grid_of(n, 256), 256, 0, st>>>(n, tchild, tcount, first, child, range, parent, perm);
+  return EOS_OK;
+}
+
+}  // namespace eos

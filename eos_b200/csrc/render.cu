@@ -81,8 +81,11 @@ __device__ f3 trace_path(const PlainParams& P, f3 o, f3 d, int32_t* hits, uint32
   return c;
 }
 
+// Registers capped at 64 (32 warps per SM with blocks of 128): the megakernel is latency-
+// bound and gains more from resident warps than it loses to spills (measured on config 2:
+// 112 registers 2,580 Mrays/s, 96 2,794, 80 2,913, 64 3,076, 56 2,987, 48 2,481).
 template <int SH>
-__global__ void k_render_plain(PlainParams P) {
+__global__ void __maxnreg__(64) k_render_plain(PlainParams P) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;

@@ -24,8 +24,14 @@ constexpr float kCull = 1.000244140625f;       // 1 + 2^-12
 constexpr float kParallelEps = 1e-30f;
 constexpr float kRayEps = 1e-3f;               // shadow / mirror ray offset, src/RayTracer.cpp:305
 
+// Ray prepared for box tests.  sx / sy / sz select the near plane of each axis in a node
+// record ([0..2] = lo.xyz, [3..5] = hi.xyz): 0 (lo) for a direction component >= 0 or a
+// parallel axis, 3 (hi) otherwise; the far plane is the other one.  The near and far
+// distances are then (near - o) / d and (far - o) / d directly, the same values the
+// min / max of the two plane distances would give.
 struct SlabRay {
   float ox, oy, oz, ix, iy, iz;
+  int sx, sy, sz;
   bool par;
 };
 
@@ -36,47 +42,55 @@ __device__ __forceinline__ SlabRay make_slab(f3 o, f3 d) {
   r.ix = px ? 0.0f : 1.0f / d.x;
   r.iy = py ? 0.0f : 1.0f / d.y;
   r.iz = pz ? 0.0f : 1.0f / d.z;
+  r.sx = (px || d.x >= 0.0f) ? 0 : 3;
+  r.sy = (py || d.y >= 0.0f) ? 0 : 3;
+  r.sz = (pz || d.z >= 0.0f) ? 0 : 3;
   r.par = px || py || pz;
   return r;
 }
 
-// Entry distance of a box, or kInf when the box is missed or starts beyond `limit`.
-// Rays with a (near-)zero direction component take the containment branch; it is
-// warp-uniform in practice (whole pixel columns share it).
-__device__ __forceinline__ float slab(const SlabRay& r, float lx, float ly, float lz, float hx, float hy, float hz,
-                                      float limit) {
-  float t0x = (lx - r.ox) * r.ix, t1x = (hx - r.ox) * r.ix;
-  float t0y = (ly - r.oy) * r.iy, t1y = (hy - r.oy) * r.iy;
-  float t0z = (lz - r.oz) * r.iz, t1z = (hz - r.oz) * r.iz;
-  float nx = fminf(t0x, t1x), fx = fmaxf(t0x, t1x);
-  float ny = fminf(t0y, t1y), fy = fmaxf(t0y, t1y);
-  float nz = fminf(t0z, t1z), fz = fmaxf(t0z, t1z);
+// Three-input min / max (sm_100): exact, like two fminf / fmaxf.
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+// Entry and exit distances of a box from its near planes (nx, ny, nz) and far planes
+// (fx, fy, fz).  Rays with a (near-)zero direction component take the containment branch
+// (near = lo, far = hi there); it is warp-uniform in practice (whole pixel columns share it).
+__device__ __forceinline__ void slab_range(const SlabRay& r, float nx, float ny, float nz, float fx, float fy,
+                                           float fz, float& tn, float& tf) {
+  float tnx = (nx - r.ox) * r.ix, tfx = (fx - r.ox) * r.ix;
+  float tny = (ny - r.oy) * r.iy, tfy = (fy - r.oy) * r.iy;
+  float tnz = (nz - r.oz) * r.iz, tfz = (fz - r.oz) * r.iz;
   if (r.par) {
-    if (r.ix == 0.0f) { nx = -kInf; fx = (r.ox >= lx && r.ox <= hx) ? kInf : -kInf; }
-    if (r.iy == 0.0f) { ny = -kInf; fy = (r.oy >= ly && r.oy <= hy) ? kInf : -kInf; }
-    if (r.iz == 0.0f) { nz = -kInf; fz = (r.oz >= lz && r.oz <= hz) ? kInf : -kInf; }
+    if (r.ix == 0.0f) { tnx = -kInf; tfx = (r.ox >= nx && r.ox <= fx) ? kInf : -kInf; }
+    if (r.iy == 0.0f) { tny = -kInf; tfy = (r.oy >= ny && r.oy <= fy) ? kInf : -kInf; }
+    if (r.iz == 0.0f) { tnz = -kInf; tfz = (r.oz >= nz && r.oz <= fz) ? kInf : -kInf; }
   }
-  float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, 0.0f));
-  float tf = fminf(fminf(fminf(fx, fy), fz) * kSlack, limit);
-  return tn <= tf ? tn : kInf;
+  tn = fmaxf(max3f(tnx, tny, tnz), 0.0f);
+  tf = min3f(tfx, tfy, tfz) * kSlack;
+}
+
+// Entry distance of a box, or kInf when the box is missed or starts beyond `limit`.
+__device__ __forceinline__ float slab(const SlabRay& r, float nx, float ny, float nz, float fx, float fy, float fz,
+                                      float limit) {
+  float tn, tf;
+  slab_range(r, nx, ny, nz, fx, fy, fz, tn, tf);
+  return tn <= fminf(tf, limit) ? tn : kInf;
 }
 
 // Hit test of a box for shadow rays (no distance limit, no entry distance needed).
-__device__ __forceinline__ bool slab_hit(const SlabRay& r, float lx, float ly, float lz, float hx, float hy,
-                                         float hz) {
-  float t0x = (lx - r.ox) * r.ix, t1x = (hx - r.ox) * r.ix;
-  float t0y = (ly - r.oy) * r.iy, t1y = (hy - r.oy) * r.iy;
-  float t0z = (lz - r.oz) * r.iz, t1z = (hz - r.oz) * r.iz;
-  float nx = fminf(t0x, t1x), fx = fmaxf(t0x, t1x);
-  float ny = fminf(t0y, t1y), fy = fmaxf(t0y, t1y);
-  float nz = fminf(t0z, t1z), fz = fmaxf(t0z, t1z);
-  if (r.par) {
-    if (r.ix == 0.0f) { nx = -kInf; fx = (r.ox >= lx && r.ox <= hx) ? kInf : -kInf; }
-    if (r.iy == 0.0f) { ny = -kInf; fy = (r.oy >= ly && r.oy <= hy) ? kInf : -kInf; }
-    if (r.iz == 0.0f) { nz = -kInf; fz = (r.oz >= lz && r.oz <= hz) ? kInf : -kInf; }
-  }
-  float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, 0.0f));
-  float tf = fminf(fminf(fx, fy), fz) * kSlack;
+__device__ __forceinline__ bool slab_hit(const SlabRay& r, float nx, float ny, float nz, float fx, float fy,
+                                         float fz) {
+  float tn, tf;
+  slab_range(r, nx, ny, nz, fx, fy, fz, tn, tf);
   return tn <= tf && tn != kInf;
 }
 
@@ -159,8 +173,8 @@ template <int SH, bool SORT>
 __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const SlabRay& r, int& cur,
                                             float limit, TraversalStack<SH>& st, unsigned& nodes) {
   const float4* nd = node_base + 8 * (size_t)cur;
-  const float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
-  const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+  const float4 lx = __ldg(nd + r.sx), ly = __ldg(nd + 1 + r.sy), lz = __ldg(nd + 2 + r.sz);  // near planes
+  const float4 hx = __ldg(nd + 3 - r.sx), hy = __ldg(nd + 4 - r.sy), hz = __ldg(nd + 5 - r.sz);  // far planes
   const int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 6);
   ++nodes;
   int c[4] = {ref.x, ref.y, ref.z, ref.w};

@@ -124,6 +124,7 @@ typedef struct eos_tuning {
   int32_t leaf_size;
   int32_t layout;
   int32_t width;
+  int32_t builder;
 } eos_tuning;
 
 /* Node layout of the LBVH: which subtrees become leaves. */
@@ -133,11 +134,20 @@ enum {
   EOS_LAYOUT_FIXED = 2    /* leaf whenever n <= leaf_size */
 };
 
+/* Hierarchy builder (both start from the Morton-sorted triangles). */
+enum {
+  EOS_BUILDER_DEFAULT = 0, /* tuned value, else PLOC */
+  EOS_BUILDER_LBVH = 1,    /* Karras 2012 radix tree over the Morton codes */
+  EOS_BUILDER_PLOC = 2     /* locally-ordered agglomerative clustering (Meister & Bittner 2018);
+                              falls back to LBVH for a tree deeper than the traversal allows */
+};
+
 typedef struct eos_build_params {
   int32_t leaf_size;    /* largest leaf, 1..32 triangles; 0 = tuned value, else 8 */
   int32_t layout;       /* EOS_LAYOUT_* */
   int32_t width;        /* children per 128-B node record: 4, or 2 (binary tree);
                            0 = tuned value, else 4 */
+  int32_t builder;      /* EOS_BUILDER_* */
 } eos_build_params;
 
 /* Per-path record of the bounce path: hit triangle id per bounce and, per bounce, the
@@ -165,15 +175,17 @@ typedef struct eos_stats {
 
 typedef struct eos_scene_info {
   uint32_t n_tris;
-  uint32_t n_nodes;       /* interior nodes of the LBVH (n_tris - 1) */
+  uint32_t n_nodes;       /* node records (128 B each) */
   uint32_t leaf_size;
   uint32_t layout;        /* EOS_LAYOUT_SAH or EOS_LAYOUT_FIXED */
   uint32_t width;         /* 2 or 4 (a 4-wide request too deep for the stack stays 2) */
   float sah_cost;         /* SAH cost of the tree, in triangle-test units */
   uint32_t n_objects;
   uint32_t n_lights;
-  float build_ms;         /* device time of the LBVH build */
+  float build_ms;         /* device time of the build */
   uint64_t device_bytes;  /* device memory held by the scene */
+  uint32_t builder;       /* EOS_BUILDER_LBVH or EOS_BUILDER_PLOC (the one used) */
+  uint32_t depth;         /* levels of the tree of node records */
 } eos_scene_info;
 
 /* One view of one scene for eos_render_batch.  Outputs follow eos_render. */

@@ -162,11 +162,13 @@ def _random_rays(n, seed, lo=-3, hi=3):
     return np.concatenate([r, ax])
 
 
-@pytest.mark.parametrize("leaf,width", [(1, 2), (4, 2), (8, 2), (1, 4), (4, 4), (16, 4)])
-def test_queries_match_oracle(ctx, leaf, width):
+@pytest.mark.parametrize("leaf,width,builder", [(1, 2, "lbvh"), (4, 2, "lbvh"), (8, 2, "lbvh"), (1, 4, "lbvh"),
+                                                (4, 4, "lbvh"), (16, 4, "lbvh"), (1, 2, "ploc"), (4, 4, "ploc"),
+                                                (16, 4, "ploc")])
+def test_queries_match_oracle(ctx, leaf, width, builder):
     sc = scenes.small_random_scene(51, n_spheres=8, level=3, lights=2)
-    dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, width=width)
-    assert dsc.info()["width"] == width
+    dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, width=width, builder=builder)
+    assert dsc.info()["width"] == width and dsc.info()["builder"] == {"lbvh": 1, "ploc": 2}[builder]
     orc = oracle.Oracle(sc)
     rays = _random_rays(20000, 9)
     ids, t = api.trace_closest(ctx, dsc, rays)

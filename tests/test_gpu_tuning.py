@@ -14,10 +14,13 @@ def test_results_invariant_under_tuning(ctx):
     sc = scenes.small_random_scene(81, n_spheres=10, level=3, lights=3, refl=0.5)
     cam = scenes.look_at((1.0, 3.0, 9.0), (0, -0.5, 0), 55.0, 200, 150)
     ref = None
-    for layout, leaf, width in (("fixed", 1, 2), ("fixed", 3, 2), ("sah", 8, 2), ("sah", 32, 2), ("fixed", 32, 2),
-                                ("fixed", 1, 4), ("sah", 8, 4), ("fixed", 16, 4)):
-        dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, layout=layout, width=width)
+    for builder, layout, leaf, width in (("lbvh", "fixed", 1, 2), ("lbvh", "fixed", 3, 2), ("lbvh", "sah", 8, 2),
+                                         ("lbvh", "sah", 32, 2), ("lbvh", "fixed", 32, 2), ("lbvh", "fixed", 1, 4),
+                                         ("lbvh", "sah", 8, 4), ("lbvh", "fixed", 16, 4), ("ploc", "fixed", 1, 2),
+                                         ("ploc", "sah", 8, 4), ("ploc", "fixed", 4, 4), ("ploc", "fixed", 32, 4)):
+        dsc = api.DeviceScene(ctx, sc, leaf_size=leaf, layout=layout, width=width, builder=builder)
         assert dsc.info()["leaf_size"] == leaf and dsc.info()["width"] == width
+        assert dsc.info()["builder"] == {"lbvh": 1, "ploc": 2}[builder]
         assert dsc.info()["sah_cost"] > 0
         for mode, refill in (("plain", False), ("wavefront", False), ("wavefront", True)):
             for block, stack, chunk in ((64, 8, 32), (128, 16, 64), (256, 32, 256)):
@@ -32,7 +35,8 @@ def test_results_invariant_under_tuning(ctx):
 
 
 def test_autotuner_writes_and_applies_table(ctx, tmp_path, monkeypatch):
-    monkeypatch.setattr(autotune, "CANDIDATES", {"width": [2, 4], "layout": ["sah", "fixed"], "leaf_size": [2, 4],
+    monkeypatch.setattr(autotune, "CANDIDATES", {"builder": ["ploc", "lbvh"], "width": [2, 4],
+                                                 "layout": ["sah", "fixed"], "leaf_size": [2, 4],
                                                  "block_size": [64, 128], "stack_depth": [8, 16],
                                                  "queue_chunk": [64, 128]})
     sc = scenes.small_random_scene(82, n_spheres=12, level=3, lights=2)
@@ -48,4 +52,4 @@ def test_autotuner_writes_and_applies_table(ctx, tmp_path, monkeypatch):
     assert dsc.info()["leaf_size"] == table[b]["setting"]["leaf_size"]
     ctx.lib.eos_ctx_clear_tuning(ctx.h)
     info = api.DeviceScene(ctx, sc, leaf_size=0).info()
-    assert info["leaf_size"] == 8 and info["layout"] == 1 and info["width"] == 4
+    assert info["leaf_size"] == 8 and info["layout"] == 1 and info["width"] == 4 and info["builder"] == 2
