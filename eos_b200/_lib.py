@@ -33,7 +33,8 @@ class EosError(RuntimeError):
 
 
 class Material(Structure):
-    _fields_ = [("kd", c_float * 3), ("ks", c_float * 3), ("shininess", c_float), ("reflectivity", c_float)]
+    _fields_ = [("kd", c_float * 3), ("ks", c_float * 3), ("shininess", c_float), ("reflectivity", c_float),
+                ("transparency", c_float), ("refractive_index", c_float)]
 
 
 class Light(Structure):
@@ -115,6 +116,7 @@ SIGNATURES = [
     ("eos_scene_destroy", c_int32, [c_void_p]),
     ("eos_scene_set_materials", c_int32, [c_void_p, c_void_p, c_uint32]),
     ("eos_scene_set_lights", c_int32, [c_void_p, c_void_p, c_uint32]),
+    ("eos_scene_set_ambient_index", c_int32, [c_void_p, c_float]),
     ("eos_scene_get_info", c_int32, [c_void_p, POINTER(SceneInfo)]),
     ("eos_scene_get_morton", c_int32, [c_void_p, c_void_p, c_void_p]),
     ("eos_render", c_int32, [c_void_p, c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,

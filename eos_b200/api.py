@@ -12,7 +12,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib as L
-from .scenes import CameraData, SceneData
+from .scenes import CameraData, SceneData, pad_materials
 
 
 def _ptr(a):
@@ -83,8 +83,17 @@ class Context:
         L.check(self.lib.eos_ctx_synchronize(self.h), "eos_ctx_synchronize")
 
 
-def materials_array(mats: np.ndarray) -> np.ndarray:
-    return np.ascontiguousarray(mats, np.float32).reshape(-1, 8)
+def materials_array(mats):
+    """Material rows in the C layout (eos_material, 10 floats): numpy rows of 8 or 10, or a
+    torch tensor (rows of 8 are padded with transparency 0, refractive index 1)."""
+    if hasattr(mats, "data_ptr"):
+        import torch
+        m = mats.float().reshape(mats.shape[0], -1)
+        if m.shape[1] == 8:
+            pad = torch.tensor([0.0, 1.0], device=m.device).expand(m.shape[0], 2)
+            m = torch.cat([m, pad], 1)
+        return m.contiguous()
+    return pad_materials(mats)
 
 
 class DeviceScene:
@@ -114,6 +123,8 @@ class DeviceScene:
                                          lights.shape[0], byref(bp), byref(h))
         L.check(code, "eos_scene_create")
         self.h = h
+        if scene.ambient_index != 1.0:
+            self.set_ambient_index(scene.ambient_index)
 
     def close(self):
         if getattr(self, "h", None):
@@ -139,8 +150,11 @@ class DeviceScene:
         return codes, order
 
     def set_materials(self, mats):
-        m = mats if hasattr(mats, "data_ptr") else materials_array(mats)
+        m = materials_array(mats)
         L.check(self.lib.eos_scene_set_materials(self.h, _ptr(m), int(m.shape[0])), "eos_scene_set_materials")
+
+    def set_ambient_index(self, refractive_index: float):
+        L.check(self.lib.eos_scene_set_ambient_index(self.h, float(refractive_index)), "eos_scene_set_ambient_index")
 
     def set_lights(self, lights):
         l = lights if hasattr(lights, "data_ptr") else np.ascontiguousarray(lights, np.float32).reshape(-1, 6)

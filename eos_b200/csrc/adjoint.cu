@@ -3,11 +3,12 @@
 // visibility frozen from the forward pass's path records (hit triangle per bounce and
 // blocked-light masks).  Nothing else of the forward pass is stored: each bounce's hit is
 // re-derived from its triangle id with the same exact-order Moller-Trumbore, hit point,
-// normal and mirror ray as the forward kernels, so the geometry matches the forward pass
-// bit for bit.
+// normal and secondary ray as the forward kernels, so the geometry matches the forward
+// pass bit for bit.
 //
 // Forward model per path (src/RayTracer.cpp:302-458): c = sum_k T_k phong_k with
-// T_k = prod_{j<k} reflectivity_j and, per unblocked light l,
+// T_k = prod_{j<k} w_j, w = reflectivity for a mirror bounce and K + (1 - K) for a
+// transparent one (its Fresnel mix of one colour), and, per unblocked light l,
 //   phong = max(0, N.L) kd*C_l + [V.R > 0] (V.R)^s C_l*ks,  L = (p_l - P)/|p_l - P|,
 //   R = w/|w|, w = 2 (N.L) N - L,  V = normalize(camera - P),  s = shininess.
 // Gradients with g = dL/dc * T_k:
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
           alive = false;
         } else {
           hit_geometry(s, o, d, h, P, N, obj);
-          m = s.mats + 8 * obj;
+          m = s.mats + kMatStride * obj;
         }
       }
     }
@@ -157,13 +158,13 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
       pending &= ~peers;
     }
     if (alive) {
-      float r = m[7];
-      if (!(r > 0.0f) || k + 1 > A.trace_depth) {
+      f3 ro, rd;
+      float w;
+      if (!secondary_ray(m, s.ambient_index, d, P, N, ro, rd, w) || k + 1 > A.trace_depth) {
         alive = false;
       } else {
-        T *= r;
-        f3 rd = norm3(reflect3(d, N));
-        o = add3(P, scale3(kRayEps, rd));
+        T *= fold_weight(w);
+        o = ro;
         d = rd;
       }
     }

@@ -314,6 +314,7 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
   sc->device_bytes += sizeof(eos_material) * n_materials + sizeof(eos_light) * std::max<uint32_t>(1, n_lights);
   sc->dev.n_obj = (int)n_materials;
   sc->dev.n_lights = (int)n_lights;
+  sc->dev.ambient_index = 1.0f;
   sc->dev.n_tris = (int)n_tris;
   if ((st = eos_scene_set_materials(sc, materials, n_materials)) != EOS_OK) return fail(st);
   if (n_lights && (st = eos_scene_set_lights(sc, lights, n_lights)) != EOS_OK) return fail(st);
@@ -351,9 +352,22 @@ eos_status eos_scene_destroy(eos_scene* sc) {
 eos_status eos_scene_set_materials(eos_scene* sc, const eos_material* m, uint32_t n) {
   if (!sc || !m || n != (uint32_t)sc->dev.n_obj) return EOS_ERR_INVALID_ARG;
   EOS_CUDA(cudaSetDevice(sc->ctx->device));
-  cudaMemcpyKind kind = is_device_ptr(m) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  EOS_CUDA(cudaMemcpyAsync(sc->d_mats, m, sizeof(eos_material) * n, kind, sc->ctx->stream));
+  // a material both reflective and transparent would need two secondary rays per hit
+  std::vector<eos_material> host(n);
+  const bool dev = is_device_ptr(m);
+  if (dev) EOS_CUDA(cudaMemcpy(host.data(), m, sizeof(eos_material) * n, cudaMemcpyDeviceToHost));
+  else std::memcpy(host.data(), m, sizeof(eos_material) * n);
+  for (const eos_material& e : host)
+    if (e.reflectivity > 0.0f && e.transparency > 0.0f) return EOS_ERR_UNSUPPORTED;
+  EOS_CUDA(cudaMemcpyAsync(sc->d_mats, m, sizeof(eos_material) * n,
+                           dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, sc->ctx->stream));
   EOS_CUDA(cudaStreamSynchronize(sc->ctx->stream));
+  return EOS_OK;
+}
+
+eos_status eos_scene_set_ambient_index(eos_scene* sc, float refractive_index) {
+  if (!sc || !(refractive_index > 0.0f)) return EOS_ERR_INVALID_ARG;
+  sc->dev.ambient_index = refractive_index;
   return EOS_OK;
 }
 

@@ -20,6 +20,7 @@ constexpr int kMaxLights = EOS_MAX_LIGHTS;
 constexpr int kStackMax = 96;
 constexpr float kInf = __builtin_huge_valf();
 constexpr int kCounters = 8;  // ray / traversal counters per call (see trace.cuh)
+constexpr int kMatStride = 10;  // floats per material (sizeof(eos_material) / 4)
 
 // Device error word bits (atomicOr'ed by kernels, read back by the host).
 enum : int {
@@ -52,11 +53,13 @@ struct DevScene {
   const float4* tris;
   const float4* shade;
   const int32_t* pos_of_id;  // triangle id -> sorted position
-  const float* mats;         // n_obj x 8: kd rgb, ks rgb, shininess, reflectivity
+  const float* mats;         // n_obj x kMatStride: kd rgb, ks rgb, shininess, reflectivity,
+                             // transparency, refractive index (eos_material)
   const float* lights;       // n_lights x 6: position xyz, colour rgb
   int32_t n_tris;
   int32_t n_obj;
   int32_t n_lights;
+  float ambient_index;       // refractive index outside transparent objects
 };
 
 struct DevBuffer {

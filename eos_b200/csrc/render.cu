@@ -26,13 +26,13 @@ struct PlainParams {
   unsigned long long* counts;  // kNumCounts traversal counters
 };
 
-// One path: colour with the reference's fold c_k = phong_k + refl_k * c_{k+1}.
+// One path: colour with the reference's fold c_k = phong_k + w_k c_{k+1} (fold_colour).
 template <int SH>
 __device__ f3 trace_path(const PlainParams& P, f3 o, f3 d, int32_t* hits, uint32_t* masks, unsigned* cnt,
                          uint2* shs, int stride) {
   const DevScene& s = P.s;
   f3 phong[kMaxBounces];
-  float refl[kMaxBounces];
+  float weight[kMaxBounces];
   int nb = 0;
   const f3 campos = mk3(P.cam[0], P.cam[1], P.cam[2]);
   for (int k = 0; k <= P.trace_depth; ++k) {
@@ -49,7 +49,7 @@ __device__ f3 trace_path(const PlainParams& P, f3 o, f3 d, int32_t* hits, uint32
     f3 Pp, N;
     int obj;
     hit_geometry(s, o, d, h, Pp, N, obj);
-    const float* m = s.mats + 8 * obj;
+    const float* m = s.mats + kMatStride * obj;
     f3 acc = mk3(0.0f, 0.0f, 0.0f);
     uint32_t mask = 0;
     for (int li = 0; li < s.n_lights; ++li) {
@@ -67,17 +67,14 @@ __device__ f3 trace_path(const PlainParams& P, f3 o, f3 d, int32_t* hits, uint32
     }
     masks[k] = mask;
     phong[k] = acc;
-    refl[k] = 0.0f;
     nb = k + 1;
-    float r = m[7];
-    if (!(r > 0.0f)) break;
-    refl[k] = r;
-    f3 rd = norm3(reflect3(d, N));
-    o = add3(Pp, scale3(kRayEps, rd));
+    f3 ro, rd;
+    if (!secondary_ray(m, s.ambient_index, d, Pp, N, ro, rd, weight[k])) break;
+    o = ro;
     d = rd;
   }
   f3 c = mk3(0.0f, 0.0f, 0.0f);
-  for (int k = nb - 1; k >= 0; --k) c = add3(phong[k], scale3(refl[k], c));
+  for (int k = nb - 1; k >= 0; --k) c = fold_colour(phong[k], weight[k], c);
   return c;
 }
 

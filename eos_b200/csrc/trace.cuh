@@ -480,6 +480,67 @@ __device__ __forceinline__ f3 phong_light(const float* m, const float* l, f3 P, 
   return diff;
 }
 
+// RayTracer::fresnel (src/RayTracer.cpp:52-64, after Bram de Greve 2006), in its float
+// order: reflectance of an interface n1 -> n2 for a unit incident direction and the normal
+// on the incident side; 1 under total internal reflection.
+__device__ __forceinline__ float fresnel(f3 incident, f3 normal, float n1, float n2) {
+  const float n = n1 / n2;
+  const float cos_i = -dot3(normal, incident);
+  const float sin_t2 = (n * n) * (1.0f - cos_i * cos_i);
+  if (sin_t2 > 1.0f) return 1.0f;
+  const float cos_t = sqrtf(1.0f - sin_t2);
+  const float r_orth = (n1 * cos_i - n2 * cos_t) / (n1 * cos_i + n2 * cos_t);
+  const float r_par = (n2 * cos_i - n1 * cos_t) / (n2 * cos_i + n1 * cos_t);
+  return (r_orth * r_orth + r_par * r_par) / 2.0f;
+}
+
+// Secondary ray of a hit with material m (RayTracer::shadeIntersection,
+// src/RayTracer.cpp:329-407).  Reflective: the mirror ray from P + 1e-3 R, weight =
+// reflectivity.  Transparent: the reference computes the Fresnel weight K and traces the
+// mirror ray about the incident-side normal from P + 1e-3 n -- twice, as "reflected" and,
+// by a slip at :403, again as "refracted" -- and mixes K c + (1 - K) c; the refracted ray
+// itself is never traced.  That ray once, with w = -K: the sign bit marks the mix.
+// Returns false when the material spawns no ray.
+__device__ __forceinline__ bool secondary_ray(const float* m, float ambient, f3 d, f3 P, f3 N, f3& ro, f3& rd,
+                                              float& w) {
+  if (m[7] > 0.0f) {
+    rd = norm3(reflect3(d, N));
+    ro = add3(P, scale3(kRayEps, rd));
+    w = m[7];
+    return true;
+  }
+  if (m[8] > 0.0f) {
+    const f3 inc = norm3(d);
+    f3 n = N;
+    float n1 = ambient, n2 = m[9];
+    if (!(dot3(inc, N) < 0.0f)) {  // leaving the material: normal flipped as 0 - N
+      n1 = m[9];
+      n2 = ambient;
+      n = sub3(mk3(0.0f, 0.0f, 0.0f), N);
+    }
+    const float K = fresnel(inc, n, n1, n2);
+    rd = norm3(reflect3(d, n));
+    ro = add3(P, scale3(kRayEps, n));
+    w = -K;
+    return true;
+  }
+  w = 0.0f;
+  return false;
+}
+
+// Colour fold of one bounce: phong + w c for a mirror (or no) bounce; for a transparent
+// one (sign bit of w set, K = -w) (phong + 0) + (K c + (1 - K) c) as the reference sums it.
+__device__ __forceinline__ f3 fold_colour(f3 phong, float w, f3 c) {
+  if (signbit(w)) {
+    const float K = -w, L = 1.0f - K;
+    return add3(phong, add3(scale3(K, c), scale3(L, c)));
+  }
+  return add3(phong, scale3(w, c));
+}
+
+// Weight of the next bounce's colour in the adjoint: d(fold)/dc.
+__device__ __forceinline__ float fold_weight(float w) { return signbit(w) ? (-w) + (1.0f - (-w)) : w; }
+
 // 8-bit quantisation of src/RayTracer.cpp:150-153: floor(c == 1 ? 255 : min(256 c, 255)).
 // 256*c, the min and the floor are exact in float, so the float form matches the
 // reference's double arithmetic bit for bit.

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;
   int* ctr = A.ctr + A.k * kCtr;
-  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // mirror rays of bounce k-1
+  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // secondary rays of bounce k-1
   const int lane = threadIdx.x & 31;
   unsigned nrays = 0, nshadow = 0, nhits = 0;
   unsigned long long nodes = 0, tests = 0;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
       bool valid = i < end;
       bool hit = false, refl = false;
       int path = -1, jb = 0, obj = -1;
-      f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1), P = o, N = o;
+      f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1), P = o, N = o, ro = o, rd = d;
       if (valid) {
         if (PRIMARY) {
           long long gp = A.c0 + i;
@@ -179,7 +179,10 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
         }
         if (hit) {
           hit_geometry(J.s, o, d, h, P, N, obj);
-          refl = J.s.mats[8 * obj + 7] > 0.0f && A.k < J.trace_depth;
+          float w;
+          refl = secondary_ray(J.s.mats + kMatStride * obj, J.s.ambient_index, d, P, N, ro, rd, w);
+          reinterpret_cast<float*>(A.acc + (size_t)path * (A.depth + 1) + A.k)[3] = w;
+          refl = refl && A.k < J.trace_depth;
         }
         HitQ hq;
         hq.a = make_float4(P.x, P.y, P.z, __int_as_float(path));
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
         }
         nshadow += nl;
       }
-      // mirror rays
+      // secondary rays (mirror, or the transparent bounce's ray)
       uint32_t rb = __ballot_sync(0xffffffffu, refl);
       if (rb) {
         int rbase = 0;
@@ -227,8 +230,6 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
           if (pos >= A.cap_r) {
             atomicOr(A.err, kErrQueue);
           } else {
-            f3 rd = norm3(reflect3(d, N));
-            f3 ro = add3(P, scale3(kRayEps, rd));
             RayQ r;
             r.a = make_float4(ro.x, ro.y, ro.z, __int_as_float(path));
             r.b = make_float4(rd.x, rd.y, rd.z, 0.0f);
@@ -247,15 +248,15 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
 
 // Emits the results of lanes whose nearest-hit ray has ended (`pending`): path record, hit
 // record, one shadow ray per light (compacted light-major inside the warp's block of the
-// queue, so a warp of the any-hit kernel mostly traces towards one light) and the mirror
-// ray (ballot / popc compaction, one atomic per warp).  Warp-uniform: every lane calls it.
+// queue, so a warp of the any-hit kernel mostly traces towards one light) and the
+// secondary ray (ballot / popc compaction, one atomic per warp).  Warp-uniform: every lane calls it.
 __device__ __forceinline__ void emit_results(const WfArgs& A, int* ctr, bool pending, int i, int path, int jb,
                                              const Hit& h, f3 o, f3 d, unsigned& nshadow, unsigned& nhits) {
   const int lane = threadIdx.x & 31;
   const DevJob& J = A.jobs[jb];
   bool hit = pending && h.pos >= 0;
   bool refl = false;
-  f3 P = mk3(0, 0, 0), N = P;
+  f3 P = mk3(0, 0, 0), N = P, ro = P, rd = P;
   int obj = -1;
   if (pending) {
     nhits += hit;
@@ -266,7 +267,10 @@ __device__ __forceinline__ void emit_results(const WfArgs& A, int* ctr, bool pen
     }
     if (hit) {
       hit_geometry(J.s, o, d, h, P, N, obj);
-      refl = J.s.mats[8 * obj + 7] > 0.0f && A.k < J.trace_depth;
+      float w;
+      refl = secondary_ray(J.s.mats + kMatStride * obj, J.s.ambient_index, d, P, N, ro, rd, w);
+      reinterpret_cast<float*>(A.acc + (size_t)path * (A.depth + 1) + A.k)[3] = w;
+      refl = refl && A.k < J.trace_depth;
     }
     HitQ hq;
     hq.a = make_float4(P.x, P.y, P.z, __int_as_float(path));
@@ -311,8 +315,6 @@ __device__ __forceinline__ void emit_results(const WfArgs& A, int* ctr, bool pen
       if (pos >= A.cap_r) {
         atomicOr(A.err, kErrQueue);
       } else {
-        f3 rd = norm3(reflect3(d, N));
-        f3 ro = add3(P, scale3(kRayEps, rd));
         RayQ r;
         r.a = make_float4(ro.x, ro.y, ro.z, __int_as_float(path));
         r.b = make_float4(rd.x, rd.y, rd.z, 0.0f);
@@ -345,7 +347,7 @@ template <bool PRIMARY, int SH>
 __global__ void k_wf_closest_refill(WfArgs A) {
   extern __shared__ uint2 shstack[];
   int* ctr = A.ctr + A.k * kCtr;
-  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // mirror rays of bounce k-1
+  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // secondary rays of bounce k-1
   const int lane = threadIdx.x & 31;
   RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
   TravScene ts{nullptr, nullptr};
@@ -513,13 +515,13 @@ __global__ void k_wf_shade(WfArgs A) {
     if (obj < 0) continue;
     f3 P = mk3(hq.a.x, hq.a.y, hq.a.z), N = mk3(hq.b.x, hq.b.y, hq.b.z);
     f3 cam = mk3(J.cam[0], J.cam[1], J.cam[2]);
-    const float* m = J.s.mats + 8 * obj;
+    const float* m = J.s.mats + kMatStride * obj;
     uint32_t mask = A.masks[i];
     f3 acc = mk3(0, 0, 0);
     for (int l = 0; l < J.s.n_lights; ++l)
       if (!(mask & (1u << l))) acc = add3(acc, phong_light(m, J.s.lights + 6 * l, P, N, cam));
-    float r = m[7] > 0.0f ? m[7] : 0.0f;
-    A.acc[(size_t)path * (A.depth + 1) + A.k] = make_float4(acc.x, acc.y, acc.z, r);
+    float4* e = A.acc + (size_t)path * (A.depth + 1) + A.k;  // .w: the bounce weight, set by the hit stage
+    *e = make_float4(acc.x, acc.y, acc.z, e->w);
     if (J.paths) {
       int x, y, smp;
       path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
@@ -562,7 +564,7 @@ __global__ void k_wf_resolve(WfArgs A) {
       f3 c = mk3(0, 0, 0);
       for (int k = A.depth; k >= 0; --k) {
         float4 e = a[k];
-        c = add3(mk3(e.x, e.y, e.z), scale3(e.w, c));
+        c = fold_colour(mk3(e.x, e.y, e.z), e.w, c);
       }
       sum = add3(sum, c);
     }

@@ -12,7 +12,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib as L
-from .scenes import LIGHT_STRIDE, MAT_STRIDE, SceneData
+from .scenes import LIGHT_STRIDE, SceneData, pad_materials
 
 
 @dataclass
@@ -81,7 +81,7 @@ def scene_from_meshes(meshes: list[MeshData], materials, lights, name: str = "me
         tris.append(m.tris.astype(np.int64) + base)
         obj.append(np.full(m.n_tris, k, np.uint32))
         base += m.verts.shape[0]
-    mats = np.asarray(materials, np.float32).reshape(-1, MAT_STRIDE)
+    mats = pad_materials(materials)
     if mats.shape[0] < len(meshes):
         raise ValueError("one material row per mesh")
     return SceneData(np.concatenate(verts), np.concatenate(normals), np.concatenate(tris).astype(np.uint32),

@@ -24,8 +24,20 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-MAT_STRIDE = 8
+MAT_STRIDE = 10  # kd rgb, ks rgb, shininess, reflectivity, transparency, refractive index
 LIGHT_STRIDE = 6
+
+
+def pad_materials(mats) -> np.ndarray:
+    """Material rows as float32 [K, 10]; rows of 8 (no transparency columns) get
+    transparency 0 and refractive index 1."""
+    m = np.asarray(mats, dtype=np.float32)
+    m = m.reshape(-1, m.shape[-1]) if m.ndim > 1 else m.reshape(1, -1) if m.size else m.reshape(0, MAT_STRIDE)
+    if m.shape[1] == 8:
+        m = np.concatenate([m, np.zeros((m.shape[0], 1), np.float32), np.ones((m.shape[0], 1), np.float32)], 1)
+    if m.shape[1] != MAT_STRIDE:
+        raise ValueError(f"material rows have {m.shape[1]} values, expected 8 or {MAT_STRIDE}")
+    return np.ascontiguousarray(m)
 
 
 def rng_for(seed: int) -> np.random.Generator:
@@ -41,13 +53,14 @@ class SceneData:
     materials: np.ndarray
     lights: np.ndarray
     name: str = "scene"
+    ambient_index: float = 1.0  # refractive index outside transparent objects
 
     def __post_init__(self):
         self.verts = np.ascontiguousarray(self.verts, dtype=np.float32).reshape(-1, 3)
         self.normals = np.ascontiguousarray(self.normals, dtype=np.float32).reshape(-1, 3)
         self.tris = np.ascontiguousarray(self.tris, dtype=np.uint32).reshape(-1, 3)
         self.tri_obj = np.ascontiguousarray(self.tri_obj, dtype=np.uint32).reshape(-1)
-        self.materials = np.ascontiguousarray(self.materials, dtype=np.float32).reshape(-1, MAT_STRIDE)
+        self.materials = pad_materials(self.materials)
         self.lights = np.ascontiguousarray(self.lights, dtype=np.float32).reshape(-1, LIGHT_STRIDE)
 
     @property
@@ -249,9 +262,9 @@ class _Builder:
                          np.asarray(lights, np.float64), name)
 
 
-def material(kd, ks, shininess, reflectivity):
+def material(kd, ks, shininess, reflectivity, transparency=0.0, refractive_index=1.0):
     ks = np.broadcast_to(np.asarray(ks, np.float64), (3,))
-    return [*kd, *ks, float(shininess), float(reflectivity)]
+    return [*kd, *ks, float(shininess), float(reflectivity), float(transparency), float(refractive_index)]
 
 
 def add_sphere(b: _Builder, level: int, center, radius: float, rot, mat):
@@ -414,13 +427,20 @@ def config5_camera(width=3840, height=2160) -> CameraData:
 
 
 def small_random_scene(seed: int, n_spheres: int = 4, level: int = 2, lights: int = 2,
-                       refl: float = 0.5) -> SceneData:
-    """A few icospheres over a quad: quick scenes for parity edge cases."""
+                       refl: float = 0.5, transparent: int = 0, ambient_index: float = 1.0) -> SceneData:
+    """A few icospheres over a quad: quick scenes for parity edge cases.  The first
+    `transparent` spheres get non-reflective transparent materials (refractive index
+    1.333, 1.52 or 2.42 in turn)."""
     rng = rng_for(seed)
     b = _Builder()
-    for _ in range(n_spheres):
-        add_sphere(b, level, rng.uniform(-2, 2, 3), rng.uniform(0.3, 1.2), random_rotation(rng),
-                   _random_material(rng, refl))
+    for k in range(n_spheres):
+        center, radius, rot = rng.uniform(-2, 2, 3), rng.uniform(0.3, 1.2), random_rotation(rng)
+        m = _random_material(rng, refl)
+        if k < transparent:
+            m[7], m[8], m[9] = 0.0, 1.0, (1.333, 1.52, 2.42)[k % 3]
+        add_sphere(b, level, center, radius, rot, m)
     b.add(*ground_quad(6.0, -2.5), _random_material(rng, refl))
     ls = [[*rng.uniform([-5, 3, -5], [5, 8, 5]), 1, 1, 1] for _ in range(lights)]
-    return b.build(ls, f"small{seed}")
+    sc = b.build(ls, f"small{seed}")
+    sc.ambient_index = float(ambient_index)
+    return sc

@@ -147,6 +147,8 @@ class Material {
     m.ks[0] = m_Specular.x; m.ks[1] = m_Specular.y; m.ks[2] = m_Specular.z;
     m.shininess = (float)m_Shininess;
     m.reflectivity = m_Reflective ? m_ReflectionIntensity : 0.0f;
+    m.transparency = m_Transparent ? 1.0f : 0.0f;
+    m.refractive_index = m_RefractiveIndex;
     return m;
   }
 
@@ -435,6 +437,7 @@ inline cudaScene_t* createCudaScene(Scene* scene, eos_ctx* ctx = nullptr) {
                          mats.data(), (uint32_t)mats.size(), lights.data(), (uint32_t)lights.size(), nullptr,
                          &cs->scene),
         "createCudaScene");
+  check(eos_scene_set_ambient_index(cs->scene, scene->getAmbientRefractiveIndex()), "createCudaScene");
   return cs.release();
 }
 

@@ -17,6 +17,7 @@
  *                                src/cudaStructures.cu:407-481)
  *   eos_scene_set_lights         Scene::addLightSource + copyLights (src/Scene.cpp:77-83,
  *                                src/cudaStructures.cu:177-218)
+ *   eos_scene_set_ambient_index  Scene::setAmbientRefractiveIndex (src/Scene.cpp:134-136)
  *   eos_render                   DeviceRenderer::renderCudaSceneToHostBufferMegaKernel and
  *                                the C wrapper rayTrace_MegaKernel (src/DeviceRenderer.cu:61-109,
  *                                src/kernelWrapper.h:30), with the CPU RayTracer's full
@@ -65,13 +66,19 @@ typedef struct eos_ctx eos_ctx;
 typedef struct eos_scene eos_scene;
 
 /* Material of one object (src/Material.h:46-78).  The reference's diffuse/specular are
- * vec4 with an unused alpha and its shininess is an int; reflective = reflectivity > 0.
- * The ambient term is unused by the reference renderer (src/RayTracer.cpp:412-413). */
+ * vec4 with an unused alpha and its shininess is an int; reflective = reflectivity > 0,
+ * transparent = transparency > 0 (the reference's m_Transparent flag; its value is not
+ * used otherwise).  A material may be reflective or transparent, not both
+ * (EOS_ERR_UNSUPPORTED): the reference traces two secondary rays for such a hit and the
+ * path record holds one per bounce.  The ambient term is unused by the reference renderer
+ * (src/RayTracer.cpp:412-413). */
 typedef struct eos_material {
   float kd[3];
   float ks[3];
   float shininess;
   float reflectivity;
+  float transparency;
+  float refractive_index;
 } eos_material;
 
 /* Point light (src/LightSource.h:27-39); the position's w is 1. */
@@ -230,6 +237,9 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
 eos_status eos_scene_destroy(eos_scene* scene);
 eos_status eos_scene_set_materials(eos_scene* scene, const eos_material* materials, uint32_t n);
 eos_status eos_scene_set_lights(eos_scene* scene, const eos_light* lights, uint32_t n);
+/* Scene::setAmbientRefractiveIndex (src/Scene.cpp:134-136): the index outside every
+ * transparent object; 1 when never set. */
+eos_status eos_scene_set_ambient_index(eos_scene* scene, float refractive_index);
 eos_status eos_scene_get_info(const eos_scene* scene, eos_scene_info* info);
 /* Test hook: Morton codes of the triangles in sorted order and the sorted triangle ids. */
 eos_status eos_scene_get_morton(const eos_scene* scene, uint32_t* codes, uint32_t* order);

@@ -59,6 +59,7 @@ def lib_oracle():
                                           POINTER(c_uint32), c_int, POINTER(c_float), c_int,
                                           POINTER(c_float), c_int]
         L.oracle_scene_destroy.argtypes = [c_void_p]
+        L.oracle_scene_set_ambient.argtypes = [c_void_p, c_float]
         L.oracle_render.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
                                     c_uint32, POINTER(c_int32), c_int, c_int, POINTER(c_float),
                                     POINTER(c_int32), POINTER(c_uint32), POINTER(c_uint32),
@@ -91,6 +92,7 @@ def lib_ref():
                                           POINTER(c_uint32), c_int, POINTER(c_float), c_int,
                                           POINTER(c_float), c_int, c_int, POINTER(c_double)]
         L.eosref_scene_destroy.argtypes = [c_void_p]
+        L.eosref_scene_set_ambient.argtypes = [c_void_p, c_float]
         L.eosref_scene_stats.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int)]
         L.eosref_render.restype = c_int
         L.eosref_render.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
@@ -149,6 +151,7 @@ class Oracle:
         self.scene = scene
         self._keep = scene
         self.h = lib_oracle().oracle_scene_create(*_scene_args(scene))
+        lib_oracle().oracle_scene_set_ambient(self.h, float(getattr(scene, "ambient_index", 1.0)))
 
     def __del__(self):
         if getattr(self, "h", None) and _lib_oracle is not None:
@@ -198,7 +201,8 @@ class Oracle:
                    light_params, g=None, nthreads=None):
         """FP64 re-render with frozen visibility; with g, also the adjoint of <g, rgb>.
 
-        mat_params: [K, 8] kd rgb, ks rgb, log shininess, reflectivity (float64)
+        mat_params: [K, 10] kd rgb, ks rgb, log shininess, reflectivity, transparency, refractive
+        index (float64; rows of 8 are opaque)
         light_params: [L, 6] position xyz, colour rgb (float64)
         Returns rgb [V*H*W, 3] and, with g, (grad_mat [K, 7], grad_light [L, 6]).
         """
@@ -208,7 +212,10 @@ class Oracle:
         npx = nv * width * height
         h = np.ascontiguousarray(hits, np.int32).reshape(npx, MAXB)
         s = np.ascontiguousarray(shadows, np.uint32).reshape(npx, MAXB)
-        mp = np.ascontiguousarray(mat_params, np.float64)
+        mp = np.asarray(mat_params, np.float64)
+        if mp.shape[1] == 8:  # no transparency columns: opaque, index 1
+            mp = np.concatenate([mp, np.zeros((mp.shape[0], 1)), np.ones((mp.shape[0], 1))], 1)
+        mp = np.ascontiguousarray(mp)
         lp = np.ascontiguousarray(light_params, np.float64)
         rgb = np.zeros((npx, 3), np.float64)
         gm = np.zeros((mp.shape[0], 7), np.float64)
@@ -231,6 +238,7 @@ class RefRenderer:
         self.scene = scene
         secs = c_double(0.0)
         self.h = L.eosref_scene_create(*_scene_args(scene), build_threads, ctypes.byref(secs))
+        L.eosref_scene_set_ambient(self.h, float(getattr(scene, "ambient_index", 1.0)))
         self.build_seconds = secs.value
         nn, ml = c_int(0), c_int(0)
         L.eosref_scene_stats(self.h, ctypes.byref(nn), ctypes.byref(ml))

@@ -64,6 +64,9 @@ static inline v3f vcross(v3f a, v3f b) {
 static inline v3f vnorm(v3f a) { float s = 1.0f / sqrtf(vdot(a, a)); return V3(a.x * s, a.y * s, a.z * s); }
 static inline float fget(v3f a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 
+/* Material record: kd rgb, ks rgb, shininess, reflectivity, transparency, refractive index. */
+#define OMAT 10
+
 typedef struct {
   float lo[3], hi[3];
   int left, right;   /* children (interior) */
@@ -75,7 +78,8 @@ typedef struct {
   v3f *v1, *v2, *v3, *e1, *e2, *n1, *n2, *n3; /* sorted (Morton) order */
   int32_t *id;                                 /* sorted position -> triangle id */
   uint32_t *obj;                               /* sorted position -> object */
-  float *mats;                                 /* nobj x 8 */
+  float *mats;                                 /* nobj x OMAT (eos_material) */
+  float ambient;                               /* refractive index outside objects */
   float *lights;                               /* nl x 6 */
   onode *nodes;
   int nnodes;
@@ -202,8 +206,9 @@ void* oracle_scene_create(const float* verts, const float* normals, int nv, cons
     s->pos_of_id[i] = p;
   }
   free(codes); free(order);
-  s->mats = malloc(sizeof(float) * 8 * (size_t)(nobj > 0 ? nobj : 1));
-  memcpy(s->mats, mats, sizeof(float) * 8 * (size_t)nobj);
+  s->mats = malloc(sizeof(float) * OMAT * (size_t)(nobj > 0 ? nobj : 1));
+  memcpy(s->mats, mats, sizeof(float) * OMAT * (size_t)nobj);
+  s->ambient = 1.0f;
   s->lights = malloc(sizeof(float) * 6 * (size_t)(nl > 0 ? nl : 1));
   memcpy(s->lights, lights, sizeof(float) * 6 * (size_t)nl);
   s->nodes = malloc(sizeof(onode) * (2 * n + 1));
@@ -211,6 +216,9 @@ void* oracle_scene_create(const float* verts, const float* normals, int nv, cons
   if (nt > 0) build_rec(s, 0, nt);
   return s;
 }
+
+/* Scene::setAmbientRefractiveIndex (src/Scene.cpp:134-136). */
+void oracle_scene_set_ambient(void* h, float ambient) { ((oscene*)h)->ambient = ambient; }
 
 void oracle_scene_destroy(void* h) {
   oscene* s = (oscene*)h;
@@ -390,12 +398,63 @@ static inline v3f phong_one(const float* m, const float* l, v3f P, v3f N, v3f ca
   return diff;
 }
 
+/* RayTracer::fresnel (src/RayTracer.cpp:52-64). */
+static inline float fresnel_f(v3f incident, v3f normal, float n1, float n2) {
+  float n = n1 / n2;
+  float cos_i = -vdot(normal, incident);
+  float sin_t2 = (n * n) * (1.0f - cos_i * cos_i);
+  if (sin_t2 > 1.0f) return 1.0f;
+  float cos_t = sqrtf(1.0f - sin_t2);
+  float r_orth = (n1 * cos_i - n2 * cos_t) / (n1 * cos_i + n2 * cos_t);
+  float r_par = (n2 * cos_i - n1 * cos_t) / (n2 * cos_i + n1 * cos_t);
+  return (r_orth * r_orth + r_par * r_par) / 2.0f;
+}
+
+static inline v3f reflect_f(v3f d, v3f n) {
+  float dn = vdot(n, d);
+  return V3(d.x - ((n.x * dn) * 2.0f), d.y - ((n.y * dn) * 2.0f), d.z - ((n.z * dn) * 2.0f));
+}
+
+/* The secondary ray of a hit (RayTracer::shadeIntersection, src/RayTracer.cpp:329-407):
+ * reflective -> mirror ray from P + 1e-3 R, weight = reflectivity; transparent -> the
+ * reference traces the mirror ray about the incident-side normal from P + 1e-3 n twice
+ * (:401 and, instead of the refracted ray, :403) and mixes K c + (1 - K) c with the
+ * Fresnel K; *K_out = K, *transp = 1 then.  Returns 0 when no ray is spawned. */
+static inline int secondary_f(const float* m, float ambient, v3f d, v3f P, v3f N, v3f* ro, v3f* rd, float* w,
+                              int* transp) {
+  const float eps = 1e-3f;
+  *transp = 0;
+  if (m[7] > 0.0f) {
+    *rd = vnorm(reflect_f(d, N));
+    *ro = vadd(P, vscale(eps, *rd));
+    *w = m[7];
+    return 1;
+  }
+  if (m[8] > 0.0f) {
+    v3f inc = vnorm(d);
+    v3f n = N;
+    float n1 = ambient, n2 = m[9];
+    if (!(vdot(inc, N) < 0.0f)) {
+      n1 = m[9];
+      n2 = ambient;
+      n = vsub(V3(0.0f, 0.0f, 0.0f), N);
+    }
+    *w = fresnel_f(inc, n, n1, n2);
+    *rd = vnorm(reflect_f(d, n));
+    *ro = vadd(P, vscale(eps, n));
+    *transp = 1;
+    return 1;
+  }
+  return 0;
+}
+
 typedef struct { long long prim, shadow, second; } counts_t;
 
 static v3f trace_path(const oscene* s, const float* cam, v3f o, v3f d, int trace_depth, int32_t* hits,
                       uint32_t* shadows, uint32_t* flags, counts_t* cnt) {
   v3f phong[MAXB];
-  float refl[MAXB];
+  float wgt[MAXB];
+  int transp[MAXB];
   int nb = 0;
   v3f campos = V3(cam[0], cam[1], cam[2]);
   const float eps = 1e-3f;
@@ -410,7 +469,7 @@ static v3f trace_path(const oscene* s, const float* cam, v3f o, v3f d, int trace
     if (h.t < 1e-3f || h.t > 999.0f) *flags |= FLAG_OUT_OF_RANGE;
     v3f P, N;
     hit_geometry(s, h.pos, o, d, h.t, h.u, h.v, &P, &N);
-    const float* m = s->mats + 8 * s->obj[h.pos];
+    const float* m = s->mats + OMAT * s->obj[h.pos];
     v3f acc = V3(0, 0, 0);
     uint32_t mask = 0;
     for (int li = 0; li < s->nl; ++li) {
@@ -430,19 +489,25 @@ static v3f trace_path(const oscene* s, const float* cam, v3f o, v3f d, int trace
     }
     shadows[k] = mask;
     phong[k] = acc;
-    refl[k] = 0.0f;
+    wgt[k] = 0.0f;
+    transp[k] = 0;
     nb = k + 1;
-    if (!(m[7] > 0.0f)) break;
-    refl[k] = m[7];
-    float dn = vdot(N, d);
-    v3f r = V3(d.x - ((N.x * dn) * 2.0f), d.y - ((N.y * dn) * 2.0f), d.z - ((N.z * dn) * 2.0f));
-    v3f rd = vnorm(r);
-    o = vadd(P, vscale(eps, rd));
+    v3f ro, rd;
+    if (!secondary_f(m, s->ambient, d, P, N, &ro, &rd, &wgt[k], &transp[k])) break;
+    o = ro;
     d = rd;
   }
-  /* c_k = phong_k + refl_k * c_{k+1} (src/RayTracer.cpp:356-357,410) */
+  /* c_k = (phong_k + refl_k c_{k+1}) + 0 for a mirror bounce, (phong_k + 0) +
+   * (K c_{k+1} + (1 - K) c_{k+1}) for a transparent one (src/RayTracer.cpp:356-357,405,410) */
   v3f c = V3(0, 0, 0);
-  for (int k = nb - 1; k >= 0; --k) c = vadd(phong[k], vscale(refl[k], c));
+  for (int k = nb - 1; k >= 0; --k) {
+    if (transp[k]) {
+      float K = wgt[k], L1 = 1.0f - K;
+      c = vadd(phong[k], vadd(vscale(K, c), vscale(L1, c)));
+    } else {
+      c = vadd(phong[k], vscale(wgt[k], c));
+    }
+  }
   return c;
 }
 
@@ -532,12 +597,13 @@ static inline double dlen(v3d a) { return sqrt(ddot(a, a)); }
 static inline v3d dnorm(v3d a) { return dsc(1.0 / dlen(a), a); }
 static inline v3d f2d(v3f a) { return D3(a.x, a.y, a.z); }
 
-/* Parameters: per object [kd r,g,b, ks r,g,b, log shininess, reflectivity] (8 doubles),
+/* Parameters: per object [kd r,g,b, ks r,g,b, log shininess, reflectivity, transparency,
+ * refractive index] (OMAT doubles),
  * per light [position xyz, colour rgb] (6 doubles).  Gradients: per object
  * [kd rgb, ks rgb, log shininess] (7), per light [colour rgb, position xyz] (6). */
 typedef struct {
   const oscene* s;
-  const double* mp;  /* nobj x 8 */
+  const double* mp;  /* nobj x OMAT */
   const double* lp;  /* nl x 6 */
 } f64ctx;
 
@@ -568,7 +634,7 @@ static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, in
     v3d P = dadd(o, dsc(t, d));
     v3d N = dnorm(dadd(dadd(dsc(1.0 - u - v, f2d(s->n1[p])), dsc(u, f2d(s->n2[p]))), dsc(v, f2d(s->n3[p]))));
     int ob = (int)s->obj[p];
-    const double* m = c->mp + 8 * ob;
+    const double* m = c->mp + OMAT * ob;
     double shin = exp(m[6]);
     v3d V = dnorm(dsub(campos, P));
     for (int li = 0; li < s->nl; ++li) {
@@ -618,13 +684,21 @@ static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, in
       }
       glo[3] += gp.x; glo[4] += gp.y; glo[5] += gp.z;
     }
-    double refl = m[7];
-    if (!(refl > 0.0) || k + 1 > trace_depth) break;
-    T *= refl;
-    v3d r = dsub(d, dsc(2.0 * ddot(N, d), N));
-    v3d rd = dnorm(r);
-    o = dadd(P, dsc(1e-3, rd));
-    d = rd;
+    if (k + 1 > trace_depth) break;
+    if (m[7] > 0.0) {
+      T *= m[7];
+      v3d rd = dnorm(dsub(d, dsc(2.0 * ddot(N, d), N)));
+      o = dadd(P, dsc(1e-3, rd));
+      d = rd;
+    } else if (m[8] > 0.0) {
+      /* transparent: the Fresnel mix K c + (1 - K) c of one colour, weight 1 */
+      v3d n = ddot(dnorm(d), N) < 0.0 ? N : dsc(-1.0, N);
+      v3d rd = dnorm(dsub(d, dsc(2.0 * ddot(n, d), n)));
+      o = dadd(P, dsc(1e-3, n));
+      d = rd;
+    } else {
+      break;
+    }
   }
   return col;
 }

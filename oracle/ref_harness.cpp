@@ -120,11 +120,22 @@ void replay_path(const RefScene& rs, Ray ray, int trace_depth, int32_t* hits,
     }
     shadows[depth] = mask;
     const Material& m = scene.getMaterialAtIndex(id);
-    if (!m.isReflective()) return;
-    glm::vec3 rd = glm::normalize(glm::reflect(ray.getDirection(), isect.getNormal()));
-    glm::vec3 ro = P + epsilon * rd;
-    ray.setOrigin(ro);
-    ray.setDirection(rd);
+    if (m.isReflective()) {  // src/RayTracer.cpp:339-351
+      glm::vec3 rd = glm::normalize(glm::reflect(ray.getDirection(), isect.getNormal()));
+      glm::vec3 ro = P + epsilon * rd;
+      ray.setOrigin(ro);
+      ray.setDirection(rd);
+    } else if (m.isTransparent()) {  // src/RayTracer.cpp:353-407: the reflected ray, traced twice
+      glm::vec3 incident = glm::normalize(ray.getDirection());
+      glm::vec3 n = isect.getNormal();
+      if (!(glm::dot(incident, n) < 0.0f)) n = glm::vec3(0.0f) - isect.getNormal();
+      glm::vec3 rd = glm::normalize(glm::reflect(ray.getDirection(), n));
+      glm::vec3 ro = P + epsilon * n;
+      ray.setOrigin(ro);
+      ray.setDirection(rd);
+    } else {
+      return;
+    }
   }
 }
 
@@ -141,14 +152,15 @@ void* eosref_scene_create(const float* verts, const float* normals, int nv, cons
   (void)nv;
   RefScene* rs = new RefScene();
   rs->object_materials.resize(nobj);
+  // materials: kd rgb, ks rgb, shininess, reflectivity, transparency, refractive index
   for (int k = 0; k < nobj; ++k) {
-    const float* m = mats + 8 * k;
+    const float* m = mats + 10 * k;
     Material mat(0.0f, glm::vec4(m[0], m[1], m[2], 1.0f), glm::vec4(m[3], m[4], m[5], 1.0f),
                  (int)m[6]);
     mat.setReflective(m[7] > 0.0f);
     mat.setReflectionIntensity(m[7]);
-    mat.setTransparent(false);
-    mat.setRefractiveIndex(1.0f);
+    mat.setTransparent(m[8] > 0.0f);
+    mat.setRefractiveIndex(m[9]);
     rs->object_materials[k] = mat;
   }
   rs->scene.setMaxTracedDepth(8);
@@ -193,6 +205,10 @@ void* eosref_scene_create(const float* verts, const float* normals, int nv, cons
   for (int i = 0; i < rs->n_nodes; ++i)
     if (nodes[i].type == BVH_LEAF) rs->max_leaf = std::max(rs->max_leaf, nodes[i].numSurfacesEncapulated);
   return rs;
+}
+
+void eosref_scene_set_ambient(void* h, float ambient) {
+  ((RefScene*)h)->scene.setAmbientRefractiveIndex(ambient);
 }
 
 void eosref_scene_stats(void* h, int* n_nodes, int* max_leaf) {

@@ -1,7 +1,7 @@
 """Thin torch.autograd.Function over eos_render / eos_render_backward (tests only).
 
-Parameters are torch tensors: materials [K, 8] (kd rgb, ks rgb, log shininess,
-reflectivity) and lights [L, 6] (position, colour).  Forward renders the views with the
+Parameters are torch tensors: materials [K, 8] or [K, 10] (kd rgb, ks rgb, log shininess,
+reflectivity[, transparency, refractive index]) and lights [L, 6] (position, colour).  Forward renders the views with the
 plain renderer and keeps the path records; backward replays them with visibility frozen.
 """
 import torch
@@ -23,6 +23,7 @@ class EosRender(torch.autograd.Function):
             paths.append(r["paths"])
         fctx.save_for_backward(torch.cat(paths))
         fctx.rctx, fctx.dscene, fctx.cams, fctx.td = rctx, dscene, cams, trace_depth
+        fctx.mat_shape = tuple(mat_params.shape)
         return torch.stack(imgs)
 
     @staticmethod
@@ -30,6 +31,6 @@ class EosRender(torch.autograd.Function):
         (paths,) = fctx.saved_tensors
         gm, gl = api.render_backward(fctx.rctx, fctx.dscene, fctx.cams, fctx.td, paths,
                                      grad_img.contiguous().float().reshape(-1, 3), pixel_offset=0.5)
-        gmat = torch.zeros((gm.shape[0], 8), device=gm.device, dtype=torch.float32)
+        gmat = torch.zeros(fctx.mat_shape, device=gm.device, dtype=torch.float32)
         gmat[:, :7] = gm
         return gmat, gl, None, None, None, None

@@ -5,8 +5,8 @@
 //   facade_render <scene.bin> <out_device_renderer.rgba> <out_raytracer.rgba>
 //
 // scene.bin: int32 n_verts, n_tris, n_mats, n_lights, width, height, trace_depth;
-// float32 verts[3n], normals[3n]; uint32 tris[3m], tri_obj[m]; float32 mats[8k],
-// lights[6l], camera[12].
+// float32 verts[3n], normals[3n]; uint32 tris[3m], tri_obj[m]; float32 mats[10k] (kd rgb,
+// ks rgb, shininess, reflectivity, transparency, refractive index), lights[6l], camera[12].
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
@@ -33,7 +33,7 @@ int main(int argc, char** argv) {
   std::vector<float> verts, normals, mats, lights, cam;
   std::vector<uint32_t> tris, obj;
   bool ok = read_n(f, verts, 3 * nv) && read_n(f, normals, 3 * nv) && read_n(f, tris, 3 * nt) && read_n(f, obj, nt) &&
-            read_n(f, mats, 8 * nm) && read_n(f, lights, 6 * nl) && read_n(f, cam, 12);
+            read_n(f, mats, 10 * nm) && read_n(f, lights, 6 * nl) && read_n(f, cam, 12);
   fclose(f);
   if (!ok) return 2;
 
@@ -42,11 +42,12 @@ int main(int argc, char** argv) {
     scene.useBvh(true);
     scene.setAmbientRefractiveIndex(1.0f);
     for (int k = 0; k < nm; ++k) {
-      const float* m = &mats[8 * k];
+      const float* m = &mats[10 * k];
       eos::Material mat(0.0f, eos::vec4(m[0], m[1], m[2], 1.0f), eos::vec4(m[3], m[4], m[5], 1.0f), (int)m[6]);
       mat.setReflective(m[7] > 0.0f);
       mat.setReflectionIntensity(m[7]);
-      mat.setTransparent(false);
+      mat.setTransparent(m[8] > 0.0f);
+      mat.setRefractiveIndex(m[9]);
       scene.addMaterial(mat);
     }
     std::vector<std::unique_ptr<eos::Triangle>> owned;

@@ -54,6 +54,9 @@ def main():
         sc = scenes.small_random_scene(seed, n_spheres=5, level=2, lights=3, refl=0.6)
         cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 96, 72)
         render_case(f"small{seed}", sc, cam, 3)
+    # transparent spheres (Fresnel-mixed secondary rays) in air
+    sc = scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3, ambient_index=1.0002)
+    render_case("transp61", sc, scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 96, 72), 4)
 
 
 if __name__ == "__main__":

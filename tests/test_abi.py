@@ -29,7 +29,7 @@ def test_library_exports_every_header_symbol():
 
 
 def test_struct_layouts_match_header():
-    assert ctypes.sizeof(L.Material) == 32
+    assert ctypes.sizeof(L.Material) == 40
     assert ctypes.sizeof(L.Light) == 24
     assert ctypes.sizeof(L.Camera) == 56
     assert ctypes.sizeof(L.RenderParams) == 36

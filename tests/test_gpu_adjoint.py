@@ -16,11 +16,15 @@ def _rel_close(a, b, rel=1e-3):
     return np.abs(a - b).max() <= rel * max(scale, 1e-12), (np.abs(a - b).max(), scale)
 
 
-@pytest.mark.parametrize("td", [1, 2])
-def test_backward_matches_fp64_adjoint(ctx, td):
+@pytest.mark.parametrize("td,transparent", [(1, False), (2, False), (2, True)])
+def test_backward_matches_fp64_adjoint(ctx, td, transparent):
     import torch
     sc = scenes.config4_scene()
     sc.materials[:, 7] = 0.3  # mirror bounces so reflected shading is differentiated too
+    if transparent:  # every third object transparent: Fresnel-mixed secondary rays
+        sc.materials[::3, 7] = 0.0
+        sc.materials[::3, 8] = 1.0
+        sc.materials[::3, 9] = 1.52
     dsc = api.DeviceScene(ctx, sc)
     cams = scenes.config4_cameras(2, 64)
     paths, rgb = [], []

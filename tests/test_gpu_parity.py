@@ -88,6 +88,8 @@ def test_plain_matches_compiled_reference_config1(ctx, c1):
     ("config1_128", lambda: scenes.config1_scene()),
     ("small11", lambda: scenes.small_random_scene(11, n_spheres=5, level=2, lights=3, refl=0.6)),
     ("small12", lambda: scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)),
+    ("transp61", lambda: scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3,
+                                                   ambient_index=1.0002)),
 ])
 def test_plain_matches_reference_golden(ctx, name, scene_fn):
     gd = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -123,6 +125,38 @@ def test_wavefront_equals_plain(ctx, spp, td):
         gh, gs = paths_split(a["paths"])
         assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
         assert np.abs(a["rgb"] - o["rgb"]).max() <= RGB_TOL
+
+
+@pytest.mark.parametrize("seed,ambient,spp", [(62, 1.0, 1), (63, 1.33, 2), (64, 1.0002, 1)])
+def test_transparent_materials_match_oracle(ctx, seed, ambient, spp):
+    """Transparent materials: Fresnel-mixed secondary rays (the reference's semantics,
+    src/RayTracer.cpp:353-407) bit-exact against the oracle in both modes."""
+    sc = scenes.small_random_scene(seed, n_spheres=6, level=3, lights=3, refl=0.5, transparent=3,
+                                   ambient_index=ambient)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 128, 96)
+    o = oracle.Oracle(sc).render(cam, 4, pixel_offset=0.5, spp=spp, jitter_seed=9)
+    for mode in ("plain", "wavefront"):
+        g = gpu_render(ctx, dsc, cam, 4, 0.5, spp=spp, jitter_seed=9, mode=mode)
+        gh, gs = paths_split(g["paths"])
+        assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"]), mode
+        assert np.abs(g["rgb"] - o["rgb"]).max() <= RGB_TOL, mode
+    transparent_tris = np.nonzero(sc.materials[sc.tri_obj, 8] > 0)[0]
+    assert np.isin(o["hits"][:, :4], transparent_tris).sum() > 100
+
+
+def test_reflective_and_transparent_material_is_unsupported(ctx):
+    from eos_b200._lib import EosError
+    sc = scenes.small_random_scene(65, n_spheres=2, level=1, lights=1)
+    sc.materials[0, 7] = 0.5
+    sc.materials[0, 8] = 1.0
+    with pytest.raises(EosError) as e:
+        api.DeviceScene(ctx, sc)
+    assert e.value.code == 7
+    # and the ambient index must be positive
+    ok = api.DeviceScene(ctx, scenes.small_random_scene(65, n_spheres=2, level=1, lights=1))
+    with pytest.raises(EosError):
+        ok.set_ambient_index(0.0)
 
 
 def test_batch_matches_single_renders(ctx):

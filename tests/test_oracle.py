@@ -50,6 +50,8 @@ def test_oracle_morton_order_is_stable_sort():
     ("config1_128", lambda: scenes.config1_scene()),
     ("small11", lambda: scenes.small_random_scene(11, n_spheres=5, level=2, lights=3, refl=0.6)),
     ("small12", lambda: scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)),
+    ("transp61", lambda: scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3,
+                                                   ambient_index=1.0002)),
 ])
 def test_oracle_matches_reference_golden(name, scene_fn):
     """Oracle paths and colours vs the reference's own renderer output (golden file)."""
@@ -68,6 +70,25 @@ def test_oracle_matches_reference_golden(name, scene_fn):
     # the restatement reproduces the reference's float colours exactly on matching paths
     assert (d[~mm] == 0).mean() > 0.999
     assert np.array_equal(r["counts"][0], g["counts"][0])
+
+
+@pytest.mark.parametrize("seed,ambient", [(62, 1.0), (63, 1.33), (64, 1.0002)])
+def test_transparent_materials_match_reference(seed, ambient):
+    """Transparent materials (src/RayTracer.cpp:353-407: Fresnel K, the mirror ray about the
+    incident-side normal traced for both halves of the mix) against the compiled reference:
+    paths and FP32 colours exact."""
+    if not oracle.ref_available():
+        pytest.skip("reference CPU build unavailable")
+    sc = scenes.small_random_scene(seed, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3,
+                                   ambient_index=ambient)
+    cam = scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 80, 60)
+    r = oracle.RefRenderer(sc).render(cam, 4, pixel_offset=0.0)
+    o = oracle.Oracle(sc).render(cam, 4, pixel_offset=0.0)
+    mm = path_mismatch(o["hits"], o["shadows"], r["hits"], r["shadows"], 5)
+    assert classify(mm, o["flags"])["unexplained"] == 0
+    assert np.abs(o["rgb"] - r["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    transparent_tris = np.nonzero(sc.materials[sc.tri_obj, 8] > 0)[0]
+    assert np.isin(o["hits"][:, :4], transparent_tris).sum() > 100  # the case is exercised
 
 
 def test_oracle_bvh_equals_brute_force():
