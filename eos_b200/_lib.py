@@ -54,6 +54,7 @@ class RenderParams(Structure):
 
 FLAG_STAGE_TIMING = 1
 FLAG_REFILL = 2
+FLAG_PACKET = 4
 
 
 class Tuning(Structure):

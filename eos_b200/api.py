@@ -36,7 +36,7 @@ def camera_struct(cam: CameraData) -> L.Camera:
 
 
 def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="plain", block_size=0,
-                  queue_chunk=0, stack_depth=0, stage_timing=False, refill=False) -> L.RenderParams:
+                  queue_chunk=0, stack_depth=0, stage_timing=False, refill=False, packet=False) -> L.RenderParams:
     p = L.RenderParams()
     p.trace_depth = int(trace_depth)
     p.pixel_offset = float(pixel_offset)
@@ -46,7 +46,8 @@ def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="p
     p.block_size = int(block_size)
     p.queue_chunk = int(queue_chunk)
     p.stack_depth = int(stack_depth)
-    p.flags = (L.FLAG_STAGE_TIMING if stage_timing else 0) | (L.FLAG_REFILL if refill else 0)
+    p.flags = ((L.FLAG_STAGE_TIMING if stage_timing else 0) | (L.FLAG_REFILL if refill else 0)
+               | (L.FLAG_PACKET if packet else 0))
     return p
 
 

@@ -503,6 +503,145 @@ __global__ void __launch_bounds__(256, 4) k_wf_any(WfArgs A) {
   warp_add_count(&A.counts[kCntTestsA], tests);
 }
 
+// Shadow stage as warp packets (EOS_FLAG_PACKET): the warp's 32 shadow rays -- one 8x4
+// pixel tile towards one light, as the closest stage emits them -- share one traversal
+// stack in shared memory.  Every stack entry carries the mask of lanes whose ray entered
+// that box; at a node each participating lane tests the four child boxes and a child is
+// taken when any lane hits it, with the ballot of those lanes as its mask.  Node and
+// triangle records are fetched once per warp (same address in every lane) and control
+// flow is warp-uniform; a lane whose ray is blocked drops out of every mask.  A ray visits
+// exactly the leaves whose boxes (and all ancestors') it enters, as in the per-lane
+// traversal, so the results are the same.
+constexpr int kPacketStack = kStackMax;
+
+template <int SH>
+__global__ void __launch_bounds__(256, 4) k_wf_any_packet(WfArgs A) {
+  extern __shared__ uint2 shstack[];
+  const int lane = threadIdx.x & 31;
+  uint2* stack = shstack + (threadIdx.x >> 5) * kPacketStack;  // (ref, lane mask) per warp
+  int* ctr = A.ctr + A.k * kCtr;
+  const int n = min(ctr[2], A.cap_s);
+  unsigned long long nodes = 0, tests = 0;
+  for (;;) {
+    const int start = grab(&ctr[4], A.qchunk);
+    if (start >= n) break;
+    const int end = min(start + A.qchunk, n);
+    for (int base = start; base < end; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < end;
+      SlabRay r;
+      f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1);
+      int hi = 0, key = 0;
+      const float4* tnodes = nullptr;
+      const float4* ttris = nullptr;
+      if (valid) {
+        ShadowQ q = A.sq[i];
+        hi = __float_as_int(q.a.w);
+        key = __float_as_int(q.b.w);
+        o = mk3(q.a.x, q.a.y, q.a.z);
+        d = mk3(q.b.x, q.b.y, q.b.z);
+        const DevScene& S = A.jobs[key >> 5].s;
+        tnodes = S.nodes;
+        ttris = S.tris;
+      }
+      r = make_slab(o, d);
+      // lanes of one packet may belong to different scenes: one packet per distinct scene
+      uint32_t todo = __ballot_sync(0xffffffffu, valid);
+      uint32_t blocked = 0;
+      while (todo) {
+        const int leader = __ffs(todo) - 1;
+        const float4* nodes_w = (const float4*)__shfl_sync(0xffffffffu, (unsigned long long)tnodes, leader);
+        const float4* tris_w = (const float4*)__shfl_sync(0xffffffffu, (unsigned long long)ttris, leader);
+        const uint32_t group = __ballot_sync(0xffffffffu, valid && tnodes == nodes_w);
+        todo &= ~group;
+        uint32_t alive = group;
+        int sp = 0;
+        int cur = 0;
+        uint32_t cmask = alive;
+        for (;;) {
+          const bool part = (cmask >> lane) & 1u;
+          if (cur >= 0) {  // interior record
+            const float4* nd = nodes_w + 8 * (size_t)cur;
+            const float4 lx = __ldg(nd + r.sx), ly = __ldg(nd + 1 + r.sy), lz = __ldg(nd + 2 + r.sz);
+            const float4 hx = __ldg(nd + 3 - r.sx), hy = __ldg(nd + 4 - r.sy), hz = __ldg(nd + 5 - r.sz);
+            const int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 6);
+            nodes += part;
+            const uint32_t m0 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x));
+            const uint32_t m1 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y));
+            const uint32_t m2 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z));
+            const uint32_t m3 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w));
+            // take the first hit child in slot order, push the others (last slot deepest)
+            int next = kDone;
+            uint32_t nmask = 0;
+            const int c[4] = {ref.x, ref.y, ref.z, ref.w};
+            const uint32_t m[4] = {m0, m1, m2, m3};
+            bool overflow = false;
+#pragma unroll
+            for (int k = 3; k >= 0; --k) {
+              if (!m[k]) continue;
+              if (next != kDone) {
+                if (sp >= kPacketStack) {
+                  overflow = true;
+                } else {
+                  if (lane == 0) stack[sp] = make_uint2((uint32_t)next, nmask);
+                  ++sp;
+                }
+              }
+              next = c[k];
+              nmask = m[k];
+            }
+            if (overflow) {
+              if (lane == 0) atomicOr(A.err, kErrStack);
+              break;
+            }
+            __syncwarp();
+            if (next != kDone) {
+              cur = next;
+              cmask = nmask;
+              continue;
+            }
+          } else if (cur != kDone) {  // leaf: the participating lanes test its triangles
+            const int first = leaf_first(cur), cnt = leaf_count(cur);
+            bool hit = false;
+            for (int p = first; p < first + cnt; ++p) {
+              f3 v1, e1, e2;
+              int id;
+              load_tri(tris_w, p, v1, e1, e2, id);
+              float t, u, v;
+              if (part && !hit) {
+                ++tests;
+                hit = mt_intersect_fast(o, d, v1, e1, e2, t, u, v);
+              }
+              if (!__any_sync(0xffffffffu, part && !hit)) break;
+            }
+            const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+            blocked |= hb;
+            alive &= ~hb;
+            if (!alive) break;
+          }
+          // pop the next entry with a lane still unblocked
+          bool found = false;
+          while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const uint32_t em = e.y & alive;
+            if (em) {
+              cur = (int)e.x;
+              cmask = em;
+              found = true;
+              break;
+            }
+          }
+          __syncwarp();
+          if (!found) break;
+        }
+      }
+      if ((blocked >> lane) & 1u) atomicOr(&A.masks[hi], 1u << (key & 31));
+    }
+  }
+  warp_add_count(&A.counts[kCntNodesA], nodes);
+  warp_add_count(&A.counts[kCntTestsA], tests);
+}
+
 __global__ void k_wf_shade(WfArgs A) {
   int* ctr = A.ctr + A.k * kCtr;
   const int n = A.k == 0 ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);
@@ -623,18 +762,20 @@ struct StageKernels {
   void (*closest_primary)(WfArgs);
   void (*closest)(WfArgs);
   void (*any)(WfArgs);
-  static StageKernels get(bool refill) {
+  static StageKernels get(int variant) {  // bit 0: lane refill, bit 1: shadow packets
+    const bool refill = variant & 1, packet = variant & 2;
     if (refill) return {k_wf_closest_refill<true, SH>, k_wf_closest_refill<false, SH>, k_wf_any_refill<SH>};
+    if (packet) return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any_packet<SH>};
     return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any<SH>};
   }
 };
 
 template <int SH>
 eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, const Chunk* chunks, int n_chunks,
-                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem, bool refill,
+                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem, int variant,
                            StageTimer tm, uint32_t& launches) {
   const int grid_lin = num_sms * 8;
-  const StageKernels<SH> K = StageKernels<SH>::get(refill);
+  const StageKernels<SH> K = StageKernels<SH>::get(variant);
   for (int ci = 0; ci < n_chunks; ++ci) {
     const Chunk& c = chunks[ci];
     WfArgs A = base;
@@ -699,13 +840,13 @@ void fill_job(const eos_job& J, long long path_off, DevJob& d) {
 
 struct LaunchConfig {
   int block, sh, qchunk, grid_c, grid_a;
-  bool refill;
+  int variant;  // bit 0: lane refill, bit 1: shadow packets
   size_t smem;
 };
 
 template <int SH>
 void configure(LaunchConfig& c, int num_sms) {
-  const StageKernels<SH> K = StageKernels<SH>::get(c.refill);
+  const StageKernels<SH> K = StageKernels<SH>::get(c.variant);
   if (c.smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
     cudaFuncSetAttribute(K.closest_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
     cudaFuncSetAttribute(K.closest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
@@ -723,7 +864,7 @@ LaunchConfig launch_config(const eos_render_params& p, int num_sms) {
   c.block = p.block_size > 0 ? std::min(512, std::max(32, (p.block_size / 32) * 32)) : 128;
   c.sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
   c.qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
-  c.refill = (p.flags & EOS_FLAG_REFILL) != 0;
+  c.variant = ((p.flags & EOS_FLAG_REFILL) ? 1 : 0) | ((p.flags & EOS_FLAG_PACKET) ? 2 : 0);
   c.smem = (size_t)c.sh * c.block * sizeof(uint2);
   if (c.sh == 8) configure<8>(c, num_sms);
   else if (c.sh == 16) configure<16>(c, num_sms);
@@ -735,12 +876,12 @@ eos_status run_sequence(cudaStream_t st, int num_sms, const LaunchConfig& lc, co
                         int n_chunks, int depth, StageTimer tm, uint32_t& launches) {
   if (lc.sh == 8)
     return launch_sequence<8>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                              lc.refill, tm, launches);
+                              lc.variant, tm, launches);
   if (lc.sh == 16)
     return launch_sequence<16>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr,
-                               lc.smem, lc.refill, tm, launches);
+                               lc.smem, lc.variant, tm, launches);
   return launch_sequence<32>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                             lc.refill, tm, launches);
+                             lc.variant, tm, launches);
 }
 
 }  // namespace
@@ -825,7 +966,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   }
 
   // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
-  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.refill,
+  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.variant,
                                 (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
                                 (long long)(size_t)acc};

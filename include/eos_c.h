@@ -122,6 +122,9 @@ typedef struct eos_render_params {
  * and finishes them all before taking more).  Measured slower on B200 for the 1080p
  * 1M-triangle workload: refilled lanes break the warps' ray coherence. */
 #define EOS_FLAG_REFILL 2
+/* Wavefront only: shadow rays traced as warp packets (one shared stack per 32 rays with
+ * per-child lane masks) instead of one traversal per lane. */
+#define EOS_FLAG_PACKET 4
 
 /* Tuned launch / layout parameters of one scene-size bucket (see eos_ctx_set_tuning). */
 typedef struct eos_tuning {
