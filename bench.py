@@ -400,9 +400,12 @@ def run_ours(args, rank, world, local):
     alg = {"closest": (closest_bytes, stage[0]), "shadow": (shadow_bytes, stage[1])}
     top = max(alg, key=lambda k: alg[k][1])
     bytes_top, ms_top = alg[top]
-    # one launch per bounce per chunk of <= 2^21 paths (8x4-pixel tiles)
+    # one launch per bounce per chunk; the library's chunk rule: at most 2^24 paths (8x4-pixel
+    # tiles) and at most 8 GB of queues at (3 x 32 + 4 + 32 x lights + 16 x (depth + 1)) B per path
     paths = sum(((c.width + 7) // 8) * ((c.height + 3) // 4) * 32 for c in cams)
-    launches_top = (td + 1) * int(np.ceil(paths / float(1 << 21)))
+    per_path = 3 * 32 + 4 + 32 * max(1, sc.n_lights) + 16 * (td + 1)
+    chunk = max(1 << 16, min(1 << 24, (8 << 30) // per_path))
+    launches_top = (td + 1) * int(np.ceil(paths / float(chunk)))
     achieved = bytes_top / (ms_top * 1e-3) / 1e9
     traffic = profile_traffic().get(top)
     rays_top = (st["shadow_rays"] if top == "shadow" else st["primary_rays"] + st["secondary_rays"])
@@ -455,7 +458,8 @@ def run_ours(args, rank, world, local):
         "gpu_launches": launches_b,
         "roofline": roof,
         "clocks": clocks,
-        "lbvh_build_ms": round(info["build_ms"], 3),
+        "build_ms": round(info["build_ms"], 3),
+        "builder": {1: "lbvh", 2: "ploc"}.get(info["builder"], "?"),
         "bvh": {"layout": {1: "sah", 2: "fixed"}.get(info["layout"], "?"), "leaf_size": info["leaf_size"],
                 "sah_cost": round(info["sah_cost"], 2), "width": info["width"], "node_records": info["n_nodes"],
                 "scene_device_mb": round(info["device_bytes"] / 1e6, 1)},
@@ -563,7 +567,7 @@ def config5_timing(ctx, stream, steps, warmup):
     info = dsc.info()
     return {"tris": sc.n_tris, "resolution": "3840x2160", "spp": 2, "depth": 4, "lights": 8, **res,
             "batched_over_plain": round(res["batched"]["mrays"] / res["plain"]["mrays"], 3),
-            "lbvh_build_ms": round(info["build_ms"], 2)}
+            "build_ms": round(info["build_ms"], 2), "builder": {1: "lbvh", 2: "ploc"}.get(info["builder"], "?")}
 
 
 def adjoint_timing(ctx, stream, reps=5):

@@ -9,8 +9,8 @@
 //      of it (distance = surface area of the merged box; ties to the lower index);
 //   2. mutual nearest neighbours merge into a new interior node at the lower position;
 //   3. the surviving clusters are compacted in order.
-// Interior nodes are numbered in creation order (deterministic: exclusive scans, no
-// atomics), the root last.  Afterwards every node's first leaf position in depth-first
+// Interior nodes are numbered in creation order (deterministic: one exclusive scan of
+// packed keep / make flags per round, no atomics), the root last.  Afterwards every node's first leaf position in depth-first
 // order (left subtree first) is found by a walk to the root, so that every subtree covers
 // a contiguous range of triangle records; the nodes are renumbered root-first into the
 // layout the refit and the node-record writer expect (interior 0..n-2 with the root 0,
@@ -71,10 +71,14 @@ __global__ void k_ploc_nn(int nc, const float4* __restrict__ lo, const float4* _
 // Cluster i survives (keep) unless it is the upper half of a mutual pair; the lower half
 // of a pair creates a node (make).  With `force` (an iteration that merged nothing) the
 // pairs (2k, 2k + 1) merge instead, which bounds the number of iterations.
-__global__ void k_ploc_flags(int nc, const int* __restrict__ nn, int force, int* __restrict__ keep,
-                             int* __restrict__ make) {
+// keep in the low 32 bits, make in the high 32 bits: one scan counts both.
+__global__ void k_ploc_flags(int nc, const int* __restrict__ nn, int force, unsigned long long* __restrict__ km) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nc) return;
+  if (i > nc) return;
+  if (i == nc) {  // the scan's total
+    km[i] = 0ull;
+    return;
+  }
   int partner;
   if (force) {
     partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
@@ -82,12 +86,13 @@ __global__ void k_ploc_flags(int nc, const int* __restrict__ nn, int force, int*
     const int j = nn[i];
     partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
   }
-  keep[i] = partner < 0 || i < partner;
-  make[i] = partner >= 0 && i < partner;
+  const unsigned long long keep = partner < 0 || i < partner;
+  const unsigned long long make = partner >= 0 && i < partner;
+  km[i] = keep | (make << 32);
 }
 
-__global__ void k_ploc_merge(int nc, const int* __restrict__ nn, int force, const int* __restrict__ keep_scan,
-                             const int* __restrict__ make_scan, int node_base, const int* __restrict__ cid,
+__global__ void k_ploc_merge(int nc, const int* __restrict__ nn, int force,
+                             const unsigned long long* __restrict__ km_scan, int node_base, const int* __restrict__ cid,
                              const float4* __restrict__ lo, const float4* __restrict__ hi, int* __restrict__ cid_out,
                              float4* __restrict__ lo_out, float4* __restrict__ hi_out, int2* __restrict__ child,
                              int* __restrict__ count, float4* __restrict__ nlo, float4* __restrict__ nhi, int n) {
@@ -101,14 +106,15 @@ __global__ void k_ploc_merge(int nc, const int* __restrict__ nn, int force, cons
     partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
   }
   if (partner >= 0 && i > partner) return;  // merged into the lower cluster
-  const int pos = keep_scan[i];
+  const unsigned long long sc = km_scan[i];
+  const int pos = (int)(sc & 0xffffffffull);
   if (partner < 0) {
     cid_out[pos] = cid[i];
     lo_out[pos] = lo[i];
     hi_out[pos] = hi[i];
     return;
   }
-  const int k = node_base + make_scan[i];
+  const int k = node_base + (int)(sc >> 32);
   const int a = cid[i], b = cid[partner];
   const float4 al = lo[i], ah = hi[i], bl = lo[partner], bh = hi[partner];
   const float4 l = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
@@ -187,10 +193,8 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   float4* clo[2] = {(float4*)scratch(ctx, "ploc.lo0", 16 * nn, &es), (float4*)scratch(ctx, "ploc.lo1", 16 * nn, &es)};
   float4* chi[2] = {(float4*)scratch(ctx, "ploc.hi0", 16 * nn, &es), (float4*)scratch(ctx, "ploc.hi1", 16 * nn, &es)};
   int* nbr = (int*)scratch(ctx, "ploc.nn", 4 * nn, &es);
-  int* keep = (int*)scratch(ctx, "ploc.keep", 4 * (nn + 1), &es);
-  int* make = (int*)scratch(ctx, "ploc.make", 4 * (nn + 1), &es);
-  int* keep_scan = (int*)scratch(ctx, "ploc.keep_scan", 4 * (nn + 1), &es);
-  int* make_scan = (int*)scratch(ctx, "ploc.make_scan", 4 * (nn + 1), &es);
+  unsigned long long* km = (unsigned long long*)scratch(ctx, "ploc.km", 8 * (nn + 1), &es);
+  unsigned long long* km_scan = (unsigned long long*)scratch(ctx, "ploc.km_scan", 8 * (nn + 1), &es);
   int2* tchild = (int2*)scratch(ctx, "ploc.child", 8 * nn, &es);
   int* tcount = (int*)scratch(ctx, "ploc.count", 4 * nn, &es);
   float4* tlo = (float4*)scratch(ctx, "ploc.nlo", 16 * nn, &es);
@@ -199,7 +203,7 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   int* first = (int*)scratch(ctx, "ploc.first", 4 * (2 * nn), &es);
   int* dmax = (int*)scratch(ctx, "ploc.depth", 4, &es);
   size_t temp_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, keep, keep_scan, n + 1, st);
+  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, km, km_scan, n + 1, st);
   void* temp = scratch(ctx, "ploc.scan_temp", std::max<size_t>(temp_bytes, 16), &es);
   if (es != EOS_OK) return es;
 
@@ -218,20 +222,17 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
     k_ploc_nn<<<grid_of(nc, kNNBlock), kNNBlock, 0, st>>>(nc, clo[cur], chi[cur], nbr);
     int force = 0;
     for (;;) {
-      k_ploc_flags<<<grid_of(nc, 256), 256, 0, st>>>(nc, nbr, force, keep, make);
-      EOS_CUDA(cudaMemsetAsync(keep + nc, 0, 4, st));
-      EOS_CUDA(cudaMemsetAsync(make + nc, 0, 4, st));
-      EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, keep, keep_scan, nc + 1, st));
-      EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, make, make_scan, nc + 1, st));
-      int made = 0, kept = 0;
-      EOS_CUDA(cudaMemcpyAsync(&made, make_scan + nc, 4, cudaMemcpyDeviceToHost, st));
-      EOS_CUDA(cudaMemcpyAsync(&kept, keep_scan + nc, 4, cudaMemcpyDeviceToHost, st));
+      k_ploc_flags<<<grid_of(nc + 1, 256), 256, 0, st>>>(nc, nbr, force, km);
+      EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, km, km_scan, nc + 1, st));
+      unsigned long long total = 0;
+      EOS_CUDA(cudaMemcpyAsync(&total, km_scan + nc, 8, cudaMemcpyDeviceToHost, st));
       EOS_CUDA(cudaStreamSynchronize(st));
+      const int kept = (int)(total & 0xffffffffull), made = (int)(total >> 32);
       if (made == 0 && !force) {
         force = 1;
         continue;
       }
-      k_ploc_merge<<<grid_of(nc, 256), 256, 0, st>>>(nc, nbr, force, keep_scan, make_scan, node_base, cid[cur],
+      k_ploc_merge<<<grid_of(nc, 256), 256, 0, st>>>(nc, nbr, force, km_scan, node_base, cid[cur],
                                                      clo[cur], chi[cur], cid[cur ^ 1], clo[cur ^ 1], chi[cur ^ 1],
                                                      tchild, tcount, tlo, thi, n);
       node_base += made;
