@@ -49,7 +49,7 @@ class Camera(Structure):
 class RenderParams(Structure):
     _fields_ = [("trace_depth", c_int32), ("pixel_offset", c_float), ("spp", c_int32), ("jitter_seed", c_uint32),
                 ("mode", c_int32), ("block_size", c_int32), ("queue_chunk", c_int32), ("stack_depth", c_int32),
-                ("flags", c_int32)]
+                ("flags", c_int32), ("row_begin", c_int32), ("row_end", c_int32)]
 
 
 FLAG_STAGE_TIMING = 1
@@ -95,7 +95,7 @@ class SceneInfo(Structure):
 class Job(Structure):
     _fields_ = [("scene", c_void_p), ("camera", Camera), ("trace_depth", c_int32), ("pixel_offset", c_float),
                 ("spp", c_int32), ("jitter_seed", c_uint32), ("rgb_out", c_void_p), ("rgba8_out", c_void_p),
-                ("paths_out", c_void_p)]
+                ("paths_out", c_void_p), ("row_begin", c_int32), ("row_end", c_int32)]
 
 
 class Grads(Structure):
@@ -106,6 +106,7 @@ class Grads(Structure):
 SIGNATURES = [
     ("eos_abi_version", c_int32, []),
     ("eos_status_string", c_char_p, [c_int32]),
+    ("eos_device_count", c_int32, [POINTER(c_int32)]),
     ("eos_ctx_create", c_int32, [c_int32, POINTER(c_void_p)]),
     ("eos_ctx_destroy", c_int32, [c_void_p]),
     ("eos_ctx_set_stream", c_int32, [c_void_p, c_void_p]),

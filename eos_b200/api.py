@@ -36,7 +36,8 @@ def camera_struct(cam: CameraData) -> L.Camera:
 
 
 def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="plain", block_size=0,
-                  queue_chunk=0, stack_depth=0, stage_timing=False, refill=False, packet=False) -> L.RenderParams:
+                  queue_chunk=0, stack_depth=0, stage_timing=False, refill=False, packet=False,
+                  rows=None) -> L.RenderParams:
     p = L.RenderParams()
     p.trace_depth = int(trace_depth)
     p.pixel_offset = float(pixel_offset)
@@ -48,6 +49,8 @@ def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="p
     p.stack_depth = int(stack_depth)
     p.flags = ((L.FLAG_STAGE_TIMING if stage_timing else 0) | (L.FLAG_REFILL if refill else 0)
                | (L.FLAG_PACKET if packet else 0))
+    if rows is not None:
+        p.row_begin, p.row_end = int(rows[0]), int(rows[1])
     return p
 
 
@@ -176,11 +179,14 @@ def render(ctx: Context, scene: DeviceScene, cam: CameraData, trace_depth: int, 
     """Render one frame; returns the requested outputs plus 'stats'.
 
     outputs: any of 'rgb' [H*W,3] f32, 'rgba8' [H,W,4] u8, 'hit' [H*W*spp] i32,
-    'paths' [H*W*spp, 16] i32 (8 hit ids then 8 shadow masks per path).
+    'paths' [H*W*spp, 16] i32 (8 hit ids then 8 shadow masks per path).  rows=(r0, r1) in
+    `tuning` renders image rows [r0, r1) only (split-frame); H is then r1 - r0.
     """
-    npx = cam.width * cam.height
+    rows = tuning.get("rows")
+    H = (rows[1] - rows[0]) if rows is not None else cam.height
+    npx = cam.width * H
     res = dict(out or {})
-    shapes = {"rgb": ((npx, 3), np.float32), "rgba8": ((cam.height, cam.width, 4), np.uint8),
+    shapes = {"rgb": ((npx, 3), np.float32), "rgba8": ((H, cam.width, 4), np.uint8),
               "hit": ((npx * spp,), np.int32), "paths": ((npx * spp, 16), np.int32)}
     for k in outputs:
         if k not in res:
@@ -203,17 +209,19 @@ class BatchJob:
     pixel_offset: float = 0.5
     spp: int = 1
     jitter_seed: int = 0
+    rows: tuple | None = None  # image rows [r0, r1) only
 
 
 def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",)):
     outs = []
     for j in jobs:
-        npx = j.camera.width * j.camera.height
+        H = (j.rows[1] - j.rows[0]) if j.rows is not None else j.camera.height
+        npx = j.camera.width * H
         o = {}
         if "rgb" in outputs:
             o["rgb"] = _alloc((npx, 3), np.float32, True)
         if "rgba8" in outputs:
-            o["rgba8"] = _alloc((j.camera.height, j.camera.width, 4), np.uint8, True)
+            o["rgba8"] = _alloc((H, j.camera.width, 4), np.uint8, True)
         if "paths" in outputs:
             o["paths"] = _alloc((npx * j.spp, 16), np.int32, True)
         outs.append(o)
@@ -234,6 +242,8 @@ def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning)
         arr[i].rgb_out = _ptr(o.get("rgb"))
         arr[i].rgba8_out = _ptr(o.get("rgba8"))
         arr[i].paths_out = _ptr(o.get("paths"))
+        if j.rows is not None:
+            arr[i].row_begin, arr[i].row_end = int(j.rows[0]), int(j.rows[1])
     p = params_struct(mode="wavefront", **tuning)
     st = L.Stats()
     L.check(ctx.lib.eos_render_batch(ctx.h, arr, len(jobs), byref(p), byref(st)), "eos_render_batch")

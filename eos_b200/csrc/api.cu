@@ -152,6 +152,10 @@ eos_status check_params(const eos_render_params* p) {
   return EOS_OK;
 }
 
+// Row band [rb, re) of an image of h rows; 0, 0 = all rows.
+bool valid_rows(int h, int rb, int re) { return (rb == 0 && re == 0) || (rb >= 0 && rb < re && re <= h); }
+int band_rows(int h, int rb, int re) { return re > 0 ? re - rb : h; }
+
 eos_status set_device(eos_ctx* ctx) {
   EOS_CUDA(cudaSetDevice(ctx->device));
   return EOS_OK;
@@ -196,6 +200,17 @@ const char* eos_status_string(eos_status s) {
     case EOS_ERR_PARSE: return "malformed input file";
   }
   return "unknown status";
+}
+
+eos_status eos_device_count(int32_t* n) {
+  if (!n) return EOS_ERR_INVALID_ARG;
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) {
+    cudaGetLastError();
+    c = 0;
+  }
+  *n = c;
+  return EOS_OK;
 }
 
 eos_status eos_ctx_create(int32_t device, eos_ctx** out) {
@@ -415,8 +430,9 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, 
   if (!ctx || !sc || !valid_camera(cam)) return EOS_ERR_INVALID_ARG;
   eos_status st = check_params(p);
   if (st != EOS_OK) return st;
+  if (!valid_rows(cam->height, p->row_begin, p->row_end)) return EOS_ERR_INVALID_ARG;
   if ((st = set_device(ctx)) != EOS_OK) return st;
-  const size_t npx = (size_t)cam->width * cam->height;
+  const size_t npx = (size_t)cam->width * band_rows(cam->height, p->row_begin, p->row_end);
   const size_t npath = npx * p->spp;
   OutBuf o_rgb, o_q, o_hit, o_paths;
   if ((st = out_buf(ctx, "out.rgb", rgb_out, 12 * npx, o_rgb)) != EOS_OK) return st;
@@ -441,6 +457,8 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, 
     job.rgb_out = (float*)o_rgb.dev;
     job.rgba8_out = (uint8_t*)o_q.dev;
     job.paths_out = (eos_path_record*)o_paths.dev;
+    job.row_begin = p->row_begin;
+    job.row_end = p->row_end;
     st = render_wavefront(ctx, &job, 1, with_tuning(ctx, *p, (uint32_t)sc->dev.n_tris), false);
   }
   if (st != EOS_OK) return st;
@@ -462,7 +480,7 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   for (uint32_t j = 0; j < n_jobs; ++j) {
     const eos_job& jb = jobs[j];
     if (!jb.scene || !valid_camera(&jb.camera) || jb.trace_depth < 0 || jb.trace_depth >= EOS_MAX_BOUNCES ||
-        jb.spp < 1 || jb.spp > 1024)
+        jb.spp < 1 || jb.spp > 1024 || !valid_rows(jb.camera.height, jb.row_begin, jb.row_end))
       return EOS_ERR_INVALID_ARG;
   }
   if ((st = set_device(ctx)) != EOS_OK) return st;
@@ -480,7 +498,7 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     staged += (bytes + 255) & ~size_t(255);
   };
   for (const eos_job& jb : dj) {
-    const size_t npx = (size_t)jb.camera.width * jb.camera.height;
+    const size_t npx = (size_t)jb.camera.width * band_rows(jb.camera.height, jb.row_begin, jb.row_end);
     plan(jb.rgb_out, 12 * npx);
     plan(jb.rgba8_out, 4 * npx);
     plan(jb.paths_out, sizeof(eos_path_record) * npx * jb.spp);
@@ -522,7 +540,7 @@ eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_came
     return EOS_ERR_INVALID_ARG;
   eos_status st = check_params(p);
   if (st != EOS_OK) return st;
-  if (p->spp != 1) return EOS_ERR_UNSUPPORTED;
+  if (p->spp != 1 || p->row_begin != 0 || p->row_end != 0) return EOS_ERR_UNSUPPORTED;
   for (uint32_t v = 0; v < n_views; ++v)
     if (!valid_camera(&cams[v]) || cams[v].width != cams[0].width || cams[v].height != cams[0].height)
       return EOS_ERR_INVALID_ARG;

@@ -16,6 +16,7 @@ struct PlainParams {
   DevScene s;
   float cam[12];
   int width, height, trace_depth, spp;
+  int y0, rows;  // image rows [y0, y0 + rows) are rendered; outputs hold those rows
   float pixel_offset;
   uint32_t jitter_seed;
   float* rgb;
@@ -92,9 +93,11 @@ __global__ void __maxnreg__(64) k_render_plain(PlainParams P) {
   const int tiles_x = (P.width + 7) >> 3;
   const int tile = g >> 5, lane = g & 31;
   const int x = (tile % tiles_x) * 8 + (lane & 7);
-  const int y = (tile / tiles_x) * 4 + (lane >> 3);
-  const int pix = y * P.width + x;
-  if (x < P.width && y < P.height) {
+  const int ly = (tile / tiles_x) * 4 + (lane >> 3);  // row within the rendered band
+  const int y = P.y0 + ly;
+  const int img_pix = y * P.width + x;  // pixel of the whole image: its sample hash
+  const int pix = ly * P.width + x;     // pixel of the outputs
+  if (x < P.width && ly < P.rows) {
     f3 sum = mk3(0.0f, 0.0f, 0.0f);
     for (int smp = 0; smp < P.spp; ++smp) {
       int32_t hits[kMaxBounces];
@@ -105,7 +108,7 @@ __global__ void __maxnreg__(64) k_render_plain(PlainParams P) {
         masks[k] = 0;
       }
       float ox, oy;
-      sample_offset((uint32_t)pix, smp, P.spp, P.jitter_seed, P.pixel_offset, ox, oy);
+      sample_offset((uint32_t)img_pix, smp, P.spp, P.jitter_seed, P.pixel_offset, ox, oy);
       f3 d = primary_direction(P.cam, P.width, P.height, x, y, ox, oy);
       f3 o = mk3(P.cam[0], P.cam[1], P.cam[2]);
       f3 c = trace_path<SH>(P, o, d, hits, masks, cnt, shs, stride);
@@ -176,6 +179,8 @@ eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam
   }
   P.width = cam.width;
   P.height = cam.height;
+  P.y0 = p.row_end > 0 ? p.row_begin : 0;
+  P.rows = p.row_end > 0 ? p.row_end - p.row_begin : cam.height;
   P.trace_depth = p.trace_depth;
   P.spp = p.spp;
   P.pixel_offset = p.pixel_offset;
@@ -188,7 +193,7 @@ eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam
   P.counts = ctx->d_counts;
   const int block = clamp_block(p.block_size);
   const int sh = pick_stack(p.stack_depth);
-  const long long n_threads = (long long)((cam.width + 7) / 8) * ((cam.height + 3) / 4) * 32;
+  const long long n_threads = (long long)((cam.width + 7) / 8) * ((P.rows + 3) / 4) * 32;
   const int grid = (int)std::max<long long>(1, (n_threads + block - 1) / block);
   const size_t smem = (size_t)sh * block * sizeof(uint2);
   cudaStream_t st = ctx->stream;

@@ -37,6 +37,7 @@ struct DevJob {
   DevScene s;
   float cam[12];
   int w, h, trace_depth, spp;
+  int y0, rows;  // image rows [y0, y0 + rows) are rendered; outputs hold those rows
   float off;
   uint32_t seed;
   float* rgb;
@@ -96,6 +97,7 @@ __device__ __forceinline__ int find_job(const DevJob* jobs, int n, long long pat
 }
 
 // Tiled path order: warp-sized 8x4 pixel tiles, samples of a pixel consecutive.
+// y is the row within the job's band (output row); the image row is j.y0 + y.
 __device__ __forceinline__ bool path_pixel(const DevJob& j, long long local, int& x, int& y, int& smp) {
   smp = (int)(local % j.spp);
   long long tp = local / j.spp;
@@ -103,7 +105,7 @@ __device__ __forceinline__ bool path_pixel(const DevJob& j, long long local, int
   int lane = (int)(tp & 31);
   x = (int)(tile % j.tiles_x) * kTileW + (lane & (kTileW - 1));
   y = (int)(tile / j.tiles_x) * kTileH + (lane >> 3);
-  return x < j.w && y < j.h;
+  return x < j.w && y < j.rows;
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -149,8 +151,8 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
           int x, y, smp;
           if (path_pixel(J, gp - J.path_off, x, y, smp)) {
             float ox, oy;
-            sample_offset((uint32_t)(y * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
-            d = primary_direction(J.cam, J.w, J.h, x, y, ox, oy);
+            sample_offset((uint32_t)((J.y0 + y) * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
+            d = primary_direction(J.cam, J.w, J.h, x, J.y0 + y, ox, oy);
             o = mk3(J.cam[0], J.cam[1], J.cam[2]);
             path = i;
           } else {
@@ -386,8 +388,8 @@ __global__ void k_wf_closest_refill(WfArgs A) {
           ok = path_pixel(J, gp - J.path_off, x, y, smp);
           if (ok) {
             float ox, oy;
-            sample_offset((uint32_t)(y * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
-            d = primary_direction(J.cam, J.w, J.h, x, y, ox, oy);
+            sample_offset((uint32_t)((J.y0 + y) * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
+            d = primary_direction(J.cam, J.w, J.h, x, J.y0 + y, ox, oy);
             o = mk3(J.cam[0], J.cam[1], J.cam[2]);
             path = k;
           }
@@ -832,8 +834,10 @@ void fill_job(const eos_job& J, long long path_off, DevJob& d) {
   d.rgb = J.rgb_out;
   d.rgba8 = J.rgba8_out;
   d.paths = J.paths_out;
+  d.y0 = J.row_end > 0 ? J.row_begin : 0;
+  d.rows = J.row_end > 0 ? J.row_end - J.row_begin : d.h;
   d.tiles_x = (d.w + kTileW - 1) / kTileW;
-  long long tiles_y = (d.h + kTileH - 1) / kTileH;
+  long long tiles_y = (d.rows + kTileH - 1) / kTileH;
   d.n_paths = (long long)d.tiles_x * tiles_y * 32 * d.spp;
   d.path_off = path_off;
 }
@@ -1109,6 +1113,12 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
   J.jitter_seed = params->jitter_seed;
   J.rgb_out = rgb_out;
   J.paths_out = paths_out;
+  const bool rows_ok = (params->row_begin == 0 && params->row_end == 0) ||
+                       (params->row_begin >= 0 && params->row_begin < params->row_end &&
+                        params->row_end <= camera->height);
+  if (!rows_ok) return EOS_ERR_INVALID_ARG;
+  J.row_begin = params->row_begin;
+  J.row_end = params->row_end;
   DevJob job;
   fill_job(J, 0, job);
   if (job.n_paths > kNoAllocMaxPaths) return EOS_ERR_INVALID_ARG;  // beyond the fixed scratch capacity

@@ -1,10 +1,14 @@
-"""Multi-GPU plumbing: one process per GPU, views sharded across ranks.
+"""Multi-GPU plumbing: one process per GPU.
 
-Rendering shards with no data-path collective: views are independent, every rank
-renders its own (the reference replicates the scene per GPU and splits frames by rows,
-src/MultiDeviceRenderer.cu:59-81,119-161).  The adjoint has one real exchange step: the
-parameter-gradient vector (per-object kd/ks/log-shininess, per-light colour/position) is
-summed over ranks with one all-reduce.
+Two ways to spread rendering over ranks, both with the scene replicated per GPU as the
+reference does (src/MultiDeviceRenderer.cu:59-81):
+* views sharded across ranks, no data-path collective (views are independent);
+* split-frame: one frame cut into horizontal bands, one per rank, each rendered with a
+  row band (eos_render_params.row_begin / row_end) and gathered to every rank with one
+  all-gather -- the reference's MultiDeviceRenderer split (src/MultiDeviceRenderer.cu:
+  119-200) across processes.
+The adjoint has one real exchange step: the parameter-gradient vector (per-object
+kd/ks/log-shininess, per-light colour/position) is summed over ranks with one all-reduce.
 """
 from __future__ import annotations
 
@@ -18,6 +22,45 @@ def shard(items, rank: int, world: int):
 
 def shard_indices(n: int, rank: int, world: int) -> np.ndarray:
     return np.arange(rank, n, world)
+
+
+def band(height: int, rank: int, world: int) -> tuple[int, int]:
+    """Rows [r0, r1) of band `rank` out of `world`: height // world rows each, the last
+    band takes the remainder (the reference drops it, src/MultiDeviceRenderer.cu:128)."""
+    per = height // world
+    r0 = rank * per
+    r1 = height if rank == world - 1 else r0 + per
+    return r0, r1
+
+
+def gather_bands(mine, height: int, group=None):
+    """All-gather of every rank's band (a [rows, W, C] tensor or array) into the whole
+    [height, W, C] frame on every rank; bands are padded to equal size for the collective."""
+    import torch
+    import torch.distributed as dist
+    as_np = not hasattr(mine, "data_ptr")
+    t = torch.as_tensor(np.asarray(mine)) if as_np else mine
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    if world == 1:
+        return mine
+    per = height // world
+    tallest = height - per * (world - 1)
+    pad = torch.zeros((tallest,) + tuple(t.shape[1:]), dtype=t.dtype, device=t.device)
+    pad[: t.shape[0]] = t
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    full = torch.cat([p[: band(height, r, world)[1] - band(height, r, world)[0]] for r, p in enumerate(parts)])
+    return full.numpy() if as_np else full
+
+
+def render_split_frame(ctx, dscene, cam, trace_depth, rank: int, world: int, pixel_offset=0.5, mode="plain"):
+    """This rank's band of one frame (RGBA8 on the device), then the whole frame on every
+    rank.  Bit-identical to rendering the frame on one GPU."""
+    from . import api
+    r0, r1 = band(cam.height, rank, world)
+    out = api.render(ctx, dscene, cam, trace_depth, pixel_offset=pixel_offset, mode=mode, outputs=("rgba8",),
+                     rows=(r0, r1))
+    return gather_bands(out["rgba8"], cam.height)
 
 
 def allreduce_grads(grad_mat, grad_light, group=None):

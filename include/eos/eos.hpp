@@ -23,8 +23,7 @@
 //    createCudaScene; with identity transforms the frame equals the reference bit for
 //    bit on hit ids and paths;
 //  * the scene must be triangles only, as the reference GPU upload requires
-//    (src/cudaStructures.cu:342-348); one GPU (the reference's split-frame multi-GPU mode
-//    is not part of this path).
+//    (src/cudaStructures.cu:342-348).
 #ifndef EOS_EOS_HPP
 #define EOS_EOS_HPP
 
@@ -33,6 +32,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../eos_c.h"
@@ -500,25 +500,69 @@ class DeviceRenderer {
   int m_TraceDepth = kDefaultTraceDepth;
 };
 
-// src/MultiDeviceRenderer.h:31-45, on one GPU.
+// src/MultiDeviceRenderer.h:31-45 / src/MultiDeviceRenderer.cu:31-200: a copy of the
+// scene on every GPU and the frame split into horizontal bands, one per GPU, rendered in
+// parallel by one host thread each straight into the caller's buffer (eos_render with a
+// row band).  The reference gives every GPU height / n rows and leaves the remainder
+// unrendered; here the last band takes it.  `bands` > 0 sets the number of bands, which
+// then cycle over the GPUs, each band with its own context.
 class MultiDeviceRenderer {
  public:
-  MultiDeviceRenderer(Scene* scene, Camera* camera, int width, int height)
-      : m_Scene(createCudaScene(scene)), m_Width(width), m_Height(height) {
+  MultiDeviceRenderer(Scene* scene, Camera* camera, int width, int height, int bands = 0)
+      : m_Width(width), m_Height(height) {
     (void)camera;
+    int32_t n_dev = 0;
+    check(eos_device_count(&n_dev), "eos_device_count");
+    if (n_dev < 1) throw Error(EOS_ERR_NO_DEVICE, "MultiDeviceRenderer");
+    const int n = bands > 0 ? bands : n_dev;
+    for (int b = 0; b < n; ++b) {
+      eos_ctx* ctx = nullptr;
+      check(eos_ctx_create(b % n_dev, &ctx), "eos_ctx_create");
+      m_Ctx.push_back(ctx);
+      m_Scenes.emplace_back(createCudaScene(scene, ctx));
+    }
   }
+  ~MultiDeviceRenderer() {
+    m_Scenes.clear();
+    for (eos_ctx* c : m_Ctx) eos_ctx_destroy(c);
+  }
+  MultiDeviceRenderer(const MultiDeviceRenderer&) = delete;
+  MultiDeviceRenderer& operator=(const MultiDeviceRenderer&) = delete;
+
   void renderSceneToHostBuffer(void* imageBuffer, Camera* hostCamera) {
     Camera c = *hostCamera;
     c.setWidth(m_Width);
     c.setHeight(m_Height);
-    render_rgba8(m_Scene->ctx, m_Scene->scene, c, m_TraceDepth, imageBuffer);
+    const eos_camera cc = c.to_c();
+    const int n = (int)m_Ctx.size();
+    std::vector<eos_status> status(n, EOS_OK);
+    std::vector<std::thread> workers;
+    for (int b = 0; b < n; ++b) {
+      workers.emplace_back([&, b] {
+        const int r0 = b * (m_Height / n), r1 = b + 1 == n ? m_Height : (b + 1) * (m_Height / n);
+        if (r0 >= r1) return;
+        eos_render_params p{};
+        p.trace_depth = m_TraceDepth;
+        p.pixel_offset = 0.0f;
+        p.spp = 1;
+        p.mode = EOS_MODE_PLAIN;
+        p.row_begin = r0;
+        p.row_end = r1;
+        status[b] = eos_render(m_Ctx[b], m_Scenes[b]->scene, &cc, &p, nullptr,
+                               (uint8_t*)imageBuffer + 4ull * r0 * m_Width, nullptr, nullptr, nullptr);
+      });
+    }
+    for (std::thread& t : workers) t.join();
+    for (eos_status s : status) check(s, "MultiDeviceRenderer::renderSceneToHostBuffer");
   }
   void setTracedDepth(int d) {
     if (d > 0) m_TraceDepth = d;
   }
+  int getNumBands() const { return (int)m_Ctx.size(); }
 
  private:
-  std::unique_ptr<cudaScene_t> m_Scene;
+  std::vector<eos_ctx*> m_Ctx;
+  std::vector<std::unique_ptr<cudaScene_t>> m_Scenes;
   int m_Width, m_Height;
   int m_TraceDepth = kDefaultTraceDepth;
 };

@@ -6,8 +6,8 @@
  * (src/cudaQualifiers.h:35-45).
  *
  * Each entry point replaces a reference interface:
- *   eos_ctx_create / destroy     cudaSetDevice + per-renderer setup
- *                                (src/MultiDeviceRenderer.cu:31-110; single GPU here)
+ *   eos_device_count,            cudaGetDeviceCount + cudaSetDevice + per-renderer setup
+ *   eos_ctx_create / destroy     (src/MultiDeviceRenderer.cu:31-110)
  *   eos_scene_create             Scene::flush + createCudaScene
  *                                (src/Scene.cpp:204-209, src/cudaStructures.cu:483-543):
  *                                uploads the triangles once and builds a Morton-code LBVH
@@ -112,6 +112,9 @@ typedef struct eos_render_params {
   int32_t queue_chunk;  /* rays taken per queue grab in the persistent kernels; 0 = default */
   int32_t stack_depth;  /* shared-memory part of the traversal stack; 0 = default */
   int32_t flags;        /* EOS_FLAG_* */
+  int32_t row_begin;    /* render image rows [row_begin, row_end) only (split-frame, as */
+  int32_t row_end;      /* src/MultiDeviceRenderer.cu:126-200 does per GPU); 0, 0 = the
+                           whole image.  Outputs then hold those rows only. */
 } eos_render_params;
 
 /* Wavefront only: run the stages eagerly (no graph) with CUDA events between them and
@@ -209,6 +212,8 @@ typedef struct eos_job {
   float* rgb_out;              /* [H*W*3], nullable */
   uint8_t* rgba8_out;          /* [H*W*4], nullable */
   eos_path_record* paths_out;  /* [H*W*spp], nullable */
+  int32_t row_begin;           /* rows [row_begin, row_end) only; 0, 0 = whole image */
+  int32_t row_end;             /* (outputs then hold (row_end - row_begin) rows) */
 } eos_job;
 
 /* Gradients of an image loss L; d_rgb = dL/drgb per pixel. */
@@ -220,6 +225,8 @@ typedef struct eos_grads {
 /* ---------------------------------------------------------------------------- context */
 int32_t eos_abi_version(void);
 const char* eos_status_string(eos_status s);
+/* Number of CUDA devices visible to the process (0 when none). */
+eos_status eos_device_count(int32_t* n);
 eos_status eos_ctx_create(int32_t device, eos_ctx** out);
 eos_status eos_ctx_destroy(eos_ctx* ctx);
 /* Use a caller stream (a cudaStream_t) instead of the context's own; NULL restores it. */

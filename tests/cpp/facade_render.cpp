@@ -2,7 +2,10 @@
 // of the reference does (src/main.cpp:340-480): Material / Triangle / LightSource /
 // Scene / Camera, createCudaScene, DeviceRenderer and RayTracer.
 //
-//   facade_render <scene.bin> <out_device_renderer.rgba> <out_raytracer.rgba>
+//   facade_render <scene.bin> <out_device_renderer.rgba> <out_raytracer.rgba> [<out_multi.rgba>]
+//
+// The optional third image comes from MultiDeviceRenderer split into 3 row bands (they
+// cycle over the visible GPUs).
 //
 // scene.bin: int32 n_verts, n_tris, n_mats, n_lights, width, height, trace_depth;
 // float32 verts[3n], normals[3n]; uint32 tris[3m], tri_obj[m]; float32 mats[10k] (kd rgb,
@@ -21,8 +24,8 @@ static bool read_n(FILE* f, std::vector<T>& v, size_t n) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 4) {
-    fprintf(stderr, "usage: %s scene.bin out_dr.rgba out_rt.rgba\n", argv[0]);
+  if (argc != 4 && argc != 5) {
+    fprintf(stderr, "usage: %s scene.bin out_dr.rgba out_rt.rgba [out_multi.rgba]\n", argv[0]);
     return 2;
   }
   FILE* f = fopen(argv[1], "rb");
@@ -92,6 +95,15 @@ int main(int argc, char** argv) {
     o = fopen(argv[3], "wb");
     fwrite(img2.data(), 1, img2.size(), o);
     fclose(o);
+    if (argc == 5) {
+      eos::MultiDeviceRenderer multi(&scene, &camera, W, H, 3);
+      multi.setTracedDepth(td);
+      std::vector<unsigned char> img3(4 * (size_t)W * H, 0);
+      multi.renderSceneToHostBuffer(img3.data(), &camera);
+      o = fopen(argv[4], "wb");
+      fwrite(img3.data(), 1, img3.size(), o);
+      fclose(o);
+    }
   } catch (const eos::Error& e) {
     fprintf(stderr, "eos error: %s\n", e.what());
     return 1;

@@ -32,12 +32,12 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(L.Material) == 40
     assert ctypes.sizeof(L.Light) == 24
     assert ctypes.sizeof(L.Camera) == 56
-    assert ctypes.sizeof(L.RenderParams) == 36
+    assert ctypes.sizeof(L.RenderParams) == 44
     assert ctypes.sizeof(L.BuildParams) == 16
     assert ctypes.sizeof(L.Tuning) == 28
     assert ctypes.sizeof(L.SceneInfo) == 56
     assert ctypes.sizeof(L.PathRecord) == 64
-    assert ctypes.sizeof(L.Job) == 8 + 56 + 16 + 24
+    assert ctypes.sizeof(L.Job) == 8 + 56 + 16 + 24 + 8
 
 
 def test_status_strings_and_version():

@@ -44,12 +44,15 @@ def test_cpp_facade_matches_c_abi_and_reference(ctx, tmp_path):
     cam = scenes.config1_camera(256, 256)
     td = 1
     _write_scene(tmp_path / "scene.bin", sc, cam, td)
-    out1, out2 = tmp_path / "dr.rgba", tmp_path / "rt.rgba"
-    r = subprocess.run([exe, str(tmp_path / "scene.bin"), str(out1), str(out2)], capture_output=True, text=True)
+    out1, out2, out3 = tmp_path / "dr.rgba", tmp_path / "rt.rgba", tmp_path / "multi.rgba"
+    r = subprocess.run([exe, str(tmp_path / "scene.bin"), str(out1), str(out2), str(out3)], capture_output=True,
+                       text=True)
     assert r.returncode == 0, r.stderr
     img_dr = np.fromfile(out1, np.uint8).reshape(cam.height, cam.width, 4)
     img_rt = np.fromfile(out2, np.uint8).reshape(cam.height, cam.width, 4)
+    img_multi = np.fromfile(out3, np.uint8).reshape(cam.height, cam.width, 4)
     assert np.array_equal(img_dr, img_rt)
+    assert np.array_equal(img_dr, img_multi)  # split-frame bands, one context each
     dsc = api.DeviceScene(ctx, sc)
     g = api.render(ctx, dsc, cam, td, pixel_offset=0.0, outputs=("rgba8",), device=False)
     assert np.array_equal(img_dr, g["rgba8"])

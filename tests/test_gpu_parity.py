@@ -159,6 +159,34 @@ def test_reflective_and_transparent_material_is_unsupported(ctx):
         ok.set_ambient_index(0.0)
 
 
+@pytest.mark.parametrize("mode,spp", [("plain", 1), ("wavefront", 2)])
+def test_row_bands_equal_the_whole_frame(ctx, mode, spp):
+    """Split-frame: bands rendered with row ranges (eos_render_params.row_begin/row_end,
+    eos_job.row_begin/row_end) are the whole frame's rows bit for bit."""
+    sc = scenes.small_random_scene(33, n_spheres=6, level=3, lights=2, refl=0.6, transparent=1)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 150, 101)
+    full = gpu_render(ctx, dsc, cam, 3, 0.5, spp=spp, jitter_seed=4, mode=mode, outputs=("rgb", "paths", "rgba8"))
+    edges = [0, 37, 38, 77, 101]
+    for r0, r1 in zip(edges[:-1], edges[1:]):
+        b = gpu_render(ctx, dsc, cam, 3, 0.5, spp=spp, jitter_seed=4, mode=mode, outputs=("rgb", "paths", "rgba8"),
+                       rows=(r0, r1))
+        W = cam.width
+        assert np.array_equal(b["rgb"], full["rgb"][r0 * W:r1 * W])
+        assert np.array_equal(b["paths"], full["paths"][r0 * W * spp:r1 * W * spp])
+        assert np.array_equal(b["rgba8"], full["rgba8"][r0:r1])
+    # the same bands as jobs of one batch
+    jobs = [api.BatchJob(dsc, cam, 3, 0.5, spp=spp, jitter_seed=4, rows=(r0, r1))
+            for r0, r1 in zip(edges[:-1], edges[1:])]
+    outs = api.make_batch_outputs(jobs, ("rgba8",))
+    api.render_batch(ctx, jobs, outs)
+    assert np.array_equal(np.concatenate([o["rgba8"].cpu().numpy() for o in outs]), full["rgba8"])
+    from eos_b200._lib import EosError
+    for bad in ((50, 40), (-1, 5), (0, 102)):
+        with pytest.raises(EosError):
+            gpu_render(ctx, dsc, cam, 3, 0.5, outputs=(), rows=bad)
+
+
 def test_batch_matches_single_renders(ctx):
     import torch
     s1 = scenes.config1_scene()

@@ -83,3 +83,35 @@ def test_shard_round_robin_covers_everything_once():
     parts = [parallel.shard(items, r, 3) for r in range(3)]
     assert sorted(sum(parts, [])) == items
     assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 1
+
+
+def _band_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sc, cams = _setup()
+    cam = cams[1]
+    r0, r1 = parallel.band(cam.height, rank, world)
+    # the oracle renders this rank's rows (its pixel list), as a GPU rank renders its band
+    pix = np.arange(r0 * cam.width, r1 * cam.width)
+    rgb = oracle.Oracle(sc).render(cam, 1, pixel_offset=0.5, pixels=pix, nthreads=1)["rgb"]
+    full = parallel.gather_bands(rgb.reshape(r1 - r0, cam.width, 3), cam.height)
+    out[rank] = (r0, r1, full)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_split_frame_bands_gather_to_the_whole_frame():
+    world = 3  # 12 rows over 3 ranks: 4 + 4 + 4; and a remainder case below
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_band_worker, args=(world, port, out), nprocs=world, start_method="spawn")
+    sc, cams = _setup()
+    whole = oracle.Oracle(sc).render(cams[1], 1, pixel_offset=0.5, nthreads=1)["rgb"].reshape(12, 16, 3)
+    for r in range(world):
+        r0, r1, full = out[r]
+        assert (r0, r1) == parallel.band(12, r, world)
+        assert np.array_equal(full, whole)
+    assert [parallel.band(10, r, 3) for r in range(3)] == [(0, 3), (3, 6), (6, 10)]
