@@ -98,6 +98,10 @@ class Job(Structure):
                 ("paths_out", c_void_p), ("row_begin", c_int32), ("row_end", c_int32)]
 
 
+class Instance(Structure):
+    _fields_ = [("mesh", c_void_p), ("transform", c_float * 12), ("material_base", c_uint32)]
+
+
 class Grads(Structure):
     _fields_ = [("materials", c_void_p), ("lights", c_void_p)]
 
@@ -130,6 +134,8 @@ SIGNATURES = [
     ("eos_trace_any", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
     ("eos_render_noalloc", c_int32, [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
                                      c_void_p, POINTER(Stats)]),
+    ("eos_scene_create_instanced", c_int32, [c_void_p, c_void_p, c_uint32, c_void_p, c_uint32, c_void_p, c_uint32,
+                                             POINTER(c_void_p)]),
     ("eos_mesh_load_obj", c_int32, [c_char_p, POINTER(c_void_p)]),
     ("eos_mesh_parse_obj", c_int32, [c_char_p, c_size_t, POINTER(c_void_p)]),
     ("eos_mesh_get_info", c_int32, [c_void_p, POINTER(MeshInfo)]),

@@ -165,6 +165,36 @@ class DeviceScene:
         L.check(self.lib.eos_scene_set_lights(self.h, _ptr(l), int(l.shape[0])), "eos_scene_set_lights")
 
 
+class InstancedScene(DeviceScene):
+    """A two-level scene (eos_scene_create_instanced): placements of mesh scenes.
+
+    meshes: DeviceScene objects used as geometry (kept alive by this object);
+    instances: (mesh index, 3x4 world-from-object transform, material base) per instance;
+    materials [K, 10] / lights [L, 6] of the whole scene.  Hit ids are global: instance k's
+    triangles follow those of instances 0..k-1."""
+
+    def __init__(self, ctx: Context, meshes: list, instances: list, materials, lights, ambient_index: float = 1.0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.meshes = list(meshes)
+        arr = (L.Instance * len(instances))()
+        for i, (mi, M, base) in enumerate(instances):
+            arr[i].mesh = self.meshes[mi].h
+            for k, v in enumerate(np.asarray(M, np.float64).reshape(3, 4).reshape(-1)):
+                arr[i].transform[k] = float(v)
+            arr[i].material_base = int(base)
+        mats = materials_array(materials)
+        lts = np.ascontiguousarray(lights, np.float32).reshape(-1, 6)
+        h = c_void_p()
+        L.check(self.lib.eos_scene_create_instanced(ctx.h, arr, len(instances), _ptr(mats), mats.shape[0], _ptr(lts),
+                                                    lts.shape[0], byref(h)), "eos_scene_create_instanced")
+        self.h = h
+        self.n_tris = sum(self.meshes[mi].scene.n_tris for mi, _, _ in instances)
+        self.scene = None
+        if ambient_index != 1.0:
+            self.set_ambient_index(ambient_index)
+
+
 def _alloc(shape, dtype, device: bool):
     if device:
         import torch

@@ -357,7 +357,7 @@ eos_status eos_scene_destroy(eos_scene* sc) {
     cudaStreamSynchronize(sc->ctx->stream);
   }
   void* bufs[] = {sc->d_nodes, sc->d_tris, sc->d_shade, sc->d_pos_of_id, sc->d_mats, sc->d_lights, sc->d_codes,
-                  sc->d_order};
+                  sc->d_order, sc->d_inst};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete sc;
@@ -415,6 +415,7 @@ eos_status eos_scene_get_info(const eos_scene* sc, eos_scene_info* info) {
 
 eos_status eos_scene_get_morton(const eos_scene* sc, uint32_t* codes, uint32_t* order) {
   if (!sc) return EOS_ERR_INVALID_ARG;
+  if (sc->instanced) return EOS_ERR_UNSUPPORTED;
   EOS_CUDA(cudaSetDevice(sc->ctx->device));
   size_t b = 4ull * sc->dev.n_tris;
   if (b == 0) return EOS_OK;
@@ -540,7 +541,7 @@ eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_came
     return EOS_ERR_INVALID_ARG;
   eos_status st = check_params(p);
   if (st != EOS_OK) return st;
-  if (p->spp != 1 || p->row_begin != 0 || p->row_end != 0) return EOS_ERR_UNSUPPORTED;
+  if (p->spp != 1 || p->row_begin != 0 || p->row_end != 0 || sc->instanced) return EOS_ERR_UNSUPPORTED;
   for (uint32_t v = 0; v < n_views; ++v)
     if (!valid_camera(&cams[v]) || cams[v].width != cams[0].width || cams[v].height != cams[0].height)
       return EOS_ERR_INVALID_ARG;

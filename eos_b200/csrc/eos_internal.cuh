@@ -48,6 +48,16 @@ enum : int {
 //  Shading record, 48 B = 3 x float4, same order:
 //    [0] n1.x n1.y n1.z n2.x   [1] n2.y n2.z n3.x n3.y   [2] n3.z obj(int) - -
 // ---------------------------------------------------------------------------------
+// One instance of a mesh in a two-level scene (eos_scene_create_instanced), 80 B.
+struct DevInstance {
+  float minv[12];       // object-from-world affine, row-major 3x4 (the inverse of the transform)
+  const float4* nodes;  // the mesh's node records, triangle and shading records
+  const float4* tris;
+  const float4* shade;
+  int32_t id_offset;    // global id of the mesh's triangle 0 in this instance
+  int32_t mat_base;     // added to the mesh's object ids
+};
+
 struct DevScene {
   const float4* nodes;
   const float4* tris;
@@ -60,6 +70,8 @@ struct DevScene {
   int32_t n_obj;
   int32_t n_lights;
   float ambient_index;       // refractive index outside transparent objects
+  const DevInstance* inst;   // two-level scene: nodes = tree over instances (leaf = one
+  int32_t n_inst;            // instance), tris / shade / pos_of_id unused; else nullptr, 0
 };
 
 struct DevBuffer {
@@ -109,6 +121,9 @@ struct eos_scene {
   void* d_lights = nullptr;
   void* d_codes = nullptr;  // sorted Morton codes (kept for the test hook)
   void* d_order = nullptr;  // sorted triangle ids
+  void* d_inst = nullptr;   // DevInstance array of a two-level scene
+  bool instanced = false;
+  int mesh_levels = 0;      // deepest mesh tree of a two-level scene (stack bound)
   uint32_t n_nodes = 0;
   int leaf_size = 8;
   int layout = EOS_LAYOUT_SAH;

@@ -422,14 +422,114 @@ __device__ __noinline__ AnyResult any_hit_call(const DevScene& s, f3 o, f3 d, ui
   return any_hit_body<SH>(s, o, d, shs, stride, err);
 }
 
+// ------------------------------------------------------------------ two-level scenes
+// A scene of instances (eos_scene_create_instanced): s.nodes is a tree over the instances'
+// world boxes whose leaves each hold one instance; reaching one moves the ray into the
+// instance's object space and continues in its mesh's tree.  A marker entry below the
+// mesh's entries on the stack (t = -inf, so no limit drops it) brings the ray back.  t is
+// the same parameter in both spaces (the direction is not renormalised), so one limit
+// culls both levels.  Nearest-hit semantics as for a flat scene, with global ids.
+constexpr int kExitMesh = (int)0xC0000001;
+
+// o' = Minv [o, 1], d' = Minv [d, 0]; row r: ((m_r0 x + m_r1 y) + m_r2 z) (+ m_r3).
+__device__ __forceinline__ void to_object(const DevInstance* I, f3 o, f3 d, f3& oo, f3& od) {
+  const float4* m = reinterpret_cast<const float4*>(I->minv);
+  const float4 a = __ldg(m), b = __ldg(m + 1), c = __ldg(m + 2);
+  oo = mk3(((a.x * o.x + a.y * o.y) + a.z * o.z) + a.w, ((b.x * o.x + b.y * o.y) + b.z * o.z) + b.w,
+           ((c.x * o.x + c.y * o.y) + c.z * o.z) + c.w);
+  od = mk3((a.x * d.x + a.y * d.y) + a.z * d.z, (b.x * d.x + b.y * d.y) + b.z * d.z,
+           (c.x * d.x + c.y * d.y) + c.z * d.z);
+}
+
+// ANY: returns at the first hit (h.pos >= 0 then); otherwise the nearest hit.
+template <int SH, bool ANY>
+__device__ __noinline__ Hit traverse_instanced(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  Hit h;
+  h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
+  const SlabRay rw = make_slab(o, d);
+  SlabRay r = rw;
+  f3 oo = o, od = d;
+  const float4* nodes = s.nodes;
+  const float4* tris = nullptr;
+  int id_off = 0;
+  bool in_mesh = false;
+  TraversalStack<SH> st(shs, stride);
+  int cur = 0;
+  for (;;) {
+    const float limit = ANY ? kInf : h.t * kCull;
+    if (cur >= 0) {
+      if (!visit_node4<SH, !ANY>(nodes, r, cur, limit, st, h.nodes)) {
+        atomicOr(err, kErrStack);
+        return h;
+      }
+      continue;
+    }
+    if (cur == kDone) return h;
+    if (cur == kExitMesh) {  // back to the instance tree
+      r = rw;
+      nodes = s.nodes;
+      in_mesh = false;
+    } else if (!in_mesh) {  // an instance: continue in its mesh, in object space
+      const DevInstance* I = s.inst + leaf_first(cur);
+      to_object(I, o, d, oo, od);
+      r = make_slab(oo, od);
+      nodes = I->nodes;
+      tris = I->tris;
+      id_off = I->id_offset;
+      if (!st.push(kExitMesh, -kInf)) {
+        atomicOr(err, kErrStack);
+        return h;
+      }
+      in_mesh = true;
+      cur = 0;
+      continue;
+    } else {  // a leaf of the mesh
+      const int first = leaf_first(cur), cnt = leaf_count(cur);
+      for (int p = first; p < first + cnt; ++p) {
+        f3 v1, e1, e2;
+        int id;
+        load_tri(tris, p, v1, e1, e2, id);
+        float t, u, v;
+        ++h.tests;
+        if (!mt_intersect_fast(oo, od, v1, e1, e2, t, u, v)) continue;
+        const int gid = id_off + id;
+        if (ANY) {
+          h.t = t; h.u = u; h.v = v; h.pos = p; h.id = gid;
+          return h;
+        }
+        if (t < h.t || (t == h.t && gid > h.id)) {
+          h.t = t; h.u = u; h.v = v; h.pos = p; h.id = gid;
+        }
+      }
+    }
+    cur = ANY ? st.next_any() : st.next(h.t * kCull);
+  }
+}
+
+// Instance holding global triangle id `gid` (instances in id order).
+__device__ __forceinline__ const DevInstance* instance_of(const DevScene& s, int gid) {
+  int lo = 0, hi = s.n_inst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&s.inst[mid].id_offset) <= gid) lo = mid;
+    else hi = mid - 1;
+  }
+  return s.inst + lo;
+}
+
 template <int SH, bool INLINE = false>
 __device__ __forceinline__ Hit closest_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  if (s.inst) return traverse_instanced<SH, false>(s, o, d, shs, stride, err);
   if (INLINE) return closest_hit_body<SH>(s, o, d, shs, stride, err);
   return closest_hit_call<SH>(s, o, d, shs, stride, err);
 }
 
 template <int SH, bool INLINE = false>
 __device__ __forceinline__ AnyResult any_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  if (s.inst) {
+    const Hit h = traverse_instanced<SH, true>(s, o, d, shs, stride, err);
+    return AnyResult{h.pos >= 0 ? 1 : 0, h.nodes, h.tests};
+  }
   if (INLINE) return any_hit_body<SH>(s, o, d, shs, stride, err);
   return any_hit_call<SH>(s, o, d, shs, stride, err);
 }
@@ -451,12 +551,20 @@ __device__ __forceinline__ void warp_add_count(unsigned long long* dst, unsigned
 // (src/Triangle.cpp:41-46, src/BVH.cpp:373-380).
 __device__ __forceinline__ void hit_geometry(const DevScene& s, f3 o, f3 d, const Hit& h, f3& P, f3& N, int& obj) {
   P = add3(o, scale3(h.t, d));
-  const float4* sr = s.shade + 3 * (size_t)h.pos;
+  const DevInstance* I = s.inst ? instance_of(s, h.id) : nullptr;
+  const float4* sr = (I ? I->shade : s.shade) + 3 * (size_t)h.pos;
   float4 a = __ldg(sr), b = __ldg(sr + 1), c = __ldg(sr + 2);
   f3 n1 = mk3(a.x, a.y, a.z), n2 = mk3(a.w, b.x, b.y), n3 = mk3(b.z, b.w, c.x);
   obj = __float_as_int(c.y);
   float w = (1.0f - h.u) - h.v;
   f3 n = norm3(add3(add3(scale3(w, n1), scale3(h.u, n2)), scale3(h.v, n3)));
+  if (I) {  // normal to world space: Minv^T n, column c of Minv: ((m_0c n.x + m_1c n.y) + m_2c n.z)
+    const float* m = I->minv;
+    n = mk3((__ldg(m + 0) * n.x + __ldg(m + 4) * n.y) + __ldg(m + 8) * n.z,
+            (__ldg(m + 1) * n.x + __ldg(m + 5) * n.y) + __ldg(m + 9) * n.z,
+            (__ldg(m + 2) * n.x + __ldg(m + 6) * n.y) + __ldg(m + 10) * n.z);
+    obj += I->mat_base;
+  }
   N = norm3(n);
 }
 

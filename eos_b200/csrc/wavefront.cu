@@ -900,6 +900,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   for (uint32_t j = 0; j < n_jobs; ++j) {
     depth = std::max(depth, jobs[j].trace_depth);
     max_lights = std::max(max_lights, (int)jobs[j].scene->dev.n_lights);
+    // the lane-refill and packet kernels traverse single-level trees only
+    if (jobs[j].scene->instanced && (p.flags & (EOS_FLAG_REFILL | EOS_FLAG_PACKET))) return EOS_ERR_UNSUPPORTED;
   }
   // queue bytes per path: two ray queues, hit records, masks, shadow queue, accumulators
   const long long per_path = 3ll * 32 + 4 + 32ll * std::max(1, max_lights) + 16ll * (depth + 1);

@@ -444,3 +444,107 @@ def small_random_scene(seed: int, n_spheres: int = 4, level: int = 2, lights: in
     sc = b.build(ls, f"small{seed}")
     sc.ambient_index = float(ambient_index)
     return sc
+
+
+# ----------------------------------------------------------------------------- instancing
+@dataclass
+class InstancedData:
+    """A two-level scene: meshes (each a SceneData whose own materials are unused), and
+    instances (mesh index, 3x4 world-from-object transform, material base)."""
+    meshes: list
+    instances: list
+    materials: np.ndarray
+    lights: np.ndarray
+    name: str = "instances"
+    ambient_index: float = 1.0
+
+    def __post_init__(self):
+        self.materials = pad_materials(self.materials)
+        self.lights = np.ascontiguousarray(self.lights, dtype=np.float32).reshape(-1, LIGHT_STRIDE)
+
+    @property
+    def n_tris(self) -> int:
+        return sum(self.meshes[m].n_tris for m, _, _ in self.instances)
+
+    def flatten(self) -> SceneData:
+        """The same triangles transformed into world space (float64, then float32)."""
+        V, N, F, O = [], [], [], []
+        nv = 0
+        for m, M, base in self.instances:
+            sc = self.meshes[m]
+            A, t = np.asarray(M, np.float64)[:, :3], np.asarray(M, np.float64)[:, 3]
+            V.append(sc.verts.astype(np.float64) @ A.T + t)
+            n = sc.normals.astype(np.float64) @ np.linalg.inv(A)
+            N.append(n / np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30))
+            F.append(sc.tris.astype(np.int64) + nv)
+            O.append(sc.tri_obj.astype(np.int64) + base)
+            nv += sc.verts.shape[0]
+        return SceneData(np.concatenate(V), np.concatenate(N), np.concatenate(F), np.concatenate(O), self.materials,
+                         self.lights, self.name + " (flattened)", self.ambient_index)
+
+
+def _affine(R, t, scale=1.0):
+    M = np.zeros((3, 4))
+    M[:, :3] = np.asarray(R, np.float64) * scale
+    M[:, 3] = t
+    return M
+
+
+def instanced_test_scene(seed: int, n_instances: int = 12, lights: int = 2, transparent: int = 0) -> InstancedData:
+    """Three meshes (a level-2 icosphere, a ground quad, a 300-triangle foliage cluster) placed
+    n_instances times: instance 0 is the identity, the others rotated, scaled (one of them
+    non-uniformly, one mirrored) and moved; one material per instance."""
+    rng = rng_for(seed)
+    meshes = []
+    v, f = icosphere(2)
+    meshes.append(SceneData(v, v, f, np.zeros(len(f)), [material((0.5, 0.5, 0.5), 0.2, 16, 0.0)], np.zeros((0, 6))))
+    qv, qn, qf = ground_quad(4.0, 0.0)
+    meshes.append(SceneData(qv, qn, qf, np.zeros(len(qf)), [material((0.5, 0.5, 0.5), 0.2, 16, 0.0)], np.zeros((0, 6))))
+    cv, cn, cf = foliage_cluster(300, rng, radius=1.0)
+    meshes.append(SceneData(cv, cn, cf, np.zeros(len(cf)), [material((0.5, 0.5, 0.5), 0.2, 16, 0.0)], np.zeros((0, 6))))
+    instances = [(1, _affine(np.eye(3), (0.0, -2.5, 0.0)), 0)]
+    mats = [_random_material(rng, 0.5)]
+    for k in range(1, n_instances):
+        R = random_rotation(rng)
+        t = rng.uniform([-3, -1.5, -3], [3, 1.5, 3])
+        s = rng.uniform(0.4, 1.2)
+        M = _affine(R, t, s)
+        if k == 1:
+            M[:, :3] = np.eye(3)  # identity placement of the sphere
+            M[:, 3] = 0.0
+        if k == 2:
+            M[:, :3] = M[:, :3] @ np.diag([1.0, 0.5, 1.5])  # non-uniform scale
+        if k == 3:
+            M[:, :3] = M[:, :3] @ np.diag([-1.0, 1.0, 1.0])  # mirrored
+        instances.append((0 if k % 2 else 2, M, k))
+        m = _random_material(rng, 0.5)
+        if k <= transparent:
+            m[7], m[8], m[9] = 0.0, 1.0, 1.52
+        mats.append(m)
+    ls = [[*rng.uniform([-5, 3, -5], [5, 8, 5]), 1, 1, 1] for _ in range(lights)]
+    return InstancedData(meshes, instances, np.array(mats), np.array(ls), f"instanced{seed}")
+
+
+def config5_instanced(seed: int = 1005, instances: int = 800, cluster_tris: int = 5000,
+                      cells: int = 512) -> InstancedData:
+    """Config 5 as instances: the height field once and the foliage cluster stored once and
+    placed 800 times (the same rotations, offsets and materials as config5_scene)."""
+    rng = rng_for(seed)
+    V, N, F = heightfield(cells, 200.0, rng)
+    mats = [_random_material(rng, 0.9)]
+    unused = [material((0.5, 0.5, 0.5), 0.2, 16, 0.0)]
+    hf = SceneData(V, N, F, np.zeros(len(F)), unused, np.zeros((0, 6)), "heightfield")
+    cV, cN, cF = foliage_cluster(cluster_tris, rng)
+    cl = SceneData(cV, cN, cF, np.zeros(len(cF)), unused, np.zeros((0, 6)), "foliage cluster")
+    inst = [(0, _affine(np.eye(3), (0.0, 0.0, 0.0)), 0)]
+    for k in range(instances):
+        R = random_rotation(rng)
+        t = rng.uniform([-200, 0, -200], [200, 50, 200])
+        inst.append((1, _affine(R, t), k + 1))
+        mats.append(_random_material(rng, 0.9))
+    lights = []
+    for _ in range(8):
+        p = rng.uniform([-200, 60, -200], [200, 150, 200])
+        i = rng.uniform(0.3, 0.8)
+        lights.append([*p, i, i, i])
+    return InstancedData([hf, cl], inst, np.array(mats), np.array(lights), "foliage800x5000+heightfield512, instanced")

@@ -27,6 +27,8 @@
  *   eos_trace_closest / any      Scene::findMinDistanceIntersectionBVH /
  *                                shadowRayVisibilityBVH (src/Scene.cpp:145-158)
  *   eos_mesh_load_obj            TriangleMesh::loadFromFile (src/triangleMesh.cpp:79-160)
+ *   eos_scene_create_instanced   per-object transformations (src/Scene.cpp:96-106,
+ *                                src/kernelInvocations.h:158-163) with shared meshes
  *
  * Buffers are owned by the caller.  A pointer argument may be host or device memory; the
  * library tells them apart with cudaPointerGetAttributes and stages host buffers through
@@ -251,6 +253,30 @@ eos_status eos_scene_set_lights(eos_scene* scene, const eos_light* lights, uint3
  * transparent object; 1 when never set. */
 eos_status eos_scene_set_ambient_index(eos_scene* scene, float refractive_index);
 eos_status eos_scene_get_info(const eos_scene* scene, eos_scene_info* info);
+/* One placement of a mesh scene in an instanced scene. */
+typedef struct eos_instance {
+  const eos_scene* mesh;     /* a scene from eos_scene_create, used as geometry only (its tree,
+                                triangles and object ids); it must outlive the instanced scene */
+  float transform[12];       /* world-from-object affine, row-major 3x4 [A | t] */
+  uint32_t material_base;    /* added to the mesh's triangle object ids */
+} eos_instance;
+
+/* A two-level scene: a tree over the instances' world boxes (built on the host), each
+ * instance's mesh traversed with the ray moved into its object space -- what the
+ * reference's GPU kernel does per triangle with the inverse of its transformation
+ * (src/kernelInvocations.h:158-163, src/Scene.cpp:96-106).  Ray r in object space:
+ * o' = A^-1 (o - t) evaluated as Minv [o, 1] (Minv = the inverse affine, computed in
+ * double from the adjugate and rounded to float), d' = Minv [d, 0], not renormalised,
+ * so t is the same parameter in both spaces.  The shading normal is
+ * normalize(Minv^T n) of the mesh's interpolated unit normal; hit ids are global:
+ * instance k's triangles are numbered after those of instances 0..k-1.  A mesh shared by
+ * many instances is stored once.  eos_render / eos_render_batch / eos_trace_* accept the
+ * scene (not EOS_FLAG_REFILL / EOS_FLAG_PACKET); eos_render_backward and
+ * eos_scene_get_morton return EOS_ERR_UNSUPPORTED. */
+eos_status eos_scene_create_instanced(eos_ctx* ctx, const eos_instance* instances, uint32_t n_instances,
+                                      const eos_material* materials, uint32_t n_materials,
+                                      const eos_light* lights, uint32_t n_lights, eos_scene** out);
+
 /* Test hook: Morton codes of the triangles in sorted order and the sorted triangle ids. */
 eos_status eos_scene_get_morton(const eos_scene* scene, uint32_t* codes, uint32_t* order);
 

@@ -60,6 +60,9 @@ def lib_oracle():
                                           POINTER(c_float), c_int]
         L.oracle_scene_destroy.argtypes = [c_void_p]
         L.oracle_scene_set_ambient.argtypes = [c_void_p, c_float]
+        L.oracle_instanced_create.restype = c_void_p
+        L.oracle_instanced_create.argtypes = [POINTER(c_void_p), POINTER(c_int32), POINTER(c_float), POINTER(c_int32),
+                                              c_int, POINTER(c_float), c_int, POINTER(c_float), c_int]
         L.oracle_render.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
                                     c_uint32, POINTER(c_int32), c_int, c_int, POINTER(c_float),
                                     POINTER(c_int32), POINTER(c_uint32), POINTER(c_uint32),
@@ -228,6 +231,27 @@ class Oracle:
         if g is None:
             return rgb
         return rgb, gm, gl
+
+
+class OracleInstanced(Oracle):
+    """The C restatement over a two-level scene (scenes.InstancedData): every instance's
+    mesh is tested with the ray in its object space (no instance tree)."""
+
+    def __init__(self, idata):
+        L = lib_oracle()
+        self.scene = idata
+        self.meshes = [Oracle(m) for m in idata.meshes]
+        n = len(idata.instances)
+        handles = (c_void_p * len(self.meshes))(*[m.h for m in self.meshes])
+        mesh_of = np.array([m for m, _, _ in idata.instances], np.int32)
+        tr = np.ascontiguousarray(np.stack([np.asarray(M, np.float64).reshape(3, 4) for _, M, _ in idata.instances]),
+                                  np.float32)
+        base = np.array([b for _, _, b in idata.instances], np.int32)
+        self._keep = (mesh_of, tr, base, idata)
+        self.h = L.oracle_instanced_create(handles, _p(mesh_of, c_int32), _p(tr, c_float), _p(base, c_int32), n,
+                                           _p(idata.materials, c_float), idata.materials.shape[0],
+                                           _p(idata.lights, c_float), idata.lights.shape[0])
+        L.oracle_scene_set_ambient(self.h, float(idata.ambient_index))
 
 
 class RefRenderer:

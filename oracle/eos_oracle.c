@@ -80,6 +80,12 @@ typedef struct {
   uint32_t *obj;                               /* sorted position -> object */
   float *mats;                                 /* nobj x OMAT (eos_material) */
   float ambient;                               /* refractive index outside objects */
+  /* two-level scene (oracle_instanced_create): ninst > 0, the arrays above unused */
+  int ninst;
+  const void** inst_mesh;                      /* per instance: its mesh (an oscene) */
+  float* inst_minv;                            /* ninst x 12: object-from-world affine */
+  int32_t* inst_id_off;                        /* global id of the mesh's triangle 0 */
+  int32_t* inst_mat_base;
   float *lights;                               /* nl x 6 */
   onode *nodes;
   int nnodes;
@@ -225,7 +231,8 @@ void oracle_scene_destroy(void* h) {
   if (!s) return;
   free(s->v1); free(s->v2); free(s->v3); free(s->e1); free(s->e2);
   free(s->n1); free(s->n2); free(s->n3); free(s->id); free(s->obj); free(s->pos_of_id);
-  free(s->mats); free(s->lights); free(s->nodes); free(s);
+  free(s->mats); free(s->lights); free(s->nodes);
+  free((void*)s->inst_mesh); free(s->inst_minv); free(s->inst_id_off); free(s->inst_mat_base); free(s);
 }
 
 /* ---------------------------------------------------------------- intersection */
@@ -287,12 +294,12 @@ static inline int box_test(const onode* n, const bray* r, float tlimit) {
 
 static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
 
-typedef struct { int pos; float t, u, v; float t2; } chit;
+typedef struct { int pos; float t, u, v; float t2; int gid, inst; } chit;
 
 /* Nearest hit with the larger-id tie rule; also tracks the second-nearest distinct hit
  * (culling by it) so near ties can be flagged. */
-static chit closest(const oscene* s, v3f o, v3f d) {
-  chit h; h.pos = -1; h.t = FLT_MAX; h.u = h.v = 0; h.t2 = FLT_MAX;
+static chit closest_flat(const oscene* s, v3f o, v3f d) {
+  chit h; h.pos = -1; h.t = FLT_MAX; h.u = h.v = 0; h.t2 = FLT_MAX; h.gid = -1; h.inst = -1;
   if (s->nt == 0) return h;
   bray br = make_bray(o, d);
   int stack[128]; int sp = 0;
@@ -308,7 +315,7 @@ static chit closest(const oscene* s, v3f o, v3f d) {
         int better = h.pos < 0 || t < h.t || (t == h.t && s->id[p] > s->id[h.pos]);
         if (better) {
           if (h.pos >= 0 && h.t < h.t2) h.t2 = h.t;
-          h.pos = p; h.t = t; h.u = u; h.v = v;
+          h.pos = p; h.t = t; h.u = u; h.v = v; h.gid = s->id[p];
         } else if (t < h.t2) {
           h.t2 = t;
         }
@@ -321,7 +328,7 @@ static chit closest(const oscene* s, v3f o, v3f d) {
   return h;
 }
 
-static int any_hit(const oscene* s, v3f o, v3f d) {
+static int any_hit_flat(const oscene* s, v3f o, v3f d) {
   if (s->nt == 0) return 0;
   bray br = make_bray(o, d);
   int stack[128]; int sp = 0;
@@ -340,6 +347,92 @@ static int any_hit(const oscene* s, v3f o, v3f d) {
     }
   }
   return 0;
+}
+
+/* ---------------------------------------------------------------- two-level scenes */
+/* A scene of instances of mesh scenes (the library's eos_scene_create_instanced): every
+ * instance's mesh is tested with the ray moved into its object space,
+ * o' = Minv [o, 1], d' = Minv [d, 0] with row r evaluated as ((m_r0 x + m_r1 y) + m_r2 z)
+ * (+ m_r3), in float; the nearest hit over all instances with the larger global id on
+ * exact ties; the normal is normalize(Minv^T n).  Minv is the inverse of the world-from-
+ * object affine [A | t] computed in double from the adjugate and rounded to float. */
+static void affine_inverse_d(const float* M, float* out) {
+  const double a00 = M[0], a01 = M[1], a02 = M[2], a10 = M[4], a11 = M[5], a12 = M[6];
+  const double a20 = M[8], a21 = M[9], a22 = M[10];
+  const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+  const double det = (a00 * c00 + a01 * c01) + a02 * c02;
+  const double inv[3][3] = {{c00 / det, (a02 * a21 - a01 * a22) / det, (a01 * a12 - a02 * a11) / det},
+                            {c01 / det, (a00 * a22 - a02 * a20) / det, (a02 * a10 - a00 * a12) / det},
+                            {c02 / det, (a01 * a20 - a00 * a21) / det, (a00 * a11 - a01 * a10) / det}};
+  const double t[3] = {M[3], M[7], M[11]};
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) out[4 * r + c] = (float)inv[r][c];
+    out[4 * r + 3] = (float)(-((inv[r][0] * t[0] + inv[r][1] * t[1]) + inv[r][2] * t[2]));
+  }
+}
+
+static inline void to_object(const float* m, v3f o, v3f d, v3f* oo, v3f* od) {
+  *oo = V3(((m[0] * o.x + m[1] * o.y) + m[2] * o.z) + m[3], ((m[4] * o.x + m[5] * o.y) + m[6] * o.z) + m[7],
+           ((m[8] * o.x + m[9] * o.y) + m[10] * o.z) + m[11]);
+  *od = V3((m[0] * d.x + m[1] * d.y) + m[2] * d.z, (m[4] * d.x + m[5] * d.y) + m[6] * d.z,
+           (m[8] * d.x + m[9] * d.y) + m[10] * d.z);
+}
+
+static chit closest(const oscene* s, v3f o, v3f d) {
+  if (!s->ninst) return closest_flat(s, o, d);
+  chit best; best.pos = -1; best.t = FLT_MAX; best.u = best.v = 0; best.t2 = FLT_MAX; best.gid = -1; best.inst = -1;
+  for (int i = 0; i < s->ninst; ++i) {
+    const oscene* m = (const oscene*)s->inst_mesh[i];
+    v3f oo, od;
+    to_object(s->inst_minv + 12 * i, o, d, &oo, &od);
+    chit h = closest_flat(m, oo, od);
+    if (h.t2 < best.t2) best.t2 = h.t2;
+    if (h.pos < 0) continue;
+    int gid = s->inst_id_off[i] + m->id[h.pos];
+    int better = best.pos < 0 || h.t < best.t || (h.t == best.t && gid > best.gid);
+    if (better) {
+      if (best.pos >= 0 && best.t < best.t2) best.t2 = best.t;
+      best.pos = h.pos; best.t = h.t; best.u = h.u; best.v = h.v; best.gid = gid; best.inst = i;
+    } else if (h.t < best.t2) {
+      best.t2 = h.t;
+    }
+  }
+  return best;
+}
+
+static int any_hit(const oscene* s, v3f o, v3f d) {
+  if (!s->ninst) return any_hit_flat(s, o, d);
+  for (int i = 0; i < s->ninst; ++i) {
+    v3f oo, od;
+    to_object(s->inst_minv + 12 * i, o, d, &oo, &od);
+    if (any_hit_flat((const oscene*)s->inst_mesh[i], oo, od)) return 1;
+  }
+  return 0;
+}
+
+void* oracle_instanced_create(void* const* meshes, const int32_t* mesh_of, const float* transforms,
+                              const int32_t* mat_base, int ninst, const float* mats, int nobj, const float* lights,
+                              int nl) {
+  oscene* s = (oscene*)calloc(1, sizeof(oscene));
+  s->ninst = ninst; s->nobj = nobj; s->nl = nl; s->ambient = 1.0f;
+  s->inst_mesh = malloc(sizeof(void*) * (size_t)ninst);
+  s->inst_minv = malloc(sizeof(float) * 12 * (size_t)ninst);
+  s->inst_id_off = malloc(sizeof(int32_t) * (size_t)ninst);
+  s->inst_mat_base = malloc(sizeof(int32_t) * (size_t)ninst);
+  int total = 0;
+  for (int i = 0; i < ninst; ++i) {
+    s->inst_mesh[i] = meshes[mesh_of[i]];
+    affine_inverse_d(transforms + 12 * i, s->inst_minv + 12 * i);
+    s->inst_id_off[i] = total;
+    s->inst_mat_base[i] = mat_base[i];
+    total += ((const oscene*)meshes[mesh_of[i]])->nt;
+  }
+  s->nt = total;
+  s->mats = malloc(sizeof(float) * OMAT * (size_t)(nobj > 0 ? nobj : 1));
+  memcpy(s->mats, mats, sizeof(float) * OMAT * (size_t)nobj);
+  s->lights = malloc(sizeof(float) * 6 * (size_t)(nl > 0 ? nl : 1));
+  memcpy(s->lights, lights, sizeof(float) * 6 * (size_t)nl);
+  return s;
 }
 
 /* ---------------------------------------------------------------- FP32 render */
@@ -377,6 +470,26 @@ static inline void hit_geometry(const oscene* s, int p, v3f o, v3f d, float t, f
   v3f a = vscale(w, s->n1[p]), b = vscale(u, s->n2[p]), c = vscale(v, s->n3[p]);
   v3f n = vnorm(vadd(vadd(a, b), c));
   *N = vnorm(n);
+}
+
+/* The hit's point, normal and object (either kind of scene). */
+static inline void hit_shading(const oscene* s, const chit* h, v3f o, v3f d, v3f* P, v3f* N, int* obj) {
+  if (!s->ninst) {
+    hit_geometry(s, h->pos, o, d, h->t, h->u, h->v, P, N);
+    *obj = (int)s->obj[h->pos];
+    return;
+  }
+  const oscene* m = (const oscene*)s->inst_mesh[h->inst];
+  const float* M = s->inst_minv + 12 * h->inst;
+  int p = h->pos;
+  *P = vadd(o, vscale(h->t, d));
+  float w = (1.0f - h->u) - h->v;
+  v3f a = vscale(w, m->n1[p]), b = vscale(h->u, m->n2[p]), c = vscale(h->v, m->n3[p]);
+  v3f n = vnorm(vadd(vadd(a, b), c));
+  v3f nw = V3((M[0] * n.x + M[4] * n.y) + M[8] * n.z, (M[1] * n.x + M[5] * n.y) + M[9] * n.z,
+              (M[2] * n.x + M[6] * n.y) + M[10] * n.z);
+  *N = vnorm(nw);
+  *obj = (int)m->obj[p] + s->inst_mat_base[h->inst];
 }
 
 /* RayTracer::calcPhong for one light (src/RayTracer.cpp:418-458). */
@@ -464,12 +577,13 @@ static v3f trace_path(const oscene* s, const float* cam, v3f o, v3f d, int trace
     if (d.x == 0.0f || d.y == 0.0f || d.z == 0.0f) *flags |= FLAG_AXIS_PARALLEL;
     chit h = closest(s, o, d);
     if (h.pos < 0) { hits[k] = HIT_NONE; break; }
-    hits[k] = s->id[h.pos];
+    hits[k] = h.gid;
     if (h.t2 < FLT_MAX && fbits(h.t2) - fbits(h.t) <= 2u) *flags |= FLAG_TIE;
     if (h.t < 1e-3f || h.t > 999.0f) *flags |= FLAG_OUT_OF_RANGE;
     v3f P, N;
-    hit_geometry(s, h.pos, o, d, h.t, h.u, h.v, &P, &N);
-    const float* m = s->mats + OMAT * s->obj[h.pos];
+    int ob;
+    hit_shading(s, &h, o, d, &P, &N, &ob);
+    const float* m = s->mats + OMAT * ob;
     v3f acc = V3(0, 0, 0);
     uint32_t mask = 0;
     for (int li = 0; li < s->nl; ++li) {
@@ -553,7 +667,7 @@ void oracle_closest(void* h, const float* rays, int n, int32_t* ids, float* ts, 
   for (int i = 0; i < n; ++i) {
     const float* r = rays + 6 * (size_t)i;
     chit c = closest(s, V3(r[0], r[1], r[2]), V3(r[3], r[4], r[5]));
-    ids[i] = c.pos < 0 ? HIT_NONE : s->id[c.pos];
+    ids[i] = c.pos < 0 ? HIT_NONE : c.gid;
     if (ts) ts[i] = c.pos < 0 ? FLT_MAX : c.t;
     if (tie) tie[i] = (c.pos >= 0 && c.t2 < FLT_MAX && fbits(c.t2) - fbits(c.t) <= 2u) ? 1 : 0;
   }
