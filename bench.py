@@ -14,7 +14,7 @@ renders the V views:
           renderCudaSceneToHostBufferMegaKernel contract)
 
 Rays = primary + shadow + secondary (mirror) rays actually traced, from the library's
-counters.  The scene (~170 MB of node / triangle / shading records) is larger than L2.
+counters.  The scene (~135 MB of node / triangle / shading records) is larger than L2.
 
 --impl reference: the reference's CPU renderer on the host cores for the same metric.
 The reference's own BVH builder aborts on this scene (heap corruption), so
@@ -532,42 +532,64 @@ def config3_timing(ctx, stream, steps, warmup):
 
 def config5_timing(ctx, stream, steps, warmup):
     """Stress workload: 3840x2160, 2 spp with jitter, depth 4, 8 lights, 4,524,288 thin
-    triangles; one frame per step, batched wavefront vs plain."""
+    triangles; one frame per step, batched wavefront vs plain.  The same scene also as
+    801 instances (the height field once, the 5,000-triangle cluster stored once and placed
+    800 times; eos_scene_create_instanced)."""
     import torch
     from eos_b200 import api, scenes
     sc = scenes.config5_scene()
     dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
     cam = scenes.config5_camera()
-    job = [api.BatchJob(dsc, cam, 3, 0.5, spp=2, jitter_seed=7)]
-    outs = api.make_batch_outputs(job, ("rgba8",))
 
-    def batched():
-        return [api.render_batch(ctx, job, outs)]
+    def measure(scene):
+        job = [api.BatchJob(scene, cam, 3, 0.5, spp=2, jitter_seed=7)]
+        outs = api.make_batch_outputs(job, ("rgba8",))
 
-    def plain():
-        return [api.render(ctx, dsc, cam, 3, pixel_offset=0.5, spp=2, jitter_seed=7, outputs=(),
-                           out=dict(outs[0]))["stats"]]
+        def batched():
+            return [api.render_batch(ctx, job, outs)]
 
-    res = {}
-    for name, fn in (("batched", batched), ("plain", plain)):
-        for _ in range(warmup):
-            fn()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        rays = 0
-        for _ in range(steps):
-            rays += sum(s["primary_rays"] + s["shadow_rays"] + s["secondary_rays"] for s in fn())
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        res[name] = {"mrays": round(rays / (ms * 1e-3) / 1e6, 1), "ms_per_frame": round(ms / steps, 2),
-                     "rays_per_frame": rays // steps}
+        def plain():
+            return [api.render(ctx, scene, cam, 3, pixel_offset=0.5, spp=2, jitter_seed=7, outputs=(),
+                               out=dict(outs[0]))["stats"]]
+
+        res = {}
+        for name, fn in (("batched", batched), ("plain", plain)):
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rays = 0
+            for _ in range(steps):
+                rays += sum(s["primary_rays"] + s["shadow_rays"] + s["secondary_rays"] for s in fn())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            res[name] = {"mrays": round(rays / (ms * 1e-3) / 1e6, 1), "ms_per_frame": round(ms / steps, 2),
+                         "rays_per_frame": rays // steps}
+        res["batched_over_plain"] = round(res["batched"]["mrays"] / res["plain"]["mrays"], 3)
+        return res
+
+    res = measure(dsc)
     info = dsc.info()
-    return {"tris": sc.n_tris, "resolution": "3840x2160", "spp": 2, "depth": 4, "lights": 8, **res,
-            "batched_over_plain": round(res["batched"]["mrays"] / res["plain"]["mrays"], 3),
-            "build_ms": round(info["build_ms"], 2), "builder": {1: "lbvh", 2: "ploc"}.get(info["builder"], "?")}
+    out = {"tris": sc.n_tris, "resolution": "3840x2160", "spp": 2, "depth": 4, "lights": 8, **res,
+           "build_ms": round(info["build_ms"], 2), "builder": {1: "lbvh", 2: "ploc"}.get(info["builder"], "?"),
+           "scene_device_mb": round(info["device_bytes"] / 1e6, 1)}
+    del dsc
+    idata = scenes.config5_instanced()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    meshes = [api.DeviceScene(ctx, m, inputs_on_device=True) for m in idata.meshes]
+    inst = api.InstancedScene(ctx, meshes, idata.instances, idata.materials, idata.lights)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    r2 = measure(inst)
+    out["instanced"] = {"instances": len(idata.instances), "stored_tris": sum(m.n_tris for m in idata.meshes),
+                        "scene_device_mb": round((inst.info()["device_bytes"] +
+                                                  sum(m.info()["device_bytes"] for m in meshes)) / 1e6, 1),
+                        "build_ms_wall": round(build_s * 1e3, 1), **r2}
+    return out
 
 
 def adjoint_timing(ctx, stream, reps=5):
