@@ -22,7 +22,7 @@ MODE_WAVEFRONT = 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error",
           4: "device loop ran out of iterations", 5: "traversal stack overflow",
-          6: "ray queue overflow", 7: "unsupported", 8: "no CUDA device", 9: "file could not be read",
+          6: "ray queue overflow", 7: "unsupported", 8: "no CUDA device", 9: "file could not be read or written",
           10: "malformed input file"}
 
 
@@ -136,6 +136,8 @@ SIGNATURES = [
                                      c_void_p, POINTER(Stats)]),
     ("eos_scene_create_instanced", c_int32, [c_void_p, c_void_p, c_uint32, c_void_p, c_uint32, c_void_p, c_uint32,
                                              POINTER(c_void_p)]),
+    ("eos_scene_save", c_int32, [c_void_p, c_char_p]),
+    ("eos_scene_load", c_int32, [c_void_p, c_char_p, POINTER(c_void_p)]),
     ("eos_mesh_load_obj", c_int32, [c_char_p, POINTER(c_void_p)]),
     ("eos_mesh_parse_obj", c_int32, [c_char_p, c_size_t, POINTER(c_void_p)]),
     ("eos_mesh_get_info", c_int32, [c_void_p, POINTER(MeshInfo)]),

@@ -6,6 +6,8 @@ buffers are numpy arrays, which the library stages through its own device memory
 from __future__ import annotations
 
 import ctypes
+import os
+import weakref
 from ctypes import byref, c_void_p
 from dataclasses import dataclass
 
@@ -63,13 +65,18 @@ def stats_dict(st: L.Stats) -> dict:
 class Context:
     def __init__(self, device: int = 0):
         self.lib = L.load()
+        self._scenes = weakref.WeakSet()  # scenes on this context, destroyed before it
         h = c_void_p()
         L.check(self.lib.eos_ctx_create(device, byref(h)), "eos_ctx_create")
         self.h = h
         self.device = device
 
     def close(self):
+        """Destroy the context and, first, every scene still open on it (a scene's
+        destroy reaches its context's stream)."""
         if getattr(self, "h", None):
+            for sc in list(getattr(self, "_scenes", ())):
+                sc.close()
             self.lib.eos_ctx_destroy(self.h)
             self.h = None
 
@@ -127,6 +134,7 @@ class DeviceScene:
                                          lights.shape[0], byref(bp), byref(h))
         L.check(code, "eos_scene_create")
         self.h = h
+        ctx._scenes.add(self)
         if scene.ambient_index != 1.0:
             self.set_ambient_index(scene.ambient_index)
 
@@ -164,6 +172,23 @@ class DeviceScene:
         l = lights if hasattr(lights, "data_ptr") else np.ascontiguousarray(lights, np.float32).reshape(-1, 6)
         L.check(self.lib.eos_scene_set_lights(self.h, _ptr(l), int(l.shape[0])), "eos_scene_set_lights")
 
+    def save(self, path):
+        """Write the built scene to a file (eos_scene_save)."""
+        L.check(self.lib.eos_scene_save(self.h, os.fsencode(path)), "eos_scene_save")
+
+    @classmethod
+    def load(cls, ctx: Context, path, scene: SceneData | None = None) -> "DeviceScene":
+        """A scene read from a file of eos_scene_save, with no build (eos_scene_load).
+        scene: the SceneData it was made from, where the caller has it (render_backward
+        and morton read its sizes)."""
+        self = cls.__new__(cls)
+        self.ctx, self.lib, self.scene = ctx, ctx.lib, scene
+        h = c_void_p()
+        L.check(self.lib.eos_scene_load(ctx.h, os.fsencode(path), byref(h)), "eos_scene_load")
+        self.h = h
+        ctx._scenes.add(self)
+        return self
+
 
 class InstancedScene(DeviceScene):
     """A two-level scene (eos_scene_create_instanced): placements of mesh scenes.
@@ -189,6 +214,7 @@ class InstancedScene(DeviceScene):
         L.check(self.lib.eos_scene_create_instanced(ctx.h, arr, len(instances), _ptr(mats), mats.shape[0], _ptr(lts),
                                                     lts.shape[0], byref(h)), "eos_scene_create_instanced")
         self.h = h
+        ctx._scenes.add(self)
         self.n_tris = sum(self.meshes[mi].scene.n_tris for mi, _, _ in instances)
         self.scene = None
         if ambient_index != 1.0:

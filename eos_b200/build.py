@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libeos_b200.so")
-SOURCES = ["api.cu", "lbvh.cu", "ploc.cu", "instances.cu", "render.cu", "wavefront.cu", "adjoint.cu", "mesh.cpp"]
+SOURCES = ["api.cu", "lbvh.cu", "ploc.cu", "instances.cu", "scene_io.cu", "render.cu", "wavefront.cu", "adjoint.cu", "mesh.cpp"]
 HEADERS = ["eos_math.cuh", "eos_internal.cuh", "trace.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -196,7 +196,7 @@ const char* eos_status_string(eos_status s) {
     case EOS_ERR_QUEUE_OVERFLOW: return "ray queue overflow";
     case EOS_ERR_UNSUPPORTED: return "unsupported";
     case EOS_ERR_NO_DEVICE: return "no CUDA device";
-    case EOS_ERR_IO: return "file could not be read";
+    case EOS_ERR_IO: return "file could not be read or written";
     case EOS_ERR_PARSE: return "malformed input file";
   }
   return "unknown status";

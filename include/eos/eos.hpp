@@ -441,6 +441,21 @@ inline cudaScene_t* createCudaScene(Scene* scene, eos_ctx* ctx = nullptr) {
   return cs.release();
 }
 
+// Scene file of a built device scene (eos_scene_save / eos_scene_load): a later run loads
+// the tree instead of building it.  No reference counterpart.
+inline void saveCudaScene(const cudaScene_t* cs, const std::string& path) {
+  if (!cs) throw Error(EOS_ERR_INVALID_ARG, "saveCudaScene");
+  check(eos_scene_save(cs->scene, path.c_str()), "saveCudaScene");
+}
+
+inline cudaScene_t* loadCudaScene(const std::string& path, eos_ctx* ctx = nullptr) {
+  if (!ctx) ctx = default_context();
+  std::unique_ptr<cudaScene_t> cs(new cudaScene_t());
+  cs->ctx = ctx;
+  check(eos_scene_load(ctx, path.c_str(), &cs->scene), "loadCudaScene");
+  return cs.release();
+}
+
 // src/DeviceCameraHandler.h: the camera travels as kernel arguments, so the "device"
 // camera is a host copy that the renderer reads at each frame.
 class DeviceCameraHandler {

@@ -29,6 +29,8 @@
  *   eos_mesh_load_obj            TriangleMesh::loadFromFile (src/triangleMesh.cpp:79-160)
  *   eos_scene_create_instanced   per-object transformations (src/Scene.cpp:96-106,
  *                                src/kernelInvocations.h:158-163) with shared meshes
+ *   eos_scene_save / load        (no reference counterpart: the reference rebuilds its
+ *                                tree in Scene::flush on every run, src/Scene.cpp:204-209)
  *
  * Buffers are owned by the caller.  A pointer argument may be host or device memory; the
  * library tells them apart with cudaPointerGetAttributes and stages host buffers through
@@ -60,7 +62,7 @@ typedef enum eos_status {
   EOS_ERR_QUEUE_OVERFLOW = 6,
   EOS_ERR_UNSUPPORTED = 7,
   EOS_ERR_NO_DEVICE = 8,
-  EOS_ERR_IO = 9,             /* a file could not be read */
+  EOS_ERR_IO = 9,             /* a file could not be opened, read or written */
   EOS_ERR_PARSE = 10          /* malformed input file */
 } eos_status;
 
@@ -246,6 +248,7 @@ eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* norma
                             const eos_material* materials, uint32_t n_materials,
                             const eos_light* lights, uint32_t n_lights,
                             const eos_build_params* build, eos_scene** out);
+/* Destroy every scene before the context it was created on (it syncs that context's stream). */
 eos_status eos_scene_destroy(eos_scene* scene);
 eos_status eos_scene_set_materials(eos_scene* scene, const eos_material* materials, uint32_t n);
 eos_status eos_scene_set_lights(eos_scene* scene, const eos_light* lights, uint32_t n);
@@ -276,6 +279,19 @@ typedef struct eos_instance {
 eos_status eos_scene_create_instanced(eos_ctx* ctx, const eos_instance* instances, uint32_t n_instances,
                                       const eos_material* materials, uint32_t n_materials,
                                       const eos_light* lights, uint32_t n_lights, eos_scene** out);
+
+/* On-disk scene file: the built scene's device records (tree, triangle and shading
+ * records, id map, Morton order), materials, lights and build settings, with a checksum
+ * (FNV-1a over 8-byte words).  eos_scene_load uploads them into a new scene on ctx's
+ * device without building anything; it renders exactly as the saved scene did (the
+ * file's materials and lights; set_materials / set_lights change them as on any scene).
+ * It needs no input mesh.  Errors: EOS_ERR_IO (the
+ * file cannot be opened, read or written), EOS_ERR_PARSE (wrong magic or version, sizes
+ * out of range, truncated, checksum mismatch), EOS_ERR_UNSUPPORTED (saving an instanced
+ * scene, which refers to other scenes).  The file holds the host's byte order; it is
+ * meant for the machine that wrote it. */
+eos_status eos_scene_save(const eos_scene* scene, const char* path);
+eos_status eos_scene_load(eos_ctx* ctx, const char* path, eos_scene** out);
 
 /* Test hook: Morton codes of the triangles in sorted order and the sorted triangle ids. */
 eos_status eos_scene_get_morton(const eos_scene* scene, uint32_t* codes, uint32_t* order);

@@ -1,6 +1,7 @@
 // Renders a scene through the C++ drop-in facade (include/eos/eos.hpp) the way a caller
 // of the reference does (src/main.cpp:340-480): Material / Triangle / LightSource /
-// Scene / Camera, createCudaScene, DeviceRenderer and RayTracer.
+// Scene / Camera, createCudaScene, DeviceRenderer and RayTracer; the DeviceRenderer frame
+// is rendered again from a saved and reloaded scene file and must not change.
 //
 //   facade_render <scene.bin> <out_device_renderer.rgba> <out_raytracer.rgba> [<out_multi.rgba>]
 //
@@ -13,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "eos/eos.hpp"
@@ -83,6 +85,17 @@ int main(int argc, char** argv) {
     renderer.setTracedDepth(td);
     std::vector<unsigned char> img(4 * (size_t)W * H, 0);
     renderer.renderCudaSceneToHostBufferMegaKernel(dscene.get(), img.data());
+
+    // the same frame from a scene file of the built scene (saveCudaScene / loadCudaScene)
+    const std::string scn = std::string(argv[2]) + ".scn";
+    eos::saveCudaScene(dscene.get(), scn);
+    std::unique_ptr<eos::cudaScene_t> loaded(eos::loadCudaScene(scn));
+    std::vector<unsigned char> img_loaded(img.size(), 0);
+    renderer.renderCudaSceneToHostBufferMegaKernel(loaded.get(), img_loaded.data());
+    if (img_loaded != img) {
+      fprintf(stderr, "the loaded scene renders a different frame\n");
+      return 3;
+    }
 
     eos::RayTracer rt;
     rt.setTracedDepth(td);

@@ -43,7 +43,7 @@ def test_struct_layouts_match_header():
 def test_status_strings_and_version():
     lib = L.load()
     assert lib.eos_abi_version() == 1
-    for code in range(9):
+    for code in range(11):
         assert lib.eos_status_string(code)
 
 
@@ -55,6 +55,8 @@ def test_null_arguments_are_rejected_without_device_work():
     assert lib.eos_render(None, None, None, None, None, None, None, None, None) == 1
     assert lib.eos_render_batch(None, None, 0, None, None) == 1
     assert lib.eos_trace_closest(None, None, None, 0, None, None) == 1
+    assert lib.eos_scene_save(None, b"x.eos") == 1
+    assert lib.eos_scene_load(None, b"x.eos", None) == 1
 
 
 def test_no_device_reports_status_not_crash():
@@ -75,3 +77,34 @@ def test_python_package_fails_loudly_without_library(tmp_path):
             L.load(str(tmp_path / "missing.so"))
     finally:
         L._lib = saved
+
+
+def test_context_close_destroys_its_scenes_first():
+    """Scenes still alive when their Context closes (e.g. held by a traceback) are destroyed
+    before the context, never after it."""
+    import weakref
+
+    from eos_b200 import api
+    calls = []
+
+    class FakeLib:
+        def eos_scene_destroy(self, h):
+            calls.append(("scene", h))
+
+        def eos_ctx_destroy(self, h):
+            calls.append(("ctx", h))
+
+    ctx = api.Context.__new__(api.Context)
+    ctx.lib, ctx.h, ctx._scenes = FakeLib(), "C", weakref.WeakSet()
+    scs = []
+    for k in range(2):
+        sc = api.DeviceScene.__new__(api.DeviceScene)
+        sc.lib, sc.h = ctx.lib, f"S{k}"
+        ctx._scenes.add(sc)
+        scs.append(sc)
+    ctx.close()
+    assert sorted(calls[:2]) == [("scene", "S0"), ("scene", "S1")] and calls[2] == ("ctx", "C")
+    ctx.close()
+    for sc in scs:
+        sc.close()
+    assert len(calls) == 3
