@@ -9,6 +9,8 @@
 //
 // Box tests are conservative so that culling never removes the exact answer:
 //  * slab far distances are widened by 1 + 2*gamma(3) (rounding of (b - o) * (1/d));
+//    shadow rays use a one-instruction-per-plane form that accepts a superset of those
+//    boxes (FmaSlabRay);
 //  * a box is culled against the current best t only beyond best * (1 + 2^-12), a margin
 //    for the rounding of the triangle test's own t;
 //  * a direction component with |d| < 1e-30 is treated as parallel: its slab is the whole
@@ -94,6 +96,49 @@ __device__ __forceinline__ bool slab_hit(const SlabRay& r, float nx, float ny, f
   return tn <= tf && tn != kInf;
 }
 
+// Box test of shadow rays in the form b = fma(p, i, c) per plane (i = 1/d), one
+// instruction where (p - o) * i takes two.  c is offset per axis: c_near = fl(c - eps),
+// c_far = fl(c + eps), c = fl(-(o i)), eps = 2^-20 |c| + 2^-126.  With u = 2^-24 and
+// x = (p - o) i: p i + c_near = x - o i d3 - eps' <= x - eps / 4 (the rounding of c is
+// <= 1.0001u|c| <= eps / 16), so b_near <= x + u|x|, and likewise b_far >= x - u|x|;
+// the (p - o) * i value a satisfies |a - x| <= 2.0001u|x|.  Hence max(b_near) <=
+// max(a_near)(1 + 3.0002u) when that is >= 0 (both entries clamp to 0 otherwise) and
+// min(b_far) >= min(a_far)(1 - 3.0002u) when min(a_far) >= 0, and the exit distance
+// times 1 + 2^-19 (>= kSlack (1 + 8u) / (1 - u)) accepts every box that slab_hit accepts.
+// Rays with a parallel axis or |o / d| above 1e30 keep the exact form (fma_slab_ok).
+struct FmaSlabRay {
+  float ix, iy, iz, nx, ny, nz, fx, fy, fz;
+  int sx, sy, sz;
+};
+
+__device__ __forceinline__ bool fma_slab_ok(const SlabRay& r) {
+  return !r.par && fabsf(r.ox * r.ix) <= 1e30f && fabsf(r.oy * r.iy) <= 1e30f && fabsf(r.oz * r.iz) <= 1e30f;
+}
+
+__device__ __forceinline__ void fma_axis(float o, float i, float& cn, float& cf) {
+  const float c = -(o * i);
+  const float eps = fabsf(c) * 0x1p-20f + 0x1p-126f;
+  cn = c - eps;
+  cf = c + eps;
+}
+
+__device__ __forceinline__ FmaSlabRay make_fma_slab(const SlabRay& r) {
+  FmaSlabRay q;
+  q.ix = r.ix; q.iy = r.iy; q.iz = r.iz;
+  q.sx = r.sx; q.sy = r.sy; q.sz = r.sz;
+  fma_axis(r.ox, r.ix, q.nx, q.fx);
+  fma_axis(r.oy, r.iy, q.ny, q.fy);
+  fma_axis(r.oz, r.iz, q.nz, q.fz);
+  return q;
+}
+
+__device__ __forceinline__ bool slab_hit(const FmaSlabRay& r, float nx, float ny, float nz, float fx, float fy,
+                                         float fz) {
+  const float tn = fmaxf(max3f(fmaf(nx, r.ix, r.nx), fmaf(ny, r.iy, r.ny), fmaf(nz, r.iz, r.nz)), 0.0f);
+  const float tf = min3f(fmaf(fx, r.ix, r.fx), fmaf(fy, r.iy, r.fy), fmaf(fz, r.iz, r.fz)) * (1.0f + 0x1p-19f);
+  return tn <= tf && tn != kInf;
+}
+
 struct Hit {
   float t, u, v;
   int pos;  // sorted position, -1 on a miss
@@ -169,8 +214,8 @@ __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p,
 // -inf (parallel axes fail the containment test), so slab() returns kInf for it and no
 // per-slot check is needed.  Returns false on stack overflow.
 
-template <int SH, bool SORT>
-__device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const SlabRay& r, int& cur,
+template <int SH, bool SORT, class Ray>
+__device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const Ray& r, int& cur,
                                             float limit, TraversalStack<SH>& st, unsigned& nodes) {
   const float4* nd = node_base + 8 * (size_t)cur;
   const float4 lx = __ldg(nd + r.sx), ly = __ldg(nd + 1 + r.sy), lz = __ldg(nd + 2 + r.sz);  // near planes
@@ -178,7 +223,7 @@ __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base
   const int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 6);
   ++nodes;
   int c[4] = {ref.x, ref.y, ref.z, ref.w};
-  if (SORT) {
+  if constexpr (SORT) {
     float t[4];
     t[0] = slab(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, limit);
     t[1] = slab(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, limit);
@@ -264,10 +309,10 @@ __device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, u
 }
 
 // Any hit at t >= 0 (shadow rays), same two-loop form; returns at the first hit.
-template <int SH>
-__device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+template <int SH, class Ray>
+__device__ __forceinline__ AnyResult any_traverse(const DevScene& s, f3 o, f3 d, const Ray& r, uint2* shs,
+                                                  int stride, int* err) {
   AnyResult res{0, 0u, 0u};
-  SlabRay r = make_slab(o, d);
   TraversalStack<SH> st(shs, stride);
   int cur = 0;
   int leaf = 0;
@@ -304,6 +349,13 @@ __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d,
     }
     if (cur == kDone) return res;
   }
+}
+
+template <int SH>
+__device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  const SlabRay r = make_slab(o, d);
+  if (fma_slab_ok(r)) return any_traverse<SH>(s, o, d, make_fma_slab(r), shs, stride, err);
+  return any_traverse<SH>(s, o, d, r, shs, stride, err);
 }
 
 // ------------------------------------------------------------------ resumable traversal

@@ -241,6 +241,80 @@ def test_queries_match_oracle(ctx, leaf, width, builder):
     assert np.array_equal(occ, orc.any(rays))
 
 
+def _adversarial_rays(sc, n, seed):
+    """Rays that stress the box tests: origins on triangle vertices (on node box planes) or
+    just off the surface, far from the world origin in the offset scene; directions
+    towards other vertices (grazing edges), or leaving the surface with one or two
+    components tiny (1e-7 .. 1e-31) or zero."""
+    rng = np.random.default_rng(seed)
+    V = sc.verts.astype(np.float64)
+    N = sc.normals.astype(np.float64)
+    pick = rng.integers(0, len(V), n)
+    o = V[pick].copy()
+    q = n // 4
+    o[q:] += N[pick[q:]] * rng.choice([1e-4, 1e-3, 1e-2], size=(n - q, 1))
+    d = V[rng.integers(0, len(V), n)] - o
+    k = slice(q, q + n // 2)
+    m = n // 2
+    dk = rng.normal(size=(m, 3))
+    dk *= np.sign(np.sum(dk * N[pick[k]], axis=1, keepdims=True))
+    tiny = rng.choice([1e-7, 1e-12, 1e-20, 1e-29, 1e-31, 0.0], size=(m, 2))
+    ax = rng.integers(0, 3, m)
+    for j in range(2):
+        dk[np.arange(m), (ax + j) % 3] = tiny[:, j] * rng.choice([-1.0, 1.0], m)
+    d[k] = dk
+    d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-30)
+    return np.concatenate([o, d], 1).astype(np.float32)
+
+
+def _exact_ray_enters_box(o, d, lo, hi):
+    """Whether the exact ray o + t d, t >= 0 (float inputs read as rationals) meets the
+    closed box [lo, hi]."""
+    from fractions import Fraction as Fr
+    tmin, tmax = Fr(0), None
+    for a in range(3):
+        oa, da, la, ha = (Fr(float(v)) for v in (o[a], d[a], lo[a], hi[a]))
+        if da == 0:
+            if oa < la or oa > ha:
+                return False
+            continue
+        t1, t2 = sorted(((la - oa) / da, (ha - oa) / da))
+        tmin = max(tmin, t1)
+        tmax = t2 if tmax is None else min(tmax, t2)
+    return tmax is None or tmin <= tmax
+
+
+@pytest.mark.parametrize("offset", [0.0, 3.0e4])
+def test_shadow_and_nearest_queries_on_adversarial_rays(ctx, offset):
+    """Box tests are conservative (the shadow form included) for rays grazing box planes,
+    nearly parallel to an axis, or far from the origin.  Any-hit answers equal the
+    oracle's.  Nearest hits equal the oracle's except where the triangle–ray test accepts a
+    triangle whose own bounding box the exact ray never enters (its rounding at edges and
+    grazing angles): such a triangle is found or not depending on how boxes are laid out,
+    in any tree; the brute-force winner is then such a triangle, and these rays are rare."""
+    sc = scenes.small_random_scene(53, n_spheres=6, level=3, lights=1)
+    sc.verts = (sc.verts.astype(np.float64) + offset).astype(np.float32)
+    dsc = api.DeviceScene(ctx, sc)
+    orc = oracle.Oracle(sc)
+    rays = _adversarial_rays(sc, 30000, 4)
+    occ = api.trace_any(ctx, dsc, rays)
+    assert np.array_equal(occ, orc.any(rays))
+    assert 0.05 < occ.mean() < 0.95
+    ids, t = api.trace_closest(ctx, dsc, rays)
+    oid, ot, _ = orc.closest(rays)
+    bad = np.nonzero(ids != oid)[0]
+    assert len(bad) <= 1e-3 * len(rays)
+    same = ids == oid
+    assert np.array_equal(t[same & (ids >= 0)], ot[same & (oid >= 0)])
+    if len(bad):
+        bid, _ = orc.closest_brute(rays[bad])
+        for k, i in enumerate(bad):
+            w = int(bid[k])
+            assert w in (int(ids[i]), int(oid[i])), i
+            V = sc.verts[sc.tris[w]]
+            assert not _exact_ray_enters_box(rays[i, :3], rays[i, 3:], V.min(0), V.max(0)), i
+
+
 def test_edge_scenes(ctx):
     cam = scenes.look_at((0, 0, 5), (0, 0, 0), 60, 33, 17)
     mat = np.array([[0.5, 0.5, 0.5, 0.2, 0.2, 0.2, 16, 0.3]], np.float32)
