@@ -9,7 +9,7 @@
 //
 // Box tests are conservative so that culling never removes the exact answer:
 //  * slab far distances are widened by 1 + 2*gamma(3) (rounding of (b - o) * (1/d));
-//    shadow rays use a one-instruction-per-plane form that accepts a superset of those
+//    the traversals use a one-instruction-per-plane form that accepts a superset of those
 //    boxes (FmaSlabRay);
 //  * a box is culled against the current best t only beyond best * (1 + 2^-12), a margin
 //    for the rounding of the triangle test's own t;
@@ -96,8 +96,8 @@ __device__ __forceinline__ bool slab_hit(const SlabRay& r, float nx, float ny, f
   return tn <= tf && tn != kInf;
 }
 
-// Box test of shadow rays in the form b = fma(p, i, c) per plane (i = 1/d), one
-// instruction where (p - o) * i takes two.  c is offset per axis: c_near = fl(c - eps),
+// Box test in the form b = fma(p, i, c) per plane (i = 1/d), one instruction where
+// (p - o) * i takes two; used by both traversals.  c is offset per axis: c_near = fl(c - eps),
 // c_far = fl(c + eps), c = fl(-(o i)), eps = 2^-20 |c| + 2^-126.  With u = 2^-24 and
 // x = (p - o) i: p i + c_near = x - o i d3 - eps' <= x - eps / 4 (the rounding of c is
 // <= 1.0001u|c| <= eps / 16), so b_near <= x + u|x|, and likewise b_far >= x - u|x|;
@@ -105,7 +105,10 @@ __device__ __forceinline__ bool slab_hit(const SlabRay& r, float nx, float ny, f
 // max(a_near)(1 + 3.0002u) when that is >= 0 (both entries clamp to 0 otherwise) and
 // min(b_far) >= min(a_far)(1 - 3.0002u) when min(a_far) >= 0, and the exit distance
 // times 1 + 2^-19 (>= kSlack (1 + 8u) / (1 - u)) accepts every box that slab_hit accepts.
-// Rays with a parallel axis or |o / d| above 1e30 keep the exact form (fma_slab_ok).
+// The entry distance exceeds the exact form's by at most 3.0002u relative, so nearest-hit
+// culling compares it with best * (kCull + 2^-19) (RayCull), which keeps every box and
+// stack entry the exact form keeps.  Rays with a parallel axis or |o / d| above 1e30 keep
+// the exact form (fma_slab_ok).
 struct FmaSlabRay {
   float ix, iy, iz, nx, ny, nz, fx, fy, fz;
   int sx, sy, sz;
@@ -138,6 +141,24 @@ __device__ __forceinline__ bool slab_hit(const FmaSlabRay& r, float nx, float ny
   const float tf = min3f(fmaf(fx, r.ix, r.fx), fmaf(fy, r.iy, r.fy), fmaf(fz, r.iz, r.fz)) * (1.0f + 0x1p-19f);
   return tn <= tf && tn != kInf;
 }
+
+__device__ __forceinline__ float slab(const FmaSlabRay& r, float nx, float ny, float nz, float fx, float fy, float fz,
+                                      float limit) {
+  const float tn = fmaxf(max3f(fmaf(nx, r.ix, r.nx), fmaf(ny, r.iy, r.ny), fmaf(nz, r.iz, r.nz)), 0.0f);
+  const float tf = min3f(fmaf(fx, r.ix, r.fx), fmaf(fy, r.iy, r.fy), fmaf(fz, r.iz, r.fz)) * (1.0f + 0x1p-19f);
+  return tn <= fminf(tf, limit) ? tn : kInf;
+}
+
+// Culling factor on the best hit distance per ray form: the fma form's entry distance can
+// exceed the exact form's by 3.0002u relative, which 2^-19 more covers.
+template <class Ray>
+struct RayCull {
+  static constexpr float k = kCull;
+};
+template <>
+struct RayCull<FmaSlabRay> {
+  static constexpr float k = 1.0f + 0x1p-12f + 0x1p-19f;
+};
 
 struct Hit {
   float t, u, v;
@@ -245,44 +266,46 @@ __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base
       if (t[i] != kInf && !st.push(c[i], t[i])) return false;
     cur = c[0];
     return true;
-  }
-  bool h[4];
-  h[0] = slab_hit(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x);
-  h[1] = slab_hit(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y);
-  h[2] = slab_hit(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z);
-  h[3] = slab_hit(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w);
-  int first = -1;
+  } else {
+    bool h[4];
+    h[0] = slab_hit(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x);
+    h[1] = slab_hit(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y);
+    h[2] = slab_hit(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z);
+    h[3] = slab_hit(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w);
+    int first = -1;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    if (!h[i]) continue;
-    if (first < 0) first = i;
-    else if (!st.push(c[i], 0.0f)) return false;
+    for (int i = 0; i < 4; ++i) {
+      if (!h[i]) continue;
+      if (first < 0) first = i;
+      else if (!st.push(c[i], 0.0f)) return false;
+    }
+    cur = first < 0 ? st.next_any() : c[first];
+    return true;
   }
-  cur = first < 0 ? st.next_any() : c[first];
-  return true;
 }
 
 // Nearest hit.  Traversal in the two-loop form of Aila & Laine ("Understanding the
 // efficiency of ray traversal on GPUs", HPG 2009): a lane that reaches a leaf parks it and
 // keeps descending until every lane of the warp holds a leaf, then the lanes intersect
 // their leaves together, so triangle tests run with full warps.
-template <int SH>
-__device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+template <int SH, class Ray>
+__device__ __forceinline__ Hit closest_traverse(const DevScene& s, f3 o, f3 d, const Ray& r, uint2* shs, int stride,
+                                               int* err) {
+  constexpr float kCullR = RayCull<Ray>::k;
   Hit h;
   h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
-  SlabRay r = make_slab(o, d);
   TraversalStack<SH> st(shs, stride);
   int cur = 0;   // interior node, leaf ref or kDone
   int leaf = 0;  // parked leaf (0 = none)
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node4<SH, true>(s.nodes, r, cur, h.t * kCull, st, h.nodes)) {
+      if (!visit_node4<SH, true>(s.nodes, r, cur, h.t * kCullR, st, h.nodes)) {
         atomicOr(err, kErrStack);
         return h;
       }
       if (cur != kDone && cur < 0 && leaf == 0) {
         leaf = cur;
-        cur = st.next(h.t * kCull);
+        cur = st.next(h.t * kCullR);
       }
       if (!__any_sync(__activemask(), leaf == 0)) break;
     }
@@ -301,11 +324,18 @@ __device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, u
       leaf = 0;
       if (cur != kDone && cur < 0) {
         leaf = cur;
-        cur = st.next(h.t * kCull);
+        cur = st.next(h.t * kCullR);
       }
     }
     if (cur == kDone) return h;
   }
+}
+
+template <int SH>
+__device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
+  const SlabRay r = make_slab(o, d);
+  if (fma_slab_ok(r)) return closest_traverse<SH>(s, o, d, make_fma_slab(r), shs, stride, err);
+  return closest_traverse<SH>(s, o, d, r, shs, stride, err);
 }
 
 // Any hit at t >= 0 (shadow rays), same two-loop form; returns at the first hit.
