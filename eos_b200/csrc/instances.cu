@@ -176,7 +176,7 @@ int write_records_host(const std::vector<BNode>& bn, int root, std::vector<float
       int* cnt = reinterpret_cast<int*>(rec + 28);
       for (int s = 0; s < 4; ++s) {
         if (s >= (int)c.size()) {
-          for (int k = 0; k < 6; ++k) rec[4 * k + s] = INFINITY;  // a box no ray enters
+          for (int k = 0; k < 6; ++k) rec[4 * k + s] = k < 3 ? INFINITY : -INFINITY;  // a box no ray enters
           ref[s] = kEmptySlot;
           cnt[s] = -1;
           continue;

@@ -337,8 +337,8 @@ __global__ void k_refit(int n, const int2* __restrict__ child, const int2* __res
 // Record, 128 B = 8 x float4 (structure of arrays over the four slots):
 //   [0] lo.x[4] [1] lo.y[4] [2] lo.z[4] [3] hi.x[4] [4] hi.y[4] [5] hi.z[4]
 //   [6] ref[4]: interior record index, packed leaf, or kEmptyRef for an unused slot
-//       (whose box is lo = hi = +inf: every slab test misses it, so the traversal needs
-//       no per-slot check)
+//       (whose box is lo = +inf, hi = -inf: every slab test misses it, so the traversal
+//       needs no per-slot check)
 //   [7] count[4]: triangles of a leaf, 0 for an interior child, -1 for an unused slot
 constexpr int kEmptyRef = (int)0xC0000000;
 
@@ -383,7 +383,7 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
   int ref[4], cnt[4];
   for (int i = 0; i < 4; ++i) {
     if (i >= k) {
-      for (int a = 0; a < 6; ++a) v[a][i] = kInf;  // a box no ray enters
+      for (int a = 0; a < 6; ++a) v[a][i] = a < 3 ? kInf : -kInf;  // a box no ray enters
       ref[i] = kEmptyRef;
       cnt[i] = -1;
       continue;
@@ -403,7 +403,7 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
       const int w = atomicAdd(w_count, 1);
       if (w >= max_nodes) {  // cannot happen: the tree has at most n - 1 records
         atomicOr(err, kErrQueue);
-        for (int a = 0; a < 6; ++a) v[a][i] = kInf;
+        for (int a = 0; a < 6; ++a) v[a][i] = a < 3 ? kInf : -kInf;
         ref[i] = kEmptyRef;
         cnt[i] = -1;
         continue;
@@ -421,7 +421,7 @@ __global__ void k_small_root(int n, const float4* __restrict__ blo, const float4
                              float4* __restrict__ nodes) {
   float v[6][4];
   for (int a = 0; a < 6; ++a)
-    for (int i = 0; i < 4; ++i) v[a][i] = kInf;
+    for (int i = 0; i < 4; ++i) v[a][i] = a < 3 ? kInf : -kInf;
   int ref[4] = {kEmptyRef, kEmptyRef, kEmptyRef, kEmptyRef};
   int cnt[4] = {-1, -1, -1, -1};
   if (n == 1) {

@@ -23,7 +23,7 @@
 namespace {
 
 constexpr char kMagic[8] = {'E', 'O', 'S', 'S', 'C', 'N', '0', '1'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;  // 2: unused child slots hold lo = +inf, hi = -inf
 constexpr size_t kChunk = 8u << 20;  // bytes per pinned chunk (a multiple of 32)
 
 struct Header {

@@ -93,7 +93,7 @@ __device__ __forceinline__ bool slab_hit(const SlabRay& r, float nx, float ny, f
                                          float fz) {
   float tn, tf;
   slab_range(r, nx, ny, nz, fx, fy, fz, tn, tf);
-  return tn <= tf && tn != kInf;
+  return tn <= tf;
 }
 
 // Box test in the form b = fma(p, i, c) per plane (i = 1/d), one instruction where
@@ -139,7 +139,7 @@ __device__ __forceinline__ bool slab_hit(const FmaSlabRay& r, float nx, float ny
                                          float fz) {
   const float tn = fmaxf(max3f(fmaf(nx, r.ix, r.nx), fmaf(ny, r.iy, r.ny), fmaf(nz, r.iz, r.nz)), 0.0f);
   const float tf = min3f(fmaf(fx, r.ix, r.fx), fmaf(fy, r.iy, r.fy), fmaf(fz, r.iz, r.fz)) * (1.0f + 0x1p-19f);
-  return tn <= tf && tn != kInf;
+  return tn <= tf;
 }
 
 __device__ __forceinline__ float slab(const FmaSlabRay& r, float nx, float ny, float nz, float fx, float fy, float fz,
@@ -199,6 +199,10 @@ struct TraversalStack {
     ++sp;
     return true;
   }
+  __device__ __forceinline__ void push_shared(int ref, float t) {
+    sh[sp * stride] = make_uint2((uint32_t)ref, __float_as_uint(t));
+    ++sp;
+  }
   __device__ __forceinline__ uint2 pop() {
     --sp;
     return sp < SH ? sh[sp * stride] : spill[sp - SH];
@@ -231,9 +235,11 @@ __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p,
 // farthest first; without SORT (shadow rays: no distance limit) only hit / miss is
 // computed and the first hit in slot order is taken, which measured faster for shadow
 // rays than nearest-first.  An unused slot holds the box
-// lo = hi = +inf: for every direction sign some slab gives an entry of +inf or an exit of
-// -inf (parallel axes fail the containment test), so slab() returns kInf for it and no
-// per-slot check is needed.  Returns false on stack overflow.
+// lo = +inf, hi = -inf: on every axis the near plane gives an entry of +inf and the far
+// plane an exit of -inf, whatever the direction's sign (parallel axes fail the containment
+// test), so both box tests reject it and no per-slot check is needed.  With three free
+// shared-memory stack entries (the most one node pushes) the pushes skip their bound
+// checks.  Returns false on stack overflow.
 
 template <int SH, bool SORT, class Ray>
 __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const Ray& r, int& cur,
@@ -261,9 +267,15 @@ __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base
       cur = st.next(limit);
       return true;
     }
+    if (st.sp + 3 <= SH) {
 #pragma unroll
-    for (int i = 3; i >= 1; --i)
-      if (t[i] != kInf && !st.push(c[i], t[i])) return false;
+      for (int i = 3; i >= 1; --i)
+        if (t[i] != kInf) st.push_shared(c[i], t[i]);
+    } else {
+#pragma unroll
+      for (int i = 3; i >= 1; --i)
+        if (t[i] != kInf && !st.push(c[i], t[i])) return false;
+    }
     cur = c[0];
     return true;
   } else {
@@ -273,11 +285,20 @@ __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base
     h[2] = slab_hit(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z);
     h[3] = slab_hit(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w);
     int first = -1;
+    if (st.sp + 3 <= SH) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      if (!h[i]) continue;
-      if (first < 0) first = i;
-      else if (!st.push(c[i], 0.0f)) return false;
+      for (int i = 0; i < 4; ++i) {
+        if (!h[i]) continue;
+        if (first < 0) first = i;
+        else st.push_shared(c[i], 0.0f);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (!h[i]) continue;
+        if (first < 0) first = i;
+        else if (!st.push(c[i], 0.0f)) return false;
+      }
     }
     cur = first < 0 ? st.next_any() : c[first];
     return true;
