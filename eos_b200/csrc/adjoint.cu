@@ -19,7 +19,9 @@
 //          + b s (V.R)^(s-1) (I - L L^T)/|u| (2 N N^T - I) (V - (V.R) R)/|w|  [V.R > 0]
 //   with a = sum_c g_c C_c kd_c, b = sum_c g_c C_c ks_c.
 // Per-object sums use a warp segmented reduction (peers by object id) and one atomic per
-// object per warp; per-light sums use a warp reduction into shared memory per block.
+// object per warp; per-light sums are reduced over the warp first (every lane takes part,
+// with zeros for blocked lights and finished paths), then one shared-memory atomic per
+// warp and component, and one global atomic per block and component.
 #include <algorithm>
 
 #include "trace.cuh"
@@ -96,50 +98,54 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
         }
       }
     }
-    if (alive) {
-      const float shin = m[6];
-      f3 V = norm3(sub3(campos, P));
-      uint32_t mask = rec.shadow[k];
+    {
+      const float shin = alive ? m[6] : 0.0f;
+      f3 V = alive ? norm3(sub3(campos, P)) : mk3(0, 0, 1);
+      uint32_t mask = alive ? rec.shadow[k] : 0xffffffffu;
       float gT[3] = {g[0] * T, g[1] * T, g[2] * T};
       for (int l = 0; l < s.n_lights; ++l) {
-        if (mask & (1u << l)) continue;
-        const float* lp = s.lights + 6 * l;
-        f3 u = sub3(mk3(lp[0], lp[1], lp[2]), P);
-        float ul = sqrtf(dot3(u, u));
-        f3 L = scale3(1.0f / ul, u);
-        float ndl = dot3(N, L);
-        f3 wv = sub3(scale3(2.0f * ndl, N), L);
-        float wl = sqrtf(dot3(wv, wv));
-        f3 R = scale3(1.0f / wl, wv);
-        float fd = ndl > 0.0f ? ndl : 0.0f;
-        float vr = dot3(V, R);
-        float fs = vr > 0.0f ? powf(vr, shin) : 0.0f;
-        float C[3] = {lp[3], lp[4], lp[5]};
-        float a = 0.0f, b = 0.0f;
-        float gl[6];
+        float gl[6] = {0, 0, 0, 0, 0, 0};
+        if (!(mask & (1u << l))) {
+          const float* lp = s.lights + 6 * l;
+          f3 u = sub3(mk3(lp[0], lp[1], lp[2]), P);
+          float ul = sqrtf(dot3(u, u));
+          f3 L = scale3(1.0f / ul, u);
+          float ndl = dot3(N, L);
+          f3 wv = sub3(scale3(2.0f * ndl, N), L);
+          float wl = sqrtf(dot3(wv, wv));
+          f3 R = scale3(1.0f / wl, wv);
+          float fd = ndl > 0.0f ? ndl : 0.0f;
+          float vr = dot3(V, R);
+          float fs = vr > 0.0f ? powf(vr, shin) : 0.0f;
+          float C[3] = {lp[3], lp[4], lp[5]};
+          float a = 0.0f, b = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          gm[c] += gT[c] * fd * C[c];
-          gm[3 + c] += gT[c] * fs * C[c];
-          gl[c] = gT[c] * (fd * m[c] + fs * m[3 + c]);
-          a += gT[c] * C[c] * m[c];
-          b += gT[c] * C[c] * m[3 + c];
+          for (int c = 0; c < 3; ++c) {
+            gm[c] += gT[c] * fd * C[c];
+            gm[3 + c] += gT[c] * fs * C[c];
+            gl[c] = gT[c] * (fd * m[c] + fs * m[3 + c]);
+            a += gT[c] * C[c] * m[c];
+            b += gT[c] * C[c] * m[3 + c];
+          }
+          if (vr > 0.0f) gm[6] += b * fs * logf(vr) * shin;
+          f3 gp = mk3(0, 0, 0);
+          if (ndl > 0.0f) gp = add3(gp, scale3(a / ul, sub3(N, scale3(ndl, L))));
+          if (vr > 0.0f) {
+            f3 q = scale3(1.0f / wl, sub3(V, scale3(vr, R)));
+            f3 q2 = sub3(scale3(2.0f * dot3(N, q), N), q);
+            f3 gs = scale3(1.0f / ul, sub3(q2, scale3(dot3(L, q2), L)));
+            float dfs = shin * powf(vr, shin - 1.0f);
+            gp = add3(gp, scale3(b * dfs, gs));
+          }
+          gl[3] = gp.x;
+          gl[4] = gp.y;
+          gl[5] = gp.z;
         }
-        if (vr > 0.0f) gm[6] += b * fs * logf(vr) * shin;
-        f3 gp = mk3(0, 0, 0);
-        if (ndl > 0.0f) gp = add3(gp, scale3(a / ul, sub3(N, scale3(ndl, L))));
-        if (vr > 0.0f) {
-          f3 q = scale3(1.0f / wl, sub3(V, scale3(vr, R)));
-          f3 q2 = sub3(scale3(2.0f * dot3(N, q), N), q);
-          f3 gs = scale3(1.0f / ul, sub3(q2, scale3(dot3(L, q2), L)));
-          float dfs = shin * powf(vr, shin - 1.0f);
-          gp = add3(gp, scale3(b * dfs, gs));
-        }
-        gl[3] = gp.x;
-        gl[4] = gp.y;
-        gl[5] = gp.z;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) atomicAdd(&sl[6 * l + c], gl[c]);
+        for (int c = 0; c < 6; ++c) {
+          const float v = warp_sum(gl[c]);
+          if (lane == 0 && v != 0.0f) atomicAdd(&sl[6 * l + c], v);
+        }
       }
     }
     // per-object segmented reduction: one leader per distinct object in the warp
