@@ -11,6 +11,8 @@
 //                                                       src/DeviceRenderer.h:33-55
 //   MultiDeviceRenderer::renderSceneToHostBuffer        src/MultiDeviceRenderer.h:31-45
 //   RayTracer::render (same call, run on the GPU)       src/RayTracer.h:38-68
+//   rayTrace_MegaKernel, rayTrace_WarpShuffle_MegaKernel,
+//   rayTrace_MultiMegaKernel (C linkage)                src/kernelWrapper.h:30-34
 // with the same names, argument meaning and output layout (RGBA8, row 0 = bottom).
 //
 // Differences a caller sees:
@@ -610,5 +612,69 @@ class RayTracer {
 };
 
 }  // namespace eos
+
+// The reference's C wrappers around its GPU kernel (src/kernelWrapper.h:30-34,
+// src/kernelInvocations.cu:668-711), with the same names and arguments.  Each renders the
+// frame that DeviceRenderer renders at its default trace depth (RayTracer semantics, see
+// above) into `imageBuffer`, host or device memory of width * height RGBA8 pixels.
+// `camera` is the facade's Camera (the copy DeviceCameraHandler hands out); the block /
+// thread counts are accepted and ignored, as the library picks its own launch shape.
+// rayTrace_MultiMegaKernel renders rows [(height / numGPUS) * gpuID, (height / numGPUS) *
+// (gpuID + 1)) into a buffer of that band only, as the reference's per-GPU kernel does, on
+// the device of the scene's context.  Errors throw eos::Error.
+#if defined(__VECTOR_TYPES_H__) || __has_include(<vector_types.h>)
+#include <vector_types.h>
+using eos_uchar4_t = uchar4;
+#else
+using eos_uchar4_t = void;
+#endif
+
+extern "C" inline void rayTrace_MegaKernel(eos::cudaScene_t* deviceScene, eos::Camera* camera, int width, int height,
+                                           eos_uchar4_t* imageBuffer, int blockdim[], int tpblock[]) {
+  (void)blockdim;
+  (void)tpblock;
+  if (!deviceScene || !camera) throw eos::Error(EOS_ERR_INVALID_ARG, "rayTrace_MegaKernel");
+  eos::Camera c = *camera;
+  c.setWidth(width);
+  c.setHeight(height);
+  eos::render_rgba8(deviceScene->ctx, deviceScene->scene, c, eos::kDefaultTraceDepth, imageBuffer, EOS_MODE_PLAIN);
+}
+
+extern "C" inline void rayTrace_WarpShuffle_MegaKernel(eos::cudaScene_t* deviceScene, eos::Camera* camera, int width,
+                                                       int height, eos_uchar4_t* imageBuffer, int blockdim[],
+                                                       int tpblock) {
+  (void)blockdim;
+  (void)tpblock;
+  if (!deviceScene || !camera) throw eos::Error(EOS_ERR_INVALID_ARG, "rayTrace_WarpShuffle_MegaKernel");
+  eos::Camera c = *camera;
+  c.setWidth(width);
+  c.setHeight(height);
+  eos::render_rgba8(deviceScene->ctx, deviceScene->scene, c, eos::kDefaultTraceDepth, imageBuffer,
+                    EOS_MODE_WAVEFRONT);
+}
+
+extern "C" inline void rayTrace_MultiMegaKernel(eos::cudaScene_t* deviceScene, eos::Camera* camera, int width,
+                                                int height, eos_uchar4_t* imageBuffer, int numGPUS, int gpuID,
+                                                int blockdimp[], int tpblock[]) {
+  (void)blockdimp;
+  (void)tpblock;
+  if (!deviceScene || !camera || numGPUS < 1 || gpuID < 0 || gpuID >= numGPUS || height / numGPUS < 1)
+    throw eos::Error(EOS_ERR_INVALID_ARG, "rayTrace_MultiMegaKernel");
+  eos::Camera cam = *camera;
+  cam.setWidth(width);
+  cam.setHeight(height);
+  const eos_camera c = cam.to_c();
+  const int rows = height / numGPUS;
+  eos_render_params p{};
+  p.trace_depth = eos::kDefaultTraceDepth;
+  p.pixel_offset = 0.0f;
+  p.spp = 1;
+  p.mode = EOS_MODE_PLAIN;
+  p.row_begin = rows * gpuID;
+  p.row_end = rows * (gpuID + 1);
+  eos::check(eos_render(deviceScene->ctx, deviceScene->scene, &c, &p, nullptr, (uint8_t*)imageBuffer, nullptr,
+                        nullptr, nullptr),
+             "rayTrace_MultiMegaKernel");
+}
 
 #endif  // EOS_EOS_HPP

@@ -1,7 +1,9 @@
 // Renders a scene through the C++ drop-in facade (include/eos/eos.hpp) the way a caller
 // of the reference does (src/main.cpp:340-480): Material / Triangle / LightSource /
 // Scene / Camera, createCudaScene, DeviceRenderer and RayTracer; the DeviceRenderer frame
-// is rendered again from a saved and reloaded scene file and must not change.
+// is rendered again from a saved and reloaded scene file and must not change, and the
+// reference's C wrappers (rayTrace_MegaKernel and its two variants) must give the same
+// frame as DeviceRenderer at its default depth.
 //
 //   facade_render <scene.bin> <out_device_renderer.rgba> <out_raytracer.rgba> [<out_multi.rgba>]
 //
@@ -95,6 +97,26 @@ int main(int argc, char** argv) {
     if (img_loaded != img) {
       fprintf(stderr, "the loaded scene renders a different frame\n");
       return 3;
+    }
+
+    // the reference's C wrappers give DeviceRenderer's frame at its default depth; two
+    // bands of rayTrace_MultiMegaKernel stitch into the same frame
+    {
+      eos::DeviceRenderer dflt(&camera, W, H);
+      std::vector<unsigned char> want(4 * (size_t)W * H, 0), got(want.size(), 1), got2(want.size(), 2);
+      dflt.renderCudaSceneToHostBufferMegaKernel(dscene.get(), want.data());
+      int blockdim[2] = {W / 16, H / 16}, tpb[2] = {16, 16};
+      rayTrace_MegaKernel(dscene.get(), &camera, W, H, (eos_uchar4_t*)got.data(), blockdim, tpb);
+      rayTrace_WarpShuffle_MegaKernel(dscene.get(), &camera, W, H, (eos_uchar4_t*)got2.data(), blockdim, 256);
+      std::vector<unsigned char> bands(want.size(), 3);
+      const size_t band_bytes = 4 * (size_t)W * (H / 2);
+      for (int g = 0; g < 2; ++g)
+        rayTrace_MultiMegaKernel(dscene.get(), &camera, W, H, (eos_uchar4_t*)(bands.data() + g * band_bytes), 2, g,
+                                 blockdim, tpb);
+      if (got != want || got2 != want || (H % 2 == 0 && bands != want)) {
+        fprintf(stderr, "the C wrappers render a different frame\n");
+        return 4;
+      }
     }
 
     eos::RayTracer rt;
