@@ -358,15 +358,13 @@ def run_ours(args, rank, world, local):
     # (b) the reference-facing per-frame call, eos_render once per view
     host_imgs = [torch.empty((c.height, c.width, 4), dtype=torch.uint8).pin_memory() for c in cams]
     host_outs = [{"rgba8": h} for h in host_imgs]
-    e2e_mode = "wavefront" if mrays_b > mrays_p else "plain"
-
     def step_e2e_batch():
         return [api.render_batch(ctx, jobs, host_outs)]
 
-    def step_e2e_view():
+    def step_e2e_view(mode):
         st = []
         for c, h in zip(cams, host_imgs):
-            st.append(api.render(ctx, dsc, c, td, pixel_offset=0.5, mode=e2e_mode, outputs=(),
+            st.append(api.render(ctx, dsc, c, td, pixel_offset=0.5, mode=mode, outputs=(),
                                  out={"rgba8": h.numpy()}, device=False)["stats"])
         return st
 
@@ -390,7 +388,9 @@ def run_ours(args, rank, world, local):
         return rays_e / e2e_s / 1e6
 
     e2e = wall_timed(step_e2e_batch)
-    e2e_view = wall_timed(step_e2e_view)
+    e2e_modes = {m: wall_timed(lambda: step_e2e_view(m)) for m in ("plain", "wavefront")}
+    e2e_mode = max(e2e_modes, key=e2e_modes.get)
+    e2e_view = e2e_modes[e2e_mode]
 
     # roofline of the dominant kernel: per-stage device time of the wavefront (eager, one step)
     st = api.render_batch(ctx, jobs, outs, stage_timing=True)
@@ -454,7 +454,8 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
                 "call": "eos_render_batch, all views of the step, pinned host RGBA8 outputs (wall clock)",
                 "h2d_bytes_per_step": len(cams) * 184 + 36, "d2h_bytes_per_step": 4 * npx_step,
-                "per_view_call": {"value": round(e2e_view, 2), "call": f"eos_render per view, {e2e_mode} mode"}},
+                "per_view_call": {"value": round(e2e_view, 2), "call": f"eos_render per view, {e2e_mode} mode",
+                                  "modes": {m: round(v, 2) for m, v in e2e_modes.items()}}},
         "gpu_launches": launches_b,
         "roofline": roof,
         "clocks": clocks,
