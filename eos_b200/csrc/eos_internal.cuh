@@ -34,14 +34,14 @@ enum : int {
 // ---------------------------------------------------------------------------------
 // HBM layout of a scene (all 16-byte aligned, read with 128-bit loads):
 //
-//  BVH node, 64 B = 4 x float4, both children's boxes in the parent:
-//    [0] c0.lo.x c0.lo.y c0.lo.z c0.hi.x
-//    [1] c0.hi.y c0.hi.z c1.lo.x c1.lo.y
-//    [2] c1.lo.z c1.hi.x c1.hi.y c1.hi.z
-//    [3] ref0 ref1 count0 count1          (int)
-//  count > 0: leaf of `count` triangles, ref = 0x80000000 | (count-1) << 25 | first
-//             (sorted positions [first, first + count); count <= 32, first < 2^25)
-//  count == 0: interior node `ref`;  count < 0: empty child
+//  Node record, 128 B = 8 x float4, the boxes of up to four children in the parent,
+//  structure of arrays over the four slots (written by lbvh.cu, read by trace.cuh):
+//    [0] lo.x[4]  [1] lo.y[4]  [2] lo.z[4]  [3] hi.x[4]  [4] hi.y[4]  [5] hi.z[4]
+//    [6] ref[4]   [7] count[4]                (int)
+//  ref: interior record index; leaf 0x80000000 | (count-1) << 25 | first (sorted positions
+//  [first, first + count), count <= 32, first < 2^25); 0xC0000000 for an unused slot,
+//  whose box is lo = +inf, hi = -inf.  count: triangles of a leaf, 0 interior, -1 unused.
+//  A binary tree (width 2) fills two slots per record.
 //
 //  Triangle record (intersection), 48 B = 3 x float4, sorted (Morton) order:
 //    [0] v1.x v1.y v1.z e1.x   [1] e1.y e1.z e2.x e2.y   [2] e2.z id(int) - -
