@@ -577,6 +577,7 @@ def config5_timing(ctx, stream, steps, warmup):
     out = {"tris": sc.n_tris, "resolution": "3840x2160", "spp": 2, "depth": 4, "lights": 8, **res,
            "build_ms": round(info["build_ms"], 2), "builder": {1: "lbvh", 2: "ploc"}.get(info["builder"], "?"),
            "scene_device_mb": round(info["device_bytes"] / 1e6, 1)}
+    out["forward_adjoint"] = config5_adjoint(ctx, stream, dsc, cam)
     del dsc
     idata = scenes.config5_instanced()
     torch.cuda.synchronize()
@@ -591,6 +592,41 @@ def config5_timing(ctx, stream, steps, warmup):
                                                   sum(m.info()["device_bytes"] for m in meshes)) / 1e6, 1),
                         "build_ms_wall": round(build_s * 1e3, 1), **r2}
     return out
+
+
+def config5_adjoint(ctx, stream, dsc, cam, reps=2):
+    """One forward + adjoint pass at config-5 scale: the 4K frame at 2 jittered samples, depth
+    4, 8 lights, path records kept (one eos_render_batch), then eos_render_backward of an
+    image loss gradient; ms per frame of each."""
+    import torch
+    from eos_b200 import api
+    npx = cam.width * cam.height
+    job = [api.BatchJob(dsc, cam, 3, 0.5, spp=2, jitter_seed=7)]
+    outs = [{"rgb": torch.empty((npx, 3), device="cuda"),
+             "paths": torch.empty((npx * 2, 16), dtype=torch.int32, device="cuda")}]
+    g = torch.full((npx, 3), 0.01, device="cuda")
+
+    def fwd():
+        api.render_batch(ctx, job, outs)
+
+    def bwd():
+        api.render_backward(ctx, dsc, [cam], 3, outs[0]["paths"], g, pixel_offset=0.5, spp=2, jitter_seed=7)
+
+    res = {}
+    for name, fn in (("fwd", fwd), ("bwd", bwd)):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / reps
+    return {"fwd_ms": round(res["fwd"], 2), "fwd_adj_ms": round(res["fwd"] + res["bwd"], 2),
+            "ratio": round((res["fwd"] + res["bwd"]) / res["fwd"], 3),
+            "calls": "eos_render_batch with path records (2 spp) + eos_render_backward"}
 
 
 def adjoint_timing(ctx, stream, reps=5):

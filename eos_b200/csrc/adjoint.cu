@@ -32,8 +32,9 @@ namespace {
 struct BwArgs {
   DevScene s;
   const float* cams;  // n_views x 12
-  int w, h, n_views, trace_depth;
+  int w, h, n_views, trace_depth, spp;
   float off;
+  uint32_t seed;  // sample jitter (spp > 1), as in the forward pass
   const eos_path_record* paths;
   const float* drgb;
   float* gmat;    // n_obj x 7
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const long long npx = (long long)A.w * A.h;
-  const long long total = npx * A.n_views;
+  const long long total = npx * A.spp * A.n_views;  // paths: pixel-major, samples consecutive
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i < total;
   const DevScene& s = A.s;
@@ -61,15 +62,21 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
   float g[3] = {0, 0, 0};
   if (active) {
     rec = A.paths[i];
-    int view = (int)(i / npx);
-    int pix = (int)(i % npx);
+    const long long px = i / A.spp;  // view * npx + pixel
+    const int smp = (int)(i % A.spp);
+    int view = (int)(px / npx);
+    int pix = (int)(px % npx);
     const float* cam = A.cams + 12 * view;
-    d = primary_direction(cam, A.w, A.h, pix % A.w, pix / A.w, A.off, A.off);
+    float ox, oy;
+    sample_offset((uint32_t)pix, smp, A.spp, A.seed, A.off, ox, oy);
+    d = primary_direction(cam, A.w, A.h, pix % A.w, pix / A.w, ox, oy);
     campos = mk3(cam[0], cam[1], cam[2]);
     o = campos;
-    g[0] = A.drgb[3 * i];
-    g[1] = A.drgb[3 * i + 1];
-    g[2] = A.drgb[3 * i + 2];
+    // the pixel is the mean of its samples: each sample's colour has weight 1 / spp
+    const float ws = A.spp > 1 ? 1.0f / (float)A.spp : 1.0f;
+    g[0] = A.drgb[3 * px] * ws;
+    g[1] = A.drgb[3 * px + 1] * ws;
+    g[2] = A.drgb[3 * px + 2] * ws;
   }
   float T = 1.0f;
   bool alive = active;
@@ -207,13 +214,15 @@ eos_status render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* 
   A.h = cams[0].height;
   A.n_views = (int)n_views;
   A.trace_depth = p.trace_depth;
+  A.spp = p.spp;
+  A.seed = p.jitter_seed;
   A.off = p.pixel_offset;
   A.paths = d_paths;
   A.drgb = d_rgb;
   A.gmat = d_gmat;
   A.glight = d_glight;
   A.err = ctx->d_err;
-  long long total = (long long)A.w * A.h * n_views;
+  long long total = (long long)A.w * A.h * p.spp * n_views;
   int grid = (int)((total + 127) / 128);
   k_backward<<<grid, 128, 0, ctx->stream>>>(A);
   EOS_CUDA(cudaGetLastError());

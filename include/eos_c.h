@@ -311,7 +311,10 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs,
                             const eos_render_params* params, eos_stats* stats);
 
 /* Adjoint of the shading with visibility frozen from the forward records.  Views are
- * n_views cameras of equal size rendered with spp 1; paths / d_rgb are [n_views*H*W]. */
+ * n_views cameras of equal size rendered with params' spp, jitter_seed and pixel_offset
+ * (the same as the forward call's); paths are [n_views*H*W*spp] (the forward's order),
+ * d_rgb is [n_views*H*W*3]: a pixel is the mean of its samples.  Whole frames only
+ * (row bands: EOS_ERR_UNSUPPORTED). */
 eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* scene, const eos_camera* cameras,
                                uint32_t n_views, const eos_render_params* params,
                                const eos_path_record* paths, const float* d_rgb, eos_grads* grads);

@@ -74,8 +74,8 @@ def lib_oracle():
                                            POINTER(c_float)]
         L.oracle_morton.argtypes = [POINTER(c_float), POINTER(c_uint32), c_int, POINTER(c_uint32),
                                     POINTER(c_int32)]
-        L.oracle_frozen_f64.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_float, c_int,
-                                        POINTER(c_int32), POINTER(c_uint32), POINTER(c_double),
+        L.oracle_frozen_f64.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_float, c_int, c_uint32,
+                                        c_int, POINTER(c_int32), POINTER(c_uint32), POINTER(c_double),
                                         POINTER(c_double), POINTER(c_double), POINTER(c_double),
                                         POINTER(c_double), POINTER(c_double), c_int]
         _lib_oracle = L
@@ -201,20 +201,23 @@ class Oracle:
         return occ
 
     def frozen_f64(self, cams, width, height, pixel_offset, trace_depth, hits, shadows, mat_params,
-                   light_params, g=None, nthreads=None):
+                   light_params, g=None, nthreads=None, spp=1, jitter_seed=0):
         """FP64 re-render with frozen visibility; with g, also the adjoint of <g, rgb>.
 
+        hits / shadows: per path, V*H*W*spp of them (samples of a pixel consecutive, the
+        forward's order); the colour of a pixel is the mean of its samples, whose offsets
+        come from jitter_seed as in the forward pass.
         mat_params: [K, 10] kd rgb, ks rgb, log shininess, reflectivity, transparency, refractive
         index (float64; rows of 8 are opaque)
         light_params: [L, 6] position xyz, colour rgb (float64)
-        Returns rgb [V*H*W, 3] and, with g, (grad_mat [K, 7], grad_light [L, 6]).
+        Returns rgb [V*H*W, 3] and, with g [V*H*W, 3], (grad_mat [K, 7], grad_light [L, 6]).
         """
         L = lib_oracle()
         cams_a = np.ascontiguousarray(np.stack([c.as_array() for c in cams]), np.float32)
         nv = len(cams)
         npx = nv * width * height
-        h = np.ascontiguousarray(hits, np.int32).reshape(npx, MAXB)
-        s = np.ascontiguousarray(shadows, np.uint32).reshape(npx, MAXB)
+        h = np.ascontiguousarray(hits, np.int32).reshape(npx * spp, MAXB)
+        s = np.ascontiguousarray(shadows, np.uint32).reshape(npx * spp, MAXB)
         mp = np.asarray(mat_params, np.float64)
         if mp.shape[1] == 8:  # no transparency columns: opaque, index 1
             mp = np.concatenate([mp, np.zeros((mp.shape[0], 1)), np.ones((mp.shape[0], 1))], 1)
@@ -224,7 +227,8 @@ class Oracle:
         gm = np.zeros((mp.shape[0], 7), np.float64)
         gl = np.zeros((lp.shape[0], 6), np.float64)
         ga = None if g is None else np.ascontiguousarray(g, np.float64).reshape(npx, 3)
-        L.oracle_frozen_f64(self.h, _p(cams_a, c_float), nv, width, height, pixel_offset, trace_depth,
+        L.oracle_frozen_f64(self.h, _p(cams_a, c_float), nv, width, height, pixel_offset, int(spp),
+                            int(jitter_seed) & 0xFFFFFFFF, trace_depth,
                             _p(h, c_int32), _p(s, c_uint32), _p(mp, c_double), _p(lp, c_double),
                             _p(rgb, c_double), _p(ga, c_double), _p(gm, c_double), _p(gl, c_double),
                             nthreads or os.cpu_count())

@@ -821,12 +821,15 @@ static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, in
  * w x hgt pixels and spp == 1 at pixel_offset).  hits / shadows: [n_views*w*hgt, 8].
  * rgb_out: [n_views*w*hgt, 3].  If g is non-NULL, also writes gradients of <g, rgb>. */
 int oracle_frozen_f64(void* h, const float* cams, int n_views, int w, int hgt, float pixel_offset,
-                      int trace_depth, const int32_t* hits, const uint32_t* shadows,
+                      int spp, uint32_t seed, int trace_depth, const int32_t* hits, const uint32_t* shadows,
                       const double* mat_params, const double* light_params, double* rgb_out,
                       const double* g, double* grad_mat, double* grad_light, int nthreads) {
+  /* Paths are per sample (pixel-major, samples of a pixel consecutive, the forward's
+   * order); a pixel's colour is the sample mean, so each sample's adjoint is g / spp. */
   const oscene* s = (const oscene*)h;
   f64ctx c = {s, mat_params, light_params};
   size_t npx = (size_t)w * hgt;
+  if (spp < 1) spp = 1;
   int nth = nthreads > 0 ? nthreads : 1;
   size_t gms = (size_t)7 * s->nobj, gls = (size_t)6 * s->nl;
   double* gmt = g ? calloc((size_t)nth * gms + 1, sizeof(double)) : NULL;
@@ -839,10 +842,19 @@ int oracle_frozen_f64(void* h, const float* cams, int n_views, int w, int hgt, f
       int view = (int)(i / (long long)npx);
       int p = (int)(i % (long long)npx);
       const float* cam = cams + 12 * view;
-      v3d col = f64_path(&c, cam, w, hgt, p % w, p / w, pixel_offset, pixel_offset, hits + MAXB * i,
-                         shadows + MAXB * i, trace_depth, g ? g + 3 * i : NULL,
-                         g ? gmt + gms * tid : NULL, g ? glt + gls * tid : NULL);
-      if (rgb_out) { rgb_out[3 * i] = col.x; rgb_out[3 * i + 1] = col.y; rgb_out[3 * i + 2] = col.z; }
+      double gs[3];
+      if (g) for (int k = 0; k < 3; ++k) gs[k] = g[3 * i + k] / spp;
+      v3d sum = D3(0, 0, 0);
+      for (int smp = 0; smp < spp; ++smp) {
+        float ox, oy;
+        sample_offset((uint32_t)p, smp, spp, seed, pixel_offset, &ox, &oy);
+        long long path = i * spp + smp;
+        v3d col = f64_path(&c, cam, w, hgt, p % w, p / w, ox, oy, hits + MAXB * path, shadows + MAXB * path,
+                           trace_depth, g ? gs : NULL, g ? gmt + gms * tid : NULL, g ? glt + gls * tid : NULL);
+        sum = dadd(sum, col);
+      }
+      sum = dsc(1.0 / spp, sum);
+      if (rgb_out) { rgb_out[3 * i] = sum.x; rgb_out[3 * i + 1] = sum.y; rgb_out[3 * i + 2] = sum.z; }
     }
   }
   if (g) {

@@ -16,8 +16,8 @@ def _rel_close(a, b, rel=1e-3):
     return np.abs(a - b).max() <= rel * max(scale, 1e-12), (np.abs(a - b).max(), scale)
 
 
-@pytest.mark.parametrize("td,transparent", [(1, False), (2, False), (2, True)])
-def test_backward_matches_fp64_adjoint(ctx, td, transparent):
+@pytest.mark.parametrize("td,transparent,spp", [(1, False, 1), (2, False, 1), (2, True, 1), (2, False, 2)])
+def test_backward_matches_fp64_adjoint(ctx, td, transparent, spp):
     import torch
     sc = scenes.config4_scene()
     sc.materials[:, 7] = 0.3  # mirror bounces so reflected shading is differentiated too
@@ -29,7 +29,8 @@ def test_backward_matches_fp64_adjoint(ctx, td, transparent):
     cams = scenes.config4_cameras(2, 64)
     paths, rgb = [], []
     for c in cams:
-        r = api.render(ctx, dsc, c, td, pixel_offset=0.5, outputs=("rgb", "paths"), device=True)
+        r = api.render(ctx, dsc, c, td, pixel_offset=0.5, spp=spp, jitter_seed=9, outputs=("rgb", "paths"),
+                       device=True)
         paths.append(r["paths"])
         rgb.append(r["rgb"])
     paths = torch.cat(paths)
@@ -37,7 +38,7 @@ def test_backward_matches_fp64_adjoint(ctx, td, transparent):
     rng = np.random.default_rng(4)
     target = torch.from_numpy(rng.uniform(0, 0.6, tuple(rgb.shape)).astype(np.float32)).cuda()
     g = 2.0 * (rgb - target)
-    gm, gl = api.render_backward(ctx, dsc, cams, td, paths, g, pixel_offset=0.5)
+    gm, gl = api.render_backward(ctx, dsc, cams, td, paths, g, pixel_offset=0.5, spp=spp, jitter_seed=9)
     torch.cuda.synchronize()
     mp = sc.materials.astype(np.float64).copy()
     mp[:, 6] = np.log(mp[:, 6])
@@ -45,7 +46,7 @@ def test_backward_matches_fp64_adjoint(ctx, td, transparent):
     orc = oracle.Oracle(sc)
     p = paths.cpu().numpy()
     rgb64, om, ol = orc.frozen_f64(cams, 64, 64, 0.5, td, p[:, :8], p[:, 8:].view(np.uint32), mp, lp,
-                                   g=g.cpu().numpy().astype(np.float64))
+                                   g=g.cpu().numpy().astype(np.float64), spp=spp, jitter_seed=9)
     # FP32 forward vs the FP64 re-render of the same frozen paths: colours up to ~4 with
     # shininess up to e^5, so pow() turns ~1e-7 direction rounding into ~1e-4 relative
     r32 = rgb.cpu().numpy()

@@ -135,16 +135,19 @@ def test_oracle_matches_compiled_reference_config1_full():
     assert d[~mm].max() <= RGB_TOL
 
 
-def test_frozen_f64_adjoint_matches_central_differences():
-    """FP64 analytic adjoint vs central differences (step 1e-3) of the FP64 frozen render."""
+@pytest.mark.parametrize("spp", [1, 2])
+def test_frozen_f64_adjoint_matches_central_differences(spp):
+    """FP64 analytic adjoint vs central differences (step 1e-3) of the FP64 frozen render;
+    with 2 jittered samples per pixel, the pixel is their mean."""
     sc = scenes.small_random_scene(21, n_spheres=4, level=2, lights=2, refl=0.4)
     cams = [scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 24, 20),
             scenes.look_at((-6.0, 4.0, 6.0), (0, -0.5, 0), 55.0, 24, 20)]
     orc = oracle.Oracle(sc)
     td = 2
+    seed = 5
     hits, shadows = [], []
     for c in cams:
-        r = orc.render(c, td, pixel_offset=0.5)
+        r = orc.render(c, td, pixel_offset=0.5, spp=spp, jitter_seed=seed)
         hits.append(r["hits"])
         shadows.append(r["shadows"])
     hits = np.concatenate(hits)
@@ -156,12 +159,15 @@ def test_frozen_f64_adjoint_matches_central_differences():
     target = rng.uniform(0, 0.5, (len(cams) * 24 * 20, 3))
 
     def loss(m, l):
-        rgb = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, m, l)
+        rgb = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, m, l, spp=spp, jitter_seed=seed)
         return float(((rgb - target) ** 2).sum()), rgb
 
     L0, rgb = loss(mp, lp)
+    if spp > 1:  # the FP64 mean of the samples is the FP32 forward's colour, up to rounding
+        r32 = np.concatenate([orc.render(c, td, pixel_offset=0.5, spp=spp, jitter_seed=seed)["rgb"] for c in cams])
+        assert np.abs(rgb - r32).max() < 1e-3
     g = 2.0 * (rgb - target)
-    _, gm, gl = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, mp, lp, g=g)
+    _, gm, gl = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, mp, lp, g=g, spp=spp, jitter_seed=seed)
     h = 1e-3
     checks = [("m", 0, 0), ("m", 1, 4), ("m", 2, 6), ("m", 4, 2), ("l", 0, 0), ("l", 1, 4), ("l", 0, 3), ("l", 1, 5)]
     for kind, i, j in checks:
