@@ -312,8 +312,9 @@ def render_backward(ctx: Context, scene: DeviceScene, cams: list[CameraData], tr
     from the forward render with the same spp / jitter_seed / pixel_offset."""
     arr = (L.Camera * len(cams))(*[camera_struct(c) for c in cams])
     p = params_struct(trace_depth, pixel_offset, spp, jitter_seed)
-    K = scene.scene.n_objects
-    NL = max(1, scene.scene.n_lights)
+    info = scene.info()
+    K = info["n_objects"]
+    NL = max(1, info["n_lights"])
     gm = _alloc((K, 7), np.float32, device)
     gl = _alloc((NL, 6), np.float32, device)
     g = L.Grads()

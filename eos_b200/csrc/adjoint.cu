@@ -3,8 +3,8 @@
 // visibility frozen from the forward pass's path records (hit triangle per bounce and
 // blocked-light masks).  Nothing else of the forward pass is stored: each bounce's hit is
 // re-derived from its triangle id with the same exact-order Moller-Trumbore, hit point,
-// normal and secondary ray as the forward kernels, so the geometry matches the forward
-// pass bit for bit.
+// normal and secondary ray as the forward kernels (in the instance's object space for a
+// two-level scene), so the geometry matches the forward pass bit for bit.
 //
 // Forward model per path (src/RayTracer.cpp:302-458): c = sum_k T_k phong_k with
 // T_k = prod_{j<k} w_j, w = reflectivity for a mirror bounce and K + (1 - K) for a
@@ -91,12 +91,7 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
         alive = false;
       } else {
         Hit h;
-        h.pos = s.pos_of_id[id];
-        h.id = id;
-        f3 v1, e1, e2;
-        int rid;
-        load_tri(s.tris, h.pos, v1, e1, e2, rid);
-        if (!mt_intersect(o, d, v1, e1, e2, h.t, h.u, h.v)) {
+        if (!hit_of_id(s, o, d, id, h)) {
           atomicOr(A.err, kErrIndex);  // record does not match this scene / camera
           alive = false;
         } else {

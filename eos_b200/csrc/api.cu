@@ -541,7 +541,7 @@ eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_came
     return EOS_ERR_INVALID_ARG;
   eos_status st = check_params(p);
   if (st != EOS_OK) return st;
-  if (p->row_begin != 0 || p->row_end != 0 || sc->instanced) return EOS_ERR_UNSUPPORTED;
+  if (p->row_begin != 0 || p->row_end != 0) return EOS_ERR_UNSUPPORTED;
   for (uint32_t v = 0; v < n_views; ++v)
     if (!valid_camera(&cams[v]) || cams[v].width != cams[0].width || cams[v].height != cams[0].height)
       return EOS_ERR_INVALID_ARG;

@@ -48,15 +48,18 @@ enum : int {
 //  Shading record, 48 B = 3 x float4, same order:
 //    [0] n1.x n1.y n1.z n2.x   [1] n2.y n2.z n3.x n3.y   [2] n3.z obj(int) - -
 // ---------------------------------------------------------------------------------
-// One instance of a mesh in a two-level scene (eos_scene_create_instanced), 80 B.
-struct DevInstance {
+// One instance of a mesh in a two-level scene (eos_scene_create_instanced), 96 B with its
+// padding: 16-byte aligned, because the traversal reads minv as three float4.
+struct __align__(16) DevInstance {
   float minv[12];       // object-from-world affine, row-major 3x4 (the inverse of the transform)
   const float4* nodes;  // the mesh's node records, triangle and shading records
   const float4* tris;
   const float4* shade;
   int32_t id_offset;    // global id of the mesh's triangle 0 in this instance
   int32_t mat_base;     // added to the mesh's object ids
+  const int32_t* pos_of_id;  // the mesh's triangle id -> sorted position (the adjoint's replay)
 };
+static_assert(sizeof(DevInstance) % 16 == 0 && alignof(DevInstance) == 16, "minv is read as float4");
 
 struct DevScene {
   const float4* nodes;

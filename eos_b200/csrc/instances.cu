@@ -234,6 +234,7 @@ extern "C" eos_status eos_scene_create_instanced(eos_ctx* ctx, const eos_instanc
     d.nodes = (const float4*)m->d_nodes;
     d.tris = (const float4*)m->d_tris;
     d.shade = (const float4*)m->d_shade;
+    d.pos_of_id = (const int32_t*)m->d_pos_of_id;
     d.id_offset = (int32_t)total;
     d.mat_base = (int32_t)I.material_base;
     total += m->dev.n_tris;

@@ -671,6 +671,30 @@ __device__ __forceinline__ void hit_geometry(const DevScene& s, f3 o, f3 d, cons
   N = norm3(n);
 }
 
+// Replay of a recorded hit (the adjoint): the hit of global triangle `id` for ray (o, d),
+// through the same exact-order test as the traversal (in the instance's object space for a
+// two-level scene), so t, u, v and the sorted position equal the forward pass's.  False if
+// the triangle does not take the ray (a record from another scene or camera).
+__device__ __forceinline__ bool hit_of_id(const DevScene& s, f3 o, f3 d, int id, Hit& h) {
+  const float4* tris = s.tris;
+  const int32_t* pos = s.pos_of_id;
+  int local = id;
+  f3 oo = o, od = d;
+  if (s.inst) {
+    const DevInstance* I = instance_of(s, id);
+    to_object(I, o, d, oo, od);
+    tris = I->tris;
+    pos = I->pos_of_id;
+    local = id - I->id_offset;
+  }
+  h.id = id;
+  h.pos = pos[local];
+  f3 v1, e1, e2;
+  int rid;
+  load_tri(tris, h.pos, v1, e1, e2, rid);
+  return mt_intersect(oo, od, v1, e1, e2, h.t, h.u, h.v);
+}
+
 // RayTracer::calcPhong + findDiffuseColor for one light (src/RayTracer.cpp:418-458):
 // diffuse max(0, L.N) kd Lc, specular [V.R > 0] pow(V.R, shininess) Lc ks with
 // R = normalize(2 (N.L) N - L) and V towards the camera position.

@@ -92,8 +92,9 @@ def render_backward_sharded(ctx, dscene, cams, trace_depth, d_rgb_fn, rank: int,
 
     from . import api
     mine = shard_indices(len(cams), rank, world)
-    K = dscene.scene.n_objects
-    NL = max(1, dscene.scene.n_lights)
+    info = dscene.info()
+    K = info["n_objects"]
+    NL = max(1, info["n_lights"])
     gm = torch.zeros((K, 7), device="cuda")
     gl = torch.zeros((NL, 6), device="cuda")
     for v in mine:

@@ -273,9 +273,9 @@ typedef struct eos_instance {
  * so t is the same parameter in both spaces.  The shading normal is
  * normalize(Minv^T n) of the mesh's interpolated unit normal; hit ids are global:
  * instance k's triangles are numbered after those of instances 0..k-1.  A mesh shared by
- * many instances is stored once.  eos_render / eos_render_batch / eos_trace_* accept the
- * scene (not EOS_FLAG_REFILL / EOS_FLAG_PACKET); eos_render_backward and
- * eos_scene_get_morton return EOS_ERR_UNSUPPORTED. */
+ * many instances is stored once.  eos_render / eos_render_batch / eos_trace_* and
+ * eos_render_backward accept the scene (not EOS_FLAG_REFILL / EOS_FLAG_PACKET);
+ * eos_scene_get_morton and eos_scene_save return EOS_ERR_UNSUPPORTED. */
 eos_status eos_scene_create_instanced(eos_ctx* ctx, const eos_instance* instances, uint32_t n_instances,
                                       const eos_material* materials, uint32_t n_materials,
                                       const eos_light* lights, uint32_t n_lights, eos_scene** out);

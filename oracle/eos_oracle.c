@@ -738,16 +738,47 @@ static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, in
   for (int k = 0; k <= trace_depth && k < MAXB; ++k) {
     int id = hits[k];
     if (id < 0) break;
-    int p = s->pos_of_id[id];
-    v3d v1 = f2d(s->v1[p]), e1 = f2d(s->e1[p]), e2 = f2d(s->e2[p]);
-    v3d Pm = dcross(d, e2);
+    /* the triangle: flat scene, or (two-level) the instance holding global id `id`, its
+     * mesh, the ray in object space (o' = Minv [o, 1], d' = Minv [d, 0]: t is the same
+     * parameter) and the normal back through Minv^T */
+    const oscene* ms = s;
+    const float* minv = NULL;
+    int base = 0, local = id;
+    if (s->ninst) {
+      int lo = 0, hi = s->ninst - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (s->inst_id_off[mid] <= id) lo = mid; else hi = mid - 1;
+      }
+      ms = (const oscene*)s->inst_mesh[lo];
+      minv = s->inst_minv + 12 * lo;
+      base = s->inst_mat_base[lo];
+      local = id - s->inst_id_off[lo];
+    }
+    int p = ms->pos_of_id[local];
+    v3d oo = o, od = d;
+    if (minv) {
+      oo = D3(minv[0] * o.x + minv[1] * o.y + minv[2] * o.z + minv[3],
+              minv[4] * o.x + minv[5] * o.y + minv[6] * o.z + minv[7],
+              minv[8] * o.x + minv[9] * o.y + minv[10] * o.z + minv[11]);
+      od = D3(minv[0] * d.x + minv[1] * d.y + minv[2] * d.z, minv[4] * d.x + minv[5] * d.y + minv[6] * d.z,
+              minv[8] * d.x + minv[9] * d.y + minv[10] * d.z);
+    }
+    v3d v1 = f2d(ms->v1[p]), e1 = f2d(ms->e1[p]), e2 = f2d(ms->e2[p]);
+    v3d Pm = dcross(od, e2);
     double det = ddot(e1, Pm);
-    v3d Tv = dsub(o, v1);
+    v3d Tv = dsub(oo, v1);
     v3d Q = dcross(Tv, e1);
-    double t = ddot(e2, Q) / det, u = ddot(Tv, Pm) / det, v = ddot(d, Q) / det;
+    double t = ddot(e2, Q) / det, u = ddot(Tv, Pm) / det, v = ddot(od, Q) / det;
     v3d P = dadd(o, dsc(t, d));
-    v3d N = dnorm(dadd(dadd(dsc(1.0 - u - v, f2d(s->n1[p])), dsc(u, f2d(s->n2[p]))), dsc(v, f2d(s->n3[p]))));
-    int ob = (int)s->obj[p];
+    v3d n = dadd(dadd(dsc(1.0 - u - v, f2d(ms->n1[p])), dsc(u, f2d(ms->n2[p]))), dsc(v, f2d(ms->n3[p])));
+    if (minv) {
+      n = dnorm(n);
+      n = D3(minv[0] * n.x + minv[4] * n.y + minv[8] * n.z, minv[1] * n.x + minv[5] * n.y + minv[9] * n.z,
+             minv[2] * n.x + minv[6] * n.y + minv[10] * n.z);
+    }
+    v3d N = dnorm(n);
+    int ob = (int)ms->obj[p] + base;
     const double* m = c->mp + OMAT * ob;
     double shin = exp(m[6]);
     v3d V = dnorm(dsub(campos, P));

@@ -119,3 +119,39 @@ def test_instanced_errors(ctx):
     with pytest.raises(EosError) as e:
         api.render(ctx, inst, cam, 1, mode="wavefront", outputs=("rgb",), device=False, refill=True)
     assert e.value.code == 7
+
+
+@pytest.mark.parametrize("spp", [1, 2])
+def test_instanced_backward_matches_fp64_adjoint(ctx, spp):
+    """The adjoint of a two-level scene (each recorded hit replayed in its instance's object
+    space) against the oracle's FP64 adjoint of the same frozen paths, within 1e-3 relative."""
+    import torch
+    d = scenes.instanced_test_scene(7, n_instances=10, lights=2, transparent=1)
+    d.materials[1:, 7] = np.where(d.materials[1:, 8] > 0, 0.0, 0.3)
+    dsc = _device(ctx, d)
+    cams = [scenes.look_at((1.0, 3.0, 9.0), (0, -0.5, 0), 55.0, 48, 40),
+            scenes.look_at((-6.0, 4.0, 5.0), (0, -0.5, 0), 55.0, 48, 40)]
+    td = 2
+    paths, rgb = [], []
+    for c in cams:
+        r = api.render(ctx, dsc, c, td, pixel_offset=0.5, spp=spp, jitter_seed=3, outputs=("rgb", "paths"), device=True)
+        paths.append(r["paths"])
+        rgb.append(r["rgb"])
+    paths = torch.cat(paths)
+    rgb = torch.cat(rgb)
+    target = torch.from_numpy(np.random.default_rng(6).uniform(0, 0.6, tuple(rgb.shape)).astype(np.float32)).cuda()
+    g = 2.0 * (rgb - target)
+    gm, gl = api.render_backward(ctx, dsc, cams, td, paths, g, pixel_offset=0.5, spp=spp, jitter_seed=3)
+    mp = np.asarray(d.materials, np.float64).copy()
+    mp[:, 6] = np.log(mp[:, 6])
+    lp = np.asarray(d.lights, np.float64)
+    p = paths.cpu().numpy()
+    rgb64, om, ol = oracle.OracleInstanced(d).frozen_f64(cams, 48, 40, 0.5, td, p[:, :8], p[:, 8:].view(np.uint32),
+                                                         mp, lp, g=g.cpu().numpy().astype(np.float64), spp=spp,
+                                                         jitter_seed=3)
+    r32 = rgb.cpu().numpy()
+    assert (np.abs(rgb64 - r32) / np.maximum(1.0, np.abs(rgb64))).max() < 1e-3
+    gm, gl = gm.cpu().numpy(), gl.cpu().numpy()
+    for name, a, b in [("materials", gm, om), ("lights", gl, ol)]:
+        err, scale = np.abs(a - b).max(), np.abs(b).max()
+        assert err <= 1e-3 * max(scale, 1e-12), (name, err, scale)

@@ -196,3 +196,39 @@ def test_instanced_oracle_agrees_with_the_flattened_scene():
     assert same.mean() > 0.995
     assert np.abs(a["rgb"] - b["rgb"]).max(1)[same].max() < 1e-4
     assert (a["hits"][:, 0] >= 0).mean() > 0.2
+
+
+def test_instanced_frozen_f64_adjoint_matches_central_differences():
+    """The FP64 adjoint of a two-level scene (hits replayed in each instance's object space,
+    normals through the inverse transpose) against central differences of its own FP64
+    frozen render."""
+    d = scenes.instanced_test_scene(7, n_instances=8, lights=2)
+    d.materials[:, 7] = 0.3
+    orc = oracle.OracleInstanced(d)
+    cams = [scenes.look_at((1.0, 3.0, 9.0), (0, -0.5, 0), 55.0, 24, 20)]
+    td = 2
+    r = orc.render(cams[0], td, pixel_offset=0.5)
+    hits, shadows = r["hits"], r["shadows"]
+    assert (hits[:, 0] >= 0).mean() > 0.3
+    mp = np.asarray(d.materials, np.float64).copy()
+    mp[:, 6] = np.log(mp[:, 6])
+    lp = np.asarray(d.lights, np.float64).copy()
+    target = np.random.default_rng(5).uniform(0, 0.5, (24 * 20, 3))
+
+    def loss(m, l):
+        rgb = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, m, l)
+        return float(((rgb - target) ** 2).sum()), rgb
+
+    _, rgb = loss(mp, lp)
+    assert np.abs(rgb - r["rgb"]).max() < 1e-3  # FP64 replay of the FP32 frame
+    _, gm, gl = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, mp, lp, g=2.0 * (rgb - target))
+    h = 1e-3
+    for kind, i, col, gcol in [("m", 1, 0, 0), ("m", 2, 4, 4), ("m", 3, 6, 6), ("l", 0, 3, 0), ("l", 1, 0, 3)]:
+        arr = (mp if kind == "m" else lp).copy()
+        arr[i, col] += h
+        Lp, _ = loss(arr, lp) if kind == "m" else loss(mp, arr)
+        arr[i, col] -= 2 * h
+        Lm, _ = loss(arr, lp) if kind == "m" else loss(mp, arr)
+        fd = (Lp - Lm) / (2 * h)
+        an = gm[i, gcol] if kind == "m" else gl[i, gcol]
+        assert abs(fd - an) <= 1e-3 * max(1.0, abs(fd)), (kind, i, col, fd, an)
