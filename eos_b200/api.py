@@ -307,11 +307,13 @@ def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning)
 
 
 def render_backward(ctx: Context, scene: DeviceScene, cams: list[CameraData], trace_depth: int, paths, d_rgb,
-                    pixel_offset: float = 0.5, device: bool = True, spp: int = 1, jitter_seed: int = 0):
+                    pixel_offset: float = 0.5, device: bool = True, spp: int = 1, jitter_seed: int = 0,
+                    rows=None):
     """Adjoint of the shading: returns (grad_materials [K,7], grad_lights [L,6]).  paths come
-    from the forward render with the same spp / jitter_seed / pixel_offset."""
+    from the forward render with the same spp / jitter_seed / pixel_offset (and row band
+    `rows`, whose gradients are that band's share of the frame's)."""
     arr = (L.Camera * len(cams))(*[camera_struct(c) for c in cams])
-    p = params_struct(trace_depth, pixel_offset, spp, jitter_seed)
+    p = params_struct(trace_depth, pixel_offset, spp, jitter_seed, rows=rows)
     info = scene.info()
     K = info["n_objects"]
     NL = max(1, info["n_lights"])

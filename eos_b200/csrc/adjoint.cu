@@ -33,6 +33,7 @@ struct BwArgs {
   DevScene s;
   const float* cams;  // n_views x 12
   int w, h, n_views, trace_depth, spp;
+  int y0, rows;   // image rows [y0, y0 + rows) of the forward records (a row band, or all)
   float off;
   uint32_t seed;  // sample jitter (spp > 1), as in the forward pass
   const eos_path_record* paths;
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
   for (int i = threadIdx.x; i < kMaxLights * 6; i += blockDim.x) sl[i] = 0.0f;
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const long long npx = (long long)A.w * A.h;
+  const long long npx = (long long)A.w * A.rows;
   const long long total = npx * A.spp * A.n_views;  // paths: pixel-major, samples consecutive
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i < total;
@@ -67,9 +68,10 @@ __global__ void __launch_bounds__(128) k_backward(BwArgs A) {
     int view = (int)(px / npx);
     int pix = (int)(px % npx);
     const float* cam = A.cams + 12 * view;
+    const int x = pix % A.w, y = A.y0 + pix / A.w;  // image row
     float ox, oy;
-    sample_offset((uint32_t)pix, smp, A.spp, A.seed, A.off, ox, oy);
-    d = primary_direction(cam, A.w, A.h, pix % A.w, pix / A.w, ox, oy);
+    sample_offset((uint32_t)(y * A.w + x), smp, A.spp, A.seed, A.off, ox, oy);
+    d = primary_direction(cam, A.w, A.h, x, y, ox, oy);
     campos = mk3(cam[0], cam[1], cam[2]);
     o = campos;
     // the pixel is the mean of its samples: each sample's colour has weight 1 / spp
@@ -209,6 +211,8 @@ eos_status render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* 
   A.h = cams[0].height;
   A.n_views = (int)n_views;
   A.trace_depth = p.trace_depth;
+  A.y0 = p.row_end > 0 ? p.row_begin : 0;
+  A.rows = p.row_end > 0 ? p.row_end - p.row_begin : A.h;
   A.spp = p.spp;
   A.seed = p.jitter_seed;
   A.off = p.pixel_offset;
@@ -217,7 +221,7 @@ eos_status render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* 
   A.gmat = d_gmat;
   A.glight = d_glight;
   A.err = ctx->d_err;
-  long long total = (long long)A.w * A.h * p.spp * n_views;
+  long long total = (long long)A.w * A.rows * p.spp * n_views;
   int grid = (int)((total + 127) / 128);
   k_backward<<<grid, 128, 0, ctx->stream>>>(A);
   EOS_CUDA(cudaGetLastError());

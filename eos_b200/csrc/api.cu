@@ -541,12 +541,12 @@ eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_came
     return EOS_ERR_INVALID_ARG;
   eos_status st = check_params(p);
   if (st != EOS_OK) return st;
-  if (p->row_begin != 0 || p->row_end != 0) return EOS_ERR_UNSUPPORTED;
   for (uint32_t v = 0; v < n_views; ++v)
     if (!valid_camera(&cams[v]) || cams[v].width != cams[0].width || cams[v].height != cams[0].height)
       return EOS_ERR_INVALID_ARG;
+  if (!valid_rows(cams[0].height, p->row_begin, p->row_end)) return EOS_ERR_INVALID_ARG;
   if ((st = set_device(ctx)) != EOS_OK) return st;
-  const size_t npx = (size_t)n_views * cams[0].width * cams[0].height;
+  const size_t npx = (size_t)n_views * cams[0].width * band_rows(cams[0].height, p->row_begin, p->row_end);
   if ((st = begin_call(ctx)) != EOS_OK) return st;
   const eos_path_record* dp = (const eos_path_record*)stage_in(ctx, "bw.paths", paths,
                                                                  sizeof(eos_path_record) * npx * p->spp, &st);

@@ -313,8 +313,9 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs,
 /* Adjoint of the shading with visibility frozen from the forward records.  Views are
  * n_views cameras of equal size rendered with params' spp, jitter_seed and pixel_offset
  * (the same as the forward call's); paths are [n_views*H*W*spp] (the forward's order),
- * d_rgb is [n_views*H*W*3]: a pixel is the mean of its samples.  Whole frames only
- * (row bands: EOS_ERR_UNSUPPORTED). */
+ * d_rgb is [n_views*H*W*3]: a pixel is the mean of its samples.  With a row band in
+ * params (the forward's), paths and d_rgb hold those rows only and the gradients are the
+ * band's share: the bands of a frame sum to its gradients. */
 eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* scene, const eos_camera* cameras,
                                uint32_t n_views, const eos_render_params* params,
                                const eos_path_record* paths, const float* d_rgb, eos_grads* grads);

@@ -60,6 +60,35 @@ def test_backward_matches_fp64_adjoint(ctx, td, transparent, spp):
         assert ok, (name, info)
 
 
+@pytest.mark.parametrize("spp", [1, 2])
+def test_row_band_gradients_sum_to_the_frame(ctx, spp):
+    """Split-frame differentiation: each band's forward records and loss gradient give that
+    band's share, and the shares of three bands add up to the whole frame's gradients."""
+    import torch
+    sc = scenes.config4_scene()
+    sc.materials[:, 7] = 0.3
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.config4_cameras(1, 64)[0]
+    td = 2
+    rng = np.random.default_rng(8)
+    target = torch.from_numpy(rng.uniform(0, 0.6, (64 * 64, 3)).astype(np.float32)).cuda()
+    r = api.render(ctx, dsc, cam, td, spp=spp, jitter_seed=4, outputs=("rgb", "paths"), device=True)
+    g = 2.0 * (r["rgb"] - target)
+    fm, fl = api.render_backward(ctx, dsc, [cam], td, r["paths"], g, spp=spp, jitter_seed=4)
+    sm = torch.zeros_like(fm)
+    sl = torch.zeros_like(fl)
+    for r0, r1 in ((0, 20), (20, 41), (41, 64)):
+        b = api.render(ctx, dsc, cam, td, spp=spp, jitter_seed=4, outputs=("rgb", "paths"), device=True,
+                       rows=(r0, r1))
+        assert torch.equal(b["rgb"], r["rgb"][r0 * 64:r1 * 64])
+        gb = 2.0 * (b["rgb"] - target[r0 * 64:r1 * 64])
+        bm, bl = api.render_backward(ctx, dsc, [cam], td, b["paths"], gb, spp=spp, jitter_seed=4, rows=(r0, r1))
+        sm += bm
+        sl += bl
+    for a, b in ((sm, fm), (sl, fl)):  # float atomics sum in another order
+        assert (a - b).abs().max() <= 1e-4 * b.abs().max()
+
+
 def test_autograd_function_inverse_shading_reduces_loss(ctx):
     """Config-4 style inverse shading: a few gradient steps from perturbed parameters."""
     import torch
