@@ -415,6 +415,9 @@ def run_ours(args, rank, world, local):
             "traffic": (round(traffic["dram_bytes_per_ray"] * rays_top / launches_top) if traffic else None),
             "traffic_source": ("ncu capture of the same kernel, cold caches, DRAM bytes per ray x rays per launch"
                                if traffic else None),
+            # what binds this kernel: instruction issue on partly divergent warps (same ncu capture)
+            "issue_active_pct": traffic.get("issue_active_pct") if traffic else None,
+            "threads_per_warp_instruction": traffic.get("threads_per_warp_instruction") if traffic else None,
             "algorithmic_bytes_per_launch": round(bytes_top / launches_top), "launches": launches_top,
             "ms_per_launch": round(ms_top / launches_top, 4), "stage_ms": [round(x, 3) for x in stage]}
 
