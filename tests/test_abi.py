@@ -5,8 +5,6 @@ import os
 import re
 from ctypes import byref, c_void_p
 
-import numpy as np
-
 from eos_b200 import _lib as L
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -7,7 +7,7 @@ import pytest
 
 import oracle
 from eos_b200 import api, scenes
-from tests.parity import RGB_TOL, classify, path_mismatch, primary_rays
+from tests.parity import RGB_TOL, classify, path_mismatch
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
