@@ -243,6 +243,11 @@ eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning*
 eos_status eos_ctx_clear_tuning(eos_ctx* ctx);
 
 /* ---------------------------------------------------------------------------- scenes */
+/* verts / normals [n_verts*3], tris [n_tris*3] vertex indices, tri_obj [n_tris] material
+ * rows.  Limits (EOS_ERR_INVALID_ARG, checked before any device work): n_tris < 2^25
+ * (leaf references hold 25-bit positions), 1 <= n_materials, n_lights <= EOS_MAX_LIGHTS,
+ * leaf_size <= 32; vertex indices < n_verts and material rows < n_materials are checked
+ * on the device and fail the call the same way.  build may be NULL (tuned values). */
 eos_status eos_scene_create(eos_ctx* ctx, const float* verts, const float* normals, uint32_t n_verts,
                             const uint32_t* tris, const uint32_t* tri_obj, uint32_t n_tris,
                             const eos_material* materials, uint32_t n_materials,

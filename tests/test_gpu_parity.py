@@ -348,6 +348,27 @@ def test_invalid_arguments_report_status(ctx):
     with pytest.raises(EosError) as e:
         api.DeviceScene(ctx, bad)
     assert e.value.code == 1
+    bad_obj = scenes.SceneData(V, V, np.array([[0, 1, 2]]), np.array([5]), mat, np.zeros((0, 6)))
+    with pytest.raises(EosError) as e:  # material row beyond the table
+        api.DeviceScene(ctx, bad_obj)
+    assert e.value.code == 1
+    # size limits are refused before anything is read: 2^25 triangles claimed over tiny buffers,
+    # 33 lights, leaves of 33
+    import ctypes
+    from eos_b200 import _lib as L
+    tri = np.array([[0, 1, 2]], np.uint32)
+    obj = np.zeros(1, np.uint32)
+    m10 = scenes.pad_materials(mat)
+    lights33 = np.zeros((33, 6), np.float32)
+    h = ctypes.c_void_p()
+    args = [ctx.h, V.ctypes.data, V.ctypes.data, 3, tri.ctypes.data, obj.ctypes.data]
+    assert ctx.lib.eos_scene_create(*args, 1 << 25, m10.ctypes.data, 1, None, 0, None, ctypes.byref(h)) == 1
+    assert ctx.lib.eos_scene_create(*args, 1, m10.ctypes.data, 1, lights33.ctypes.data, 33, None,
+                                    ctypes.byref(h)) == 1
+    bp = L.BuildParams()
+    bp.leaf_size = 33
+    assert ctx.lib.eos_scene_create(*args, 1, m10.ctypes.data, 1, None, 0, ctypes.byref(bp), ctypes.byref(h)) == 1
+    assert not h.value
     sc = scenes.small_random_scene(3)
     dsc = api.DeviceScene(ctx, sc)
     cam = scenes.look_at((0, 0, 5), (0, 0, 0), 60, 8, 8)
