@@ -36,6 +36,12 @@ __device__ __forceinline__ float merged_area(float4 al, float4 ah, float4 bl, fl
   return dx * dy + dy * dz + dz * dx;
 }
 
+// Leaf p's node id in the refit's numbering (n - 1 + p): the initial clusters.
+__global__ void k_ploc_leaf_ids(int n, int* __restrict__ cid) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) cid[p] = n - 1 + p;
+}
+
 // Nearest neighbour of every cluster within kRadius places (boxes staged in shared memory).
 __global__ void k_ploc_nn(int nc, const float4* __restrict__ lo, const float4* __restrict__ hi,
                           int* __restrict__ nn) {
@@ -210,12 +216,7 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   // clusters = leaves in Morton order
   EOS_CUDA(cudaMemcpyAsync(clo[0], blo + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
   EOS_CUDA(cudaMemcpyAsync(chi[0], bhi + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
-  {
-    std::vector<int> ids(nn);
-    for (int p = 0; p < n; ++p) ids[p] = n - 1 + p;
-    EOS_CUDA(cudaMemcpyAsync(cid[0], ids.data(), 4 * nn, cudaMemcpyHostToDevice, st));
-    EOS_CUDA(cudaStreamSynchronize(st));
-  }
+  k_ploc_leaf_ids<<<grid_of(n, 256), 256, 0, st>>>(n, cid[0]);
   int nc = n, cur = 0, node_base = 0, iters = 0;
   while (nc > 1) {
     if (++iters > 4 * n + 8) return EOS_ERR_TIMEOUT;  // cannot happen: every round merges
