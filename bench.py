@@ -457,6 +457,9 @@ def run_ours(args, rank, world, local):
         "batched_refill": {"value": round(mrays_c, 2), "unit": "Mrays/s",
                            "note": "same batch, persistent kernels with lane refill (EOS_FLAG_REFILL)"},
         "rays_per_step": {"total": rays_b / args.steps / world},
+        # the headline split by ray type: this rank's per-step counts at the whole-job step time
+        "mrays_by_type": {k: round(st[k + "_rays"] * world / (ms_b / args.steps * 1e-3) / 1e6, 2)
+                          for k in ("primary", "shadow", "secondary")},
         "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
                 "call": "eos_render_batch, all views of the step, pinned host RGBA8 outputs (wall clock)",
                 "h2d_bytes_per_step": len(cams) * 184 + 36, "d2h_bytes_per_step": 4 * npx_step,
