@@ -14,6 +14,9 @@ eos_ctx::~eos_ctx() {
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);
+  if (ring_host) cudaFreeHost(ring_host);
+  for (cudaEvent_t e : ring_ev)
+    if (e) cudaEventDestroy(e);
   if (d_err) cudaFree(d_err);
   if (d_counts) cudaFree(d_counts);
   if (ev0) cudaEventDestroy(ev0);

@@ -95,6 +95,11 @@ struct eos_ctx {
   std::map<std::string, eos::DevBuffer> scratch;
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
+  // PLOC round read-back ring (made on first use): mapped pinned slots the merge kernel
+  // writes, and one event per slot
+  int* ring_host = nullptr;
+  int* ring_dev = nullptr;
+  cudaEvent_t ring_ev[4] = {};
   // autotuner table: min triangle count -> tuned parameters
   std::map<uint32_t, eos_tuning> tuning;
   // per-call bookkeeping reported in eos_stats

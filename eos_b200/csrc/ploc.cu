@@ -43,9 +43,10 @@ __global__ void k_ploc_leaf_ids(int n, int* __restrict__ cid) {
 }
 
 // Nearest neighbour of every cluster within kRadius places (boxes staged in shared memory).
-__global__ void k_ploc_nn(int nc, const float4* __restrict__ lo, const float4* __restrict__ hi,
+__global__ void k_ploc_nn(const int* __restrict__ state, const float4* __restrict__ lo, const float4* __restrict__ hi,
                           int* __restrict__ nn) {
   __shared__ float4 slo[kNNBlock + 2 * kRadius], shi[kNNBlock + 2 * kRadius];
+  const int nc = state[0];
   const int b0 = blockIdx.x * kNNBlock;
   for (int t = threadIdx.x; t < kNNBlock + 2 * kRadius; t += blockDim.x) {
     const int g = b0 - kRadius + t;
@@ -78,10 +79,14 @@ __global__ void k_ploc_nn(int nc, const float4* __restrict__ lo, const float4* _
 // of a pair creates a node (make).  With `force` (an iteration that merged nothing) the
 // pairs (2k, 2k + 1) merge instead, which bounds the number of iterations.
 // keep in the low 32 bits, make in the high 32 bits: one scan counts both.
-__global__ void k_ploc_flags(int nc, const int* __restrict__ nn, int force, unsigned long long* __restrict__ km) {
+// The scan runs over nc_ub + 1 entries (nc_ub: the host's upper bound of nc); the entries
+// from nc on are 0, so the scan's value at nc is the round's total.
+__global__ void k_ploc_flags(const int* __restrict__ state, int nc_ub, const int* __restrict__ nn, int force,
+                             unsigned long long* __restrict__ km) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nc) return;
-  if (i == nc) {  // the scan's total
+  const int nc = state[0];
+  if (i > nc_ub) return;
+  if (i >= nc) {
     km[i] = 0ull;
     return;
   }
@@ -97,13 +102,24 @@ __global__ void k_ploc_flags(int nc, const int* __restrict__ nn, int force, unsi
   km[i] = keep | (make << 32);
 }
 
-__global__ void k_ploc_merge(int nc, const int* __restrict__ nn, int force,
-                             const unsigned long long* __restrict__ km_scan, int node_base, const int* __restrict__ cid,
+// Also writes the next round's state (clusters kept, nodes made so far, nodes made by this
+// round) to state_out and to the host's read-back slot.
+__global__ void k_ploc_merge(const int* __restrict__ state, int* __restrict__ state_out, int* __restrict__ slot,
+                             const int* __restrict__ nn, int force,
+                             const unsigned long long* __restrict__ km_scan, const int* __restrict__ cid,
                              const float4* __restrict__ lo, const float4* __restrict__ hi, int* __restrict__ cid_out,
                              float4* __restrict__ lo_out, float4* __restrict__ hi_out, int2* __restrict__ child,
                              int* __restrict__ count, float4* __restrict__ nlo, float4* __restrict__ nhi, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = state[0], node_base = state[1];
   if (i >= nc) return;
+  if (i == 0) {
+    const unsigned long long total = km_scan[nc];
+    const int kept = (int)(total & 0xffffffffull), made = (int)(total >> 32);
+    state_out[0] = slot[0] = kept;
+    state_out[1] = slot[1] = node_base + made;
+    state_out[2] = slot[2] = made;
+  }
   int partner;
   if (force) {
     partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
@@ -132,6 +148,15 @@ __global__ void k_ploc_merge(int nc, const int* __restrict__ nn, int force,
   cid_out[pos] = k;
   lo_out[pos] = l;
   hi_out[pos] = h;
+}
+
+// Round state on the device: [0] clusters, [1] interior nodes made so far, [2] nodes made
+// by the last round.  Rounds are launched ahead of the host, which reads the state back a
+// few rounds later (build_ploc).
+__global__ void k_ploc_state_init(int* __restrict__ state, int n) {
+  state[0] = n;
+  state[1] = 0;
+  state[2] = 1;
 }
 
 __global__ void k_ploc_parents(int n, const int2* __restrict__ child, int* __restrict__ parent) {
@@ -217,31 +242,69 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   EOS_CUDA(cudaMemcpyAsync(clo[0], blo + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
   EOS_CUDA(cudaMemcpyAsync(chi[0], bhi + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
   k_ploc_leaf_ids<<<grid_of(n, 256), 256, 0, st>>>(n, cid[0]);
-  int nc = n, cur = 0, node_base = 0, iters = 0;
-  while (nc > 1) {
-    if (++iters > 4 * n + 8) return EOS_ERR_TIMEOUT;  // cannot happen: every round merges
-    k_ploc_nn<<<grid_of(nc, kNNBlock), kNNBlock, 0, st>>>(nc, clo[cur], chi[cur], nbr);
-    int force = 0;
-    for (;;) {
-      k_ploc_flags<<<grid_of(nc + 1, 256), 256, 0, st>>>(nc, nbr, force, km);
-      EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, km, km_scan, nc + 1, st));
-      unsigned long long total = 0;
-      EOS_CUDA(cudaMemcpyAsync(&total, km_scan + nc, 8, cudaMemcpyDeviceToHost, st));
-      EOS_CUDA(cudaStreamSynchronize(st));
-      const int kept = (int)(total & 0xffffffffull), made = (int)(total >> 32);
-      if (made == 0 && !force) {
-        force = 1;
-        continue;
-      }
-      k_ploc_merge<<<grid_of(nc, 256), 256, 0, st>>>(nc, nbr, force, km_scan, node_base, cid[cur],
-                                                     clo[cur], chi[cur], cid[cur ^ 1], clo[cur ^ 1], chi[cur ^ 1],
-                                                     tchild, tcount, tlo, thi, n);
-      node_base += made;
-      nc = kept;
-      cur ^= 1;
-      break;
+  // Rounds run ahead of the host: grids are sized by an upper bound of the cluster count
+  // (the last one read back; it only falls), and the host reads each round's state
+  // kAhead rounds later instead of waiting after every round.  A round that merges nothing
+  // changes nothing, so the rounds queued behind one repeat it harmlessly; when the host
+  // sees it, it waits for the queue and runs the forced round (as a synchronous loop
+  // would right away), so the tree is the same.
+  constexpr int kAhead = 4;
+  static_assert(kAhead <= (int)(sizeof(ctx->ring_ev) / sizeof(ctx->ring_ev[0])), "one event per slot");
+  int* state = (int*)scratch(ctx, "ploc.state", 32, &es);  // two states, by round parity
+  if (es != EOS_OK) return es;
+  if (!ctx->ring_host) {
+    if (cudaHostAlloc(&ctx->ring_host, 16 * kAhead, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&ctx->ring_dev, ctx->ring_host, 0) != cudaSuccess) {
+      cudaGetLastError();
+      if (ctx->ring_host) cudaFreeHost(ctx->ring_host);
+      ctx->ring_host = ctx->ring_dev = nullptr;
+      return EOS_ERR_OOM;
     }
   }
+  for (cudaEvent_t& e : ctx->ring_ev)
+    if (!e) EOS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  volatile int* snap = ctx->ring_host;
+  k_ploc_state_init<<<1, 1, 0, st>>>(state, n);
+  int nc_ub = n, cur = 0;
+  long long issued = 0, read = 0;
+  auto enqueue = [&](int force) {
+    if (!force) k_ploc_nn<<<grid_of(nc_ub, kNNBlock), kNNBlock, 0, st>>>(state + 4 * cur, clo[cur], chi[cur], nbr);
+    k_ploc_flags<<<grid_of(nc_ub + 1, 256), 256, 0, st>>>(state + 4 * cur, nc_ub, nbr, force, km);
+    if (cub::DeviceScan::ExclusiveSum(temp, temp_bytes, km, km_scan, nc_ub + 1, st) != cudaSuccess) return false;
+    const int slot = (int)(issued % kAhead);
+    k_ploc_merge<<<grid_of(nc_ub, 256), 256, 0, st>>>(state + 4 * cur, state + 4 * (cur ^ 1), ctx->ring_dev + 4 * slot,
+                                                     nbr, force, km_scan, cid[cur], clo[cur], chi[cur], cid[cur ^ 1],
+                                                     clo[cur ^ 1], chi[cur ^ 1], tchild, tcount, tlo, thi, n);
+    if (cudaEventRecord(ctx->ring_ev[slot], st) != cudaSuccess) return false;
+    cur ^= 1;
+    ++issued;
+    return true;
+  };
+  bool ok = true;
+  for (;;) {
+    if (issued - read == kAhead || !ok) {  // read the oldest round in flight
+      const int slot = (int)(read % kAhead);
+      if (!ok || cudaEventSynchronize(ctx->ring_ev[slot]) != cudaSuccess) return EOS_ERR_CUDA;
+      ++read;
+      const int nc = snap[4 * slot], made = snap[4 * slot + 2];
+      nc_ub = std::min(nc_ub, nc);
+      if (nc <= 1) break;
+      if (made == 0) {  // stalled: drain, then the forced round
+        EOS_CUDA(cudaStreamSynchronize(st));
+        if (!enqueue(1)) return EOS_ERR_CUDA;
+        EOS_CUDA(cudaStreamSynchronize(st));
+        read = issued;
+        nc_ub = std::min(nc_ub, (int)snap[4 * (int)((issued - 1) % kAhead)]);
+        if (nc_ub <= 1) break;
+      }
+    }
+    if (issued > 4ll * n + 8) return EOS_ERR_TIMEOUT;  // cannot happen: every round or its forced repeat merges
+    ok = enqueue(0);
+  }
+  int final_state[4] = {0, 0, 0, 0};
+  EOS_CUDA(cudaMemcpyAsync(final_state, state + 4 * cur, 16, cudaMemcpyDeviceToHost, st));
+  EOS_CUDA(cudaStreamSynchronize(st));
+  const int node_base = final_state[1];
   if (node_base != n - 1) return EOS_ERR_CUDA;
   EOS_CUDA(cudaMemsetAsync(tparent, 0xff, 4 * (2 * nn), st));
   EOS_CUDA(cudaMemsetAsync(dmax, 0, 4, st));
