@@ -10,6 +10,8 @@
 // Primitive order = stable sort by (code, triangle id).
 #include <algorithm>
 
+#include <cub/device/device_scan.cuh>
+
 #include "eos_internal.cuh"
 
 namespace eos {
@@ -349,16 +351,23 @@ __device__ __forceinline__ void write_record(float4* o, const float (&v)[6][4], 
   o[7] = make_float4(__int_as_float(cnt[0]), __int_as_float(cnt[1]), __int_as_float(cnt[2]), __int_as_float(cnt[3]));
 }
 
-__global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* __restrict__ range,
-                             const float4* __restrict__ blo, const float4* __restrict__ bhi,
-                             const int2* __restrict__ frontier_in, int n_in, int2* __restrict__ frontier_out,
-                             int* __restrict__ n_out, int* __restrict__ w_count, float4* __restrict__ wnodes,
-                             int max_nodes, int max_children, int* err) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_in) return;
-  const int2 item = frontier_in[t];
-  int c[4];
-  int2 ch = child[item.x];
+// One level of the wide records, in two passes over the frontier (binary node, record):
+// k_wide_select opens each frontier node's children greedily (the largest-area interior
+// child is replaced by its two children until max_children) and counts those that get a
+// record of their own; after an exclusive scan of the counts, k_wide_write numbers them
+// base + scan[t] + j and writes the record.  Records come out level by level, each node's
+// children in consecutive records, the same on every run.
+__global__ void k_wide_select(int n, const int2* __restrict__ child, const float4* __restrict__ blo,
+                              const float4* __restrict__ bhi, const int2* __restrict__ frontier_in, int n_in,
+                              int max_children, int4* __restrict__ sel, int* __restrict__ n_interior) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > n_in) return;
+  if (t == n_in) {  // the scan's total
+    n_interior[t] = 0;
+    return;
+  }
+  int c[4] = {-1, -1, -1, -1};
+  const int2 ch = child[frontier_in[t].x];
   c[0] = ch.x;
   c[1] = ch.y;
   int k = 2;
@@ -379,16 +388,31 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
     c[best] = g.x;
     c[k++] = g.y;
   }
+  int m = 0;
+  for (int i = 0; i < k; ++i) m += c[i] < n - 1 && bhi[c[i]].w == 0.0f;
+  sel[t] = make_int4(c[0], c[1], c[2], c[3]);
+  n_interior[t] = m;
+}
+
+__global__ void k_wide_write(int n, const int2* __restrict__ range, const float4* __restrict__ blo,
+                             const float4* __restrict__ bhi, const int2* __restrict__ frontier_in, int n_in,
+                             const int4* __restrict__ sel, const int* __restrict__ first, int base,
+                             int2* __restrict__ frontier_out, float4* __restrict__ wnodes, int max_nodes, int* err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_in) return;
+  const int4 s4 = sel[t];
+  const int c[4] = {s4.x, s4.y, s4.z, s4.w};
+  int next = first[t];
   float v[6][4];
   int ref[4], cnt[4];
   for (int i = 0; i < 4; ++i) {
-    if (i >= k) {
+    const int ci = c[i];
+    if (ci < 0) {
       for (int a = 0; a < 6; ++a) v[a][i] = a < 3 ? kInf : -kInf;  // a box no ray enters
       ref[i] = kEmptyRef;
       cnt[i] = -1;
       continue;
     }
-    const int ci = c[i];
     const float4 l = blo[ci], h = bhi[ci];
     v[0][i] = l.x; v[1][i] = l.y; v[2][i] = l.z;
     v[3][i] = h.x; v[4][i] = h.y; v[5][i] = h.z;
@@ -400,20 +424,21 @@ __global__ void k_wide_level(int n, const int2* __restrict__ child, const int2* 
       cnt[i] = r.y - r.x + 1;
       ref[i] = pack_leaf(r.x, cnt[i]);
     } else {
-      const int w = atomicAdd(w_count, 1);
-      if (w >= max_nodes) {  // cannot happen: the tree has at most n - 1 records
+      const int w = base + next;
+      if (w >= max_nodes) {  // cannot happen: the tree has at most n - 1 records (the host stops)
         atomicOr(err, kErrQueue);
         for (int a = 0; a < 6; ++a) v[a][i] = a < 3 ? kInf : -kInf;
         ref[i] = kEmptyRef;
         cnt[i] = -1;
+        ++next;
         continue;
       }
-      frontier_out[atomicAdd(n_out, 1)] = make_int2(ci, w);
+      frontier_out[next++] = make_int2(ci, w);
       ref[i] = w;
       cnt[i] = 0;
     }
   }
-  write_record(wnodes + 8 * (size_t)item.y, v, ref, cnt);
+  write_record(wnodes + 8 * (size_t)frontier_in[t].y, v, ref, cnt);
 }
 
 // Root record of a scene with 0 or 1 triangle (no binary interior node exists).
@@ -436,32 +461,41 @@ __global__ void k_small_root(int n, const float4* __restrict__ blo, const float4
 
 inline int grid_for(size_t n, int block) { return (int)std::max<size_t>(1, (n + block - 1) / block); }
 
-// Writes the node records of the binary tree in the given width (top-down, one launch per
-// level).  Returns the number of levels through *levels (kStackMax * 4 + 1 when the walk
+// Writes the node records of the binary tree in the given width (top-down, one select /
+// scan / write per level).  Returns the number of levels through *levels (kStackMax * 4 + 1 when the walk
 // did not end, which cannot happen for a tree of depth <= kStackMax).
 eos_status write_records(eos_ctx* ctx, int n, const int2* child, const int2* range, const float4* blo,
                          const float4* bhi, int width, float4* out, int max_nodes, int* levels, int* n_records) {
   cudaStream_t st = ctx->stream;
   eos_status es = EOS_OK;
-  int2* fa = (int2*)scratch(ctx, "lbvh.wide.fa", 8 * (size_t)n, &es);
-  int2* fb = (int2*)scratch(ctx, "lbvh.wide.fb", 8 * (size_t)n, &es);
-  int* cnt = (int*)scratch(ctx, "lbvh.wide.cnt", 8, &es);
+  const size_t nn = (size_t)n;
+  int2* fa = (int2*)scratch(ctx, "lbvh.wide.fa", 8 * nn, &es);
+  int2* fb = (int2*)scratch(ctx, "lbvh.wide.fb", 8 * nn, &es);
+  int4* sel = (int4*)scratch(ctx, "lbvh.wide.sel", 16 * nn, &es);
+  int* m = (int*)scratch(ctx, "lbvh.wide.m", 4 * (nn + 1), &es);
+  int* first = (int*)scratch(ctx, "lbvh.wide.first", 4 * (nn + 1), &es);
+  size_t temp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, m, first, n + 1, st);
+  void* temp = scratch(ctx, "lbvh.wide.scan_temp", std::max<size_t>(temp_bytes, 16), &es);
   if (es != EOS_OK) return es;
-  int h_init[2] = {1, 0};  // record count (the root is record 0), frontier size
-  int2 root = make_int2(0, 0);
-  EOS_CUDA(cudaMemcpyAsync(cnt, h_init, sizeof h_init, cudaMemcpyHostToDevice, st));
+  const int2 root = make_int2(0, 0);  // the binary root becomes record 0
   EOS_CUDA(cudaMemcpyAsync(fa, &root, sizeof root, cudaMemcpyHostToDevice, st));
-  int n_in = 1, lv = 0;
+  int n_in = 1, base = 1, lv = 0;
   while (n_in > 0 && lv <= 4 * kStackMax) {  // bounded: the depth is at most the binary depth
-    EOS_CUDA(cudaMemsetAsync(cnt + 1, 0, sizeof(int), st));
-    k_wide_level<<<grid_for(n_in, 128), 128, 0, st>>>(n, child, range, blo, bhi, fa, n_in, fb, cnt + 1, cnt, out,
-                                                       max_nodes, width, ctx->d_err);
+    k_wide_select<<<grid_for((size_t)n_in + 1, 128), 128, 0, st>>>(n, child, blo, bhi, fa, n_in, width, sel, m);
+    EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, m, first, n_in + 1, st));
+    k_wide_write<<<grid_for(n_in, 128), 128, 0, st>>>(n, range, blo, bhi, fa, n_in, sel, first, base, fb, out,
+                                                       max_nodes, ctx->d_err);
     ++lv;
-    EOS_CUDA(cudaMemcpyAsync(&n_in, cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int n_out = 0;
+    EOS_CUDA(cudaMemcpyAsync(&n_out, first + n_in, sizeof(int), cudaMemcpyDeviceToHost, st));
     EOS_CUDA(cudaStreamSynchronize(st));
+    if ((long long)base + n_out > max_nodes) return EOS_ERR_QUEUE_OVERFLOW;  // cannot happen, as above
+    base += n_out;
+    n_in = n_out;
     std::swap(fa, fb);
   }
-  EOS_CUDA(cudaMemcpy(n_records, cnt, sizeof(int), cudaMemcpyDeviceToHost));
+  *n_records = std::min(base, max_nodes);
   *levels = n_in > 0 ? 4 * kStackMax + 1 : lv;
   return EOS_OK;
 }

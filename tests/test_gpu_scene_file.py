@@ -2,7 +2,7 @@
 records as the one saved, so every render, batch and query of it equals the original's
 bit for bit (gradients up to the order of their float atomics), and the loaded scene
 alone still matches the oracle.  A missing, truncated, altered or foreign file is refused
-with a status and leaves no scene behind."""
+with a status and leaves no scene behind.  Two builds of one scene save the same bytes."""
 import ctypes
 
 import numpy as np
@@ -50,6 +50,21 @@ def test_loaded_scene_renders_like_the_built_one(ctx, tmp_path, build):
     p = _np(rb["paths"])
     assert np.array_equal(p[:, :8], o["hits"]) and np.array_equal(p[:, 8:].view(np.uint32), o["shadows"])
     assert np.abs(_np(rb["rgb"]) - o["rgb"]).max() <= RGB_TOL
+
+
+@pytest.mark.parametrize("build", [{}, {"builder": "lbvh"}, {"width": 2, "leaf_size": 1}])
+def test_builds_are_reproducible(ctx, tmp_path, build):
+    """Two builds of one scene write the same file, byte for byte, but for the build time
+    in the header (bytes 56..59): the records are numbered by scans, not by atomics."""
+    sc = scenes.small_random_scene(11, n_spheres=40, level=4, lights=2)
+    raw = []
+    for k in range(2):
+        d = api.DeviceScene(ctx, sc, **build)
+        d.save(tmp_path / f"b{k}.eos")
+        d.close()
+        raw.append((tmp_path / f"b{k}.eos").read_bytes())
+    assert len(raw[0]) == len(raw[1]) > 128 * 1000
+    assert raw[0][:56] == raw[1][:56] and raw[0][60:] == raw[1][60:]
 
 
 def test_loaded_scene_in_batches_queries_and_gradients(ctx, tmp_path):
