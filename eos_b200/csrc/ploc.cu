@@ -27,6 +27,7 @@ namespace {
 
 constexpr int kRadius = 16;        // neighbours searched on each side
 constexpr int kNNBlock = 256;
+constexpr int kTail = 1024;  // clusters at or below which one block runs the remaining rounds
 constexpr int kMaxWalk = 4 * kStackMax;  // bound of the walks to the root
 
 __device__ __forceinline__ float merged_area(float4 al, float4 ah, float4 bl, float4 bh) {
@@ -159,6 +160,122 @@ __global__ void k_ploc_state_init(int* __restrict__ state, int n) {
   state[2] = 1;
 }
 
+// The rounds left once at most kTail clusters remain, in one block with the clusters in
+// shared memory: the same neighbour search, pair rule, forced round after a round that
+// merged nothing, and creation-order numbering as the per-round kernels, so the tree is
+// the same; what it saves is the launches of the last ~30 rounds.
+__global__ void __launch_bounds__(kTail) k_ploc_tail(int* __restrict__ state, const int* __restrict__ cid_in,
+                                                     const float4* __restrict__ lo_in, const float4* __restrict__ hi_in,
+                                                     int2* __restrict__ child, int* __restrict__ count,
+                                                     float4* __restrict__ nlo, float4* __restrict__ nhi, int n,
+                                                     int* __restrict__ err) {
+  __shared__ float4 slo[kTail], shi[kTail];
+  __shared__ int scid[kTail], snn[kTail];
+  __shared__ int wsum[kTail / 32];
+  const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
+  int nc = state[0], node_base = state[1];
+  int force = state[2] == 0 && nc > 1;  // the last round merged nothing: the forced round is next
+  if (nc > kTail) {  // the host launches this only at or below kTail
+    if (i == 0) atomicOr(err, kErrIndex);
+    return;
+  }
+  if (i < nc) {
+    slo[i] = lo_in[i];
+    shi[i] = hi_in[i];
+    scid[i] = cid_in[i];
+  }
+  __syncthreads();
+  int made = 1, iters = 0;
+  while (nc > 1) {
+    if (++iters > 4 * kTail + 8) {  // cannot happen: every round or its forced repeat merges
+      if (i == 0) atomicOr(err, kErrTimeout);
+      break;
+    }
+    if (!force && i < nc) {
+      const float4 al = slo[i], ah = shi[i];
+      float best = kInf;
+      int bj = i == 0 ? 1 : i - 1;
+      const int j0 = max(0, i - kRadius), j1 = min(nc - 1, i + kRadius);
+      for (int j = j0; j <= j1; ++j) {
+        if (j == i) continue;
+        const float a = merged_area(al, ah, slo[j], shi[j]);
+        if (a < best) {
+          best = a;
+          bj = j;
+        }
+      }
+      snn[i] = bj;
+    }
+    __syncthreads();
+    int partner = -1;
+    if (i < nc) {
+      if (force) {
+        partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
+      } else {
+        const int j = snn[i];
+        partner = (j >= 0 && j < nc && snn[j] == i) ? j : -1;
+      }
+    }
+    const int keep = i < nc && (partner < 0 || i < partner);
+    const int make = i < nc && partner >= 0 && i < partner;
+    // block exclusive scan of keep (low 16 bits) and make (high 16 bits)
+    const int v = keep | (make << 16);
+    int inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= d) inc += u;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < kTail / 32; ++w) {
+      const int t = wsum[w];
+      before += w < warp ? t : 0;
+      total += t;
+    }
+    const int ex = before + inc - v;
+    const int pos = ex & 0xffff, mk = ex >> 16;
+    const int kept = total & 0xffff;
+    made = total >> 16;
+    int out_id = 0;
+    float4 ol = make_float4(0.0f, 0.0f, 0.0f, 0.0f), oh = ol;
+    if (keep) {
+      if (partner < 0) {
+        out_id = scid[i];
+        ol = slo[i];
+        oh = shi[i];
+      } else {
+        const int k = node_base + mk;
+        const int a = scid[i], b = scid[partner];
+        const float4 al = slo[i], ah = shi[i], bl = slo[partner], bh = shi[partner];
+        ol = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
+        oh = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f);
+        child[k] = make_int2(a, b);
+        count[k] = (a >= n - 1 ? 1 : count[a]) + (b >= n - 1 ? 1 : count[b]);
+        nlo[k] = ol;
+        nhi[k] = oh;
+        out_id = k;
+      }
+    }
+    __syncthreads();  // every read of this round's clusters is done
+    if (keep) {
+      scid[pos] = out_id;
+      slo[pos] = ol;
+      shi[pos] = oh;
+    }
+    __syncthreads();
+    node_base += made;
+    nc = kept;
+    force = made == 0 && !force;
+  }
+  if (i == 0) {
+    state[0] = nc;
+    state[1] = node_base;
+    state[2] = made;
+  }
+}
+
 __global__ void k_ploc_parents(int n, const int2* __restrict__ child, int* __restrict__ parent) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n - 1) return;
@@ -242,7 +359,8 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   EOS_CUDA(cudaMemcpyAsync(clo[0], blo + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
   EOS_CUDA(cudaMemcpyAsync(chi[0], bhi + (n - 1), 16 * nn, cudaMemcpyDeviceToDevice, st));
   k_ploc_leaf_ids<<<grid_of(n, 256), 256, 0, st>>>(n, cid[0]);
-  // Rounds run ahead of the host: grids are sized by an upper bound of the cluster count
+  // Rounds run ahead of the host until at most kTail clusters are left (k_ploc_tail does the
+  // rest): grids are sized by an upper bound of the cluster count
   // (the last one read back; it only falls), and the host reads each round's state
   // kAhead rounds later instead of waiting after every round.  A round that merges nothing
   // changes nothing, so the rounds queued behind one repeat it harmlessly; when the host
@@ -297,6 +415,11 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
         nc_ub = std::min(nc_ub, (int)snap[4 * (int)((issued - 1) % kAhead)]);
         if (nc_ub <= 1) break;
       }
+    }
+    if (nc_ub <= kTail) {  // the rest in one block, behind the rounds in flight
+      k_ploc_tail<<<1, kTail, 0, st>>>(state + 4 * cur, cid[cur], clo[cur], chi[cur], tchild, tcount, tlo, thi, n,
+                                       ctx->d_err);
+      break;
     }
     if (issued > 4ll * n + 8) return EOS_ERR_TIMEOUT;  // cannot happen: every round or its forced repeat merges
     ok = enqueue(0);
