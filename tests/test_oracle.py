@@ -232,3 +232,29 @@ def test_instanced_frozen_f64_adjoint_matches_central_differences():
         fd = (Lp - Lm) / (2 * h)
         an = gm[i, gcol] if kind == "m" else gl[i, gcol]
         assert abs(fd - an) <= 1e-3 * max(1.0, abs(fd)), (kind, i, col, fd, an)
+
+
+def test_ploc_restatement_small_cases():
+    """The PLOC restatement on hand-checked inputs: two pairs of unit boxes far apart merge
+    pairwise, then into the root; any input gives a permutation with contiguous subtrees."""
+    from oracle import ploc
+    lo = np.array([[0, 0, 0], [1, 0, 0], [10, 0, 0], [11, 0, 0]], np.float32)
+    child, count, pos = ploc.build(lo, lo + 1)
+    assert child.tolist() == [[3, 4], [5, 6], [0, 1]] and count.tolist() == [2, 2, 4]
+    assert pos.tolist() == [0, 1, 2, 3]
+    child, count, pos = ploc.build(lo[:2], lo[:2] + 1)
+    assert child.tolist() == [[1, 2]] and pos.tolist() == [0, 1]
+    rng = np.random.default_rng(3)
+    c = rng.uniform(-5, 5, (700, 3)).astype(np.float32)
+    child, count, pos = ploc.build(c, c + rng.uniform(0, 1, (700, 3)).astype(np.float32))
+    n = 700
+    assert sorted(pos.tolist()) == list(range(n)) and count[n - 2] == n
+    leaves = {}
+    for k in range(n - 1):  # children are made before their parents
+        s = []
+        for c in child[k]:
+            assert c >= n - 1 or c < k
+            s += [c - (n - 1)] if c >= n - 1 else leaves[c]
+        leaves[k] = s
+        p = np.sort(pos[s])
+        assert p[-1] - p[0] + 1 == len(s) == count[k]  # each subtree a contiguous range
