@@ -2,7 +2,8 @@
 rules (oracle/ploc.py): every triangle's record position -- the tree's depth-first leaf
 order, which the clustering decides merge by merge -- is equal, on scenes that the
 builder finishes in its one-block tail alone (at most 1,024 clusters), after a few
-per-round launches, and after ~40 of them (205k triangles), and on a grid of equal
+per-round launches, and after ~40 of them (205k triangles and the 1.06M-triangle
+benchmark scene), and on a grid of equal
 triangles where merged areas tie exactly.  A PLOC tree too deep for the refit's walk falls
 back to the LBVH."""
 import numpy as np
@@ -76,3 +77,19 @@ def test_too_deep_ploc_tree_falls_back_to_lbvh(ctx, tmp_path):
         d.save(tmp_path / f"{builder}.eos")
         raw.append((tmp_path / f"{builder}.eos").read_bytes())
     assert raw[0][:56] == raw[1][:56] and raw[0][60:] == raw[1][60:]
+
+
+def test_ploc_tree_matches_oracle_at_full_size(ctx, tmp_path):
+    """The 1,056,768-triangle scene of the 1080p benchmark: every triangle's record position
+    equals the restatement's (about 10 s of numpy)."""
+    sc = scenes.config2_scene()
+    d = api.DeviceScene(ctx, sc, builder="ploc")
+    assert d.info()["builder"] == L.BUILDER_PLOC
+    _, order = d.morton()
+    lo, hi = oracle_ploc.leaf_boxes(sc.verts, sc.tris, order)
+    _, count, position = oracle_ploc.build(lo, hi)
+    assert count[-1] == sc.n_tris
+    d.save(tmp_path / "c2.eos")
+    expect = np.empty(sc.n_tris, np.int64)
+    expect[order.astype(np.int64)] = position
+    assert np.array_equal(_pos_of_id(tmp_path / "c2.eos"), expect)
