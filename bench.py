@@ -16,10 +16,12 @@ renders the V views:
 Rays = primary + shadow + secondary (mirror) rays actually traced, from the library's
 counters.  The scene (~135 MB of node / triangle / shading records) is larger than L2.
 
---impl reference: the reference's CPU renderer on the host cores for the same metric.
-The reference's own BVH builder aborts on this scene (heap corruption), so
-the CPU arm times the oracle's C port of the same render path on all host threads, on a
-bounded sample of rows; --impl reference reports it with kind "port".
+--impl reference: the reference's own CPU renderer (compiled from its sources into
+oracle/_ref/libeosref.so) on all host cores for the same metric and view: RayTracer::rayTrace
+per pixel over a band of rows per step, with the tree the reference's builder made for this
+scene (built once, saved as oracle/_ref/config2_tree.npz and restored; the build takes ~10
+minutes on one core).  The cpu_baseline of the GPU line is the same measurement, with the
+oracle's C port beside it.
 
 Multi-GPU (torchrun, N ranks): views are independent, every rank renders its own V views
 (weak scaling, no data-path collective); timing = max over ranks.
@@ -185,7 +187,76 @@ def profile_traffic():
     return {}
 
 
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_renderer(sc):
+    """The reference's own CPU renderer over scene sc with the tree its builder made for it
+    (saved once by oracle/make_ref_tree.py), or None when that tree file is absent."""
+    import oracle
+    from oracle import make_ref_tree
+    if not oracle.ref_available():
+        return None
+    tree = make_ref_tree.load(sc)
+    if tree is None:
+        return None
+    return oracle.RefRenderer(sc, tree=tree)
+
+
+def ref_sample(ref, cam, trace_depth, target_s, nthreads):
+    """A band of rows around the middle of the view sized for about target_s seconds of the
+    reference's RayTracer::rayTrace per pixel on nthreads threads, and its ray count (primary
+    + shadow + secondary, replayed once outside any timing)."""
+    import numpy as np
+    W, H = cam.width, cam.height
+
+    def band(rows):
+        y0 = max(0, H // 2 - rows // 2)
+        return np.arange(y0 * W, min(H, y0 + rows) * W, dtype=np.int32)
+
+    probe = band(8)
+    r = ref.render(cam, trace_depth, pixel_offset=0.5, pixels=probe, nthreads=nthreads, paths=False)
+    rows = int(min(H, max(8, 8 * target_s / max(r["seconds"], 1e-3))))
+    pix = band(rows)
+    counts = ref.render(cam, trace_depth, pixel_offset=0.5, pixels=pix, nthreads=nthreads)["counts"]
+    return pix, int(counts.sum()), rows
+
+
+def ref_timed(ref, cam, trace_depth, pix, nthreads):
+    r = ref.render(cam, trace_depth, pixel_offset=0.5, pixels=pix, nthreads=nthreads, paths=False)
+    return r["seconds"]
+
+
 def cpu_baseline(sc, cam, trace_depth, budget_s=15.0):
+    """The reference's own CPU renderer on all host threads on a bounded band of rows
+    (kind "reference"), with the oracle's C port on a sample of the same view beside it."""
+    nthreads = os.cpu_count()
+    port = port_baseline(sc, cam, trace_depth, budget_s=min(budget_s, 6.0))
+    ref = ref_renderer(sc)
+    if ref is None:
+        port["note"] = "reference tree file absent (oracle/make_ref_tree.py): the port is reported"
+        return port
+    pix, rays, rows = ref_sample(ref, cam, trace_depth, budget_s / 3.0, nthreads)
+    secs = [ref_timed(ref, cam, trace_depth, pix, nthreads) for _ in range(3)]
+    sec = statistics.median(secs)
+    return {"value": rays / sec / 1e6, "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
+            "cpu": cpu_model(),
+            "sample": f"rows {rows} x {cam.width} px around the middle of the 1080p view through the reference's "
+                      f"RayTracer::rayTrace (oracle/_ref/libeosref.so, its own tree), {nthreads} threads, "
+                      f"median of 3",
+            "rays": rays, "seconds": sec,
+            "port": {"value": round(port["value"], 3), "unit": "Mrays/s", "cores": port["cores"],
+                     "sample": port["sample"]}}
+
+
+def port_baseline(sc, cam, trace_depth, budget_s=15.0):
     """The oracle's C port of the render path on all host threads, on a bounded sample of rows."""
     import numpy as np
     import oracle
@@ -209,26 +280,45 @@ def cpu_baseline(sc, cam, trace_depth, budget_s=15.0):
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU renderer on the host cores for the same metric and view: one
+    step = a band of rows of the 1080p view (about 3 s of work) through RayTracer::rayTrace,
+    all host threads; the tree is the one the reference's builder made for this scene,
+    restored from oracle/_ref/config2_tree.npz (the build itself takes ~10 min on one core)."""
     if rank != 0:
         return
     from eos_b200 import scenes
     sc = scenes.config2_scene()
     cam = scenes.config2_camera()
-    res = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_baseline(sc, cam, 2, budget_s=4.0)
-        if i >= args.warmup:
-            res.append(info["value"])
-    v = statistics.median(res)
+    nthreads = os.cpu_count()
+    ref = ref_renderer(sc)
+    workload = ("1920x1080 view of the 1,056,768-tri scene (height field 128^2 + 200 level-4 icospheres), "
+                "depth 3, 4 lights, 1 spp at pixel centres")
+    if ref is not None:
+        pix, rays, rows = ref_sample(ref, cam, 2, 3.0, nthreads)
+        secs = []
+        for i in range(args.warmup + args.steps):
+            sec = ref_timed(ref, cam, 2, pix, nthreads)
+            if i >= args.warmup:
+                secs.append(sec)
+        v = rays * len(secs) / sum(secs) / 1e6
+        cpu = {"value": v, "unit": "Mrays/s", "cores": nthreads, "kind": "reference", "cpu": cpu_model(),
+               "sample": f"per step rows {rows} x {cam.width} px around the middle of the view through the "
+                         f"reference's RayTracer::rayTrace (oracle/_ref/libeosref.so, its own tree)"}
+    else:
+        res, info = [], None
+        for i in range(args.warmup + args.steps):
+            info = port_baseline(sc, cam, 2, budget_s=4.0)
+            if i >= args.warmup:
+                res.append(info["value"])
+        v = statistics.median(res)
+        cpu = {"value": v, "unit": "Mrays/s", "cores": info["cores"], "kind": "port", "cpu": cpu_model(),
+               "sample": info["sample"] + " per step; the reference's tree file oracle/_ref/config2_tree.npz "
+                                          "is absent"}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-            "config": {"workload": "1920x1080 view, 1,056,768 tris (height field 128^2 + 200 ico4), depth 3, "
-                                   "4 lights, 1 spp", "mode": "CPU"},
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": info["cores"], "kind": "port",
-                             "sample": info["sample"] + " per step; the reference's own BVH builder aborts "
-                                       "(heap corruption) on this 1M-triangle scene"},
+            "config": {"workload": workload, "mode": "CPU"},
+            "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -325,9 +415,6 @@ def run_ours(args, rank, world, local):
             rays = float(r)
         return ms, rays, launches
 
-    def step_refill():
-        return api.render_batch(ctx, jobs, outs, refill=True)
-
     b0 = None
     if args.profile:
         # bounce 0 of view 0 alone, before anything else: the launches that an ncu capture with
@@ -338,13 +425,10 @@ def run_ours(args, rank, world, local):
     clk = ClockSampler(dev).__enter__()
     for _ in range(args.warmup):
         step_batched()
-        step_refill()
         step_plain()
     ms_b, rays_b, launches_b = timed(step_batched, args.steps)
-    ms_c, rays_c, _ = timed(step_refill, args.steps)
     ms_p, rays_p, launches_p = timed(step_plain, args.steps)
     mrays_b = rays_b / (ms_b * 1e-3) / 1e6
-    mrays_c = rays_c / (ms_c * 1e-3) / 1e6
     mrays_p = rays_p / (ms_p * 1e-3) / 1e6
     if args.profile:
         clk.__exit__(None, None, None)
@@ -454,8 +538,6 @@ def run_ours(args, rank, world, local):
                    "tuning": "eos_b200/tuning_b200.json" if tuned else "defaults"},
         "plain": {"value": round(mrays_p, 2), "unit": "Mrays/s", "ms_per_step": round(ms_p / args.steps, 3)},
         "batched_over_plain": round(mrays_b / mrays_p, 3),
-        "batched_refill": {"value": round(mrays_c, 2), "unit": "Mrays/s",
-                           "note": "same batch, persistent kernels with lane refill (EOS_FLAG_REFILL)"},
         "rays_per_step": {"total": rays_b / args.steps / world},
         # the headline split by ray type: this rank's per-step counts at the whole-job step time
         "mrays_by_type": {k: round(st[k + "_rays"] * world / (ms_b / args.steps * 1e-3) / 1e6, 2)

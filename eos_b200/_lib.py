@@ -53,8 +53,6 @@ class RenderParams(Structure):
 
 
 FLAG_STAGE_TIMING = 1
-FLAG_REFILL = 2
-FLAG_PACKET = 4
 
 
 class Tuning(Structure):
@@ -102,6 +100,10 @@ class Instance(Structure):
     _fields_ = [("mesh", c_void_p), ("transform", c_float * 12), ("material_base", c_uint32)]
 
 
+class Limits(Structure):
+    _fields_ = [("queue_entries", c_int32), ("work_budget", c_int32), ("small_stack", c_int32)]
+
+
 class Grads(Structure):
     _fields_ = [("materials", c_void_p), ("lights", c_void_p)]
 
@@ -117,6 +119,7 @@ SIGNATURES = [
     ("eos_ctx_synchronize", c_int32, [c_void_p]),
     ("eos_ctx_set_tuning", c_int32, [c_void_p, c_uint32, POINTER(Tuning)]),
     ("eos_ctx_clear_tuning", c_int32, [c_void_p]),
+    ("eos_ctx_set_limits", c_int32, [c_void_p, POINTER(Limits)]),
     ("eos_scene_create", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_uint32,
                                    c_void_p, c_uint32, c_void_p, c_uint32, POINTER(BuildParams), POINTER(c_void_p)]),
     ("eos_scene_destroy", c_int32, [c_void_p]),

@@ -38,8 +38,7 @@ def camera_struct(cam: CameraData) -> L.Camera:
 
 
 def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="plain", block_size=0,
-                  queue_chunk=0, stack_depth=0, stage_timing=False, refill=False, packet=False,
-                  rows=None) -> L.RenderParams:
+                  queue_chunk=0, stack_depth=0, stage_timing=False, rows=None) -> L.RenderParams:
     p = L.RenderParams()
     p.trace_depth = int(trace_depth)
     p.pixel_offset = float(pixel_offset)
@@ -49,8 +48,7 @@ def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="p
     p.block_size = int(block_size)
     p.queue_chunk = int(queue_chunk)
     p.stack_depth = int(stack_depth)
-    p.flags = ((L.FLAG_STAGE_TIMING if stage_timing else 0) | (L.FLAG_REFILL if refill else 0)
-               | (L.FLAG_PACKET if packet else 0))
+    p.flags = L.FLAG_STAGE_TIMING if stage_timing else 0
     if rows is not None:
         p.row_begin, p.row_end = int(rows[0]), int(rows[1])
     return p
@@ -92,6 +90,11 @@ class Context:
 
     def synchronize(self):
         L.check(self.lib.eos_ctx_synchronize(self.h), "eos_ctx_synchronize")
+
+    def set_limits(self, queue_entries: int = 0, work_budget: int = 0, small_stack: bool = False):
+        """Test limits of the wavefront kernels (eos_ctx_set_limits); no arguments clears them."""
+        lim = L.Limits(int(queue_entries), int(work_budget), 1 if small_stack else 0)
+        L.check(self.lib.eos_ctx_set_limits(self.h, byref(lim)), "eos_ctx_set_limits")
 
 
 def materials_array(mats):

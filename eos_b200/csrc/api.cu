@@ -109,15 +109,6 @@ eos_status begin_call(eos_ctx* ctx) {
   return EOS_OK;
 }
 
-eos_status err_to_status(int e) {
-  if (e & kErrStack) return EOS_ERR_STACK_OVERFLOW;
-  if (e & kErrQueue) return EOS_ERR_QUEUE_OVERFLOW;
-  if (e & kErrIndex) return EOS_ERR_INVALID_ARG;
-  if (e & kErrTimeout) return EOS_ERR_TIMEOUT;
-  if (e & kErrDepth) return EOS_ERR_STACK_OVERFLOW;
-  return EOS_OK;
-}
-
 // Waits for the call, reads the error word (and counters into stats).
 eos_status end_call(eos_ctx* ctx, eos_stats* stats) {
   struct {
@@ -152,6 +143,7 @@ eos_status check_params(const eos_render_params* p) {
   if (p->trace_depth < 0 || p->trace_depth >= EOS_MAX_BOUNCES) return EOS_ERR_INVALID_ARG;
   if (p->spp < 1 || p->spp > 1024) return EOS_ERR_INVALID_ARG;
   if (p->mode != EOS_MODE_PLAIN && p->mode != EOS_MODE_WAVEFRONT) return EOS_ERR_INVALID_ARG;
+  if (p->flags & ~EOS_FLAG_STAGE_TIMING) return EOS_ERR_INVALID_ARG;
   return EOS_OK;
 }
 
@@ -172,8 +164,10 @@ eos_tuning tuned_for(const eos_ctx* ctx, uint32_t n) {
   return t;
 }
 
+}  // namespace
+
 // Parameters left at 0 take the tuned value.
-eos_render_params with_tuning(const eos_ctx* ctx, const eos_render_params& p, uint32_t n_tris) {
+eos_render_params eos::with_tuning(const eos_ctx* ctx, const eos_render_params& p, uint32_t n_tris) {
   eos_render_params q = p;
   eos_tuning t = tuned_for(ctx, n_tris);
   if (q.block_size <= 0) q.block_size = t.block_size;
@@ -181,8 +175,6 @@ eos_render_params with_tuning(const eos_ctx* ctx, const eos_render_params& p, ui
   if (q.stack_depth <= 0) q.stack_depth = t.stack_depth;
   return q;
 }
-
-}  // namespace
 
 extern "C" {
 
@@ -282,6 +274,13 @@ eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning*
 eos_status eos_ctx_clear_tuning(eos_ctx* ctx) {
   if (!ctx) return EOS_ERR_INVALID_ARG;
   ctx->tuning.clear();
+  return EOS_OK;
+}
+
+eos_status eos_ctx_set_limits(eos_ctx* ctx, const eos_limits* lim) {
+  if (!ctx) return EOS_ERR_INVALID_ARG;
+  if (lim && (lim->queue_entries < 0 || lim->work_budget < 0)) return EOS_ERR_INVALID_ARG;
+  ctx->limits = lim ? *lim : eos_limits{0, 0, 0};
   return EOS_OK;
 }
 

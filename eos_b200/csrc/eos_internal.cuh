@@ -31,6 +31,15 @@ enum : int {
   kErrDepth = 1 << 4,
 };
 
+// Status of a call from its device error word; every entry point maps it the same way.
+inline eos_status err_to_status(int e) {
+  if (e & (kErrStack | kErrDepth)) return EOS_ERR_STACK_OVERFLOW;
+  if (e & kErrQueue) return EOS_ERR_QUEUE_OVERFLOW;
+  if (e & kErrIndex) return EOS_ERR_INVALID_ARG;
+  if (e & kErrTimeout) return EOS_ERR_TIMEOUT;
+  return EOS_OK;
+}
+
 // ---------------------------------------------------------------------------------
 // HBM layout of a scene (all 16-byte aligned, read with 128-bit loads):
 //
@@ -102,6 +111,8 @@ struct eos_ctx {
   cudaEvent_t ring_ev[4] = {};
   // autotuner table: min triangle count -> tuned parameters
   std::map<uint32_t, eos_tuning> tuning;
+  // test limits of the wavefront kernels (eos_ctx_set_limits); zeros = none
+  eos_limits limits{0, 0, 0};
   // per-call bookkeeping reported in eos_stats
   uint32_t launches = 0;
   float stage_ms[3] = {0, 0, 0};
@@ -159,6 +170,9 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
 // Morton position p, *depth = tree depth (above 4 * kStackMax nothing is written).
 eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi, int2* child, int2* range,
                       int* parent, uint32_t* perm, int* depth);
+
+// Parameters left at 0 take the context's tuned values for a scene of n_tris triangles.
+eos_render_params with_tuning(const eos_ctx* ctx, const eos_render_params& p, uint32_t n_tris);
 
 // Renderers (render.cu).
 struct RenderArgs {

@@ -183,18 +183,20 @@ __device__ __forceinline__ int leaf_count(int r) { return ((r >> 25) & 31) + 1; 
 
 // Per-thread traversal stack of (child ref, entry distance): the first SH entries live in
 // shared memory (column threadIdx.x of a [SH][blockDim] array), deeper entries spill to
-// local memory, kStackMax in total.
-template <int SH>
+// local memory, CAP in total (kStackMax; CAP = SH, no spill, is the small stack of the
+// error-path test limit, eos_limits.small_stack).
+template <int SH, int CAP = kStackMax>
 struct TraversalStack {
+  static_assert(CAP >= SH, "the shared part is the bottom of the stack");
   uint2* sh;
   int stride;
   int sp;
-  uint2 spill[kStackMax - SH];
+  uint2 spill[CAP > SH ? CAP - SH : 1];
   __device__ __forceinline__ TraversalStack(uint2* base, int str) : sh(base), stride(str), sp(0) {}
   __device__ __forceinline__ bool push(int ref, float t) {
     uint2 v = make_uint2((uint32_t)ref, __float_as_uint(t));
     if (sp < SH) sh[sp * stride] = v;
-    else if (sp < kStackMax) spill[sp - SH] = v;
+    else if (sp < CAP) spill[sp - SH] = v;
     else return false;
     ++sp;
     return true;
@@ -241,9 +243,9 @@ __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p,
 // shared-memory stack entries (the most one node pushes) the pushes skip their bound
 // checks.  Returns false on stack overflow.
 
-template <int SH, bool SORT, class Ray>
+template <int SH, bool SORT, class Ray, int CAP>
 __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const Ray& r, int& cur,
-                                            float limit, TraversalStack<SH>& st, unsigned& nodes) {
+                                            float limit, TraversalStack<SH, CAP>& st, unsigned& nodes) {
   const float4* nd = node_base + 8 * (size_t)cur;
   const float4 lx = __ldg(nd + r.sx), ly = __ldg(nd + 1 + r.sy), lz = __ldg(nd + 2 + r.sz);  // near planes
   const float4 hx = __ldg(nd + 3 - r.sx), hy = __ldg(nd + 4 - r.sy), hz = __ldg(nd + 5 - r.sz);  // far planes
@@ -309,13 +311,13 @@ __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base
 // efficiency of ray traversal on GPUs", HPG 2009): a lane that reaches a leaf parks it and
 // keeps descending until every lane of the warp holds a leaf, then the lanes intersect
 // their leaves together, so triangle tests run with full warps.
-template <int SH, class Ray>
+template <int SH, int CAP, class Ray>
 __device__ __forceinline__ Hit closest_traverse(const DevScene& s, f3 o, f3 d, const Ray& r, uint2* shs, int stride,
                                                int* err) {
   constexpr float kCullR = RayCull<Ray>::k;
   Hit h;
   h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
-  TraversalStack<SH> st(shs, stride);
+  TraversalStack<SH, CAP> st(shs, stride);
   int cur = 0;   // interior node, leaf ref or kDone
   int leaf = 0;  // parked leaf (0 = none)
   for (;;) {
@@ -352,19 +354,19 @@ __device__ __forceinline__ Hit closest_traverse(const DevScene& s, f3 o, f3 d, c
   }
 }
 
-template <int SH>
+template <int SH, int CAP = kStackMax>
 __device__ __forceinline__ Hit closest_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
   const SlabRay r = make_slab(o, d);
-  if (fma_slab_ok(r)) return closest_traverse<SH>(s, o, d, make_fma_slab(r), shs, stride, err);
-  return closest_traverse<SH>(s, o, d, r, shs, stride, err);
+  if (fma_slab_ok(r)) return closest_traverse<SH, CAP>(s, o, d, make_fma_slab(r), shs, stride, err);
+  return closest_traverse<SH, CAP>(s, o, d, r, shs, stride, err);
 }
 
 // Any hit at t >= 0 (shadow rays), same two-loop form; returns at the first hit.
-template <int SH, class Ray>
+template <int SH, int CAP, class Ray>
 __device__ __forceinline__ AnyResult any_traverse(const DevScene& s, f3 o, f3 d, const Ray& r, uint2* shs,
                                                   int stride, int* err) {
   AnyResult res{0, 0u, 0u};
-  TraversalStack<SH> st(shs, stride);
+  TraversalStack<SH, CAP> st(shs, stride);
   int cur = 0;
   int leaf = 0;
   for (;;) {
@@ -402,116 +404,11 @@ __device__ __forceinline__ AnyResult any_traverse(const DevScene& s, f3 o, f3 d,
   }
 }
 
-template <int SH>
+template <int SH, int CAP = kStackMax>
 __device__ __forceinline__ AnyResult any_hit_body(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
   const SlabRay r = make_slab(o, d);
-  if (fma_slab_ok(r)) return any_traverse<SH>(s, o, d, make_fma_slab(r), shs, stride, err);
-  return any_traverse<SH>(s, o, d, r, shs, stride, err);
-}
-
-// ------------------------------------------------------------------ resumable traversal
-// Per-lane traversal state for persistent kernels that refill lanes: a lane whose ray
-// ends takes the next ray from the queue while the other lanes of its warp continue, so
-// no lane idles until the slowest ray of its group ends.  One step = one round of the
-// two-loop traversal above (descend until the warp holds leaves, then intersect them).
-struct TravScene {
-  const float4* nodes;
-  const float4* tris;
-};
-
-template <int SH>
-struct RayTraversal {
-  SlabRay r;
-  f3 o, d;
-  TraversalStack<SH> st;
-  int cur, leaf;
-  __device__ __forceinline__ RayTraversal(uint2* base, int stride) : st(base, stride), cur(kDone), leaf(0) {}
-  __device__ __forceinline__ void start(f3 o_, f3 d_) {
-    o = o_;
-    d = d_;
-    r = make_slab(o_, d_);
-    st.sp = 0;
-    cur = 0;
-    leaf = 0;
-  }
-  __device__ __forceinline__ bool done() const { return cur == kDone && leaf == 0; }
-  __device__ __forceinline__ void finish() {
-    cur = kDone;
-    leaf = 0;
-  }
-};
-
-// One step of a nearest-hit traversal; h accumulates across steps.
-template <int SH>
-__device__ __forceinline__ void closest_step(const TravScene& s, RayTraversal<SH>& T, Hit& h, int* err) {
-  while (T.cur >= 0) {
-    if (!visit_node4<SH, true>(s.nodes, T.r, T.cur, h.t * kCull, T.st, h.nodes)) {
-      atomicOr(err, kErrStack);
-      T.finish();
-      return;
-    }
-    if (T.cur != kDone && T.cur < 0 && T.leaf == 0) {
-      T.leaf = T.cur;
-      T.cur = T.st.next(h.t * kCull);
-    }
-    if (!__any_sync(__activemask(), T.leaf == 0)) break;
-  }
-  while (T.leaf != 0) {
-    const int first = leaf_first(T.leaf), cnt = leaf_count(T.leaf);
-    h.tests += cnt;
-    for (int p = first; p < first + cnt; ++p) {
-      f3 v1, e1, e2;
-      int id;
-      load_tri(s.tris, p, v1, e1, e2, id);
-      float t, u, v;
-      if (mt_intersect_fast(T.o, T.d, v1, e1, e2, t, u, v) && (t < h.t || (t == h.t && id > h.id))) {
-        h.t = t; h.u = u; h.v = v; h.pos = p; h.id = id;
-      }
-    }
-    T.leaf = 0;
-    if (T.cur != kDone && T.cur < 0) {
-      T.leaf = T.cur;
-      T.cur = T.st.next(h.t * kCull);
-    }
-  }
-}
-
-// One step of a shadow-ray traversal; returns true when the ray is blocked (it ends).
-template <int SH>
-__device__ __forceinline__ bool any_step(const TravScene& s, RayTraversal<SH>& T, unsigned& nodes, unsigned& tests,
-                                         int* err) {
-  while (T.cur >= 0) {
-    if (!visit_node4<SH, false>(s.nodes, T.r, T.cur, kInf, T.st, nodes)) {
-      atomicOr(err, kErrStack);
-      T.finish();
-      return false;
-    }
-    if (T.cur != kDone && T.cur < 0 && T.leaf == 0) {
-      T.leaf = T.cur;
-      T.cur = T.st.next_any();
-    }
-    if (!__any_sync(__activemask(), T.leaf == 0)) break;
-  }
-  while (T.leaf != 0) {
-    const int first = leaf_first(T.leaf), cnt = leaf_count(T.leaf);
-    for (int p = first; p < first + cnt; ++p) {
-      f3 v1, e1, e2;
-      int id;
-      load_tri(s.tris, p, v1, e1, e2, id);
-      float t, u, v;
-      ++tests;
-      if (mt_intersect_fast(T.o, T.d, v1, e1, e2, t, u, v)) {
-        T.finish();
-        return true;
-      }
-    }
-    T.leaf = 0;
-    if (T.cur != kDone && T.cur < 0) {
-      T.leaf = T.cur;
-      T.cur = T.st.next_any();
-    }
-  }
-  return false;
+  if (fma_slab_ok(r)) return any_traverse<SH, CAP>(s, o, d, make_fma_slab(r), shs, stride, err);
+  return any_traverse<SH, CAP>(s, o, d, r, shs, stride, err);
 }
 
 // Out-of-line copies for the plain megakernel, which calls both traversals: keeping them
@@ -620,20 +517,21 @@ __device__ __forceinline__ const DevInstance* instance_of(const DevScene& s, int
   return s.inst + lo;
 }
 
-template <int SH, bool INLINE = false>
+// CAP (inline traversals of flat scenes only): total stack entries, see TraversalStack.
+template <int SH, bool INLINE = false, int CAP = kStackMax>
 __device__ __forceinline__ Hit closest_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
   if (s.inst) return traverse_instanced<SH, false>(s, o, d, shs, stride, err);
-  if (INLINE) return closest_hit_body<SH>(s, o, d, shs, stride, err);
+  if (INLINE) return closest_hit_body<SH, CAP>(s, o, d, shs, stride, err);
   return closest_hit_call<SH>(s, o, d, shs, stride, err);
 }
 
-template <int SH, bool INLINE = false>
+template <int SH, bool INLINE = false, int CAP = kStackMax>
 __device__ __forceinline__ AnyResult any_hit(const DevScene& s, f3 o, f3 d, uint2* shs, int stride, int* err) {
   if (s.inst) {
     const Hit h = traverse_instanced<SH, true>(s, o, d, shs, stride, err);
     return AnyResult{h.pos >= 0 ? 1 : 0, h.nodes, h.tests};
   }
-  if (INLINE) return any_hit_body<SH>(s, o, d, shs, stride, err);
+  if (INLINE) return any_hit_body<SH, CAP>(s, o, d, shs, stride, err);
   return any_hit_call<SH>(s, o, d, shs, stride, err);
 }
 

@@ -82,6 +82,7 @@ struct WfArgs {
   int* ctr;      // [depth+1][kCtr]
   int cap_r, cap_s;
   int qchunk;
+  int work_limit;  // queue entries a persistent launch traces (test limit; INT_MAX = all)
   int* err;
   unsigned long long* counts;
 };
@@ -121,15 +122,28 @@ __device__ __forceinline__ int grab(int* ctr, int qchunk) {
   return __shfl_sync(0xffffffffu, s, 0);
 }
 
+// Work budget of a persistent launch (eos_limits.work_budget): its loop over the queue
+// stops after work_limit entries and raises the timeout bit when entries are left.  The
+// entries beyond stay untraced and the shading stage reads no further than the budget
+// either: their path records keep EOS_HIT_UNTRACED and no stale queue entry is read.
+__device__ __forceinline__ int budget(int n, int work_limit, int* err) {
+  if (n <= work_limit) return n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, kErrTimeout);
+  return work_limit;
+}
+
 // The wavefront traversal kernels are capped at 64 registers (blocks up to 256, 4 per SM):
-// measured faster than no cap (77 registers) and than caps of 56 or 48 (spills).
-template <bool PRIMARY, int SH>
+// measured faster than no cap (77 registers) and than caps of 56 or 48 (spills).  CAP is
+// the traversal stack's size (TraversalStack): kStackMax, or SH for the small-stack test
+// limit.
+template <bool PRIMARY, int SH, int CAP = kStackMax>
 __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;
   int* ctr = A.ctr + A.k * kCtr;
-  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // secondary rays of bounce k-1
+  // primary rays of the chunk, or the secondary rays of bounce k-1
+  const int n_in = budget(PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r), A.work_limit, A.err);
   const int lane = threadIdx.x & 31;
   unsigned nrays = 0, nshadow = 0, nhits = 0;
   unsigned long long nodes = 0, tests = 0;
@@ -169,7 +183,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
       const DevJob& J = A.jobs[jb];
       if (valid) {
         ++nrays;
-        Hit h = closest_hit<SH, true>(J.s, o, d, shs, stride, A.err);
+        Hit h = closest_hit<SH, true, CAP>(J.s, o, d, shs, stride, A.err);
         nodes += h.nodes;
         tests += h.tests;
         hit = h.pos >= 0;
@@ -248,254 +262,25 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
   warp_add_count(&A.counts[kCntTestsC], tests);
 }
 
-// Emits the results of lanes whose nearest-hit ray has ended (`pending`): path record, hit
-// record, one shadow ray per light (compacted light-major inside the warp's block of the
-// queue, so a warp of the any-hit kernel mostly traces towards one light) and the
-// secondary ray (ballot / popc compaction, one atomic per warp).  Warp-uniform: every lane calls it.
-__device__ __forceinline__ void emit_results(const WfArgs& A, int* ctr, bool pending, int i, int path, int jb,
-                                             const Hit& h, f3 o, f3 d, unsigned& nshadow, unsigned& nhits) {
-  const int lane = threadIdx.x & 31;
-  const DevJob& J = A.jobs[jb];
-  bool hit = pending && h.pos >= 0;
-  bool refl = false;
-  f3 P = mk3(0, 0, 0), N = P, ro = P, rd = P;
-  int obj = -1;
-  if (pending) {
-    nhits += hit;
-    if (J.paths) {
-      int x, y, smp;
-      path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
-      J.paths[((size_t)y * J.w + x) * J.spp + smp].hit[A.k] = hit ? h.id : EOS_HIT_NONE;
-    }
-    if (hit) {
-      hit_geometry(J.s, o, d, h, P, N, obj);
-      float w;
-      refl = secondary_ray(J.s.mats + kMatStride * obj, J.s.ambient_index, d, P, N, ro, rd, w);
-      reinterpret_cast<float*>(A.acc + (size_t)path * (A.depth + 1) + A.k)[3] = w;
-      refl = refl && A.k < J.trace_depth;
-    }
-    HitQ hq;
-    hq.a = make_float4(P.x, P.y, P.z, __int_as_float(path));
-    hq.b = make_float4(N.x, N.y, N.z, __int_as_float(hit ? obj : -1));
-    A.hits[i] = hq;
-    A.masks[i] = 0u;
-  }
-  int nl = hit ? J.s.n_lights : 0;
-  int maxl = nl;
-  for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(0xffffffffu, maxl, off));
-  if (maxl > 0) {
-    int total = nl;
-    for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
-    int wbase = 0;
-    if (lane == 0) wbase = atomicAdd(&ctr[2], total);
-    wbase = __shfl_sync(0xffffffffu, wbase, 0);
-    bool fits = wbase + total <= A.cap_s;
-    if (!fits && lane == 0) atomicOr(A.err, kErrQueue);
-    int prefix = 0;
-    for (int l = 0; l < maxl; ++l) {
-      uint32_t bl = __ballot_sync(0xffffffffu, l < nl);
-      if (l < nl && fits) {
-        const float* lp = J.s.lights + 6 * l;
-        f3 sd = norm3(sub3(mk3(lp[0], lp[1], lp[2]), P));
-        f3 so = add3(P, scale3(kRayEps, sd));
-        ShadowQ s;
-        s.a = make_float4(so.x, so.y, so.z, __int_as_float(i));
-        s.b = make_float4(sd.x, sd.y, sd.z, __int_as_float((jb << 5) | l));
-        A.sq[wbase + prefix + __popc(bl & lanemask_lt())] = s;
-      }
-      prefix += __popc(bl);
-    }
-    nshadow += nl;
-  }
-  uint32_t rb = __ballot_sync(0xffffffffu, refl);
-  if (rb) {
-    int rbase = 0;
-    if (lane == 0) rbase = atomicAdd(&ctr[1], __popc(rb));
-    rbase = __shfl_sync(0xffffffffu, rbase, 0);
-    if (refl) {
-      int pos = rbase + __popc(rb & lanemask_lt());
-      if (pos >= A.cap_r) {
-        atomicOr(A.err, kErrQueue);
-      } else {
-        RayQ r;
-        r.a = make_float4(ro.x, ro.y, ro.z, __int_as_float(path));
-        r.b = make_float4(rd.x, rd.y, rd.z, 0.0f);
-        A.rout[pos] = r;
-      }
-    }
-  }
-}
-
-// Warp-level pool of queue entries for the refill kernels: when the pool is empty, lane 0
-// takes the next `chunk` entries with one atomic.  Returns true when the pool holds
-// entries.  pool, pool_end and more stay warp-uniform.
-__device__ __forceinline__ bool refill_pool(int* counter, int chunk, int n, int lane, int& pool, int& pool_end,
-                                            bool& more) {
-  if (pool >= pool_end && more) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(counter, chunk);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    pool = base;
-    pool_end = min(base + chunk, n);
-    if (pool_end >= n) more = false;
-  }
-  return pool < pool_end;
-}
-
-// Nearest-hit stage with lane refill: each iteration (1) emits the results of lanes whose
-// ray ended, (2) gives idle lanes new rays from the warp's pool of queue entries (refilled
-// `queue_chunk` entries at a time), (3) advances every active lane by one traversal step.
-template <bool PRIMARY, int SH>
-__global__ void k_wf_closest_refill(WfArgs A) {
-  extern __shared__ uint2 shstack[];
-  int* ctr = A.ctr + A.k * kCtr;
-  const int n_in = PRIMARY ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);  // secondary rays of bounce k-1
-  const int lane = threadIdx.x & 31;
-  RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
-  TravScene ts{nullptr, nullptr};
-  Hit h;
-  h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
-  int i = -1, path = -1, jb = 0;
-  bool pending = false;
-  bool more = true;              // warp-uniform: the queue may still have rays
-  int pool = 0, pool_end = 0;    // warp-uniform: queue entries taken by this warp, not yet started
-  unsigned nrays = 0, nshadow = 0, nhits = 0;
-  unsigned long long nodes = 0, tests = 0;
-  for (;;) {
-    if (__any_sync(0xffffffffu, pending)) {
-      emit_results(A, ctr, pending, i, path, jb, h, T.o, T.d, nshadow, nhits);
-      if (pending) {
-        nodes += h.nodes;
-        tests += h.tests;
-        pending = false;
-        i = -1;
-      }
-    }
-    const uint32_t idle = __ballot_sync(0xffffffffu, i < 0);
-    if (idle && refill_pool(&ctr[3], A.qchunk, n_in, lane, pool, pool_end, more)) {
-      const int rank = __popc(idle & lanemask_lt());
-      const int avail = pool_end - pool;
-      const int k = pool + rank;
-      pool += min(__popc(idle), avail);
-      if (i < 0 && rank < avail) {
-        f3 o, d;
-        bool ok = true;
-        if (PRIMARY) {
-          long long gp = A.c0 + k;
-          jb = find_job(A.jobs, A.n_jobs, gp);
-          const DevJob& J = A.jobs[jb];
-          int x, y, smp;
-          ok = path_pixel(J, gp - J.path_off, x, y, smp);
-          if (ok) {
-            float ox, oy;
-            sample_offset((uint32_t)((J.y0 + y) * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
-            d = primary_direction(J.cam, J.w, J.h, x, J.y0 + y, ox, oy);
-            o = mk3(J.cam[0], J.cam[1], J.cam[2]);
-            path = k;
-          }
-        } else {
-          RayQ r = A.rin[k];
-          o = mk3(r.a.x, r.a.y, r.a.z);
-          d = mk3(r.b.x, r.b.y, r.b.z);
-          path = __float_as_int(r.a.w);
-          jb = find_job(A.jobs, A.n_jobs, A.c0 + path);
-        }
-        if (ok) {
-          i = k;
-          ++nrays;
-          ts.nodes = A.jobs[jb].s.nodes;
-          ts.tris = A.jobs[jb].s.tris;
-          T.start(o, d);
-          h.t = kInf; h.u = h.v = 0.0f; h.pos = -1; h.id = -1; h.nodes = 0; h.tests = 0;
-        }
-      }
-    }
-    if (__ballot_sync(0xffffffffu, i >= 0) == 0) {
-      if (!more && pool >= pool_end) break;
-      continue;
-    }
-    if (i >= 0) {
-      closest_step<SH>(ts, T, h, A.err);
-      if (T.done()) pending = true;
-    }
-  }
-  warp_add_count(&A.counts[A.k == 0 ? kCntPrimary : kCntSecondary], nrays);
-  warp_add_count(&A.counts[kCntShadow], nshadow);
-  warp_add_count(&A.counts[kCntHits], nhits);
-  warp_add_count(&A.counts[kCntNodesC], nodes);
-  warp_add_count(&A.counts[kCntTestsC], tests);
-}
-
-// Shadow stage with lane refill (see k_wf_closest_refill).
-template <int SH>
-__global__ void k_wf_any_refill(WfArgs A) {
-  extern __shared__ uint2 shstack[];
-  int* ctr = A.ctr + A.k * kCtr;
-  const int n = min(ctr[2], A.cap_s);
-  const int lane = threadIdx.x & 31;
-  RayTraversal<SH> T(shstack + threadIdx.x, blockDim.x);
-  TravScene ts{nullptr, nullptr};
-  int i = -1, hi = 0, key = 0;
-  bool more = true;
-  int pool = 0, pool_end = 0;
-  unsigned nn = 0, nt = 0;
-  unsigned long long nodes = 0, tests = 0;
-  for (;;) {
-    const uint32_t idle = __ballot_sync(0xffffffffu, i < 0);
-    if (idle && refill_pool(&ctr[4], A.qchunk, n, lane, pool, pool_end, more)) {
-      const int rank = __popc(idle & lanemask_lt());
-      const int avail = pool_end - pool;
-      const int k = pool + rank;
-      pool += min(__popc(idle), avail);
-      if (i < 0 && rank < avail) {
-        ShadowQ s = A.sq[k];
-        i = k;
-        hi = __float_as_int(s.a.w);
-        key = __float_as_int(s.b.w);
-        const DevScene& S = A.jobs[key >> 5].s;
-        ts.nodes = S.nodes;
-        ts.tris = S.tris;
-        T.start(mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z));
-      }
-    }
-    if (__ballot_sync(0xffffffffu, i >= 0) == 0) {
-      if (!more && pool >= pool_end) break;
-      continue;
-    }
-    if (i >= 0) {
-      if (any_step<SH>(ts, T, nn, nt, A.err)) {
-        atomicOr(&A.masks[hi], 1u << (key & 31));
-        i = -1;
-      } else if (T.done()) {
-        i = -1;
-      }
-    }
-  }
-  nodes += nn;
-  tests += nt;
-  warp_add_count(&A.counts[kCntNodesA], nodes);
-  warp_add_count(&A.counts[kCntTestsA], tests);
-}
-
-template <int SH>
+template <int SH, int CAP = kStackMax>
 __global__ void __launch_bounds__(256, 4) k_wf_any(WfArgs A) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
   const int stride = blockDim.x;
   int* ctr = A.ctr + A.k * kCtr;
-  const int n = min(ctr[2], A.cap_s);
-  const int lane = threadIdx.x & 31;
+  const int n = budget(min(ctr[2], A.cap_s), A.work_limit, A.err);
   unsigned long long nodes = 0, tests = 0;
   for (;;) {
     int start = grab(&ctr[4], A.qchunk);
     if (start >= n) break;
     int end = min(start + A.qchunk, n);
-    for (int i = start + lane; i < end; i += 32) {
+    for (int i = start + (threadIdx.x & 31); i < end; i += 32) {
       ShadowQ s = A.sq[i];
       int hi = __float_as_int(s.a.w);
       int key = __float_as_int(s.b.w);
       const DevJob& J = A.jobs[key >> 5];
-      AnyResult ar = any_hit<SH, true>(J.s, mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z), shs, stride, A.err);
+      AnyResult ar =
+          any_hit<SH, true, CAP>(J.s, mk3(s.a.x, s.a.y, s.a.z), mk3(s.b.x, s.b.y, s.b.z), shs, stride, A.err);
       nodes += ar.nodes;
       tests += ar.tests;
       if (ar.hit) atomicOr(&A.masks[hi], 1u << (key & 31));
@@ -505,148 +290,10 @@ __global__ void __launch_bounds__(256, 4) k_wf_any(WfArgs A) {
   warp_add_count(&A.counts[kCntTestsA], tests);
 }
 
-// Shadow stage as warp packets (EOS_FLAG_PACKET): the warp's 32 shadow rays -- one 8x4
-// pixel tile towards one light, as the closest stage emits them -- share one traversal
-// stack in shared memory.  Every stack entry carries the mask of lanes whose ray entered
-// that box; at a node each participating lane tests the four child boxes and a child is
-// taken when any lane hits it, with the ballot of those lanes as its mask.  Node and
-// triangle records are fetched once per warp (same address in every lane) and control
-// flow is warp-uniform; a lane whose ray is blocked drops out of every mask.  A ray visits
-// exactly the leaves whose boxes (and all ancestors') it enters, as in the per-lane
-// traversal, so the results are the same.
-constexpr int kPacketStack = kStackMax;
-
-template <int SH>
-__global__ void __launch_bounds__(256, 4) k_wf_any_packet(WfArgs A) {
-  extern __shared__ uint2 shstack[];
-  const int lane = threadIdx.x & 31;
-  uint2* stack = shstack + (threadIdx.x >> 5) * kPacketStack;  // (ref, lane mask) per warp
-  int* ctr = A.ctr + A.k * kCtr;
-  const int n = min(ctr[2], A.cap_s);
-  unsigned long long nodes = 0, tests = 0;
-  for (;;) {
-    const int start = grab(&ctr[4], A.qchunk);
-    if (start >= n) break;
-    const int end = min(start + A.qchunk, n);
-    for (int base = start; base < end; base += 32) {
-      const int i = base + lane;
-      const bool valid = i < end;
-      SlabRay r;
-      f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1);
-      int hi = 0, key = 0;
-      const float4* tnodes = nullptr;
-      const float4* ttris = nullptr;
-      if (valid) {
-        ShadowQ q = A.sq[i];
-        hi = __float_as_int(q.a.w);
-        key = __float_as_int(q.b.w);
-        o = mk3(q.a.x, q.a.y, q.a.z);
-        d = mk3(q.b.x, q.b.y, q.b.z);
-        const DevScene& S = A.jobs[key >> 5].s;
-        tnodes = S.nodes;
-        ttris = S.tris;
-      }
-      r = make_slab(o, d);
-      // lanes of one packet may belong to different scenes: one packet per distinct scene
-      uint32_t todo = __ballot_sync(0xffffffffu, valid);
-      uint32_t blocked = 0;
-      while (todo) {
-        const int leader = __ffs(todo) - 1;
-        const float4* nodes_w = (const float4*)__shfl_sync(0xffffffffu, (unsigned long long)tnodes, leader);
-        const float4* tris_w = (const float4*)__shfl_sync(0xffffffffu, (unsigned long long)ttris, leader);
-        const uint32_t group = __ballot_sync(0xffffffffu, valid && tnodes == nodes_w);
-        todo &= ~group;
-        uint32_t alive = group;
-        int sp = 0;
-        int cur = 0;
-        uint32_t cmask = alive;
-        for (;;) {
-          const bool part = (cmask >> lane) & 1u;
-          if (cur >= 0) {  // interior record
-            const float4* nd = nodes_w + 8 * (size_t)cur;
-            const float4 lx = __ldg(nd + r.sx), ly = __ldg(nd + 1 + r.sy), lz = __ldg(nd + 2 + r.sz);
-            const float4 hx = __ldg(nd + 3 - r.sx), hy = __ldg(nd + 4 - r.sy), hz = __ldg(nd + 5 - r.sz);
-            const int4 ref = __ldg(reinterpret_cast<const int4*>(nd) + 6);
-            nodes += part;
-            const uint32_t m0 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x));
-            const uint32_t m1 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y));
-            const uint32_t m2 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z));
-            const uint32_t m3 = __ballot_sync(0xffffffffu, part && slab_hit(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w));
-            // take the first hit child in slot order, push the others (last slot deepest)
-            int next = kDone;
-            uint32_t nmask = 0;
-            const int c[4] = {ref.x, ref.y, ref.z, ref.w};
-            const uint32_t m[4] = {m0, m1, m2, m3};
-            bool overflow = false;
-#pragma unroll
-            for (int k = 3; k >= 0; --k) {
-              if (!m[k]) continue;
-              if (next != kDone) {
-                if (sp >= kPacketStack) {
-                  overflow = true;
-                } else {
-                  if (lane == 0) stack[sp] = make_uint2((uint32_t)next, nmask);
-                  ++sp;
-                }
-              }
-              next = c[k];
-              nmask = m[k];
-            }
-            if (overflow) {
-              if (lane == 0) atomicOr(A.err, kErrStack);
-              break;
-            }
-            __syncwarp();
-            if (next != kDone) {
-              cur = next;
-              cmask = nmask;
-              continue;
-            }
-          } else if (cur != kDone) {  // leaf: the participating lanes test its triangles
-            const int first = leaf_first(cur), cnt = leaf_count(cur);
-            bool hit = false;
-            for (int p = first; p < first + cnt; ++p) {
-              f3 v1, e1, e2;
-              int id;
-              load_tri(tris_w, p, v1, e1, e2, id);
-              float t, u, v;
-              if (part && !hit) {
-                ++tests;
-                hit = mt_intersect_fast(o, d, v1, e1, e2, t, u, v);
-              }
-              if (!__any_sync(0xffffffffu, part && !hit)) break;
-            }
-            const uint32_t hb = __ballot_sync(0xffffffffu, hit);
-            blocked |= hb;
-            alive &= ~hb;
-            if (!alive) break;
-          }
-          // pop the next entry with a lane still unblocked
-          bool found = false;
-          while (sp > 0) {
-            const uint2 e = stack[--sp];
-            const uint32_t em = e.y & alive;
-            if (em) {
-              cur = (int)e.x;
-              cmask = em;
-              found = true;
-              break;
-            }
-          }
-          __syncwarp();
-          if (!found) break;
-        }
-      }
-      if ((blocked >> lane) & 1u) atomicOr(&A.masks[hi], 1u << (key & 31));
-    }
-  }
-  warp_add_count(&A.counts[kCntNodesA], nodes);
-  warp_add_count(&A.counts[kCntTestsA], tests);
-}
-
 __global__ void k_wf_shade(WfArgs A) {
   int* ctr = A.ctr + A.k * kCtr;
-  const int n = A.k == 0 ? A.n_chunk : min(ctr[1 - kCtr], A.cap_r);
+  // primary hit records beyond the work budget keep k_wf_init's padding marks
+  const int n = A.k == 0 ? A.n_chunk : min(min(ctr[1 - kCtr], A.cap_r), A.work_limit);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     HitQ hq = A.hits[i];
     int path = __float_as_int(hq.a.w);
@@ -757,27 +404,28 @@ struct StageTimer {
     if (s_ != EOS_OK) return s_;    \
   } while (0)
 
-// The nearest-hit / shadow kernels of one configuration: the chunked form (default; a
-// warp takes `queue_chunk` rays and finishes all before taking more) or lane refill.
+// The nearest-hit / shadow kernels of one configuration: a warp takes `queue_chunk` rays
+// and finishes all before taking more.  small_stack selects the test instantiation whose
+// traversal stack is its SH shared-memory entries only (launch_config pins SH = 8 then).
 template <int SH>
 struct StageKernels {
   void (*closest_primary)(WfArgs);
   void (*closest)(WfArgs);
   void (*any)(WfArgs);
-  static StageKernels get(int variant) {  // bit 0: lane refill, bit 1: shadow packets
-    const bool refill = variant & 1, packet = variant & 2;
-    if (refill) return {k_wf_closest_refill<true, SH>, k_wf_closest_refill<false, SH>, k_wf_any_refill<SH>};
-    if (packet) return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any_packet<SH>};
+  static StageKernels get(bool small_stack) {
+    if constexpr (SH == 8) {
+      if (small_stack) return {k_wf_closest<true, 8, 8>, k_wf_closest<false, 8, 8>, k_wf_any<8, 8>};
+    }
     return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any<SH>};
   }
 };
 
 template <int SH>
 eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, const Chunk* chunks, int n_chunks,
-                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem, int variant,
-                           StageTimer tm, uint32_t& launches) {
+                           int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem,
+                           bool small_stack, StageTimer tm, uint32_t& launches) {
   const int grid_lin = num_sms * 8;
-  const StageKernels<SH> K = StageKernels<SH>::get(variant);
+  const StageKernels<SH> K = StageKernels<SH>::get(small_stack);
   for (int ci = 0; ci < n_chunks; ++ci) {
     const Chunk& c = chunks[ci];
     WfArgs A = base;
@@ -844,13 +492,13 @@ void fill_job(const eos_job& J, long long path_off, DevJob& d) {
 
 struct LaunchConfig {
   int block, sh, qchunk, grid_c, grid_a;
-  int variant;  // bit 0: lane refill, bit 1: shadow packets
+  bool small_stack;  // test limit: 8-entry traversal stacks
   size_t smem;
 };
 
 template <int SH>
 void configure(LaunchConfig& c, int num_sms) {
-  const StageKernels<SH> K = StageKernels<SH>::get(c.variant);
+  const StageKernels<SH> K = StageKernels<SH>::get(c.small_stack);
   if (c.smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
     cudaFuncSetAttribute(K.closest_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
     cudaFuncSetAttribute(K.closest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
@@ -863,12 +511,13 @@ void configure(LaunchConfig& c, int num_sms) {
   c.grid_a = num_sms * std::max(1, occ_a);
 }
 
-LaunchConfig launch_config(const eos_render_params& p, int num_sms) {
+LaunchConfig launch_config(const eos_render_params& p, int num_sms, bool small_stack) {
   LaunchConfig c;
   c.block = p.block_size > 0 ? std::min(512, std::max(32, (p.block_size / 32) * 32)) : 128;
   c.sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
   c.qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
-  c.variant = ((p.flags & EOS_FLAG_REFILL) ? 1 : 0) | ((p.flags & EOS_FLAG_PACKET) ? 2 : 0);
+  c.small_stack = small_stack;
+  if (small_stack) c.sh = 8;
   c.smem = (size_t)c.sh * c.block * sizeof(uint2);
   if (c.sh == 8) configure<8>(c, num_sms);
   else if (c.sh == 16) configure<16>(c, num_sms);
@@ -880,12 +529,12 @@ eos_status run_sequence(cudaStream_t st, int num_sms, const LaunchConfig& lc, co
                         int n_chunks, int depth, StageTimer tm, uint32_t& launches) {
   if (lc.sh == 8)
     return launch_sequence<8>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                              lc.variant, tm, launches);
+                              lc.small_stack, tm, launches);
   if (lc.sh == 16)
     return launch_sequence<16>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr,
-                               lc.smem, lc.variant, tm, launches);
+                               lc.smem, false, tm, launches);
   return launch_sequence<32>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                             lc.variant, tm, launches);
+                             false, tm, launches);
 }
 
 }  // namespace
@@ -900,8 +549,6 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   for (uint32_t j = 0; j < n_jobs; ++j) {
     depth = std::max(depth, jobs[j].trace_depth);
     max_lights = std::max(max_lights, (int)jobs[j].scene->dev.n_lights);
-    // the lane-refill and packet kernels traverse single-level trees only
-    if (jobs[j].scene->instanced && (p.flags & (EOS_FLAG_REFILL | EOS_FLAG_PACKET))) return EOS_ERR_UNSUPPORTED;
   }
   // queue bytes per path: two ray queues, hit records, masks, shadow queue, accumulators
   const long long per_path = 3ll * 32 + 4 + 32ll * std::max(1, max_lights) + 16ll * (depth + 1);
@@ -939,7 +586,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   if (es != EOS_OK) return es;
   EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
 
-  const LaunchConfig lc = launch_config(p, ctx->num_sms);
+  const eos_limits& lim = ctx->limits;
+  const LaunchConfig lc = launch_config(p, ctx->num_sms, lim.small_stack != 0);
   const int block = lc.block, sh = lc.sh, qchunk = lc.qchunk;
 
   WfArgs A;
@@ -956,7 +604,12 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   A.ctr = ctr;
   A.cap_r = max_chunk;
   A.cap_s = (int)std::min<size_t>(cap_s, 0x7fffffff);
+  if (lim.queue_entries > 0) {
+    A.cap_r = std::min(A.cap_r, (int)lim.queue_entries);
+    A.cap_s = std::min(A.cap_s, (int)lim.queue_entries);
+  }
   A.qchunk = qchunk;
+  A.work_limit = lim.work_budget > 0 ? lim.work_budget : 0x7fffffff;
   A.err = ctx->d_err;
   A.counts = ctx->d_counts;
 
@@ -972,7 +625,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   }
 
   // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
-  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.variant,
+  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
+                                A.cap_r, A.cap_s, A.work_limit,
                                 (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
                                 (long long)(size_t)acc};
@@ -1073,14 +727,6 @@ eos_status noalloc_base(int dev, unsigned char** out) {
   return EOS_OK;
 }
 
-eos_status na_error_status(int e) {
-  if (e & (kErrStack | kErrDepth)) return EOS_ERR_STACK_OVERFLOW;
-  if (e & kErrQueue) return EOS_ERR_QUEUE_OVERFLOW;
-  if (e & kErrIndex) return EOS_ERR_INVALID_ARG;
-  if (e & kErrTimeout) return EOS_ERR_TIMEOUT;
-  return EOS_OK;
-}
-
 }  // namespace
 }  // namespace eos
 
@@ -1093,7 +739,7 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
       camera->height > kNoAllocMaxPaths)
     return EOS_ERR_INVALID_ARG;
   if (params->trace_depth < 0 || params->trace_depth >= EOS_MAX_BOUNCES || params->spp < 1 ||
-      params->spp > kNoAllocMaxPaths)
+      params->spp > kNoAllocMaxPaths || (params->flags & ~EOS_FLAG_STAGE_TIMING))
     return EOS_ERR_INVALID_ARG;
   if (scene->dev.n_lights > kNoAllocMaxLights) return EOS_ERR_INVALID_ARG;
   if ((rgb_out && !is_device_ptr(rgb_out)) || (paths_out && !is_device_ptr(paths_out))) return EOS_ERR_INVALID_ARG;
@@ -1144,8 +790,11 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
   A.ctr = (int*)(base + kNaCtr);
   A.cap_r = kNoAllocMaxPaths;
   A.cap_s = kNoAllocMaxPaths * kNoAllocMaxLights;
-  const LaunchConfig lc = launch_config(*params, num_sms);
+  // the scene context's tuning table, as eos_render applies it (the table is read here
+  // only; it is changed by eos_ctx_set_tuning calls, which callers serialise with renders)
+  const LaunchConfig lc = launch_config(with_tuning(scene->ctx, *params, (uint32_t)scene->dev.n_tris), num_sms, false);
   A.qchunk = lc.qchunk;
+  A.work_limit = 0x7fffffff;
   A.err = (int*)(base + kNaErr);
   A.counts = (unsigned long long*)(base + kNaCounts);
   Chunk ch{0, (int)job.n_paths};
@@ -1174,5 +823,5 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
     stats->error_flags = h.err;
     stats->kernel_launches = launches;
   }
-  return na_error_status(h.err);
+  return err_to_status(h.err);
 }

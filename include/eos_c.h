@@ -122,16 +122,9 @@ typedef struct eos_render_params {
 } eos_render_params;
 
 /* Wavefront only: run the stages eagerly (no graph) with CUDA events between them and
- * report per-stage device time in eos_stats.stage_ms. */
+ * report per-stage device time in eos_stats.stage_ms.  Other flag bits are refused
+ * (EOS_ERR_INVALID_ARG). */
 #define EOS_FLAG_STAGE_TIMING 1
-/* Wavefront only: lane refill (a lane whose ray ends takes the next ray from the queue at
- * once) instead of the default chunked persistent kernels (a warp takes queue_chunk rays
- * and finishes them all before taking more).  Measured slower on B200 for the 1080p
- * 1M-triangle workload: refilled lanes break the warps' ray coherence. */
-#define EOS_FLAG_REFILL 2
-/* Wavefront only: shadow rays traced as warp packets (one shared stack per 32 rays with
- * per-child lane masks) instead of one traversal per lane. */
-#define EOS_FLAG_PACKET 4
 
 /* Tuned launch / layout parameters of one scene-size bucket (see eos_ctx_set_tuning). */
 typedef struct eos_tuning {
@@ -242,6 +235,25 @@ eos_status eos_ctx_synchronize(eos_ctx* ctx);
 eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning* tuning);
 eos_status eos_ctx_clear_tuning(eos_ctx* ctx);
 
+/* Test limits of the wavefront kernels (no reference counterpart; the reference exits on
+ * any error, src/cudaQualifiers.h:35-45).  They make the device error paths reachable on
+ * ordinary scenes without faulting anything: a call that runs into a limit stops the work
+ * it cannot do, returns the status below and leaves the context usable.  All zero (or
+ * limits NULL) = no limits, the default.
+ *   queue_entries  > 0: each secondary-ray and shadow-ray queue holds at most this many
+ *                  entries; a bounce that emits more -> EOS_ERR_QUEUE_OVERFLOW
+ *   work_budget    > 0: queue entries one persistent launch traces; the loop over the
+ *                  queue leaves the entries beyond untraced -> EOS_ERR_TIMEOUT
+ *   small_stack    != 0: traversal stacks of flat scenes hold 8 entries (the shared-memory
+ *                  part only, no spill); a deeper traversal -> EOS_ERR_STACK_OVERFLOW
+ * eos_render in wavefront mode and eos_render_batch apply them; eos_render_noalloc does not. */
+typedef struct eos_limits {
+  int32_t queue_entries;
+  int32_t work_budget;
+  int32_t small_stack;
+} eos_limits;
+eos_status eos_ctx_set_limits(eos_ctx* ctx, const eos_limits* limits);
+
 /* ---------------------------------------------------------------------------- scenes */
 /* verts / normals [n_verts*3], tris [n_tris*3] vertex indices, tri_obj [n_tris] material
  * rows.  Limits (EOS_ERR_INVALID_ARG, checked before any device work): n_tris < 2^25
@@ -279,8 +291,8 @@ typedef struct eos_instance {
  * normalize(Minv^T n) of the mesh's interpolated unit normal; hit ids are global:
  * instance k's triangles are numbered after those of instances 0..k-1.  A mesh shared by
  * many instances is stored once.  eos_render / eos_render_batch / eos_trace_* and
- * eos_render_backward accept the scene (not EOS_FLAG_REFILL / EOS_FLAG_PACKET);
- * eos_scene_get_morton and eos_scene_save return EOS_ERR_UNSUPPORTED. */
+ * eos_render_backward accept the scene; eos_scene_get_morton and eos_scene_save return
+ * EOS_ERR_UNSUPPORTED. */
 eos_status eos_scene_create_instanced(eos_ctx* ctx, const eos_instance* instances, uint32_t n_instances,
                                       const eos_material* materials, uint32_t n_materials,
                                       const eos_light* lights, uint32_t n_lights, eos_scene** out);
@@ -372,10 +384,13 @@ eos_status eos_mesh_destroy(eos_mesh* mesh);
  * Limits: at most EOS_NOALLOC_MAX_PATHS paths counted in 8x4-pixel tiles times spp
  * (128x128 at 1 spp) and at most EOS_NOALLOC_MAX_LIGHTS lights; larger requests return
  * EOS_ERR_INVALID_ARG without touching the GPU.  rgb_out [H*W*3] and paths_out [H*W*spp]
- * must be device memory (either may be NULL); stats may be NULL.  The call waits for its
- * stream.  The first call on a device looks up the array's device address (make that
- * first call before any stream capture).  All calls share the one array: calls that
- * overlap on the GPU race, so serialise them. */
+ * must be device memory (either may be NULL); stats may be NULL.  params->mode is not
+ * read: the call always renders with the wavefront kernels (the same image as either
+ * mode); block size, queue chunk and stack depth left at 0 take the scene context's tuned
+ * values, as in eos_render; flags other than EOS_FLAG_STAGE_TIMING (ignored here) are
+ * refused.  The call waits for its stream.  The first call on a device looks up the
+ * array's device address (make that first call before any stream capture).  All calls
+ * share the one array: calls that overlap on the GPU race, so serialise them. */
 #define EOS_NOALLOC_MAX_PATHS 16384
 #define EOS_NOALLOC_MAX_LIGHTS 8
 eos_status eos_render_noalloc(const eos_scene* scene, const eos_camera* camera,

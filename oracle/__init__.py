@@ -12,7 +12,8 @@ Two checkers live here:
   forward + adjoint.
 * :class:`RefRenderer` -- ``_ref/libeosref.so``, the reference's own CPU renderer
   (src/RayTracer.cpp, src/Scene.cpp, src/BVH.cpp, ...) compiled from its sources by
-  ``oracle/Makefile`` with the one-line shadow fix documented there.
+  ``oracle/Makefile`` with the two one-line fixes documented there (the shadow ray's
+  uninitialised distance, the leaf index overrun).
 """
 from __future__ import annotations
 
@@ -26,7 +27,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libeosref.so")
-REF_SRC = "/root/reference/src"
+# the reference's source tree, present where the checkers are built (not on the GPU box)
+REF_ROOT = os.environ.get("EOS_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "src")
 MAXB = 8
 HIT_NONE = -1
 HIT_UNTRACED = -2
@@ -106,6 +109,13 @@ def lib_ref():
         L.eosref_closest_hit.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_float)]
         L.eosref_any_hit.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_uint8)]
         L.eosref_morton3.argtypes = [POINTER(c_uint32), c_int, POINTER(c_uint32)]
+        L.eosref_tree_export.argtypes = [c_void_p, POINTER(c_int32), POINTER(c_int32)]
+        L.eosref_tree_boxes.argtypes = [c_void_p, POINTER(c_float)]
+        L.eosref_scene_create_from_tree.restype = c_void_p
+        L.eosref_scene_create_from_tree.argtypes = [POINTER(c_float), POINTER(c_float), c_int, POINTER(c_uint32),
+                                                    POINTER(c_uint32), c_int, POINTER(c_float), c_int,
+                                                    POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_int32),
+                                                    c_int]
         _lib_ref = L
     return _lib_ref
 
@@ -259,18 +269,44 @@ class OracleInstanced(Oracle):
 
 
 class RefRenderer:
-    """The reference's own CPU renderer, compiled from its sources, over one scene."""
+    """The reference's own CPU renderer, compiled from its sources, over one scene.
 
-    def __init__(self, scene, build_threads: int = 1):
+    tree: (perm, nodes) from :meth:`export_tree` of an earlier build of the same scene;
+    the tree is then restored instead of built (see :func:`ref_tree_cached`)."""
+
+    def __init__(self, scene, build_threads: int = 1, tree=None):
         L = lib_ref()
         self.scene = scene
         secs = c_double(0.0)
-        self.h = L.eosref_scene_create(*_scene_args(scene), build_threads, ctypes.byref(secs))
+        if tree is None:
+            self.h = L.eosref_scene_create(*_scene_args(scene), build_threads, ctypes.byref(secs))
+        else:
+            perm = np.ascontiguousarray(tree[0], np.int32)
+            nodes = np.ascontiguousarray(tree[1], np.int32).reshape(-1, 6)
+            if perm.shape[0] != scene.n_tris:
+                raise ValueError("tree was built for another scene")
+            self.h = L.eosref_scene_create_from_tree(*_scene_args(scene), _p(perm, c_int32), _p(nodes, c_int32),
+                                                     nodes.shape[0])
+            if not self.h:
+                raise ValueError("tree arrays do not describe a tree over this scene")
         L.eosref_scene_set_ambient(self.h, float(getattr(scene, "ambient_index", 1.0)))
         self.build_seconds = secs.value
         nn, ml = c_int(0), c_int(0)
         L.eosref_scene_stats(self.h, ctypes.byref(nn), ctypes.byref(ml))
         self.n_nodes, self.max_leaf = nn.value, ml.value
+
+    def export_tree(self):
+        """(perm [n_tris], nodes [n_nodes, 6]) of the reference's tree (eosref_tree_export)."""
+        perm = np.zeros(self.scene.n_tris, np.int32)
+        nodes = np.zeros((self.n_nodes, 6), np.int32)
+        lib_ref().eosref_tree_export(self.h, _p(perm, c_int32), _p(nodes, c_int32))
+        return perm, nodes
+
+    def boxes(self):
+        """[n_nodes, 6] boxes of the reference's flat node buffer."""
+        b = np.zeros((self.n_nodes, 6), np.float32)
+        lib_ref().eosref_tree_boxes(self.h, _p(b, c_float))
+        return b
 
     def __del__(self):
         if getattr(self, "h", None) and _lib_ref is not None:

@@ -139,17 +139,9 @@ void replay_path(const RefScene& rs, Ray ray, int trace_depth, int32_t* hits,
   }
 }
 
-}  // namespace
-
-extern "C" {
-
-// Builds the reference Scene and its BVH (Scene::flush, src/Scene.cpp:204-209).
-// build_threads = 1 gives a deterministic tree: the SAH sweep's OpenMP loop races on
-// shared temporaries otherwise (src/BVH.cpp:454-480).
-void* eosref_scene_create(const float* verts, const float* normals, int nv, const uint32_t* tris,
-                          const uint32_t* tri_obj, int nt, const float* mats, int nobj,
-                          const float* lights, int nl, int build_threads, double* build_seconds) {
-  (void)nv;
+// The reference Scene with its surfaces, materials and lights, before Scene::flush.
+RefScene* make_scene(const float* verts, const float* normals, const uint32_t* tris, const uint32_t* tri_obj,
+                     int nt, const float* mats, int nobj, const float* lights, int nl) {
   RefScene* rs = new RefScene();
   rs->object_materials.resize(nobj);
   // materials: kd rgb, ks rgb, shininess, reflectivity, transparency, refractive index
@@ -192,6 +184,30 @@ void* eosref_scene_create(const float* verts, const float* normals, int nv, cons
     rs->lights.push_back(ls);
     rs->scene.addLightSource(ls);
   }
+  return rs;
+}
+
+void scan_leaves(RefScene* rs) {
+  const BVH& bvh = rs->scene.getBVH();
+  BvhNode* nodes = bvh.getNodesBuffer();
+  rs->n_nodes = bvh.getNodesBufferSize();
+  rs->max_leaf = 0;
+  for (int i = 0; i < rs->n_nodes; ++i)
+    if (nodes[i].type == BVH_LEAF) rs->max_leaf = std::max(rs->max_leaf, nodes[i].numSurfacesEncapulated);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Builds the reference Scene and its BVH (Scene::flush, src/Scene.cpp:204-209).
+// build_threads = 1 gives a deterministic tree: the SAH sweep's OpenMP loop races on
+// shared temporaries otherwise (src/BVH.cpp:454-480).
+void* eosref_scene_create(const float* verts, const float* normals, int nv, const uint32_t* tris,
+                          const uint32_t* tri_obj, int nt, const float* mats, int nobj,
+                          const float* lights, int nl, int build_threads, double* build_seconds) {
+  (void)nv;
+  RefScene* rs = make_scene(verts, normals, tris, tri_obj, nt, mats, nobj, lights, nl);
   int prev = omp_get_max_threads();
   omp_set_num_threads(build_threads > 0 ? build_threads : 1);
   double t0 = getRealTime();
@@ -199,12 +215,99 @@ void* eosref_scene_create(const float* verts, const float* normals, int nv, cons
   double t1 = getRealTime();
   omp_set_num_threads(prev);
   if (build_seconds) *build_seconds = t1 - t0;
-  const BVH& bvh = rs->scene.getBVH();
-  BvhNode* nodes = bvh.getNodesBuffer();
-  rs->n_nodes = bvh.getNodesBufferSize();
-  for (int i = 0; i < rs->n_nodes; ++i)
-    if (nodes[i].type == BVH_LEAF) rs->max_leaf = std::max(rs->max_leaf, nodes[i].numSurfacesEncapulated);
+  scan_leaves(rs);
   return rs;
+}
+
+// The tree the reference's builder made, as plain arrays, so that a scene whose build
+// takes minutes on one core (the 1.06M-triangle benchmark scene) is built once and
+// restored afterwards.  perm [nt]: triangle id at each position of the scene's surface
+// array after the build's in-place sorts.  nodes [n_nodes * 6]: per entry of the
+// reference's flat node buffer (src/BVH.cpp:742-784) type, numSurfacesEncapulated,
+// leftChildIndex, rightChildIndex, surfacesIndices[0] (leaves; -1 otherwise), splitAxis.
+void eosref_tree_export(void* h, int32_t* perm, int32_t* nodes) {
+  RefScene* rs = (RefScene*)h;
+  const int nt = rs->scene.getNumSurfaces();
+  Surface** surf = rs->scene.getFirstSurfaceAddress();
+  for (int i = 0; i < nt; ++i) perm[i] = surf[i]->getMaterialIndex();
+  const BvhNode* nb = rs->scene.getBVH().getNodesBuffer();
+  for (int i = 0; i < rs->n_nodes; ++i) {
+    const BvhNode& n = nb[i];
+    int32_t* o = nodes + 6 * i;
+    o[0] = n.type;
+    o[1] = n.numSurfacesEncapulated;
+    o[2] = n.type == BVH_LEAF ? -1 : n.leftChildIndex;
+    o[3] = n.type == BVH_LEAF ? -1 : n.rightChildIndex;
+    o[4] = n.type == BVH_LEAF ? n.surfacesIndices[0] : -1;
+    o[5] = n.type == BVH_LEAF ? 0 : n.splitAxis;
+  }
+}
+
+// The scene with the tree restored from eosref_tree_export's arrays instead of built:
+// the surface array is put in the exported order and the flat node buffer is refilled
+// (leaves as the patched createLeaf writes them, src/BVH.cpp:325-340); every node's box is
+// recomputed by the builder's own BVH::computeBoxWithSurfaces over the node's surface
+// range (src/BVH.cpp:144-159), a min / max union over the same surfaces and so the box the
+// build computed.  Returns NULL when the arrays do not describe a tree over nt surfaces.
+void* eosref_scene_create_from_tree(const float* verts, const float* normals, int nv, const uint32_t* tris,
+                                    const uint32_t* tri_obj, int nt, const float* mats, int nobj,
+                                    const float* lights, int nl, const int32_t* perm, const int32_t* nodes,
+                                    int n_nodes) {
+  (void)nv;
+  if (n_nodes < 2 || nt < 1) return nullptr;
+  std::vector<char> seen(nt, 0);
+  for (int i = 0; i < nt; ++i) {
+    if (perm[i] < 0 || perm[i] >= nt || seen[perm[i]]) return nullptr;
+    seen[perm[i]] = 1;
+  }
+  // first surface of every node: a leaf's own, an interior node's leftmost leaf's; in the
+  // preorder buffer a child comes after its parent, so one backwards pass fills them
+  std::vector<int> first(n_nodes, -1);
+  for (int i = n_nodes - 1; i >= 0; --i) {
+    const int32_t* n = nodes + 6 * i;
+    if (n[0] == BVH_LEAF) {
+      first[i] = n[4];
+    } else {
+      if (n[2] <= i || n[2] >= n_nodes || n[3] <= i || n[3] >= n_nodes) return nullptr;
+      first[i] = first[n[2]];
+    }
+    if (first[i] < 0 || n[1] < 1 || first[i] + n[1] > nt) return nullptr;
+  }
+  RefScene* rs = make_scene(verts, normals, tris, tri_obj, nt, mats, nobj, lights, nl);
+  std::vector<Surface*>& so = rs->scene.m_SurfaceObjects;
+  std::vector<Surface*> by_id(so.begin(), so.end());
+  for (int i = 0; i < nt; ++i) so[i] = by_id[perm[i]];
+  BVH& bvh = rs->scene.m_Bvh;
+  bvh.m_NodesBuffer = new BvhNode[n_nodes];
+  bvh.m_FlatTreePointers.assign(n_nodes, nullptr);
+  bvh.m_Root = nullptr;
+  for (int i = 0; i < n_nodes; ++i) {
+    const int32_t* n = nodes + 6 * i;
+    BvhNode& b = bvh.m_NodesBuffer[i];
+    b.type = n[0];
+    b.numSurfacesEncapulated = n[1];
+    b.leftChild = nullptr;
+    b.rightChild = nullptr;
+    b.leftChildIndex = n[2];
+    b.rightChildIndex = n[3];
+    b.splitAxis = n[5];
+    for (int k = 0; k < SURFACES_PER_LEAF; ++k) b.surfacesIndices[k] = k < n[1] ? first[i] + k : 0;
+    b.aabb = bvh.computeBoxWithSurfaces(&so[0], first[i], first[i] + n[1]);
+  }
+  scan_leaves(rs);
+  return rs;
+}
+
+// Boxes of the flat node buffer, [n_nodes * 6] min xyz, max xyz (to check a restore).
+void eosref_tree_boxes(void* h, float* boxes) {
+  RefScene* rs = (RefScene*)h;
+  const BvhNode* nb = rs->scene.getBVH().getNodesBuffer();
+  for (int i = 0; i < rs->n_nodes; ++i) {
+    const glm::vec3 lo = nb[i].aabb.getMinVertex(), hi = nb[i].aabb.getMaxVertex();
+    float* o = boxes + 6 * i;
+    o[0] = lo.x; o[1] = lo.y; o[2] = lo.z;
+    o[3] = hi.x; o[4] = hi.y; o[5] = hi.z;
+  }
 }
 
 void eosref_scene_set_ambient(void* h, float ambient) {

@@ -5,7 +5,8 @@ oracle/Makefile from the reference tree) and its EncodeMorton3 on seeded inputs 
 stores the outputs as small .npz files.  The GPU box has no reference tree, so the
 tests read these files there.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (all fixtures)
+    python tests/golden/make_golden.py config2    (the 1.06M-triangle sample only)
 """
 from __future__ import annotations
 
@@ -46,8 +47,31 @@ def morton_case():
     print("morton3", codes[:10])
 
 
+def config2_case(n_sample=30_000):
+    """30,000 seeded pixels of the 1080p view of the 1,056,768-triangle scene (depth 3, 4
+    lights, pixel centres) through the reference's renderer, with the tree its own builder
+    made (saved once by oracle/make_ref_tree.py and restored here)."""
+    from oracle import make_ref_tree
+    sc = scenes.config2_scene()
+    tree = make_ref_tree.load(sc)
+    if tree is None:
+        raise SystemExit("run `python -m oracle.make_ref_tree` first (builds the reference's tree once)")
+    ref = oracle.RefRenderer(sc, tree=tree)
+    cam = scenes.config2_camera()
+    rng = np.random.default_rng(2002)
+    pix = np.sort(rng.choice(cam.width * cam.height, n_sample, replace=False)).astype(np.int32)
+    r = ref.render(cam, 2, pixel_offset=0.5, pixels=pix, nthreads=os.cpu_count())
+    np.savez_compressed(os.path.join(HERE, "config2_sample.npz"), pixels=pix, rgb=r["rgb"], hits=r["hits"][:, :3],
+                        shadows=r["shadows"][:, :3].astype(np.uint8), counts=r["counts"], cam=cam.as_array(),
+                        size=np.array([cam.width, cam.height, 2]), ref_nodes=np.array([ref.n_nodes, ref.max_leaf]))
+    print("config2_sample", r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
+
+
 def main():
     oracle.build(ref=True)
+    if sys.argv[1:] == ["config2"]:
+        config2_case()
+        return
     morton_case()
     render_case("config1_128", scenes.config1_scene(), scenes.config1_camera(128, 128), 1)
     for seed in (11, 12):
@@ -57,6 +81,7 @@ def main():
     # transparent spheres (Fresnel-mixed secondary rays) in air
     sc = scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3, ambient_index=1.0002)
     render_case("transp61", sc, scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 96, 72), 4)
+    config2_case()
 
 
 if __name__ == "__main__":

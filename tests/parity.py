@@ -47,4 +47,8 @@ def classify(mismatch, flags):
         "near_origin": int((mismatch & ((flags & oracle.FLAG_NEAR_ORIGIN) != 0)).sum()),
         "unexplained": int((mismatch & (flags == 0)).sum()),
     }
+    # the classes beyond the 2-ulp rule: flagged paths that are not also near ties
+    no_tie = mismatch & ((flags & oracle.FLAG_TIE) == 0)
+    out["axis_parallel_not_tie"] = int((no_tie & ((flags & oracle.FLAG_AXIS_PARALLEL) != 0)).sum())
+    out["near_origin_not_tie"] = int((no_tie & ((flags & oracle.FLAG_NEAR_ORIGIN) != 0)).sum())
     return out

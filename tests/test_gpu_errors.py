@@ -1,0 +1,92 @@
+"""Device error paths, made to fire on ordinary scenes by the context's test limits
+(eos_ctx_set_limits) -- no fault, trap or hang: each limited call returns its status, and
+the same context renders the frame correctly right afterwards.
+
+  queue_entries  -> EOS_ERR_QUEUE_OVERFLOW (6)
+  work_budget    -> EOS_ERR_TIMEOUT (4), the persistent loops' iteration budget
+  small_stack    -> EOS_ERR_STACK_OVERFLOW (5)
+"""
+import numpy as np
+import pytest
+
+from eos_b200 import api, scenes
+from eos_b200._lib import EosError
+
+pytestmark = pytest.mark.gpu
+
+TIMEOUT, STACK, QUEUE = 4, 5, 6
+
+
+@pytest.fixture(scope="module")
+def big(ctx):
+    """A 300k-triangle mixed scene: its 4-wide tree is deep enough for an 8-entry stack to
+    overflow on shadow rays."""
+    sc = scenes.mixed_scene(scenes.rng_for(4243), 300_000, "mixed300k")
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 256, 192)
+    ref = api.render(ctx, dsc, cam, 2, mode="wavefront", outputs=("rgb", "paths"), device=False)
+    return dsc, cam, ref
+
+
+def _limited(ctx, fn, **lim):
+    ctx.set_limits(**lim)
+    try:
+        with pytest.raises(EosError) as e:
+            fn()
+        return e.value.code
+    finally:
+        ctx.set_limits()
+
+
+def _same(a, b):
+    assert np.array_equal(a["paths"], b["paths"])
+    assert np.array_equal(a["rgb"], b["rgb"])
+
+
+@pytest.mark.parametrize("lim,code", [(dict(queue_entries=64), QUEUE), (dict(work_budget=1000), TIMEOUT),
+                                      (dict(small_stack=True), STACK)])
+def test_limit_gives_its_status_and_the_context_stays_usable(ctx, big, lim, code):
+    dsc, cam, ref = big
+    assert ref["stats"]["error_flags"] == 0
+    # eos_render in wavefront mode
+    got = _limited(ctx, lambda: api.render(ctx, dsc, cam, 2, mode="wavefront", outputs=("rgb", "paths"),
+                                           device=False), **lim)
+    assert got == code
+    _same(api.render(ctx, dsc, cam, 2, mode="wavefront", outputs=("rgb", "paths"), device=False), ref)
+    # eos_render_batch (graph-captured; the limits are part of the graph's key)
+    jobs = [api.BatchJob(dsc, cam, 2, 0.5)]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    got = _limited(ctx, lambda: api.render_batch(ctx, jobs, outs), **lim)
+    assert got == code
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    api.render_batch(ctx, jobs, outs)
+    assert np.array_equal(outs[0]["paths"].cpu().numpy(), ref["paths"])
+    assert np.array_equal(outs[0]["rgb"].cpu().numpy(), ref["rgb"])
+
+
+def test_work_budget_leaves_untraced_paths_marked(ctx, big):
+    """Past the budget the queue entries stay untraced: their path records keep
+    EOS_HIT_UNTRACED (-2) and the traced ones equal the unlimited render's."""
+    dsc, cam, ref = big
+    out = {}
+    npx = cam.width * cam.height
+    paths = np.zeros((npx, 16), np.int32)
+    out["paths"] = paths
+    ctx.set_limits(work_budget=4096)
+    try:
+        with pytest.raises(EosError) as e:
+            api.render(ctx, dsc, cam, 2, mode="wavefront", outputs=(), out=out, device=False)
+        assert e.value.code == TIMEOUT
+    finally:
+        ctx.set_limits()
+    prim = paths[:, 0]
+    traced = prim != -2
+    assert 0 < traced.sum() < npx
+    assert np.array_equal(prim[traced], ref["paths"][traced, 0])
+
+
+def test_limits_reject_negative_values(ctx):
+    with pytest.raises(EosError) as e:
+        ctx.set_limits(queue_entries=-1)
+    assert e.value.code == 1
+    ctx.set_limits()

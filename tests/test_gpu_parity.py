@@ -77,6 +77,11 @@ def test_plain_matches_compiled_reference_config1(ctx, c1):
     c = classify(mm, o["flags"])
     print("config1 512^2 vs reference:", c)
     assert c["unexplained"] == 0, c
+    # the tree-dependent reference artefacts stay at their recorded counts: axis-parallel
+    # paths that are not also 2-ulp ties (the reference's NaN slab culling, src/Box.cu:234-255)
+    # and shadow rays blocked within 1e-3 of their origin (its [0.001, 999] box window,
+    # src/BVH.cpp:668-683); 2-ulp ties are excused by the parity bar itself
+    assert c["axis_parallel_not_tie"] <= 5 and c["near_origin_not_tie"] <= 9, c
     d = np.abs(g["rgb"] - ref["rgb"]).max(1)
     assert d[~mm].max() <= RGB_TOL
     rgba, _ = refr.render_rgba8(cam, 1)
@@ -399,3 +404,34 @@ def test_config2_sampled_pixels_match_oracle(ctx, width):
     st = g["stats"]
     assert st["primary_rays"] == cam.width * cam.height
     assert st["shadow_rays"] > st["primary_rays"]
+
+
+def test_config2_sample_matches_reference_golden(ctx):
+    """The reference's own renderer on the 1,056,768-triangle 1080p view (30,000 seeded pixel
+    centres, depth 3, 4 lights; tests/golden/config2_sample.npz, from make_golden.py with the
+    tree the reference's builder made): hit ids and bounce paths bit-exact except the
+    classes the oracle flags, colours within RGB_TOL on every other path; the plain and
+    the batched wavefront path agree."""
+    path = os.path.join(GOLDEN, "config2_sample.npz")
+    if not os.path.exists(path):
+        pytest.skip("config2_sample.npz not generated")
+    gd = np.load(path)
+    pix = gd["pixels"]
+    sc = scenes.config2_scene()
+    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
+    cam = scenes.config2_camera()
+    g = api.render(ctx, dsc, cam, 2, pixel_offset=0.5, outputs=("rgb", "paths"), device=True)
+    jobs = [api.BatchJob(dsc, cam, 2, 0.5)]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    api.render_batch(ctx, jobs, outs)
+    assert np.array_equal(outs[0]["paths"].cpu().numpy(), g["paths"].cpu().numpy())
+    gp = g["paths"].cpu().numpy()[pix]
+    gh, gs = paths_split(gp)
+    o = oracle.Oracle(sc).render(cam, 2, pixel_offset=0.5, pixels=pix)
+    mm = path_mismatch(gh, gs, gd["hits"], gd["shadows"], 3)
+    c = classify(mm, o["flags"])
+    print("config2 30k sample vs reference:", c)
+    assert c["unexplained"] == 0, c
+    assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 30, c
+    assert np.abs(g["rgb"].cpu().numpy()[pix] - gd["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])

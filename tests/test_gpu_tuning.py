@@ -22,12 +22,10 @@ def test_results_invariant_under_tuning(ctx):
         assert dsc.info()["leaf_size"] == leaf and dsc.info()["width"] == width
         assert dsc.info()["builder"] == {"lbvh": 1, "ploc": 2}[builder]
         assert dsc.info()["sah_cost"] > 0
-        for mode, refill, packet in (("plain", False, False), ("wavefront", False, False),
-                                     ("wavefront", True, False), ("wavefront", False, True)):
+        for mode in ("plain", "wavefront"):
             for block, stack, chunk in ((64, 8, 32), (128, 16, 64), (256, 32, 256)):
                 r = api.render(ctx, dsc, cam, 2, pixel_offset=0.5, mode=mode, outputs=("rgb", "paths"),
-                               device=False, block_size=block, stack_depth=stack, queue_chunk=chunk,
-                               refill=refill, packet=packet)
+                               device=False, block_size=block, stack_depth=stack, queue_chunk=chunk)
                 if ref is None:
                     ref = r
                     continue

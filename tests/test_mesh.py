@@ -11,11 +11,12 @@ import pytest
 
 from eos_b200 import mesh
 from eos_b200._lib import EosError
+import oracle
 from oracle import mesh_oracle
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "meshes", "*.obj")))
-REF_MODELS = "/root/reference/objmodels"
+REF_MODELS = os.path.join(oracle.REF_ROOT, "objmodels")
 
 
 def _bits(a):

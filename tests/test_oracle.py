@@ -72,6 +72,43 @@ def test_oracle_matches_reference_golden(name, scene_fn):
     assert np.array_equal(r["counts"][0], g["counts"][0])
 
 
+def test_oracle_matches_reference_config2_sample():
+    """The oracle against the reference's renderer on 30,000 sampled paths of the
+    1,056,768-triangle 1080p view (golden file recorded with the reference's own tree)."""
+    path = os.path.join(os.path.dirname(__file__), "golden", "config2_sample.npz")
+    if not os.path.exists(path):
+        pytest.skip("config2_sample.npz not generated")
+    g = np.load(path)
+    sc = scenes.config2_scene()
+    cam = scenes.config2_camera()
+    r = oracle.Oracle(sc).render(cam, 2, pixel_offset=0.5, pixels=g["pixels"])
+    mm = path_mismatch(r["hits"], r["shadows"], g["hits"], g["shadows"], 3)
+    c = classify(mm, r["flags"])
+    print("oracle vs reference, config 2 sample:", c)
+    assert c["unexplained"] == 0, c
+    assert np.abs(r["rgb"] - g["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    assert np.array_equal(r["counts"][0], g["counts"][0])
+
+
+def test_reference_tree_restore_equals_build():
+    """The reference's tree exported after its own build and restored (boxes recomputed by
+    BVH::computeBoxWithSurfaces) gives the same node buffer boxes and the same renders."""
+    if not oracle.ref_available():
+        pytest.skip("reference CPU build unavailable")
+    sc = scenes.small_random_scene(71, n_spheres=8, level=3, lights=2, refl=0.5, transparent=1)
+    built = oracle.RefRenderer(sc)
+    perm, nodes = built.export_tree()
+    restored = oracle.RefRenderer(sc, tree=(perm, nodes))
+    assert restored.n_nodes == built.n_nodes and restored.max_leaf == built.max_leaf
+    assert np.array_equal(built.boxes().view(np.uint32), restored.boxes().view(np.uint32))
+    cam = scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 64, 48)
+    a, b = built.render(cam, 3), restored.render(cam, 3)
+    assert np.array_equal(a["hits"], b["hits"]) and np.array_equal(a["shadows"], b["shadows"])
+    assert np.array_equal(a["rgb"].view(np.uint32), b["rgb"].view(np.uint32))
+    with pytest.raises(ValueError):  # a tree of another scene is refused
+        oracle.RefRenderer(scenes.small_random_scene(72, n_spheres=2), tree=(perm, nodes))
+
+
 @pytest.mark.parametrize("seed,ambient", [(62, 1.0), (63, 1.33), (64, 1.0002)])
 def test_transparent_materials_match_reference(seed, ambient):
     """Transparent materials (src/RayTracer.cpp:353-407: Fresnel K, the mirror ray about the

@@ -21,10 +21,11 @@ from tests.parity import RGB_TOL
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(ctx, dsc, cam, td, rgb, paths, spp=1):
+def _noalloc(ctx, dsc, cam, td, rgb, paths, spp=1, rows=None, jitter_seed=0, flags=0):
     import torch
     c = api.camera_struct(cam)
-    p = api.params_struct(td, 0.5, spp)
+    p = api.params_struct(td, 0.5, spp, jitter_seed, rows=rows)
+    p.flags = flags
     st = L.Stats()
     stream = torch.cuda.current_stream().cuda_stream
     code = ctx.lib.eos_render_noalloc(dsc.h, byref(c), byref(p), ctypes.c_void_p(stream),
@@ -74,3 +75,59 @@ def test_noalloc_rejects_sizes_beyond_its_capacity(ctx):
     rgb2 = torch.zeros((64 * 64, 3), device="cuda")
     code, st = _noalloc(ctx, dsc, small, 1, rgb2, None)
     assert code == 0 and st.primary_rays == 64 * 64
+
+
+def _check_against_render(ctx, dsc, cam, td, spp=1, rows=None, jitter_seed=0):
+    """Two calls in a row of the allocation-free entry point against eos_render (wavefront
+    mode, context scratch) on the same frame: paths bit for bit, colours within RGB_TOL."""
+    import torch
+    H = rows[1] - rows[0] if rows else cam.height
+    npx = cam.width * H
+    ref = api.render(ctx, dsc, cam, td, pixel_offset=0.5, spp=spp, jitter_seed=jitter_seed, mode="wavefront",
+                     outputs=("rgb", "paths"), device=True, rows=rows)
+    for call in range(2):
+        rgb = torch.full((npx, 3), -1.0, device="cuda")
+        paths = torch.zeros((npx * spp, 16), dtype=torch.int32, device="cuda")
+        code, st = _noalloc(ctx, dsc, cam, td, rgb, paths, spp=spp, rows=rows, jitter_seed=jitter_seed)
+        assert code == 0, (call, code)
+        torch.cuda.synchronize()
+        assert np.abs(rgb.cpu().numpy() - ref["rgb"].cpu().numpy()).max() <= RGB_TOL, call
+        assert np.array_equal(paths.cpu().numpy(), ref["paths"].cpu().numpy()), call
+        assert st.primary_rays == ref["stats"]["primary_rays"] == npx * spp
+        assert st.shadow_rays == ref["stats"]["shadow_rays"]
+        assert st.secondary_rays == ref["stats"]["secondary_rays"]
+
+
+def test_noalloc_two_samples_per_pixel(ctx):
+    sc = scenes.small_random_scene(63, n_spheres=5, level=3, lights=2, refl=0.5, transparent=1)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 96, 80)  # 2 x 7,680 paths <= 16,384
+    _check_against_render(ctx, dsc, cam, 3, spp=2, jitter_seed=77)
+
+
+def test_noalloc_row_band(ctx):
+    sc = scenes.small_random_scene(64, n_spheres=6, level=3, lights=3, refl=0.6)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 320, 240)  # the whole frame is too large,
+    _check_against_render(ctx, dsc, cam, 2, rows=(101, 141))             # a 40-row band fits
+
+
+def test_noalloc_instanced_scene(ctx):
+    d = scenes.instanced_test_scene(11, n_instances=8, lights=2, transparent=1)
+    meshes = [api.DeviceScene(ctx, m) for m in d.meshes]
+    inst = api.InstancedScene(ctx, meshes, d.instances, d.materials, d.lights)
+    cam = scenes.look_at((1.0, 3.0, 9.0), (0, 0, 0), 50.0, 128, 96)
+    _check_against_render(ctx, inst, cam, 2)
+
+
+def test_noalloc_refuses_unknown_flags(ctx):
+    import torch
+    sc = scenes.small_random_scene(65, n_spheres=2, level=2, lights=1)
+    dsc = api.DeviceScene(ctx, sc)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 32, 32)
+    rgb = torch.zeros((32 * 32, 3), device="cuda")
+    for bad in (2, 4, 1 << 30):
+        code, _ = _noalloc(ctx, dsc, cam, 1, rgb, None, flags=bad)
+        assert code == 1, bad
+    code, st = _noalloc(ctx, dsc, cam, 1, rgb, None, flags=1)  # stage timing is accepted and ignored
+    assert code == 0 and st.primary_rays == 32 * 32
