@@ -18,7 +18,7 @@ counters.  The scene (~135 MB of node / triangle / shading records) is larger th
 
 --impl reference: the reference's own CPU renderer (compiled from its sources into
 oracle/_ref/libeosref.so) on all host cores for the same metric and view: RayTracer::rayTrace
-per pixel over a band of rows per step, with the tree the reference's builder made for this
+per pixel over a strided sample of the view's pixels per step, with the tree the reference's builder made for this
 scene (built once, saved as oracle/_ref/config2_tree.npz and restored; the build takes ~10
 minutes on one core).  The cpu_baseline of the GPU line is the same measurement, with the
 oracle's C port beside it.
@@ -180,11 +180,69 @@ def algorithmic_bytes(st, width):
 
 
 def profile_traffic():
-    """Per-ray DRAM traffic of the top kernels from the committed ncu summary, if present."""
+    """Per-ray counters of the top kernels from the committed ncu summary (profiles/traffic.json):
+    warp instructions, L1 / L2 / DRAM bytes per ray, and the per-cycle peaks of the part."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         return json.load(open(p))
     return {}
+
+
+def roofline(tr, st, stage_ms, shadow_bytes, closest_bytes, launches, sm_hz):
+    """Roofline of the wavefront's two traversal stages against the ceiling that binds them.
+
+    Both are gathers through a tree whose node and triangle records are mostly served by L1
+    and L2, not streams from HBM; the ncu captures show instruction issue as the limit
+    (issue slots ~70 % busy, 18-25 of 32 lanes active per instruction).  So the headline
+    fraction is issue: warp instructions per ray (ncu capture of the same kernel) x this
+    step's rays of the stage / the stage's CUDA-event time, against the part's issue peak
+    (sm__inst_issued.sum.peak_sustained = 592 warp instructions per cycle) at the SM clock
+    sampled under load.  Beside it the same rays' L1, L2 and DRAM bytes against their peaks
+    (ncu per-cycle peaks; HBM: the measured copy bandwidth), and the algorithmic bytes."""
+    hbm_peak, hbm_kind = measured_peak()
+    peaks = tr.get("peaks_per_cycle", {})
+    out = {}
+    for key, kern, ms, alg, rays in (
+            ("shadow", "k_wf_any", stage_ms[1], shadow_bytes, st["shadow_rays"]),
+            ("closest", "k_wf_closest", stage_ms[0], closest_bytes, st["primary_rays"] + st["secondary_rays"])):
+        c = tr.get(key)
+        sec = ms * 1e-3
+        e = {"kernel": kern, "stage_ms": round(ms, 4), "launches": launches, "rays": rays,
+             "ms_per_launch": round(ms / launches, 4),
+             "algorithmic_bytes_per_launch": round(alg / launches),
+             "algorithmic_note": "node / triangle record bytes requested (28 B per child box, 40 B per test, "
+                                 "32 B ray in, result out): an L1-level request count, mostly served by L1 / L2"}
+        if c and peaks:
+            inst = c["warp_inst_per_ray"] * rays
+            issue_peak = peaks["issue_warp_inst"] * sm_hz
+            l1_peak = peaks["l1_bytes"] * sm_hz
+            l2_peak = peaks["l2_bytes"] * peaks["l2_clock_hz"]
+            e.update({
+                "bound": "issue", "achieved": round(inst / sec / 1e9, 1),
+                "peak": round(issue_peak / 1e9, 1), "unit": "Gwarp-inst/s",
+                "frac": round(inst / sec / issue_peak, 4),
+                "peak_kind": "ncu sm__inst_issued.sum.peak_sustained (592 warp instructions per cycle) x the "
+                             "median SM clock sampled during this run",
+                "traffic": round(c["dram_bytes_per_ray"] * rays / launches),
+                "traffic_source": "ncu capture of the same kernel: DRAM bytes per ray x rays per launch "
+                                  "(cold caches: an upper bound)",
+                "ceilings": {
+                    "issue": round(inst / sec / issue_peak, 4),
+                    "l1_bytes": round(c["l1_bytes_per_ray"] * rays / sec / l1_peak, 4),
+                    "l2_bytes": round(c["l2_bytes_per_ray"] * rays / sec / l2_peak, 4),
+                    "hbm_bytes": round(c["dram_bytes_per_ray"] * rays / sec / (hbm_peak * 1e9), 4)},
+                "hbm_peak_gbs": hbm_peak, "hbm_peak_kind": hbm_kind,
+                "per_ray": {k: c[k] for k in ("warp_inst_per_ray", "l1_bytes_per_ray", "l2_bytes_per_ray",
+                                              "dram_bytes_per_ray")},
+                "ncu": {k: c[k] for k in ("issue_active_pct", "l1tex_throughput_pct", "threads_per_warp_instruction",
+                                          "warps_active_pct")}})
+        out[key] = e
+    top = max(out, key=lambda k: out[k]["stage_ms"])
+    roof = dict(out[top])
+    roof["stages"] = {k: {x: v for x, v in out[k].items() if x not in ("algorithmic_note", "peak_kind",
+                                                                        "traffic_source")} for k in out}
+    roof["stage_ms"] = [round(x, 3) for x in stage_ms]
+    return roof
 
 
 def cpu_model() -> str:
@@ -211,22 +269,24 @@ def ref_renderer(sc):
 
 
 def ref_sample(ref, cam, trace_depth, target_s, nthreads):
-    """A band of rows around the middle of the view sized for about target_s seconds of the
-    reference's RayTracer::rayTrace per pixel on nthreads threads, and its ray count (primary
-    + shadow + secondary, replayed once outside any timing)."""
+    """Pixels spread evenly over the whole view (every k-th pixel), as many as the reference's
+    RayTracer::rayTrace renders in about target_s seconds on nthreads threads, and their ray
+    count (primary + shadow + secondary, replayed once outside any timing).  The reference
+    is slow on this scene (its depth-limited tree has leaves of up to 438 triangles), so the
+    sample is a small strided subset of the frame."""
     import numpy as np
-    W, H = cam.width, cam.height
+    n = cam.width * cam.height
 
-    def band(rows):
-        y0 = max(0, H // 2 - rows // 2)
-        return np.arange(y0 * W, min(H, y0 + rows) * W, dtype=np.int32)
+    def strided(count):
+        step = max(1, n // max(1, count))
+        return np.arange(step // 2, n, step, dtype=np.int32)[:count]
 
-    probe = band(8)
+    probe = strided(512)
     r = ref.render(cam, trace_depth, pixel_offset=0.5, pixels=probe, nthreads=nthreads, paths=False)
-    rows = int(min(H, max(8, 8 * target_s / max(r["seconds"], 1e-3))))
-    pix = band(rows)
+    count = int(min(n, max(256, len(probe) * target_s / max(r["seconds"], 1e-3))))
+    pix = strided(count)
     counts = ref.render(cam, trace_depth, pixel_offset=0.5, pixels=pix, nthreads=nthreads)["counts"]
-    return pix, int(counts.sum()), rows
+    return pix, int(counts.sum())
 
 
 def ref_timed(ref, cam, trace_depth, pix, nthreads):
@@ -243,14 +303,14 @@ def cpu_baseline(sc, cam, trace_depth, budget_s=15.0):
     if ref is None:
         port["note"] = "reference tree file absent (oracle/make_ref_tree.py): the port is reported"
         return port
-    pix, rays, rows = ref_sample(ref, cam, trace_depth, budget_s / 3.0, nthreads)
+    pix, rays = ref_sample(ref, cam, trace_depth, budget_s / 4.0, nthreads)
     secs = [ref_timed(ref, cam, trace_depth, pix, nthreads) for _ in range(3)]
     sec = statistics.median(secs)
     return {"value": rays / sec / 1e6, "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
             "cpu": cpu_model(),
-            "sample": f"rows {rows} x {cam.width} px around the middle of the 1080p view through the reference's "
-                      f"RayTracer::rayTrace (oracle/_ref/libeosref.so, its own tree), {nthreads} threads, "
-                      f"median of 3",
+            "sample": f"{len(pix)} pixels spread evenly over the 1080p view ({rays} rays) through the reference's "
+                      f"RayTracer::rayTrace (oracle/_ref/libeosref.so, the tree of its own builder), "
+                      f"{nthreads} threads, median of 3",
             "rays": rays, "seconds": sec,
             "port": {"value": round(port["value"], 3), "unit": "Mrays/s", "cores": port["cores"],
                      "sample": port["sample"]}}
@@ -281,8 +341,8 @@ def port_baseline(sc, cam, trace_depth, budget_s=15.0):
 
 def run_reference(args, rank, world):
     """The reference's own CPU renderer on the host cores for the same metric and view: one
-    step = a band of rows of the 1080p view (about 3 s of work) through RayTracer::rayTrace,
-    all host threads; the tree is the one the reference's builder made for this scene,
+    step = a strided sample of the 1080p view's pixels (about 3 s of work) through
+    RayTracer::rayTrace, all host threads; the tree is the one the reference's builder made for this scene,
     restored from oracle/_ref/config2_tree.npz (the build itself takes ~10 min on one core)."""
     if rank != 0:
         return
@@ -294,7 +354,7 @@ def run_reference(args, rank, world):
     workload = ("1920x1080 view of the 1,056,768-tri scene (height field 128^2 + 200 level-4 icospheres), "
                 "depth 3, 4 lights, 1 spp at pixel centres")
     if ref is not None:
-        pix, rays, rows = ref_sample(ref, cam, 2, 3.0, nthreads)
+        pix, rays = ref_sample(ref, cam, 2, 3.0, nthreads)
         secs = []
         for i in range(args.warmup + args.steps):
             sec = ref_timed(ref, cam, 2, pix, nthreads)
@@ -302,8 +362,9 @@ def run_reference(args, rank, world):
                 secs.append(sec)
         v = rays * len(secs) / sum(secs) / 1e6
         cpu = {"value": v, "unit": "Mrays/s", "cores": nthreads, "kind": "reference", "cpu": cpu_model(),
-               "sample": f"per step rows {rows} x {cam.width} px around the middle of the view through the "
-                         f"reference's RayTracer::rayTrace (oracle/_ref/libeosref.so, its own tree)"}
+               "sample": f"per step {len(pix)} pixels spread evenly over the view ({rays} rays) through the "
+                         f"reference's RayTracer::rayTrace (oracle/_ref/libeosref.so, the tree of its own "
+                         f"builder)"}
     else:
         res, info = [], None
         for i in range(args.warmup + args.steps):
@@ -481,32 +542,16 @@ def run_ours(args, rank, world, local):
 
     # roofline of the dominant kernel: per-stage device time of the wavefront (eager, one step)
     st = api.render_batch(ctx, jobs, outs, stage_timing=True)
-    peak, peak_kind = measured_peak()
     shadow_bytes, closest_bytes = algorithmic_bytes(st, info["width"])
     stage = st["stage_ms"]
-    alg = {"closest": (closest_bytes, stage[0]), "shadow": (shadow_bytes, stage[1])}
-    top = max(alg, key=lambda k: alg[k][1])
-    bytes_top, ms_top = alg[top]
     # one launch per bounce per chunk; the library's chunk rule: at most 2^24 paths (8x4-pixel
     # tiles) and at most 8 GB of queues at (3 x 32 + 4 + 32 x lights + 16 x (depth + 1)) B per path
     paths = sum(((c.width + 7) // 8) * ((c.height + 3) // 4) * 32 for c in cams)
     per_path = 3 * 32 + 4 + 32 * max(1, sc.n_lights) + 16 * (td + 1)
     chunk = max(1 << 16, min(1 << 24, (8 << 30) // per_path))
-    launches_top = (td + 1) * int(np.ceil(paths / float(chunk)))
-    achieved = bytes_top / (ms_top * 1e-3) / 1e9
-    traffic = profile_traffic().get(top)
-    rays_top = (st["shadow_rays"] if top == "shadow" else st["primary_rays"] + st["secondary_rays"])
-    roof = {"bound": "hbm", "kernel": "k_wf_any" if top == "shadow" else "k_wf_closest",
-            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "peak_kind": peak_kind,
-            "traffic": (round(traffic["dram_bytes_per_ray"] * rays_top / launches_top) if traffic else None),
-            "traffic_source": ("ncu capture of the same kernel, cold caches, DRAM bytes per ray x rays per launch"
-                               if traffic else None),
-            # what binds this kernel: instruction issue on partly divergent warps (same ncu capture)
-            "issue_active_pct": traffic.get("issue_active_pct") if traffic else None,
-            "threads_per_warp_instruction": traffic.get("threads_per_warp_instruction") if traffic else None,
-            "algorithmic_bytes_per_launch": round(bytes_top / launches_top), "launches": launches_top,
-            "ms_per_launch": round(ms_top / launches_top, 4), "stage_ms": [round(x, 3) for x in stage]}
+    launches_stage = (td + 1) * int(np.ceil(paths / float(chunk)))
+    sm_hz = (clk.summary()["sm_mhz"] or 1965.0) * 1e6
+    roof = roofline(profile_traffic(), st, stage, shadow_bytes, closest_bytes, launches_stage, sm_hz)
 
     # adjoint: forward (with path records) + backward per view, config-4 style parameters
     adj = None
@@ -570,8 +615,8 @@ def run_ours(args, rank, world, local):
     if stress5:
         line["config5_stress"] = stress5
     if cpu:
-        line["cpu_baseline"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items()
-                                if k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"] = {k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in cpu.items()
+                                if k in ("value", "unit", "cores", "kind", "sample", "cpu", "port", "note")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.set_stream(None)

@@ -53,6 +53,8 @@ class RenderParams(Structure):
 
 
 FLAG_STAGE_TIMING = 1
+FLAG_TREE_RECORDS = 2
+FLAG_AA_GRID = 4
 
 
 class Tuning(Structure):
@@ -112,6 +114,7 @@ class Grads(Structure):
 SIGNATURES = [
     ("eos_abi_version", c_int32, []),
     ("eos_status_string", c_char_p, [c_int32]),
+    ("eos_last_error_detail", c_char_p, []),
     ("eos_device_count", c_int32, [POINTER(c_int32)]),
     ("eos_ctx_create", c_int32, [c_int32, POINTER(c_void_p)]),
     ("eos_ctx_destroy", c_int32, [c_void_p]),
@@ -174,4 +177,7 @@ def load(path: str = LIB_PATH):
 
 def check(code: int, where: str) -> None:
     if code != 0:
-        raise EosError(code, where)
+        detail = ""
+        if code in (2, 3) and _lib is not None:
+            detail = (_lib.eos_last_error_detail() or b"").decode()
+        raise EosError(code, where + (f" [{detail}]" if detail else ""))

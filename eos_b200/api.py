@@ -37,8 +37,14 @@ def camera_struct(cam: CameraData) -> L.Camera:
     return c
 
 
+def tree_nodes(trace_depth: int) -> int:
+    """Nodes of a tree-form path record: 2^(trace_depth + 1) - 1 (EOS_TREE_NODES)."""
+    return (1 << (int(trace_depth) + 1)) - 1
+
+
 def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="plain", block_size=0,
-                  queue_chunk=0, stack_depth=0, stage_timing=False, rows=None) -> L.RenderParams:
+                  queue_chunk=0, stack_depth=0, stage_timing=False, rows=None,
+                  tree_records=False, aa_grid=False) -> L.RenderParams:
     p = L.RenderParams()
     p.trace_depth = int(trace_depth)
     p.pixel_offset = float(pixel_offset)
@@ -48,7 +54,8 @@ def params_struct(trace_depth=1, pixel_offset=0.5, spp=1, jitter_seed=0, mode="p
     p.block_size = int(block_size)
     p.queue_chunk = int(queue_chunk)
     p.stack_depth = int(stack_depth)
-    p.flags = L.FLAG_STAGE_TIMING if stage_timing else 0
+    p.flags = ((L.FLAG_STAGE_TIMING if stage_timing else 0) | (L.FLAG_TREE_RECORDS if tree_records else 0)
+               | (L.FLAG_AA_GRID if aa_grid else 0))
     if rows is not None:
         p.row_begin, p.row_end = int(rows[0]), int(rows[1])
     return p
@@ -238,15 +245,19 @@ def render(ctx: Context, scene: DeviceScene, cam: CameraData, trace_depth: int, 
     """Render one frame; returns the requested outputs plus 'stats'.
 
     outputs: any of 'rgb' [H*W,3] f32, 'rgba8' [H,W,4] u8, 'hit' [H*W*spp] i32,
-    'paths' [H*W*spp, 16] i32 (8 hit ids then 8 shadow masks per path).  rows=(r0, r1) in
-    `tuning` renders image rows [r0, r1) only (split-frame); H is then r1 - r0.
+    'paths' [H*W*spp, 16] i32 (8 hit ids then 8 shadow masks per path; with
+    tree_records=True in `tuning`, [H*W*spp, tree_nodes(trace_depth), 2]: hit id and shadow
+    mask per ray-tree node).  rows=(r0, r1) in `tuning` renders image rows [r0, r1) only
+    (split-frame); H is then r1 - r0.
     """
     rows = tuning.get("rows")
     H = (rows[1] - rows[0]) if rows is not None else cam.height
     npx = cam.width * H
     res = dict(out or {})
     shapes = {"rgb": ((npx, 3), np.float32), "rgba8": ((H, cam.width, 4), np.uint8),
-              "hit": ((npx * spp,), np.int32), "paths": ((npx * spp, 16), np.int32)}
+              "hit": ((npx * spp,), np.int32),
+              "paths": ((npx * spp, tree_nodes(trace_depth), 2) if tuning.get("tree_records") else (npx * spp, 16),
+                        np.int32)}
     for k in outputs:
         if k not in res:
             res[k] = _alloc(shapes[k][0], shapes[k][1], device)
@@ -271,7 +282,7 @@ class BatchJob:
     rows: tuple | None = None  # image rows [r0, r1) only
 
 
-def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",)):
+def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",), tree_records: bool = False):
     outs = []
     for j in jobs:
         H = (j.rows[1] - j.rows[0]) if j.rows is not None else j.camera.height
@@ -282,7 +293,8 @@ def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",)):
         if "rgba8" in outputs:
             o["rgba8"] = _alloc((H, j.camera.width, 4), np.uint8, True)
         if "paths" in outputs:
-            o["paths"] = _alloc((npx * j.spp, 16), np.int32, True)
+            shape = (npx * j.spp, tree_nodes(j.trace_depth), 2) if tree_records else (npx * j.spp, 16)
+            o["paths"] = _alloc(shape, np.int32, True)
         outs.append(o)
     return outs
 
@@ -311,12 +323,13 @@ def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning)
 
 def render_backward(ctx: Context, scene: DeviceScene, cams: list[CameraData], trace_depth: int, paths, d_rgb,
                     pixel_offset: float = 0.5, device: bool = True, spp: int = 1, jitter_seed: int = 0,
-                    rows=None):
+                    rows=None, tree_records: bool = False, aa_grid: bool = False):
     """Adjoint of the shading: returns (grad_materials [K,7], grad_lights [L,6]).  paths come
     from the forward render with the same spp / jitter_seed / pixel_offset (and row band
     `rows`, whose gradients are that band's share of the frame's)."""
     arr = (L.Camera * len(cams))(*[camera_struct(c) for c in cams])
-    p = params_struct(trace_depth, pixel_offset, spp, jitter_seed, rows=rows)
+    p = params_struct(trace_depth, pixel_offset, spp, jitter_seed, rows=rows, tree_records=tree_records,
+                      aa_grid=aa_grid)
     info = scene.info()
     K = info["n_objects"]
     NL = max(1, info["n_lights"])

@@ -22,7 +22,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libeos_b200.so")
 SOURCES = ["api.cu", "lbvh.cu", "ploc.cu", "instances.cu", "scene_io.cu", "render.cu", "wavefront.cu", "adjoint.cu", "mesh.cpp"]
-HEADERS = ["eos_math.cuh", "eos_internal.cuh", "trace.cuh"]
+HEADERS = ["eos_math.cuh", "eos_internal.cuh", "trace.cuh", "scan.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -65,7 +65,9 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
             raise RuntimeError(f"nvcc failed: {' '.join(c)}")
     if force or jobs or not os.path.exists(LIB) or _mtime(LIB) < max(_mtime(o) for o in objs):
         tmp = LIB + ".tmp"
-        cmd = [nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-cudart", "static"]
+        # -z defs: a symbol left undefined fails the link instead of the first load
+        cmd = [nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-cudart", "static",
+                                                             "-Xlinker", "-z", "-Xlinker", "defs"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

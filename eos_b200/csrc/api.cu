@@ -2,6 +2,7 @@
 // staging, error words and statistics.  The kernels live in lbvh.cu, render.cu,
 // wavefront.cu and adjoint.cu.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -44,6 +45,16 @@ void* scratch(eos_ctx* ctx, const char* name, size_t bytes, eos_status* st) {
   }
   b.bytes = want;
   return b.ptr;
+}
+
+namespace {
+thread_local char g_error_detail[192] = "";
+}
+
+void note_cuda_error(cudaError_t e, const char* file, int line) {
+  const char* base = std::strrchr(file, '/');
+  std::snprintf(g_error_detail, sizeof g_error_detail, "%s (%s) at %s:%d", cudaGetErrorName(e),
+                cudaGetErrorString(e), base ? base + 1 : file, line);
 }
 
 bool is_device_ptr(const void* p) {
@@ -143,8 +154,15 @@ eos_status check_params(const eos_render_params* p) {
   if (p->trace_depth < 0 || p->trace_depth >= EOS_MAX_BOUNCES) return EOS_ERR_INVALID_ARG;
   if (p->spp < 1 || p->spp > 1024) return EOS_ERR_INVALID_ARG;
   if (p->mode != EOS_MODE_PLAIN && p->mode != EOS_MODE_WAVEFRONT) return EOS_ERR_INVALID_ARG;
-  if (p->flags & ~EOS_FLAG_STAGE_TIMING) return EOS_ERR_INVALID_ARG;
+  if (p->flags & ~(EOS_FLAG_STAGE_TIMING | EOS_FLAG_TREE_RECORDS | EOS_FLAG_AA_GRID)) return EOS_ERR_INVALID_ARG;
+  if ((p->flags & EOS_FLAG_AA_GRID) && aa_grid_side(p->spp) == 0) return EOS_ERR_INVALID_ARG;
   return EOS_OK;
+}
+
+// Bytes of one path record: eos_path_record, or the tree form's nodes.
+size_t record_bytes(int flags, int trace_depth) {
+  return (flags & EOS_FLAG_TREE_RECORDS) ? sizeof(eos_tree_node) * EOS_TREE_NODES(trace_depth)
+                                         : sizeof(eos_path_record);
 }
 
 // Row band [rb, re) of an image of h rows; 0, 0 = all rows.
@@ -179,6 +197,8 @@ eos_render_params eos::with_tuning(const eos_ctx* ctx, const eos_render_params& 
 extern "C" {
 
 int32_t eos_abi_version(void) { return EOS_ABI_VERSION; }
+
+const char* eos_last_error_detail(void) { return g_error_detail; }
 
 const char* eos_status_string(eos_status s) {
   switch (s) {
@@ -369,16 +389,16 @@ eos_status eos_scene_destroy(eos_scene* sc) {
 eos_status eos_scene_set_materials(eos_scene* sc, const eos_material* m, uint32_t n) {
   if (!sc || !m || n != (uint32_t)sc->dev.n_obj) return EOS_ERR_INVALID_ARG;
   EOS_CUDA(cudaSetDevice(sc->ctx->device));
-  // a material both reflective and transparent would need two secondary rays per hit
+  // a material both reflective and transparent spawns two secondary rays per hit: the
+  // scene then renders in ray-tree form
   std::vector<eos_material> host(n);
   const bool dev = is_device_ptr(m);
   if (dev) EOS_CUDA(cudaMemcpy(host.data(), m, sizeof(eos_material) * n, cudaMemcpyDeviceToHost));
   else std::memcpy(host.data(), m, sizeof(eos_material) * n);
-  for (const eos_material& e : host)
-    if (e.reflectivity > 0.0f && e.transparency > 0.0f) return EOS_ERR_UNSUPPORTED;
   EOS_CUDA(cudaMemcpyAsync(sc->d_mats, m, sizeof(eos_material) * n,
                            dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, sc->ctx->stream));
   EOS_CUDA(cudaStreamSynchronize(sc->ctx->stream));
+  sc->branching = has_branching(host.data(), n);
   return EOS_OK;
 }
 
@@ -434,6 +454,8 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, 
   eos_status st = check_params(p);
   if (st != EOS_OK) return st;
   if (!valid_rows(cam->height, p->row_begin, p->row_end)) return EOS_ERR_INVALID_ARG;
+  const bool tree_records = (p->flags & EOS_FLAG_TREE_RECORDS) != 0;
+  if (paths_out && sc->branching && !tree_records) return EOS_ERR_UNSUPPORTED;  // one hit per bounce cannot hold a tree
   if ((st = set_device(ctx)) != EOS_OK) return st;
   const size_t npx = (size_t)cam->width * band_rows(cam->height, p->row_begin, p->row_end);
   const size_t npath = npx * p->spp;
@@ -441,13 +463,13 @@ eos_status eos_render(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cam, 
   if ((st = out_buf(ctx, "out.rgb", rgb_out, 12 * npx, o_rgb)) != EOS_OK) return st;
   if ((st = out_buf(ctx, "out.rgba8", rgba8_out, 4 * npx, o_q)) != EOS_OK) return st;
   if ((st = out_buf(ctx, "out.hit", hit_out, 4 * npath, o_hit)) != EOS_OK) return st;
-  if ((st = out_buf(ctx, "out.paths", paths_out, sizeof(eos_path_record) * npath, o_paths)) != EOS_OK) return st;
+  if ((st = out_buf(ctx, "out.paths", paths_out, record_bytes(p->flags, p->trace_depth) * npath, o_paths)) != EOS_OK)
+    return st;
   if ((st = begin_call(ctx)) != EOS_OK) return st;
   EOS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   if (p->mode == EOS_MODE_PLAIN) {
     st = render_plain(ctx, sc, *cam, with_tuning(ctx, *p, (uint32_t)sc->dev.n_tris), (float*)o_rgb.dev,
-                      (uint8_t*)o_q.dev, (int32_t*)o_hit.dev,
-                      (eos_path_record*)o_paths.dev);
+                      (uint8_t*)o_q.dev, (int32_t*)o_hit.dev, o_paths.dev, tree_records || sc->branching);
   } else {
     if (hit_out) return EOS_ERR_UNSUPPORTED;  // per-path hits come from paths_out in this mode
     eos_job job;
@@ -485,6 +507,8 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     if (!jb.scene || !valid_camera(&jb.camera) || jb.trace_depth < 0 || jb.trace_depth >= EOS_MAX_BOUNCES ||
         jb.spp < 1 || jb.spp > 1024 || !valid_rows(jb.camera.height, jb.row_begin, jb.row_end))
       return EOS_ERR_INVALID_ARG;
+    if (jb.paths_out && jb.scene->branching && !(p->flags & EOS_FLAG_TREE_RECORDS)) return EOS_ERR_UNSUPPORTED;
+    if ((p->flags & EOS_FLAG_AA_GRID) && aa_grid_side(jb.spp) == 0) return EOS_ERR_INVALID_ARG;
   }
   if ((st = set_device(ctx)) != EOS_OK) return st;
   // host output buffers are staged through one device buffer and copied back at the end
@@ -504,7 +528,7 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     const size_t npx = (size_t)jb.camera.width * band_rows(jb.camera.height, jb.row_begin, jb.row_end);
     plan(jb.rgb_out, 12 * npx);
     plan(jb.rgba8_out, 4 * npx);
-    plan(jb.paths_out, sizeof(eos_path_record) * npx * jb.spp);
+    plan(jb.paths_out, record_bytes(p->flags, jb.trace_depth) * npx * jb.spp);
   }
   char* stage = nullptr;
   if (staged) {
@@ -547,11 +571,11 @@ eos_status eos_render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_came
     if (!valid_camera(&cams[v]) || cams[v].width != cams[0].width || cams[v].height != cams[0].height)
       return EOS_ERR_INVALID_ARG;
   if (!valid_rows(cams[0].height, p->row_begin, p->row_end)) return EOS_ERR_INVALID_ARG;
+  if (sc->branching && !(p->flags & EOS_FLAG_TREE_RECORDS)) return EOS_ERR_UNSUPPORTED;  // chain records of a tree
   if ((st = set_device(ctx)) != EOS_OK) return st;
   const size_t npx = (size_t)n_views * cams[0].width * band_rows(cams[0].height, p->row_begin, p->row_end);
   if ((st = begin_call(ctx)) != EOS_OK) return st;
-  const eos_path_record* dp = (const eos_path_record*)stage_in(ctx, "bw.paths", paths,
-                                                                 sizeof(eos_path_record) * npx * p->spp, &st);
+  const void* dp = stage_in(ctx, "bw.paths", paths, record_bytes(p->flags, p->trace_depth) * npx * p->spp, &st);
   const float* dg = (const float*)stage_in(ctx, "bw.drgb", d_rgb, 12 * npx, &st);
   if (st != EOS_OK) return st;
   OutBuf o_m, o_l;

@@ -142,6 +142,7 @@ struct eos_scene {
   void* d_order = nullptr;  // sorted triangle ids
   void* d_inst = nullptr;   // DevInstance array of a two-level scene
   bool instanced = false;
+  bool branching = false;   // some material is both reflective and transparent: ray trees
   int mesh_levels = 0;      // deepest mesh tree of a two-level scene (stack bound)
   uint32_t n_nodes = 0;
   int leaf_size = 8;
@@ -171,6 +172,13 @@ eos_status build_scene(eos_ctx* ctx, eos_scene* sc, const float* d_verts, const 
 eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi, int2* child, int2* range,
                       int* parent, uint32_t* perm, int* depth);
 
+// True when some material is both reflective and transparent (the scene renders ray trees).
+inline bool has_branching(const eos_material* m, uint32_t n) {
+  for (uint32_t i = 0; i < n; ++i)
+    if (m[i].reflectivity > 0.0f && m[i].transparency > 0.0f) return true;
+  return false;
+}
+
 // Parameters left at 0 take the context's tuned values for a scene of n_tris triangles.
 eos_render_params with_tuning(const eos_ctx* ctx, const eos_render_params& p, uint32_t n_tris);
 
@@ -189,7 +197,7 @@ struct RenderArgs {
 };
 eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam,
                         const eos_render_params& p, float* rgb, uint8_t* rgba8, int32_t* hit,
-                        eos_path_record* paths);
+                        void* paths, bool tree);
 eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs,
                             const eos_render_params& p, bool use_graph);
 eos_status trace_closest(eos_ctx* ctx, const eos_scene* sc, const float* d_rays, uint32_t n,
@@ -197,15 +205,21 @@ eos_status trace_closest(eos_ctx* ctx, const eos_scene* sc, const float* d_rays,
 eos_status trace_any(eos_ctx* ctx, const eos_scene* sc, const float* d_rays, uint32_t n,
                      uint8_t* d_occ);
 eos_status render_backward(eos_ctx* ctx, const eos_scene* sc, const eos_camera* cams, uint32_t n_views,
-                           const eos_render_params& p, const eos_path_record* d_paths,
+                           const eos_render_params& p, const void* d_paths,
                            const float* d_rgb, float* d_gmat, float* d_glight);
 
+}  // namespace eos
+
+namespace eos {
+// Records a failing CUDA call for eos_last_error_detail (per host thread).
+void note_cuda_error(cudaError_t e, const char* file, int line);
 }  // namespace eos
 
 #define EOS_CUDA(call)                                   \
   do {                                                   \
     cudaError_t e_ = (call);                             \
     if (e_ != cudaSuccess) {                             \
+      eos::note_cuda_error(e_, __FILE__, __LINE__);      \
       if (e_ == cudaErrorMemoryAllocation) return EOS_ERR_OOM; \
       return EOS_ERR_CUDA;                               \
     }                                                    \

@@ -118,9 +118,30 @@ EOS_HD uint32_t hash32(uint32_t x) {
   return x;
 }
 
+// Side of the reference's anti-aliasing grid for spp samples per pixel (EOS_FLAG_AA_GRID):
+// n with n * n == spp, else 0.
+EOS_HD int aa_grid_side(int spp) {
+  int n = 1;
+  while (n * n < spp) ++n;
+  return n * n == spp ? n : 0;
+}
+
+// 1 / n as the reference computes it, `1.0 / (float) aaSamples` (double, then float).
+EOS_HD float aa_grid_step(int n) { return (float)(1.0 / (double)(float)n); }
+
 // Sub-pixel position of sample `s` of pixel `p`: the fixed offset for one sample per
-// pixel, a hashed jitter in [0, 1) otherwise.
-EOS_HD void sample_offset(uint32_t p, int s, int spp, uint32_t seed, float off, float& ox, float& oy) {
+// pixel; with grid = n > 0 the reference's n x n anti-aliasing grid
+// (RayTracer::renderWithAA, src/RayTracer.cpp:214-233): sample s = q n + p at
+// ((p + ksi) step, (q + ksi) step), ksi = rand() / RAND_MAX in integer arithmetic = 0;
+// otherwise a hashed jitter in [0, 1).
+EOS_HD void sample_offset(uint32_t p, int s, int spp, uint32_t seed, float off, float& ox, float& oy,
+                          int grid = 0) {
+  if (grid > 0) {
+    const float step = aa_grid_step(grid);
+    ox = (float)(s % grid) * step;
+    oy = (float)(s / grid) * step;
+    return;
+  }
   if (spp <= 1) {
     ox = off;
     oy = off;
@@ -130,6 +151,16 @@ EOS_HD void sample_offset(uint32_t p, int s, int spp, uint32_t seed, float off, 
   uint32_t h2 = hash32(h1 ^ 0x68E31DA4u);
   ox = (float)(h1 >> 8) * (1.0f / 16777216.0f);
   oy = (float)(h2 >> 8) * (1.0f / 16777216.0f);
+}
+
+// Weight of one sample in its pixel: 1 / spp, or on the reference's grid its
+// inv_aaSamplesSquared = step * step (src/RayTracer.cpp:212,237).
+EOS_HD float sample_weight(int spp, int grid) {
+  if (grid > 0) {
+    const float step = aa_grid_step(grid);
+    return step * step;
+  }
+  return 1.0f / (float)spp;
 }
 
 // 30-bit Morton code: two zero bits inserted after each of the 10 low bits of x, y, z,

@@ -10,9 +10,9 @@
 // Primitive order = stable sort by (code, triangle id).
 #include <algorithm>
 
-#include <cub/device/device_scan.cuh>
 
 #include "eos_internal.cuh"
+#include "scan.cuh"
 
 namespace eos {
 namespace {
@@ -357,17 +357,14 @@ __device__ __forceinline__ void write_record(float4* o, const float (&v)[6][4], 
 // record of their own; after an exclusive scan of the counts, k_wide_write numbers them
 // base + scan[t] + j and writes the record.  Records come out level by level, each node's
 // children in consecutive records, the same on every run.
-__global__ void k_wide_select(int n, const int2* __restrict__ child, const float4* __restrict__ blo,
-                              const float4* __restrict__ bhi, const int2* __restrict__ frontier_in, int n_in,
-                              int max_children, int4* __restrict__ sel, int* __restrict__ n_interior) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t > n_in) return;
-  if (t == n_in) {  // the scan's total
-    n_interior[t] = 0;
-    return;
-  }
+// Greedy opening of one frontier node (k_wide_select): its children, then the children of
+// the largest-area interior child until max_children are reached; returns how many of
+// them get records of their own.
+__device__ __forceinline__ int wide_select_one(int n, const int2* __restrict__ child, const float4* __restrict__ blo,
+                                               const float4* __restrict__ bhi, int node, int max_children,
+                                               int4& sel) {
   int c[4] = {-1, -1, -1, -1};
-  const int2 ch = child[frontier_in[t].x];
+  const int2 ch = child[node];
   c[0] = ch.x;
   c[1] = ch.y;
   int k = 2;
@@ -390,19 +387,39 @@ __global__ void k_wide_select(int n, const int2* __restrict__ child, const float
   }
   int m = 0;
   for (int i = 0; i < k; ++i) m += c[i] < n - 1 && bhi[c[i]].w == 0.0f;
-  sel[t] = make_int4(c[0], c[1], c[2], c[3]);
-  n_interior[t] = m;
+  sel = make_int4(c[0], c[1], c[2], c[3]);
+  return m;
 }
 
-__global__ void k_wide_write(int n, const int2* __restrict__ range, const float4* __restrict__ blo,
-                             const float4* __restrict__ bhi, const int2* __restrict__ frontier_in, int n_in,
-                             const int4* __restrict__ sel, const int* __restrict__ first, int base,
-                             int2* __restrict__ frontier_out, float4* __restrict__ wnodes, int max_nodes, int* err) {
+__global__ void __launch_bounds__(kScanBlock) k_wide_select(int n, const int2* __restrict__ child,
+                                                            const float4* __restrict__ blo,
+                                                            const float4* __restrict__ bhi,
+                                                            const int2* __restrict__ frontier_in, int n_in,
+                                                            int max_children, int4* __restrict__ sel,
+                                                            int* __restrict__ n_interior, int* __restrict__ bsum) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = t < n_in ? wide_select_one(n, child, blo, bhi, frontier_in[t].x, max_children, sel[t]) : 0;
+  if (t < n_in) n_interior[t] = m;
+  block_total(m, bsum);  // the scan's first step (scan.cuh)
+}
+
+// The first record number of frontier node t's children: its block's exclusive scan of n_interior
+// plus the block's scanned sum (bsum after k_scan_totals); same grid as k_wide_select.
+__global__ void __launch_bounds__(kScanBlock) k_wide_write(int n, const int2* __restrict__ range,
+                                                           const float4* __restrict__ blo,
+                                                           const float4* __restrict__ bhi,
+                                                           const int2* __restrict__ frontier_in, int n_in,
+                                                           const int4* __restrict__ sel,
+                                                           const int* __restrict__ n_interior,
+                                                           const int* __restrict__ bsum, int base,
+                                                           int2* __restrict__ frontier_out,
+                                                           float4* __restrict__ wnodes, int max_nodes, int* err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int block_sum;
+  int next = bsum[blockIdx.x] + block_exclusive_scan(t < n_in ? n_interior[t] : 0, block_sum);
   if (t >= n_in) return;
   const int4 s4 = sel[t];
   const int c[4] = {s4.x, s4.y, s4.z, s4.w};
-  int next = first[t];
   float v[6][4];
   int ref[4], cnt[4];
   for (int i = 0; i < 4; ++i) {
@@ -473,22 +490,21 @@ eos_status write_records(eos_ctx* ctx, int n, const int2* child, const int2* ran
   int2* fb = (int2*)scratch(ctx, "lbvh.wide.fb", 8 * nn, &es);
   int4* sel = (int4*)scratch(ctx, "lbvh.wide.sel", 16 * nn, &es);
   int* m = (int*)scratch(ctx, "lbvh.wide.m", 4 * (nn + 1), &es);
-  int* first = (int*)scratch(ctx, "lbvh.wide.first", 4 * (nn + 1), &es);
-  size_t temp_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, m, first, n + 1, st);
-  void* temp = scratch(ctx, "lbvh.wide.scan_temp", std::max<size_t>(temp_bytes, 16), &es);
+  int* bsum = (int*)scratch(ctx, "lbvh.wide.bsum", 4 * ((size_t)scan_blocks(n + 1) + 1), &es);
   if (es != EOS_OK) return es;
   const int2 root = make_int2(0, 0);  // the binary root becomes record 0
   EOS_CUDA(cudaMemcpyAsync(fa, &root, sizeof root, cudaMemcpyHostToDevice, st));
   int n_in = 1, base = 1, lv = 0;
   while (n_in > 0 && lv <= 4 * kStackMax) {  // bounded: the depth is at most the binary depth
-    k_wide_select<<<grid_for((size_t)n_in + 1, 128), 128, 0, st>>>(n, child, blo, bhi, fa, n_in, width, sel, m);
-    EOS_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, m, first, n_in + 1, st));
-    k_wide_write<<<grid_for(n_in, 128), 128, 0, st>>>(n, range, blo, bhi, fa, n_in, sel, first, base, fb, out,
-                                                       max_nodes, ctx->d_err);
+    const int nb = scan_blocks(n_in);
+    k_wide_select<<<nb, kScanBlock, 0, st>>>(n, child, blo, bhi, fa, n_in, width, sel, m, bsum);
+    k_scan_totals<<<1, 1024, 0, st>>>(bsum, nb);
+    k_wide_write<<<nb, kScanBlock, 0, st>>>(n, range, blo, bhi, fa, n_in, sel, m, bsum, base, fb, out, max_nodes,
+                                            ctx->d_err);
+    EOS_CUDA(cudaGetLastError());
     ++lv;
     int n_out = 0;
-    EOS_CUDA(cudaMemcpyAsync(&n_out, first + n_in, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EOS_CUDA(cudaMemcpyAsync(&n_out, bsum + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
     EOS_CUDA(cudaStreamSynchronize(st));
     if ((long long)base + n_out > max_nodes) return EOS_ERR_QUEUE_OVERFLOW;  // cannot happen, as above
     base += n_out;

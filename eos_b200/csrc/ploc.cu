@@ -18,9 +18,9 @@
 #include <algorithm>
 #include <vector>
 
-#include <cub/device/device_scan.cuh>
 
 #include "eos_internal.cuh"
+#include "scan.cuh"
 
 namespace eos {
 namespace {
@@ -81,41 +81,48 @@ __global__ void k_ploc_nn(const int* __restrict__ state, const float4* __restric
 // pairs (2k, 2k + 1) merge instead, which bounds the number of iterations.
 // keep in the low 32 bits, make in the high 32 bits: one scan counts both.
 // The scan runs over nc_ub + 1 entries (nc_ub: the host's upper bound of nc); the entries
-// from nc on are 0, so the scan's value at nc is the round's total.
-__global__ void k_ploc_flags(const int* __restrict__ state, int nc_ub, const int* __restrict__ nn, int force,
-                             unsigned long long* __restrict__ km) {
+// from nc on are 0, so the scan's value at nc is the round's total.  Each block of
+// kScanBlock entries also writes its sum to bsum (the scan's first step, scan.cuh).
+__global__ void __launch_bounds__(kScanBlock) k_ploc_flags(const int* __restrict__ state, int nc_ub,
+                                                           const int* __restrict__ nn, int force,
+                                                           unsigned long long* __restrict__ km,
+                                                           unsigned long long* __restrict__ bsum) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = state[0];
-  if (i > nc_ub) return;
-  if (i >= nc) {
-    km[i] = 0ull;
-    return;
+  unsigned long long v = 0ull;
+  if (i < nc) {
+    int partner;
+    if (force) {
+      partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
+    } else {
+      const int j = nn[i];
+      partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
+    }
+    const unsigned long long keep = partner < 0 || i < partner;
+    const unsigned long long make = partner >= 0 && i < partner;
+    v = keep | (make << 32);
   }
-  int partner;
-  if (force) {
-    partner = (i & 1) ? i - 1 : (i + 1 < nc ? i + 1 : -1);
-  } else {
-    const int j = nn[i];
-    partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
-  }
-  const unsigned long long keep = partner < 0 || i < partner;
-  const unsigned long long make = partner >= 0 && i < partner;
-  km[i] = keep | (make << 32);
+  if (i <= nc_ub) km[i] = v;
+  block_total(v, bsum);
 }
 
 // Also writes the next round's state (clusters kept, nodes made so far, nodes made by this
-// round) to state_out and to the host's read-back slot.
-__global__ void k_ploc_merge(const int* __restrict__ state, int* __restrict__ state_out, int* __restrict__ slot,
-                             const int* __restrict__ nn, int force,
-                             const unsigned long long* __restrict__ km_scan, const int* __restrict__ cid,
-                             const float4* __restrict__ lo, const float4* __restrict__ hi, int* __restrict__ cid_out,
-                             float4* __restrict__ lo_out, float4* __restrict__ hi_out, int2* __restrict__ child,
-                             int* __restrict__ count, float4* __restrict__ nlo, float4* __restrict__ nhi, int n) {
+// round) to state_out and to the host's read-back slot.  The exclusive scan of km is this
+// block's scan of its entries plus the block's scanned sum (bsum after k_scan_totals;
+// bsum[n_blocks] = the round's total); same grid as k_ploc_flags.
+__global__ void __launch_bounds__(kScanBlock) k_ploc_merge(
+    const int* __restrict__ state, int* __restrict__ state_out, int* __restrict__ slot, const int* __restrict__ nn,
+    int force, int nc_ub, const unsigned long long* __restrict__ km, const unsigned long long* __restrict__ bsum,
+    int n_blocks, const int* __restrict__ cid, const float4* __restrict__ lo, const float4* __restrict__ hi,
+    int* __restrict__ cid_out, float4* __restrict__ lo_out, float4* __restrict__ hi_out, int2* __restrict__ child,
+    int* __restrict__ count, float4* __restrict__ nlo, float4* __restrict__ nhi, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = state[0], node_base = state[1];
+  unsigned long long block_sum;
+  const unsigned long long sc = bsum[blockIdx.x] + block_exclusive_scan(i <= nc_ub ? km[i] : 0ull, block_sum);
   if (i >= nc) return;
   if (i == 0) {
-    const unsigned long long total = km_scan[nc];
+    const unsigned long long total = bsum[n_blocks];
     const int kept = (int)(total & 0xffffffffull), made = (int)(total >> 32);
     state_out[0] = slot[0] = kept;
     state_out[1] = slot[1] = node_base + made;
@@ -129,7 +136,6 @@ __global__ void k_ploc_merge(const int* __restrict__ state, int* __restrict__ st
     partner = (j >= 0 && j < nc && nn[j] == i) ? j : -1;
   }
   if (partner >= 0 && i > partner) return;  // merged into the lower cluster
-  const unsigned long long sc = km_scan[i];
   const int pos = (int)(sc & 0xffffffffull);
   if (partner < 0) {
     cid_out[pos] = cid[i];
@@ -342,7 +348,7 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   float4* chi[2] = {(float4*)scratch(ctx, "ploc.hi0", 16 * nn, &es), (float4*)scratch(ctx, "ploc.hi1", 16 * nn, &es)};
   int* nbr = (int*)scratch(ctx, "ploc.nn", 4 * nn, &es);
   unsigned long long* km = (unsigned long long*)scratch(ctx, "ploc.km", 8 * (nn + 1), &es);
-  unsigned long long* km_scan = (unsigned long long*)scratch(ctx, "ploc.km_scan", 8 * (nn + 1), &es);
+  unsigned long long* bsum = (unsigned long long*)scratch(ctx, "ploc.bsum", 8 * ((size_t)scan_blocks(n + 1) + 1), &es);
   int2* tchild = (int2*)scratch(ctx, "ploc.child", 8 * nn, &es);
   int* tcount = (int*)scratch(ctx, "ploc.count", 4 * nn, &es);
   float4* tlo = (float4*)scratch(ctx, "ploc.nlo", 16 * nn, &es);
@@ -350,9 +356,6 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   int* tparent = (int*)scratch(ctx, "ploc.parent", 4 * (2 * nn), &es);
   int* first = (int*)scratch(ctx, "ploc.first", 4 * (2 * nn), &es);
   int* dmax = (int*)scratch(ctx, "ploc.depth", 4, &es);
-  size_t temp_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, km, km_scan, n + 1, st);
-  void* temp = scratch(ctx, "ploc.scan_temp", std::max<size_t>(temp_bytes, 16), &es);
   if (es != EOS_OK) return es;
 
   // clusters = leaves in Morton order
@@ -387,12 +390,14 @@ eos_status build_ploc(eos_ctx* ctx, int n, const float4* blo, const float4* bhi,
   long long issued = 0, read = 0;
   auto enqueue = [&](int force) {
     if (!force) k_ploc_nn<<<grid_of(nc_ub, kNNBlock), kNNBlock, 0, st>>>(state + 4 * cur, clo[cur], chi[cur], nbr);
-    k_ploc_flags<<<grid_of(nc_ub + 1, 256), 256, 0, st>>>(state + 4 * cur, nc_ub, nbr, force, km);
-    if (cub::DeviceScan::ExclusiveSum(temp, temp_bytes, km, km_scan, nc_ub + 1, st) != cudaSuccess) return false;
+    const int nb = scan_blocks(nc_ub + 1);
+    k_ploc_flags<<<nb, kScanBlock, 0, st>>>(state + 4 * cur, nc_ub, nbr, force, km, bsum);
+    k_scan_totals<<<1, 1024, 0, st>>>(bsum, nb);
     const int slot = (int)(issued % kAhead);
-    k_ploc_merge<<<grid_of(nc_ub, 256), 256, 0, st>>>(state + 4 * cur, state + 4 * (cur ^ 1), ctx->ring_dev + 4 * slot,
-                                                     nbr, force, km_scan, cid[cur], clo[cur], chi[cur], cid[cur ^ 1],
-                                                     clo[cur ^ 1], chi[cur ^ 1], tchild, tcount, tlo, thi, n);
+    k_ploc_merge<<<nb, kScanBlock, 0, st>>>(state + 4 * cur, state + 4 * (cur ^ 1), ctx->ring_dev + 4 * slot, nbr,
+                                            force, nc_ub, km, bsum, nb, cid[cur], clo[cur], chi[cur], cid[cur ^ 1],
+                                            clo[cur ^ 1], chi[cur ^ 1], tchild, tcount, tlo, thi, n);
+    if (cudaGetLastError() != cudaSuccess) return false;
     if (cudaEventRecord(ctx->ring_ev[slot], st) != cudaSuccess) return false;
     cur ^= 1;
     ++issued;

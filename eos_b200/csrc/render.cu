@@ -19,10 +19,12 @@ struct PlainParams {
   int y0, rows;  // image rows [y0, y0 + rows) are rendered; outputs hold those rows
   float pixel_offset;
   uint32_t jitter_seed;
+  int grid;  // side of the reference's AA grid (EOS_FLAG_AA_GRID), 0 = jitter
   float* rgb;
   uint8_t* rgba8;
   int32_t* hit;
   eos_path_record* paths;
+  eos_tree_node* tree;         // tree-form records (TREE kernel): EOS_TREE_NODES(trace_depth) per path
   int* err;
   unsigned long long* counts;  // kNumCounts traversal counters
 };
@@ -79,10 +81,117 @@ __device__ f3 trace_path(const PlainParams& P, f3 o, f3 d, int32_t* hits, uint32
   return c;
 }
 
+// One shaded node of a ray tree waiting for its children (trace_tree).
+struct TreeFrame {
+  f3 phong, cR;   // the node's Phong sum; its mirror child's colour once known
+  f3 to, td;      // its transparent child's ray
+  float wR, K;    // reflectivity (0: no mirror ray), Fresnel weight of the transparent ray
+  int node, depth;
+  bool has_t;     // transparent ray present
+  bool in_t;      // the child being traced is the transparent one
+};
+
+// A path as a ray tree (materials both reflective and transparent trace both secondary
+// rays, src/RayTracer.cpp:339-407): a post-order walk with an explicit stack of shaded
+// nodes (at most one per bounce), mirror child first as the reference recurses; node
+// colours by tree_colour.  rec (nullable): the path's tree record, heap order.
+template <int SH>
+__device__ f3 trace_tree(const PlainParams& P, f3 o, f3 d, eos_tree_node* rec, int& root_hit, unsigned* cnt,
+                         uint2* shs, int stride) {
+  const DevScene& s = P.s;
+  const f3 campos = mk3(P.cam[0], P.cam[1], P.cam[2]);
+  const f3 zero = mk3(0.0f, 0.0f, 0.0f);
+  TreeFrame st[kMaxBounces];
+  int sp = 0, node = 0, depth = 0;
+  for (;;) {
+    // trace the ray of (node, depth <= trace_depth) and shade its hit
+    f3 c = zero;
+    cnt[depth == 0 ? kCntPrimary : kCntSecondary]++;
+    Hit h = closest_hit<SH>(s, o, d, shs, stride, P.err);
+    cnt[kCntNodesC] += h.nodes;
+    cnt[kCntTestsC] += h.tests;
+    if (node == 0) root_hit = h.pos < 0 ? EOS_HIT_NONE : h.id;
+    if (h.pos < 0) {
+      if (rec) rec[node].hit = EOS_HIT_NONE;
+    } else {
+      cnt[kCntHits]++;
+      f3 Pp, N;
+      int obj;
+      hit_geometry(s, o, d, h, Pp, N, obj);
+      const float* m = s.mats + kMatStride * obj;
+      TreeFrame F;
+      F.phong = zero;
+      uint32_t mask = 0;
+      for (int li = 0; li < s.n_lights; ++li) {
+        const float* l = s.lights + 6 * li;
+        f3 sd = norm3(sub3(mk3(l[0], l[1], l[2]), Pp));
+        f3 so = add3(Pp, scale3(kRayEps, sd));
+        cnt[kCntShadow]++;
+        AnyResult ar = any_hit<SH>(s, so, sd, shs, stride, P.err);
+        cnt[kCntNodesA] += ar.nodes;
+        cnt[kCntTestsA] += ar.tests;
+        if (ar.hit) mask |= 1u << li;
+        else F.phong = add3(F.phong, phong_light(m, l, Pp, N, campos));
+      }
+      if (rec) {
+        rec[node].hit = h.id;
+        rec[node].shadow = mask;
+      }
+      f3 ro = zero, rd = zero;
+      const bool has_r = m[7] > 0.0f;
+      F.wR = has_r ? m[7] : 0.0f;
+      if (has_r) mirror_ray(d, Pp, N, ro, rd);
+      F.has_t = m[8] > 0.0f;
+      F.K = F.has_t ? transparent_ray(m, s.ambient_index, d, Pp, N, F.to, F.td) : 0.0f;
+      F.cR = zero;
+      F.node = node;
+      F.depth = depth;
+      if (depth < P.trace_depth && (has_r || F.has_t)) {
+        F.in_t = !has_r;
+        st[sp++] = F;
+        if (has_r) {
+          o = ro;
+          d = rd;
+          node = 2 * node + 1;
+        } else {
+          o = F.to;
+          d = F.td;
+          node = 2 * node + 2;
+        }
+        ++depth;
+        continue;
+      }
+      c = tree_colour(F.phong, F.wR, zero, F.has_t, F.K, zero);  // children beyond the trace depth
+    }
+    // hand the colour up until a node still has its transparent child to trace
+    bool next = false;
+    while (sp > 0) {
+      TreeFrame& F = st[sp - 1];
+      if (!F.in_t) {
+        F.cR = c;
+        if (F.has_t) {
+          F.in_t = true;
+          o = F.to;
+          d = F.td;
+          node = 2 * F.node + 2;
+          depth = F.depth + 1;
+          next = true;
+          break;
+        }
+        c = tree_colour(F.phong, F.wR, F.cR, false, 0.0f, zero);
+      } else {
+        c = tree_colour(F.phong, F.wR, F.cR, true, F.K, c);
+      }
+      --sp;
+    }
+    if (!next) return c;
+  }
+}
+
 // Registers capped at 64 (32 warps per SM with blocks of 128): the megakernel is latency-
 // bound and gains more from resident warps than it loses to spills (measured on config 2:
 // 112 registers 2,580 Mrays/s, 96 2,794, 80 2,913, 64 3,076, 56 2,987, 48 2,481).
-template <int SH>
+template <int SH, bool TREE = false>
 __global__ void __maxnreg__(64) k_render_plain(PlainParams P) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
@@ -100,32 +209,43 @@ __global__ void __maxnreg__(64) k_render_plain(PlainParams P) {
   if (x < P.width && ly < P.rows) {
     f3 sum = mk3(0.0f, 0.0f, 0.0f);
     for (int smp = 0; smp < P.spp; ++smp) {
-      int32_t hits[kMaxBounces];
-      uint32_t masks[kMaxBounces];
-#pragma unroll
-      for (int k = 0; k < kMaxBounces; ++k) {
-        hits[k] = EOS_HIT_UNTRACED;
-        masks[k] = 0;
-      }
       float ox, oy;
-      sample_offset((uint32_t)img_pix, smp, P.spp, P.jitter_seed, P.pixel_offset, ox, oy);
+      sample_offset((uint32_t)img_pix, smp, P.spp, P.jitter_seed, P.pixel_offset, ox, oy, P.grid);
       f3 d = primary_direction(P.cam, P.width, P.height, x, y, ox, oy);
       f3 o = mk3(P.cam[0], P.cam[1], P.cam[2]);
-      f3 c = trace_path<SH>(P, o, d, hits, masks, cnt, shs, stride);
-      sum = add3(sum, c);
       size_t path = (size_t)pix * P.spp + smp;
-      if (P.hit) P.hit[path] = hits[0];
-      if (P.paths) {
-        eos_path_record rec;
+      if constexpr (TREE) {
+        const int nn = EOS_TREE_NODES(P.trace_depth);
+        eos_tree_node* rec = P.tree ? P.tree + path * nn : nullptr;
+        if (rec)
+          for (int k = 0; k < nn; ++k) rec[k] = eos_tree_node{EOS_HIT_UNTRACED, 0u};
+        int root_hit = EOS_HIT_NONE;
+        f3 c = trace_tree<SH>(P, o, d, rec, root_hit, cnt, shs, stride);
+        sum = add3(sum, c);
+        if (P.hit) P.hit[path] = root_hit;
+      } else {
+        int32_t hits[kMaxBounces];
+        uint32_t masks[kMaxBounces];
 #pragma unroll
         for (int k = 0; k < kMaxBounces; ++k) {
-          rec.hit[k] = hits[k];
-          rec.shadow[k] = masks[k];
+          hits[k] = EOS_HIT_UNTRACED;
+          masks[k] = 0;
         }
-        P.paths[path] = rec;
+        f3 c = trace_path<SH>(P, o, d, hits, masks, cnt, shs, stride);
+        sum = add3(sum, c);
+        if (P.hit) P.hit[path] = hits[0];
+        if (P.paths) {
+          eos_path_record rec;
+#pragma unroll
+          for (int k = 0; k < kMaxBounces; ++k) {
+            rec.hit[k] = hits[k];
+            rec.shadow[k] = masks[k];
+          }
+          P.paths[path] = rec;
+        }
       }
     }
-    if (P.spp > 1) sum = scale3(1.0f / (float)P.spp, sum);
+    if (P.spp > 1 || P.grid > 0) sum = scale3(sample_weight(P.spp, P.grid), sum);
     if (P.rgb) {
       P.rgb[3 * (size_t)pix] = sum.x;
       P.rgb[3 * (size_t)pix + 1] = sum.y;
@@ -167,8 +287,27 @@ inline int pick_stack(int d) { return d <= 0 ? 16 : (d <= 8 ? 8 : (d <= 16 ? 16 
 
 }  // namespace
 
+namespace {
+
+template <bool TREE>
+void launch_plain(const PlainParams& P, int sh, int grid, int block, size_t smem, cudaStream_t st) {
+  if (smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
+    if (sh == 8) cudaFuncSetAttribute(k_render_plain<8, TREE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else if (sh == 16)
+      cudaFuncSetAttribute(k_render_plain<16, TREE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else cudaFuncSetAttribute(k_render_plain<32, TREE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  if (sh == 8) k_render_plain<8, TREE><<<grid, block, smem, st>>>(P);
+  else if (sh == 16) k_render_plain<16, TREE><<<grid, block, smem, st>>>(P);
+  else k_render_plain<32, TREE><<<grid, block, smem, st>>>(P);
+}
+
+}  // namespace
+
+// tree: ray-tree kernel (scenes with materials both reflective and transparent, or tree
+// records asked for); paths then points at tree-form records.
 eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam, const eos_render_params& p,
-                        float* rgb, uint8_t* rgba8, int32_t* hit, eos_path_record* paths) {
+                        float* rgb, uint8_t* rgba8, int32_t* hit, void* paths, bool tree) {
   PlainParams P;
   P.s = sc->dev;
   for (int k = 0; k < 3; ++k) {
@@ -185,10 +324,12 @@ eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam
   P.spp = p.spp;
   P.pixel_offset = p.pixel_offset;
   P.jitter_seed = p.jitter_seed;
+  P.grid = (p.flags & EOS_FLAG_AA_GRID) ? aa_grid_side(p.spp) : 0;
   P.rgb = rgb;
   P.rgba8 = rgba8;
   P.hit = hit;
-  P.paths = paths;
+  P.paths = tree ? nullptr : (eos_path_record*)paths;
+  P.tree = tree ? (eos_tree_node*)paths : nullptr;
   P.err = ctx->d_err;
   P.counts = ctx->d_counts;
   const int block = clamp_block(p.block_size);
@@ -196,15 +337,8 @@ eos_status render_plain(eos_ctx* ctx, const eos_scene* sc, const eos_camera& cam
   const long long n_threads = (long long)((cam.width + 7) / 8) * ((P.rows + 3) / 4) * 32;
   const int grid = (int)std::max<long long>(1, (n_threads + block - 1) / block);
   const size_t smem = (size_t)sh * block * sizeof(uint2);
-  cudaStream_t st = ctx->stream;
-  if (smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
-    if (sh == 8) cudaFuncSetAttribute(k_render_plain<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else if (sh == 16) cudaFuncSetAttribute(k_render_plain<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else cudaFuncSetAttribute(k_render_plain<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  }
-  if (sh == 8) k_render_plain<8><<<grid, block, smem, st>>>(P);
-  else if (sh == 16) k_render_plain<16><<<grid, block, smem, st>>>(P);
-  else k_render_plain<32><<<grid, block, smem, st>>>(P);
+  if (tree) launch_plain<true>(P, sh, grid, block, smem, ctx->stream);
+  else launch_plain<false>(P, sh, grid, block, smem, ctx->stream);
   EOS_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return EOS_OK;

@@ -265,6 +265,13 @@ extern "C" eos_status eos_scene_load(eos_ctx* ctx, const char* path, eos_scene**
   sc->dev.pos_of_id = (const int32_t*)sc->d_pos_of_id;
   sc->dev.mats = (const float*)sc->d_mats;
   sc->dev.lights = (const float*)sc->d_lights;
+  std::vector<eos_material> mats(h.n_obj);
+  if (h.n_obj && cudaMemcpy(mats.data(), sc->d_mats, sizeof(eos_material) * h.n_obj, cudaMemcpyDeviceToHost) !=
+                     cudaSuccess) {
+    eos_scene_destroy(sc);  // the file is closed already
+    return EOS_ERR_CUDA;
+  }
+  sc->branching = eos::has_branching(mats.data(), h.n_obj);
   *out = sc;
   return EOS_OK;
 }

@@ -188,6 +188,7 @@ __device__ __forceinline__ int leaf_count(int r) { return ((r >> 25) & 31) + 1; 
 template <int SH, int CAP = kStackMax>
 struct TraversalStack {
   static_assert(CAP >= SH, "the shared part is the bottom of the stack");
+  static constexpr int kShared = SH;
   uint2* sh;
   int stride;
   int sp;
@@ -219,7 +220,11 @@ struct TraversalStack {
   }
   // Next entry, any distance (shadow rays), or kDone.
   __device__ __forceinline__ int next_any() { return sp > 0 ? (int)pop().x : kDone; }
+  // Entries without a distance (any-hit traversal).
+  __device__ __forceinline__ bool push_ref(int ref) { return push(ref, 0.0f); }
+  __device__ __forceinline__ void push_ref_shared(int ref) { push_shared(ref, 0.0f); }
 };
+
 
 __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p, f3& v1, f3& e1, f3& e2, int& id) {
   float4 a = __ldg(tris + 3 * (size_t)p);
@@ -243,9 +248,10 @@ __device__ __forceinline__ void load_tri(const float4* __restrict__ tris, int p,
 // shared-memory stack entries (the most one node pushes) the pushes skip their bound
 // checks.  Returns false on stack overflow.
 
-template <int SH, bool SORT, class Ray, int CAP>
+template <bool SORT, class Ray, class Stack>
 __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base, const Ray& r, int& cur,
-                                            float limit, TraversalStack<SH, CAP>& st, unsigned& nodes) {
+                                            float limit, Stack& st, unsigned& nodes) {
+  constexpr int SH = Stack::kShared;
   const float4* nd = node_base + 8 * (size_t)cur;
   const float4 lx = __ldg(nd + r.sx), ly = __ldg(nd + 1 + r.sy), lz = __ldg(nd + 2 + r.sz);  // near planes
   const float4 hx = __ldg(nd + 3 - r.sx), hy = __ldg(nd + 4 - r.sy), hz = __ldg(nd + 5 - r.sz);  // far planes
@@ -292,14 +298,14 @@ __device__ __forceinline__ bool visit_node4(const float4* __restrict__ node_base
       for (int i = 0; i < 4; ++i) {
         if (!h[i]) continue;
         if (first < 0) first = i;
-        else st.push_shared(c[i], 0.0f);
+        else st.push_ref_shared(c[i]);
       }
     } else {
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         if (!h[i]) continue;
         if (first < 0) first = i;
-        else if (!st.push(c[i], 0.0f)) return false;
+        else if (!st.push_ref(c[i])) return false;
       }
     }
     cur = first < 0 ? st.next_any() : c[first];
@@ -322,7 +328,7 @@ __device__ __forceinline__ Hit closest_traverse(const DevScene& s, f3 o, f3 d, c
   int leaf = 0;  // parked leaf (0 = none)
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node4<SH, true>(s.nodes, r, cur, h.t * kCullR, st, h.nodes)) {
+      if (!visit_node4<true>(s.nodes, r, cur, h.t * kCullR, st, h.nodes)) {
         atomicOr(err, kErrStack);
         return h;
       }
@@ -371,7 +377,7 @@ __device__ __forceinline__ AnyResult any_traverse(const DevScene& s, f3 o, f3 d,
   int leaf = 0;
   for (;;) {
     while (cur >= 0) {
-      if (!visit_node4<SH, false>(s.nodes, r, cur, kInf, st, res.nodes)) {
+      if (!visit_node4<false>(s.nodes, r, cur, kInf, st, res.nodes)) {
         atomicOr(err, kErrStack);
         return res;
       }
@@ -458,7 +464,7 @@ __device__ __noinline__ Hit traverse_instanced(const DevScene& s, f3 o, f3 d, ui
   for (;;) {
     const float limit = ANY ? kInf : h.t * kCull;
     if (cur >= 0) {
-      if (!visit_node4<SH, !ANY>(nodes, r, cur, limit, st, h.nodes)) {
+      if (!visit_node4<!ANY>(nodes, r, cur, limit, st, h.nodes)) {
         atomicOr(err, kErrStack);
         return h;
       }
@@ -634,31 +640,51 @@ __device__ __forceinline__ float fresnel(f3 incident, f3 normal, float n1, float
 // by a slip at :403, again as "refracted" -- and mixes K c + (1 - K) c; the refracted ray
 // itself is never traced.  That ray once, with w = -K: the sign bit marks the mix.
 // Returns false when the material spawns no ray.
+// The mirror ray of a reflective hit: normalize(reflect(d, N)) from P + 1e-3 of it (:339-351).
+__device__ __forceinline__ void mirror_ray(f3 d, f3 P, f3 N, f3& ro, f3& rd) {
+  rd = norm3(reflect3(d, N));
+  ro = add3(P, scale3(kRayEps, rd));
+}
+
+// The ray of a transparent hit (:353-407) and its Fresnel weight K.
+__device__ __forceinline__ float transparent_ray(const float* m, float ambient, f3 d, f3 P, f3 N, f3& ro, f3& rd) {
+  const f3 inc = norm3(d);
+  f3 n = N;
+  float n1 = ambient, n2 = m[9];
+  if (!(dot3(inc, N) < 0.0f)) {  // leaving the material: normal flipped as 0 - N
+    n1 = m[9];
+    n2 = ambient;
+    n = sub3(mk3(0.0f, 0.0f, 0.0f), N);
+  }
+  const float K = fresnel(inc, n, n1, n2);
+  rd = norm3(reflect3(d, n));
+  ro = add3(P, scale3(kRayEps, n));
+  return K;
+}
+
 __device__ __forceinline__ bool secondary_ray(const float* m, float ambient, f3 d, f3 P, f3 N, f3& ro, f3& rd,
                                               float& w) {
   if (m[7] > 0.0f) {
-    rd = norm3(reflect3(d, N));
-    ro = add3(P, scale3(kRayEps, rd));
+    mirror_ray(d, P, N, ro, rd);
     w = m[7];
     return true;
   }
   if (m[8] > 0.0f) {
-    const f3 inc = norm3(d);
-    f3 n = N;
-    float n1 = ambient, n2 = m[9];
-    if (!(dot3(inc, N) < 0.0f)) {  // leaving the material: normal flipped as 0 - N
-      n1 = m[9];
-      n2 = ambient;
-      n = sub3(mk3(0.0f, 0.0f, 0.0f), N);
-    }
-    const float K = fresnel(inc, n, n1, n2);
-    rd = norm3(reflect3(d, n));
-    ro = add3(P, scale3(kRayEps, n));
-    w = -K;
+    w = -transparent_ray(m, ambient, d, P, N, ro, rd);
     return true;
   }
   w = 0.0f;
   return false;
+}
+
+// Colour of a ray-tree node (a material that is both reflective and transparent traces
+// both rays, src/RayTracer.cpp:339-407) as :410 sums it: (phong + wR c_mirror) +
+// (K c_t + (1 - K) c_t); a term the material lacks is 0 (wR = 0, has_t false), a child not
+// traced (beyond the trace depth, or a miss) has colour 0.  For a node with one secondary
+// ray this equals fold_colour bit for bit (x + 0 = x for the non-negative sums here).
+__device__ __forceinline__ f3 tree_colour(f3 phong, float wR, f3 cR, bool has_t, float K, f3 cT) {
+  const f3 refr = has_t ? add3(scale3(K, cT), scale3(1.0f - K, cT)) : mk3(0.0f, 0.0f, 0.0f);
+  return add3(add3(phong, scale3(wR, cR)), refr);
 }
 
 // Colour fold of one bounce: phong + w c for a mirror (or no) bounce; for a transparent

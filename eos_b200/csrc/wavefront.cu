@@ -40,9 +40,12 @@ struct DevJob {
   int y0, rows;  // image rows [y0, y0 + rows) are rendered; outputs hold those rows
   float off;
   uint32_t seed;
+  int grid;  // side of the reference's AA grid (EOS_FLAG_AA_GRID), 0 = jitter
   float* rgb;
   uint8_t* rgba8;
   eos_path_record* paths;
+  eos_tree_node* tree;  // tree-form records instead of paths (EOS_FLAG_TREE_RECORDS)
+  int tree_nn;          // nodes per tree record: EOS_TREE_NODES(trace_depth)
   long long path_off;  // first global path index of this job
   long long n_paths;   // tiled, padded path count
   int tiles_x;
@@ -51,12 +54,21 @@ struct DevJob {
 
 struct RayQ {
   float4 a;  // origin xyz, path (int)
-  float4 b;  // direction xyz, -
+  float4 b;  // direction xyz, ray-tree node (int; tree mode)
 };
 struct HitQ {
-  float4 a;  // P xyz, path (int)
+  float4 a;  // P xyz, path (int; tree mode: path | node << 24, all ones = padding)
   float4 b;  // N xyz, obj (int; -1 = miss)
 };
+
+// Ray-tree mode (materials both reflective and transparent, or tree-form records): a hit
+// may emit a mirror ray (node 2j + 1) and a transparent one (node 2j + 2); accumulators
+// hold one entry per node (phong rgb, weight of the edge into the node: reflectivity, or
+// -K for a transparent ray with its sign marking the mix) and k_wf_resolve folds each
+// path's tree bottom-up.  Paths of a chunk are < 2^24 and nodes < 2^8, so a hit record
+// packs both into one word.
+constexpr uint32_t kTreePad = 0xFFFFFFFFu;
+__device__ __forceinline__ uint32_t tree_pack(int path, int node) { return (uint32_t)path | ((uint32_t)node << 24); }
 struct ShadowQ {
   float4 a;  // origin xyz, hit index (int)
   float4 b;  // direction xyz, light (int)
@@ -78,9 +90,10 @@ struct WfArgs {
   HitQ* hits;
   uint32_t* masks;
   ShadowQ* sq;
-  float4* acc;   // [n_chunk][depth+1] phong rgb, reflectivity
+  float4* acc;   // [n_chunk][depth+1] phong rgb, reflectivity (tree mode: [n_chunk][nn], see above)
   int* ctr;      // [depth+1][kCtr]
   int cap_r, cap_s;
+  int nn;         // tree mode: nodes per path (EOS_TREE_NODES of the deepest job)
   int qchunk;
   int work_limit;  // queue entries a persistent launch traces (test limit; INT_MAX = all)
   int* err;
@@ -136,7 +149,31 @@ __device__ __forceinline__ int budget(int n, int work_limit, int* err) {
 // measured faster than no cap (77 registers) and than caps of 56 or 48 (spills).  CAP is
 // the traversal stack's size (TraversalStack): kStackMax, or SH for the small-stack test
 // limit.
-template <bool PRIMARY, int SH, int CAP = kStackMax>
+// Appends the secondary rays of the lanes with `want` to R_k+1 (ballot / popc compaction,
+// one atomic per warp); node = the ray-tree node of the ray (0 outside tree mode).
+// Warp-uniform: every lane calls it.
+__device__ __forceinline__ void emit_secondary(const WfArgs& A, int* ctr, bool want, int path, int node, f3 ro,
+                                               f3 rd) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t rb = __ballot_sync(0xffffffffu, want);
+  if (!rb) return;
+  int rbase = 0;
+  if (lane == 0) rbase = atomicAdd(&ctr[1], __popc(rb));
+  rbase = __shfl_sync(0xffffffffu, rbase, 0);
+  if (want) {
+    const int pos = rbase + __popc(rb & lanemask_lt());
+    if (pos >= A.cap_r) {
+      atomicOr(A.err, kErrQueue);
+    } else {
+      RayQ r;
+      r.a = make_float4(ro.x, ro.y, ro.z, __int_as_float(path));
+      r.b = make_float4(rd.x, rd.y, rd.z, __int_as_float(node));
+      A.rout[pos] = r;
+    }
+  }
+}
+
+template <bool PRIMARY, int SH, int CAP = kStackMax, bool TREE = false>
 __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
   extern __shared__ uint2 shstack[];
   uint2* shs = shstack + threadIdx.x;
@@ -154,9 +191,9 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
     for (int base = start; base < end; base += 32) {
       int i = base + lane;
       bool valid = i < end;
-      bool hit = false, refl = false;
-      int path = -1, jb = 0, obj = -1;
-      f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1), P = o, N = o, ro = o, rd = d;
+      bool hit = false, refl = false, transp = false;
+      int path = -1, jb = 0, obj = -1, node = 0;
+      f3 o = mk3(0, 0, 0), d = mk3(0, 0, 1), P = o, N = o, ro = o, rd = d, to = o, td = d;
       if (valid) {
         if (PRIMARY) {
           long long gp = A.c0 + i;
@@ -165,7 +202,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
           int x, y, smp;
           if (path_pixel(J, gp - J.path_off, x, y, smp)) {
             float ox, oy;
-            sample_offset((uint32_t)((J.y0 + y) * J.w + x), smp, J.spp, J.seed, J.off, ox, oy);
+            sample_offset((uint32_t)((J.y0 + y) * J.w + x), smp, J.spp, J.seed, J.off, ox, oy, J.grid);
             d = primary_direction(J.cam, J.w, J.h, x, J.y0 + y, ox, oy);
             o = mk3(J.cam[0], J.cam[1], J.cam[2]);
             path = i;
@@ -177,6 +214,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
           o = mk3(r.a.x, r.a.y, r.a.z);
           d = mk3(r.b.x, r.b.y, r.b.z);
           path = __float_as_int(r.a.w);
+          if constexpr (TREE) node = __float_as_int(r.b.w);
           jb = find_job(A.jobs, A.n_jobs, A.c0 + path);
         }
       }
@@ -188,20 +226,44 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
         tests += h.tests;
         hit = h.pos >= 0;
         nhits += hit;
-        if (J.paths) {
-          int x, y, smp;
-          path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
-          J.paths[((size_t)y * J.w + x) * J.spp + smp].hit[A.k] = hit ? h.id : EOS_HIT_NONE;
-        }
-        if (hit) {
-          hit_geometry(J.s, o, d, h, P, N, obj);
-          float w;
-          refl = secondary_ray(J.s.mats + kMatStride * obj, J.s.ambient_index, d, P, N, ro, rd, w);
-          reinterpret_cast<float*>(A.acc + (size_t)path * (A.depth + 1) + A.k)[3] = w;
-          refl = refl && A.k < J.trace_depth;
+        if constexpr (TREE) {
+          if (J.tree) {
+            int x, y, smp;
+            path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
+            J.tree[(((size_t)y * J.w + x) * J.spp + smp) * J.tree_nn + node].hit = hit ? h.id : EOS_HIT_NONE;
+          }
+          if (hit) {
+            hit_geometry(J.s, o, d, h, P, N, obj);
+            const float* m = J.s.mats + kMatStride * obj;
+            if (A.k < J.trace_depth) {  // children only within the trace depth: nodes < tree_nn
+              float* row = reinterpret_cast<float*>(A.acc + (size_t)path * A.nn);
+              if (m[7] > 0.0f) {
+                mirror_ray(d, P, N, ro, rd);
+                refl = true;
+                row[4 * (2 * node + 1) + 3] = m[7];
+              }
+              if (m[8] > 0.0f) {
+                row[4 * (2 * node + 2) + 3] = -transparent_ray(m, J.s.ambient_index, d, P, N, to, td);
+                transp = true;
+              }
+            }
+          }
+        } else {
+          if (J.paths) {
+            int x, y, smp;
+            path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
+            J.paths[((size_t)y * J.w + x) * J.spp + smp].hit[A.k] = hit ? h.id : EOS_HIT_NONE;
+          }
+          if (hit) {
+            hit_geometry(J.s, o, d, h, P, N, obj);
+            float w;
+            refl = secondary_ray(J.s.mats + kMatStride * obj, J.s.ambient_index, d, P, N, ro, rd, w);
+            reinterpret_cast<float*>(A.acc + (size_t)path * (A.depth + 1) + A.k)[3] = w;
+            refl = refl && A.k < J.trace_depth;
+          }
         }
         HitQ hq;
-        hq.a = make_float4(P.x, P.y, P.z, __int_as_float(path));
+        hq.a = make_float4(P.x, P.y, P.z, TREE ? __uint_as_float(tree_pack(path, node)) : __int_as_float(path));
         hq.b = make_float4(N.x, N.y, N.z, __int_as_float(hit ? obj : -1));
         A.hits[i] = hq;
         A.masks[i] = 0u;
@@ -235,23 +297,12 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
         }
         nshadow += nl;
       }
-      // secondary rays (mirror, or the transparent bounce's ray)
-      uint32_t rb = __ballot_sync(0xffffffffu, refl);
-      if (rb) {
-        int rbase = 0;
-        if (lane == 0) rbase = atomicAdd(&ctr[1], __popc(rb));
-        rbase = __shfl_sync(0xffffffffu, rbase, 0);
-        if (refl) {
-          int pos = rbase + __popc(rb & lanemask_lt());
-          if (pos >= A.cap_r) {
-            atomicOr(A.err, kErrQueue);
-          } else {
-            RayQ r;
-            r.a = make_float4(ro.x, ro.y, ro.z, __int_as_float(path));
-            r.b = make_float4(rd.x, rd.y, rd.z, 0.0f);
-            A.rout[pos] = r;
-          }
-        }
+      // secondary rays (mirror, or the transparent bounce's ray; both in tree mode)
+      if constexpr (TREE) {
+        emit_secondary(A, ctr, refl, path, 2 * node + 1, ro, rd);
+        emit_secondary(A, ctr, transp, path, 2 * node + 2, to, td);
+      } else {
+        emit_secondary(A, ctr, refl, path, 0, ro, rd);
       }
     }
   }
@@ -290,15 +341,24 @@ __global__ void __launch_bounds__(256, 4) k_wf_any(WfArgs A) {
   warp_add_count(&A.counts[kCntTestsA], tests);
 }
 
+template <bool TREE = false>
 __global__ void k_wf_shade(WfArgs A) {
   int* ctr = A.ctr + A.k * kCtr;
   // primary hit records beyond the work budget keep k_wf_init's padding marks
   const int n = A.k == 0 ? A.n_chunk : min(min(ctr[1 - kCtr], A.cap_r), A.work_limit);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     HitQ hq = A.hits[i];
-    int path = __float_as_int(hq.a.w);
+    int path, node = 0;
+    if constexpr (TREE) {
+      const uint32_t w = __float_as_uint(hq.a.w);
+      if (w == kTreePad) continue;  // tile padding (primary only)
+      path = (int)(w & 0xFFFFFFu);
+      node = (int)(w >> 24);
+    } else {
+      path = __float_as_int(hq.a.w);
+      if (path < 0) continue;  // tile padding (primary only)
+    }
     int obj = __float_as_int(hq.b.w);
-    if (path < 0) continue;  // tile padding (primary only)
     const DevJob& J = A.jobs[find_job(A.jobs, A.n_jobs, A.c0 + path)];
     if (obj < 0) continue;
     f3 P = mk3(hq.a.x, hq.a.y, hq.a.z), N = mk3(hq.b.x, hq.b.y, hq.b.z);
@@ -308,28 +368,37 @@ __global__ void k_wf_shade(WfArgs A) {
     f3 acc = mk3(0, 0, 0);
     for (int l = 0; l < J.s.n_lights; ++l)
       if (!(mask & (1u << l))) acc = add3(acc, phong_light(m, J.s.lights + 6 * l, P, N, cam));
-    float4* e = A.acc + (size_t)path * (A.depth + 1) + A.k;  // .w: the bounce weight, set by the hit stage
+    // .w: the bounce weight (tree mode: the weight of the edge into the node), set by the hit stage
+    float4* e = TREE ? A.acc + (size_t)path * A.nn + node : A.acc + (size_t)path * (A.depth + 1) + A.k;
     *e = make_float4(acc.x, acc.y, acc.z, e->w);
-    if (J.paths) {
+    if (J.paths || (TREE && J.tree)) {
       int x, y, smp;
       path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
-      J.paths[((size_t)y * J.w + x) * J.spp + smp].shadow[A.k] = mask;
+      const size_t rec = ((size_t)y * J.w + x) * J.spp + smp;
+      if (TREE) J.tree[rec * J.tree_nn + node].shadow = mask;
+      else J.paths[rec].shadow[A.k] = mask;
     }
   }
 }
 
 // Marks every padding entry of the primary hit queue and clears path records / acc.
+template <bool TREE = false>
 __global__ void k_wf_init(WfArgs A) {
+  const int slots = TREE ? A.nn : A.depth + 1;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_chunk; i += gridDim.x * blockDim.x) {
     long long gp = A.c0 + i;
     const DevJob& J = A.jobs[find_job(A.jobs, A.n_jobs, gp)];
-    for (int k = 0; k <= A.depth; ++k) A.acc[(size_t)i * (A.depth + 1) + k] = make_float4(0, 0, 0, 0);
+    for (int k = 0; k < slots; ++k) A.acc[(size_t)i * slots + k] = make_float4(0, 0, 0, 0);
     HitQ hq;
-    hq.a = make_float4(0, 0, 0, __int_as_float(-1));
+    hq.a = make_float4(0, 0, 0, TREE ? __uint_as_float(kTreePad) : __int_as_float(-1));
     hq.b = make_float4(0, 0, 0, __int_as_float(-1));
     A.hits[i] = hq;
     int x, y, smp;
-    if (J.paths && path_pixel(J, gp - J.path_off, x, y, smp)) {
+    if (TREE && J.tree && path_pixel(J, gp - J.path_off, x, y, smp)) {
+      eos_tree_node* rec = J.tree + (((size_t)y * J.w + x) * J.spp + smp) * J.tree_nn;
+      for (int k = 0; k < J.tree_nn; ++k) rec[k] = eos_tree_node{EOS_HIT_UNTRACED, 0u};
+    }
+    if (!TREE && J.paths && path_pixel(J, gp - J.path_off, x, y, smp)) {
       eos_path_record rec;
       for (int k = 0; k < kMaxBounces; ++k) {
         rec.hit[k] = EOS_HIT_UNTRACED;
@@ -340,6 +409,38 @@ __global__ void k_wf_init(WfArgs A) {
   }
 }
 
+// Colour of one path: the chain fold c_k = fold_colour(phong_k, w_k, c_k+1), or in tree
+// mode the bottom-up fold of its nodes in place (children 2j + 1 and 2j + 2 come after j).
+template <bool TREE>
+__device__ __forceinline__ f3 path_colour(const WfArgs& A, long long path) {
+  if constexpr (TREE) {
+    float4* a = A.acc + (size_t)path * A.nn;
+    for (int j = A.nn - 1; j >= 0; --j) {
+      const float4 e = a[j];
+      f3 c = mk3(e.x, e.y, e.z);
+      if (2 * j + 1 < A.nn) {
+        const float4 r = a[2 * j + 1], t = a[2 * j + 2];
+        // r.w = reflectivity of the mirror ray (0: none); t.w = -K of the transparent one
+        // (+0: none; the sign bit marks it, -0 for K = 0)
+        c = tree_colour(c, r.w, mk3(r.x, r.y, r.z), signbit(t.w), -t.w, mk3(t.x, t.y, t.z));
+      } else {
+        c = tree_colour(c, 0.0f, mk3(0, 0, 0), false, 0.0f, mk3(0, 0, 0));
+      }
+      a[j] = make_float4(c.x, c.y, c.z, e.w);
+    }
+    return mk3(a[0].x, a[0].y, a[0].z);
+  } else {
+    const float4* a = A.acc + (size_t)path * (A.depth + 1);
+    f3 c = mk3(0, 0, 0);
+    for (int k = A.depth; k >= 0; --k) {
+      float4 e = a[k];
+      c = fold_colour(mk3(e.x, e.y, e.z), e.w, c);
+    }
+    return c;
+  }
+}
+
+template <bool TREE = false>
 __global__ void k_wf_resolve(WfArgs A) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_chunk; i += gridDim.x * blockDim.x) {
     long long gp = A.c0 + i;
@@ -347,16 +448,8 @@ __global__ void k_wf_resolve(WfArgs A) {
     int x, y, smp;
     if (!path_pixel(J, gp - J.path_off, x, y, smp) || smp != 0) continue;
     f3 sum = mk3(0, 0, 0);
-    for (int s = 0; s < J.spp; ++s) {
-      const float4* a = A.acc + (size_t)(i + s) * (A.depth + 1);
-      f3 c = mk3(0, 0, 0);
-      for (int k = A.depth; k >= 0; --k) {
-        float4 e = a[k];
-        c = fold_colour(mk3(e.x, e.y, e.z), e.w, c);
-      }
-      sum = add3(sum, c);
-    }
-    if (J.spp > 1) sum = scale3(1.0f / (float)J.spp, sum);
+    for (int s = 0; s < J.spp; ++s) sum = add3(sum, path_colour<TREE>(A, i + s));
+    if (J.spp > 1 || J.grid > 0) sum = scale3(sample_weight(J.spp, J.grid), sum);
     size_t pix = (size_t)y * J.w + x;
     if (J.rgb) {
       J.rgb[3 * pix] = sum.x;
@@ -404,28 +497,38 @@ struct StageTimer {
     if (s_ != EOS_OK) return s_;    \
   } while (0)
 
-// The nearest-hit / shadow kernels of one configuration: a warp takes `queue_chunk` rays
-// and finishes all before taking more.  small_stack selects the test instantiation whose
-// traversal stack is its SH shared-memory entries only (launch_config pins SH = 8 then).
+// The kernels of one configuration: a warp of the nearest-hit / shadow kernels takes
+// `queue_chunk` rays and finishes all before taking more.  small_stack selects the test
+// instantiation whose traversal stack is its SH shared-memory entries only (launch_config
+// pins SH = 8 then); tree the ray-tree mode.
 template <int SH>
 struct StageKernels {
   void (*closest_primary)(WfArgs);
   void (*closest)(WfArgs);
   void (*any)(WfArgs);
-  static StageKernels get(bool small_stack) {
+  void (*shade)(WfArgs);
+  void (*init)(WfArgs);
+  void (*resolve)(WfArgs);
+  static StageKernels get(bool small_stack, bool tree) {
+    if (tree)
+      return {k_wf_closest<true, SH, kStackMax, true>, k_wf_closest<false, SH, kStackMax, true>, k_wf_any<SH>,
+              k_wf_shade<true>, k_wf_init<true>, k_wf_resolve<true>};
     if constexpr (SH == 8) {
-      if (small_stack) return {k_wf_closest<true, 8, 8>, k_wf_closest<false, 8, 8>, k_wf_any<8, 8>};
+      if (small_stack)
+        return {k_wf_closest<true, 8, 8>, k_wf_closest<false, 8, 8>, k_wf_any<8, 8>,
+                k_wf_shade<false>, k_wf_init<false>, k_wf_resolve<false>};
     }
-    return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any<SH>};
+    return {k_wf_closest<true, SH>, k_wf_closest<false, SH>, k_wf_any<SH>,
+            k_wf_shade<false>, k_wf_init<false>, k_wf_resolve<false>};
   }
 };
 
 template <int SH>
 eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, const Chunk* chunks, int n_chunks,
                            int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem,
-                           bool small_stack, StageTimer tm, uint32_t& launches) {
+                           bool small_stack, bool tree, StageTimer tm, uint32_t& launches) {
   const int grid_lin = num_sms * 8;
-  const StageKernels<SH> K = StageKernels<SH>::get(small_stack);
+  const StageKernels<SH> K = StageKernels<SH>::get(small_stack, tree);
   for (int ci = 0; ci < n_chunks; ++ci) {
     const Chunk& c = chunks[ci];
     WfArgs A = base;
@@ -433,7 +536,7 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
     A.n_chunk = c.n;
     EOS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int) * kCtr * (depth + 1), st));
     EOS_TRY(tm.begin());
-    k_wf_init<<<grid_lin, 256, 0, st>>>(A);
+    K.init<<<grid_lin, 256, 0, st>>>(A);
     EOS_TRY(tm.end(2));
     ++launches;
     const RayQ* rin = nullptr;
@@ -449,13 +552,13 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
       K.any<<<grid_any, block, smem, st>>>(A);
       EOS_TRY(tm.end(1));
       EOS_TRY(tm.begin());
-      k_wf_shade<<<grid_lin, 256, 0, st>>>(A);
+      K.shade<<<grid_lin, 256, 0, st>>>(A);
       EOS_TRY(tm.end(2));
       launches += 3;
       rin = A.rout;
     }
     EOS_TRY(tm.begin());
-    k_wf_resolve<<<grid_lin, 256, 0, st>>>(A);
+    K.resolve<<<grid_lin, 256, 0, st>>>(A);
     EOS_TRY(tm.end(2));
     ++launches;
   }
@@ -463,8 +566,9 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
   return EOS_OK;
 }
 
-// Device job record of one view (tiled, padded path count).
-void fill_job(const eos_job& J, long long path_off, DevJob& d) {
+// Device job record of one view (tiled, padded path count).  tree_records: paths_out holds
+// tree-form records (EOS_FLAG_TREE_RECORDS).
+void fill_job(const eos_job& J, long long path_off, bool tree_records, bool aa_grid, DevJob& d) {
   memset(&d, 0, sizeof d);
   d.s = J.scene->dev;
   for (int k = 0; k < 3; ++k) {
@@ -479,9 +583,12 @@ void fill_job(const eos_job& J, long long path_off, DevJob& d) {
   d.spp = J.spp;
   d.off = J.pixel_offset;
   d.seed = J.jitter_seed;
+  d.grid = aa_grid ? aa_grid_side(J.spp) : 0;
   d.rgb = J.rgb_out;
   d.rgba8 = J.rgba8_out;
-  d.paths = J.paths_out;
+  d.paths = tree_records ? nullptr : J.paths_out;
+  d.tree = tree_records ? reinterpret_cast<eos_tree_node*>(J.paths_out) : nullptr;
+  d.tree_nn = EOS_TREE_NODES(J.trace_depth);
   d.y0 = J.row_end > 0 ? J.row_begin : 0;
   d.rows = J.row_end > 0 ? J.row_end - J.row_begin : d.h;
   d.tiles_x = (d.w + kTileW - 1) / kTileW;
@@ -492,13 +599,14 @@ void fill_job(const eos_job& J, long long path_off, DevJob& d) {
 
 struct LaunchConfig {
   int block, sh, qchunk, grid_c, grid_a;
-  bool small_stack;  // test limit: 8-entry traversal stacks
+  bool small_stack;  // test limit: 8-entry traversal stacks (chain mode)
+  bool tree;         // ray-tree mode
   size_t smem;
 };
 
 template <int SH>
 void configure(LaunchConfig& c, int num_sms) {
-  const StageKernels<SH> K = StageKernels<SH>::get(c.small_stack);
+  const StageKernels<SH> K = StageKernels<SH>::get(c.small_stack, c.tree);
   if (c.smem > 48 * 1024) {  // opt in to more than the default 48 KB of dynamic shared memory
     cudaFuncSetAttribute(K.closest_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
     cudaFuncSetAttribute(K.closest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
@@ -511,13 +619,14 @@ void configure(LaunchConfig& c, int num_sms) {
   c.grid_a = num_sms * std::max(1, occ_a);
 }
 
-LaunchConfig launch_config(const eos_render_params& p, int num_sms, bool small_stack) {
+LaunchConfig launch_config(const eos_render_params& p, int num_sms, bool small_stack, bool tree) {
   LaunchConfig c;
   c.block = p.block_size > 0 ? std::min(512, std::max(32, (p.block_size / 32) * 32)) : 128;
   c.sh = p.stack_depth <= 0 ? 16 : (p.stack_depth <= 8 ? 8 : (p.stack_depth <= 16 ? 16 : 32));
   c.qchunk = p.queue_chunk > 0 ? std::max(32, (p.queue_chunk / 32) * 32) : 64;
-  c.small_stack = small_stack;
-  if (small_stack) c.sh = 8;
+  c.tree = tree;
+  c.small_stack = small_stack && !tree;
+  if (c.small_stack) c.sh = 8;
   c.smem = (size_t)c.sh * c.block * sizeof(uint2);
   if (c.sh == 8) configure<8>(c, num_sms);
   else if (c.sh == 16) configure<16>(c, num_sms);
@@ -529,12 +638,12 @@ eos_status run_sequence(cudaStream_t st, int num_sms, const LaunchConfig& lc, co
                         int n_chunks, int depth, StageTimer tm, uint32_t& launches) {
   if (lc.sh == 8)
     return launch_sequence<8>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                              lc.small_stack, tm, launches);
+                              lc.small_stack, lc.tree, tm, launches);
   if (lc.sh == 16)
     return launch_sequence<16>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr,
-                               lc.smem, false, tm, launches);
+                               lc.smem, false, lc.tree, tm, launches);
   return launch_sequence<32>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                             false, tm, launches);
+                             false, lc.tree, tm, launches);
 }
 
 }  // namespace
@@ -546,16 +655,22 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   long long total = 0;
   int depth = 0, max_lights = 0;
   std::vector<Chunk> chunks;
+  const bool tree_records = (p.flags & EOS_FLAG_TREE_RECORDS) != 0;
+  bool tree = tree_records;
   for (uint32_t j = 0; j < n_jobs; ++j) {
     depth = std::max(depth, jobs[j].trace_depth);
     max_lights = std::max(max_lights, (int)jobs[j].scene->dev.n_lights);
+    tree = tree || jobs[j].scene->branching;
   }
-  // queue bytes per path: two ray queues, hit records, masks, shadow queue, accumulators
-  const long long per_path = 3ll * 32 + 4 + 32ll * std::max(1, max_lights) + 16ll * (depth + 1);
+  // Per path: rays per bounce (1, or up to 2^depth in tree mode) x (two ray queues, hit
+  // record, mask, shadow queue) + accumulators (one per bounce, or per tree node).
+  const long long width = tree ? 1ll << depth : 1;
+  const int nn = EOS_TREE_NODES(depth);
+  const long long per_path = width * (3ll * 32 + 4 + 32ll * std::max(1, max_lights)) + 16ll * (tree ? nn : depth + 1);
   const long long chunk_paths = std::max(1ll << 16, std::min(kChunkPathsMax, kQueueBudget / per_path));
   for (uint32_t j = 0; j < n_jobs; ++j) {
     DevJob& d = dj[j];
-    fill_job(jobs[j], total, d);
+    fill_job(jobs[j], total, tree_records, (p.flags & EOS_FLAG_AA_GRID) != 0, d);
     // chunks aligned to whole pixels of this job
     long long unit = 32ll * d.spp;
     long long per = std::max(unit, (chunk_paths / unit) * unit);
@@ -575,19 +690,20 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
 
   eos_status es = EOS_OK;
   DevJob* d_jobs = (DevJob*)scratch(ctx, "wf.jobs", sizeof(DevJob) * n_jobs, &es);
-  RayQ* r0 = (RayQ*)scratch(ctx, "wf.r0", sizeof(RayQ) * (size_t)max_chunk, &es);
-  RayQ* r1 = (RayQ*)scratch(ctx, "wf.r1", sizeof(RayQ) * (size_t)max_chunk, &es);
-  HitQ* hits = (HitQ*)scratch(ctx, "wf.hits", sizeof(HitQ) * (size_t)max_chunk, &es);
-  uint32_t* masks = (uint32_t*)scratch(ctx, "wf.masks", 4 * (size_t)max_chunk, &es);
-  size_t cap_s = (size_t)max_chunk * std::max(1, max_lights);
+  const size_t cap_q = (size_t)max_chunk * width;  // rays of one bounce
+  RayQ* r0 = (RayQ*)scratch(ctx, "wf.r0", sizeof(RayQ) * cap_q, &es);
+  RayQ* r1 = (RayQ*)scratch(ctx, "wf.r1", sizeof(RayQ) * cap_q, &es);
+  HitQ* hits = (HitQ*)scratch(ctx, "wf.hits", sizeof(HitQ) * cap_q, &es);
+  uint32_t* masks = (uint32_t*)scratch(ctx, "wf.masks", 4 * cap_q, &es);
+  size_t cap_s = cap_q * std::max(1, max_lights);
   ShadowQ* sq = (ShadowQ*)scratch(ctx, "wf.sq", sizeof(ShadowQ) * cap_s, &es);
-  float4* acc = (float4*)scratch(ctx, "wf.acc", 16 * (size_t)max_chunk * (depth + 1), &es);
+  float4* acc = (float4*)scratch(ctx, "wf.acc", 16 * (size_t)max_chunk * (tree ? nn : depth + 1), &es);
   int* ctr = (int*)scratch(ctx, "wf.ctr", sizeof(int) * kCtr * (depth + 1), &es);
   if (es != EOS_OK) return es;
   EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
 
   const eos_limits& lim = ctx->limits;
-  const LaunchConfig lc = launch_config(p, ctx->num_sms, lim.small_stack != 0);
+  const LaunchConfig lc = launch_config(p, ctx->num_sms, lim.small_stack != 0, tree);
   const int block = lc.block, sh = lc.sh, qchunk = lc.qchunk;
 
   WfArgs A;
@@ -602,8 +718,9 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   A.sq = sq;
   A.acc = acc;
   A.ctr = ctr;
-  A.cap_r = max_chunk;
+  A.cap_r = (int)std::min<size_t>(cap_q, 0x7fffffff);
   A.cap_s = (int)std::min<size_t>(cap_s, 0x7fffffff);
+  A.nn = nn;
   if (lim.queue_entries > 0) {
     A.cap_r = std::min(A.cap_r, (int)lim.queue_entries);
     A.cap_s = std::min(A.cap_s, (int)lim.queue_entries);
@@ -626,7 +743,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
 
   // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
   std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
-                                A.cap_r, A.cap_s, A.work_limit,
+                                (long long)lc.tree, A.cap_r, A.cap_s, A.work_limit,
                                 (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
                                 (long long)(size_t)acc};
@@ -739,8 +856,11 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
       camera->height > kNoAllocMaxPaths)
     return EOS_ERR_INVALID_ARG;
   if (params->trace_depth < 0 || params->trace_depth >= EOS_MAX_BOUNCES || params->spp < 1 ||
-      params->spp > kNoAllocMaxPaths || (params->flags & ~EOS_FLAG_STAGE_TIMING))
+      params->spp > kNoAllocMaxPaths ||
+      (params->flags & ~(EOS_FLAG_STAGE_TIMING | EOS_FLAG_TREE_RECORDS | EOS_FLAG_AA_GRID)))
     return EOS_ERR_INVALID_ARG;
+  // the fixed array holds the one-ray-per-bounce queues only
+  if ((params->flags & EOS_FLAG_TREE_RECORDS) || scene->branching) return EOS_ERR_UNSUPPORTED;
   if (scene->dev.n_lights > kNoAllocMaxLights) return EOS_ERR_INVALID_ARG;
   if ((rgb_out && !is_device_ptr(rgb_out)) || (paths_out && !is_device_ptr(paths_out))) return EOS_ERR_INVALID_ARG;
   const int dev = scene->ctx->device;
@@ -768,7 +888,8 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
   J.row_begin = params->row_begin;
   J.row_end = params->row_end;
   DevJob job;
-  fill_job(J, 0, job);
+  if ((params->flags & EOS_FLAG_AA_GRID) && aa_grid_side(params->spp) == 0) return EOS_ERR_INVALID_ARG;
+  fill_job(J, 0, false, (params->flags & EOS_FLAG_AA_GRID) != 0, job);
   if (job.n_paths > kNoAllocMaxPaths) return EOS_ERR_INVALID_ARG;  // beyond the fixed scratch capacity
 
   cudaStream_t s = (cudaStream_t)stream;
@@ -792,7 +913,8 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
   A.cap_s = kNoAllocMaxPaths * kNoAllocMaxLights;
   // the scene context's tuning table, as eos_render applies it (the table is read here
   // only; it is changed by eos_ctx_set_tuning calls, which callers serialise with renders)
-  const LaunchConfig lc = launch_config(with_tuning(scene->ctx, *params, (uint32_t)scene->dev.n_tris), num_sms, false);
+  const LaunchConfig lc =
+      launch_config(with_tuning(scene->ctx, *params, (uint32_t)scene->dev.n_tris), num_sms, false, false);
   A.qchunk = lc.qchunk;
   A.work_limit = 0x7fffffff;
   A.err = (int*)(base + kNaErr);

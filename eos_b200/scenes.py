@@ -427,10 +427,13 @@ def config5_camera(width=3840, height=2160) -> CameraData:
 
 
 def small_random_scene(seed: int, n_spheres: int = 4, level: int = 2, lights: int = 2,
-                       refl: float = 0.5, transparent: int = 0, ambient_index: float = 1.0) -> SceneData:
+                       refl: float = 0.5, transparent: int = 0, ambient_index: float = 1.0,
+                       both: int = 0) -> SceneData:
     """A few icospheres over a quad: quick scenes for parity edge cases.  The first
     `transparent` spheres get non-reflective transparent materials (refractive index
-    1.333, 1.52 or 2.42 in turn)."""
+    1.333, 1.52 or 2.42 in turn); the next `both` spheres get materials that are both
+    reflective (0.35) and transparent (index 1.45, 1.6 or 1.333 in turn), whose hits spawn
+    two secondary rays."""
     rng = rng_for(seed)
     b = _Builder()
     for k in range(n_spheres):
@@ -438,6 +441,8 @@ def small_random_scene(seed: int, n_spheres: int = 4, level: int = 2, lights: in
         m = _random_material(rng, refl)
         if k < transparent:
             m[7], m[8], m[9] = 0.0, 1.0, (1.333, 1.52, 2.42)[k % 3]
+        elif k < transparent + both:
+            m[7], m[8], m[9] = 0.35, 1.0, (1.45, 1.6, 1.333)[k % 3]
         add_sphere(b, level, center, radius, rot, m)
     b.add(*ground_quad(6.0, -2.5), _random_material(rng, refl))
     ls = [[*rng.uniform([-5, 3, -5], [5, 8, 5]), 1, 1, 1] for _ in range(lights)]

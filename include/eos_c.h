@@ -72,10 +72,10 @@ typedef struct eos_scene eos_scene;
 /* Material of one object (src/Material.h:46-78).  The reference's diffuse/specular are
  * vec4 with an unused alpha and its shininess is an int; reflective = reflectivity > 0,
  * transparent = transparency > 0 (the reference's m_Transparent flag; its value is not
- * used otherwise).  A material may be reflective or transparent, not both
- * (EOS_ERR_UNSUPPORTED): the reference traces two secondary rays for such a hit and the
- * path record holds one per bounce.  The ambient term is unused by the reference renderer
- * (src/RayTracer.cpp:412-413). */
+ * used otherwise).  A material that is both reflective and transparent makes a hit spawn
+ * two secondary rays, as the reference traces them (src/RayTracer.cpp:339-407): the path
+ * becomes a binary tree of rays, whose records need the tree form (EOS_FLAG_TREE_RECORDS).
+ * The ambient term is unused by the reference renderer (src/RayTracer.cpp:412-413). */
 typedef struct eos_material {
   float kd[3];
   float ks[3];
@@ -122,9 +122,21 @@ typedef struct eos_render_params {
 } eos_render_params;
 
 /* Wavefront only: run the stages eagerly (no graph) with CUDA events between them and
- * report per-stage device time in eos_stats.stage_ms.  Other flag bits are refused
- * (EOS_ERR_INVALID_ARG). */
+ * report per-stage device time in eos_stats.stage_ms. */
 #define EOS_FLAG_STAGE_TIMING 1
+/* Path records in tree form: paths_out (eos_render, eos_job, eos_render_backward) holds
+ * EOS_TREE_NODES(trace_depth) eos_tree_node entries per path instead of one
+ * eos_path_record.  Required for path records of a scene with a material that is both
+ * reflective and transparent (chain records of such a scene: EOS_ERR_UNSUPPORTED); any
+ * scene may use it. */
+#define EOS_FLAG_TREE_RECORDS 2
+/* Samples on the reference's anti-aliasing grid (RayTracer::setAASamples / renderWithAA,
+ * src/RayTracer.cpp:176-265): spp = n * n samples per pixel at offsets (p, q) / n,
+ * p, q = 0..n-1, row by row, and the pixel is their sum times (1/n)^2 in the reference's
+ * float order; pixel_offset and jitter_seed are not used.  spp must be a square
+ * (EOS_ERR_INVALID_ARG otherwise).  Without the flag, spp > 1 samples at hashed jitter. */
+#define EOS_FLAG_AA_GRID 4
+/* Other flag bits are refused (EOS_ERR_INVALID_ARG). */
 
 /* Tuned launch / layout parameters of one scene-size bucket (see eos_ctx_set_tuning). */
 typedef struct eos_tuning {
@@ -167,6 +179,16 @@ typedef struct eos_path_record {
   int32_t hit[EOS_MAX_BOUNCES];
   uint32_t shadow[EOS_MAX_BOUNCES];
 } eos_path_record;
+
+/* One node of a tree-form path record.  Nodes in heap order: node 0 the primary ray; node
+ * j's mirror ray is node 2j + 1, its transparent bounce's ray node 2j + 2; node j lies at
+ * bounce floor(log2(j + 1)).  hit: triangle id, EOS_HIT_NONE or EOS_HIT_UNTRACED; shadow:
+ * the blocked-light mask of the node's hit. */
+typedef struct eos_tree_node {
+  int32_t hit;
+  uint32_t shadow;
+} eos_tree_node;
+#define EOS_TREE_NODES(trace_depth) ((1 << ((trace_depth) + 1)) - 1)
 
 typedef struct eos_stats {
   uint64_t primary_rays;
@@ -222,6 +244,10 @@ typedef struct eos_grads {
 /* ---------------------------------------------------------------------------- context */
 int32_t eos_abi_version(void);
 const char* eos_status_string(eos_status s);
+/* The CUDA error behind the calling thread's last EOS_ERR_CUDA / EOS_ERR_OOM: its name,
+ * text and the library source line ("" when none).  No reference counterpart: the
+ * reference prints the error and exits (src/cudaQualifiers.h:35-45). */
+const char* eos_last_error_detail(void);
 /* Number of CUDA devices visible to the process (0 when none). */
 eos_status eos_device_count(int32_t* n);
 eos_status eos_ctx_create(int32_t device, eos_ctx** out);
@@ -387,8 +413,10 @@ eos_status eos_mesh_destroy(eos_mesh* mesh);
  * must be device memory (either may be NULL); stats may be NULL.  params->mode is not
  * read: the call always renders with the wavefront kernels (the same image as either
  * mode); block size, queue chunk and stack depth left at 0 take the scene context's tuned
- * values, as in eos_render; flags other than EOS_FLAG_STAGE_TIMING (ignored here) are
- * refused.  The call waits for its stream.  The first call on a device looks up the
+ * values, as in eos_render; EOS_FLAG_STAGE_TIMING is ignored, EOS_FLAG_AA_GRID applies,
+ * EOS_FLAG_TREE_RECORDS and scenes with a material both reflective and transparent (ray
+ * trees need more than one ray per path and bounce) give EOS_ERR_UNSUPPORTED, other flags
+ * EOS_ERR_INVALID_ARG.  The call waits for its stream.  The first call on a device looks up the
  * array's device address (make that first call before any stream capture).  All calls
  * share the one array: calls that overlap on the GPU race, so serialise them. */
 #define EOS_NOALLOC_MAX_PATHS 16384

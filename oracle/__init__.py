@@ -43,6 +43,19 @@ def build(ref: bool = True) -> None:
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
 
 
+def grid_side(spp: int) -> int:
+    """n for spp = n * n samples on the reference's anti-aliasing grid."""
+    n = int(round(spp ** 0.5))
+    if n * n != spp:
+        raise ValueError("the anti-aliasing grid needs a square number of samples")
+    return n
+
+
+def tree_nodes(trace_depth: int) -> int:
+    """Nodes of a tree record: 2^(trace_depth + 1) - 1 (heap order)."""
+    return (1 << (trace_depth + 1)) - 1
+
+
 def _p(a, ct):
     return a.ctypes.data_as(POINTER(ct)) if a is not None else None
 
@@ -69,7 +82,7 @@ def lib_oracle():
         L.oracle_render.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
                                     c_uint32, POINTER(c_int32), c_int, c_int, POINTER(c_float),
                                     POINTER(c_int32), POINTER(c_uint32), POINTER(c_uint32),
-                                    POINTER(c_longlong)]
+                                    POINTER(c_longlong), c_int]
         L.oracle_closest.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_float),
                                      POINTER(c_uint8)]
         L.oracle_any.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_uint8)]
@@ -80,7 +93,9 @@ def lib_oracle():
         L.oracle_frozen_f64.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_float, c_int, c_uint32,
                                         c_int, POINTER(c_int32), POINTER(c_uint32), POINTER(c_double),
                                         POINTER(c_double), POINTER(c_double), POINTER(c_double),
-                                        POINTER(c_double), POINTER(c_double), c_int]
+                                        POINTER(c_double), POINTER(c_double), c_int, c_int, c_int]
+        L.oracle_render_tree.restype = c_int
+        L.oracle_render_tree.argtypes = L.oracle_render.argtypes
         _lib_oracle = L
     return _lib_oracle
 
@@ -105,10 +120,18 @@ def lib_ref():
                                     POINTER(c_int32), c_int, POINTER(c_float), POINTER(c_int32),
                                     POINTER(c_uint32), POINTER(c_longlong), POINTER(c_double)]
         L.eosref_render_rgba8.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_int,
-                                          POINTER(c_uint8), POINTER(c_double)]
+                                          POINTER(c_uint8), POINTER(c_double), c_int]
+        L.eosref_render_aa.restype = c_int
+        L.eosref_render_aa.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_int, c_int, c_int,
+                                       POINTER(c_int32), c_int, POINTER(c_float), POINTER(c_int32),
+                                       POINTER(c_uint32), POINTER(c_longlong)]
         L.eosref_closest_hit.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_float)]
         L.eosref_any_hit.argtypes = [c_void_p, POINTER(c_float), c_int, POINTER(c_uint8)]
         L.eosref_morton3.argtypes = [POINTER(c_uint32), c_int, POINTER(c_uint32)]
+        L.eosref_render_tree.restype = c_int
+        L.eosref_render_tree.argtypes = [c_void_p, POINTER(c_float), c_int, c_int, c_float, c_int, c_int,
+                                         POINTER(c_int32), c_int, POINTER(c_float), POINTER(c_int32),
+                                         POINTER(c_uint32), POINTER(c_longlong)]
         L.eosref_tree_export.argtypes = [c_void_p, POINTER(c_int32), POINTER(c_int32)]
         L.eosref_tree_boxes.argtypes = [c_void_p, POINTER(c_float)]
         L.eosref_scene_create_from_tree.restype = c_void_p
@@ -172,7 +195,8 @@ class Oracle:
             self.h = None
 
     def render(self, cam, trace_depth: int, pixel_offset: float = 0.5, spp: int = 1, jitter_seed: int = 0,
-               pixels=None, nthreads: int | None = None):
+               pixels=None, nthreads: int | None = None, aa_grid: bool = False):
+        """aa_grid: the reference's n x n anti-aliasing grid (spp = n * n), else hashed jitter."""
         L = lib_oracle()
         px, npix = _pix(pixels)
         n = npix if px is not None else cam.width * cam.height
@@ -184,7 +208,29 @@ class Oracle:
         c12 = cam.as_array()
         L.oracle_render(self.h, _p(c12, c_float), cam.width, cam.height, pixel_offset, trace_depth, spp,
                         jitter_seed, _p(px, c_int32), npix, nthreads or os.cpu_count(), _p(rgb, c_float),
-                        _p(hits, c_int32), _p(shadows, c_uint32), _p(flags, c_uint32), _p(counts, c_longlong))
+                        _p(hits, c_int32), _p(shadows, c_uint32), _p(flags, c_uint32), _p(counts, c_longlong),
+                        grid_side(spp) if aa_grid else 0)
+        return dict(rgb=rgb, hits=hits, shadows=shadows, flags=flags, counts=counts)
+
+    def render_tree(self, cam, trace_depth: int, pixel_offset: float = 0.5, spp: int = 1, jitter_seed: int = 0,
+                    pixels=None, nthreads: int | None = None, aa_grid: bool = False):
+        """As render, with ray trees (materials both reflective and transparent trace both
+        secondary rays): hits / shadows [n*spp, 2^(trace_depth+1) - 1] in heap order (node j's
+        mirror child 2j + 1, transparent child 2j + 2)."""
+        L = lib_oracle()
+        px, npix = _pix(pixels)
+        n = npix if px is not None else cam.width * cam.height
+        nn = tree_nodes(trace_depth)
+        rgb = np.zeros((n, 3), np.float32)
+        hits = np.zeros((n * spp, nn), np.int32)
+        shadows = np.zeros((n * spp, nn), np.uint32)
+        flags = np.zeros(n * spp, np.uint32)
+        counts = np.zeros(3, np.int64)
+        c12 = cam.as_array()
+        L.oracle_render_tree(self.h, _p(c12, c_float), cam.width, cam.height, pixel_offset, trace_depth, spp,
+                             jitter_seed, _p(px, c_int32), npix, nthreads or os.cpu_count(), _p(rgb, c_float),
+                             _p(hits, c_int32), _p(shadows, c_uint32), _p(flags, c_uint32), _p(counts, c_longlong),
+                             grid_side(spp) if aa_grid else 0)
         return dict(rgb=rgb, hits=hits, shadows=shadows, flags=flags, counts=counts)
 
     def closest(self, rays):
@@ -211,12 +257,13 @@ class Oracle:
         return occ
 
     def frozen_f64(self, cams, width, height, pixel_offset, trace_depth, hits, shadows, mat_params,
-                   light_params, g=None, nthreads=None, spp=1, jitter_seed=0):
+                   light_params, g=None, nthreads=None, spp=1, jitter_seed=0, tree=False, aa_grid=False):
         """FP64 re-render with frozen visibility; with g, also the adjoint of <g, rgb>.
 
         hits / shadows: per path, V*H*W*spp of them (samples of a pixel consecutive, the
         forward's order); the colour of a pixel is the mean of its samples, whose offsets
-        come from jitter_seed as in the forward pass.
+        come from jitter_seed as in the forward pass.  Chain records (8 bounces per path)
+        or, with tree=True, tree records (2^(trace_depth+1) - 1 heap-order nodes).
         mat_params: [K, 10] kd rgb, ks rgb, log shininess, reflectivity, transparency, refractive
         index (float64; rows of 8 are opaque)
         light_params: [L, 6] position xyz, colour rgb (float64)
@@ -226,8 +273,9 @@ class Oracle:
         cams_a = np.ascontiguousarray(np.stack([c.as_array() for c in cams]), np.float32)
         nv = len(cams)
         npx = nv * width * height
-        h = np.ascontiguousarray(hits, np.int32).reshape(npx * spp, MAXB)
-        s = np.ascontiguousarray(shadows, np.uint32).reshape(npx * spp, MAXB)
+        slots = tree_nodes(trace_depth) if tree else MAXB
+        h = np.ascontiguousarray(hits, np.int32).reshape(npx * spp, slots)
+        s = np.ascontiguousarray(shadows, np.uint32).reshape(npx * spp, slots)
         mp = np.asarray(mat_params, np.float64)
         if mp.shape[1] == 8:  # no transparency columns: opaque, index 1
             mp = np.concatenate([mp, np.zeros((mp.shape[0], 1)), np.ones((mp.shape[0], 1))], 1)
@@ -241,7 +289,7 @@ class Oracle:
                             int(jitter_seed) & 0xFFFFFFFF, trace_depth,
                             _p(h, c_int32), _p(s, c_uint32), _p(mp, c_double), _p(lp, c_double),
                             _p(rgb, c_double), _p(ga, c_double), _p(gm, c_double), _p(gl, c_double),
-                            nthreads or os.cpu_count())
+                            nthreads or os.cpu_count(), 1 if tree else 0, grid_side(spp) if aa_grid else 0)
         if g is None:
             return rgb
         return rgb, gm, gl
@@ -331,14 +379,50 @@ class RefRenderer:
             raise ValueError("reference renderer rejected trace_depth (it cannot be set below 1)")
         return dict(rgb=rgb, hits=hits, shadows=shadows, counts=counts, seconds=secs.value)
 
-    def render_rgba8(self, cam, trace_depth: int, nthreads=None):
+    def render_tree(self, cam, trace_depth: int, pixel_offset: float = 0.0, pixels=None, nthreads=None):
+        """FP32 colours and ray-tree records (heap order, tree_nodes(trace_depth) per path)."""
+        L = lib_ref()
+        px, npix = _pix(pixels)
+        n = npix if px is not None else cam.width * cam.height
+        nn = tree_nodes(trace_depth)
+        rgb = np.zeros((n, 3), np.float32)
+        hits = np.zeros((n, nn), np.int32)
+        shadows = np.zeros((n, nn), np.uint32)
+        counts = np.zeros(3, np.int64)
+        c12 = cam.as_array()
+        rc = L.eosref_render_tree(self.h, _p(c12, c_float), cam.width, cam.height, pixel_offset, trace_depth,
+                                  nthreads or os.cpu_count(), _p(px, c_int32), npix, _p(rgb, c_float),
+                                  _p(hits, c_int32), _p(shadows, c_uint32), _p(counts, c_longlong))
+        if rc != 0:
+            raise ValueError("reference renderer rejected trace_depth")
+        return dict(rgb=rgb, hits=hits, shadows=shadows, counts=counts)
+
+    def render_rgba8(self, cam, trace_depth: int, nthreads=None, aa: int = 0):
+        """RayTracer::render into RGBA8; aa > 0 = setAASamples(aa) (its anti-aliasing grid)."""
         L = lib_ref()
         out = np.zeros((cam.height, cam.width, 4), np.uint8)
         secs = c_double(0.0)
         c12 = cam.as_array()
         L.eosref_render_rgba8(self.h, _p(c12, c_float), cam.width, cam.height, trace_depth,
-                              nthreads or os.cpu_count(), _p(out, c_uint8), ctypes.byref(secs))
+                              nthreads or os.cpu_count(), _p(out, c_uint8), ctypes.byref(secs), int(aa))
         return out, secs.value
+
+    def render_aa(self, cam, trace_depth: int, aa: int, pixels=None, nthreads=None):
+        """FP32 colours and per-sample paths on the reference's aa x aa grid."""
+        L = lib_ref()
+        px, npix = _pix(pixels)
+        n = npix if px is not None else cam.width * cam.height
+        rgb = np.zeros((n, 3), np.float32)
+        hits = np.zeros((n * aa * aa, MAXB), np.int32)
+        shadows = np.zeros((n * aa * aa, MAXB), np.uint32)
+        counts = np.zeros(3, np.int64)
+        c12 = cam.as_array()
+        rc = L.eosref_render_aa(self.h, _p(c12, c_float), cam.width, cam.height, trace_depth, int(aa),
+                                nthreads or os.cpu_count(), _p(px, c_int32), npix, _p(rgb, c_float),
+                                _p(hits, c_int32), _p(shadows, c_uint32), _p(counts, c_longlong))
+        if rc != 0:
+            raise ValueError("reference renderer rejected trace_depth or aa")
+        return dict(rgb=rgb, hits=hits, shadows=shadows, counts=counts)
 
     def closest(self, rays):
         r = _rays(rays)

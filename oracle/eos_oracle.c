@@ -441,15 +441,33 @@ static inline uint32_t hash32(uint32_t x) {
   return x;
 }
 
-/* Sub-pixel offsets of sample `s` of pixel `p`: the pixel offset for spp == 1, else a
- * hashed jitter in [0, 1). */
+/* 1 / n as RayTracer::renderWithAA computes it: `1.0 / (float) aaSamples`, a double
+ * division stored as float (src/RayTracer.cpp:211). */
+static inline float grid_step(int n) { return (float)(1.0 / (double)(float)n); }
+
+/* Sub-pixel offsets of sample `s` of pixel `p`: the pixel offset for spp == 1; with grid n
+ * the reference's n x n anti-aliasing grid, sample s = q n + p at (p + ksi, q + ksi) / n with
+ * ksi = rand() / RAND_MAX, integer division, 0 (src/RayTracer.cpp:214-227); else a hashed
+ * jitter in [0, 1). */
 static inline void sample_offset(uint32_t p, int smp, int spp, uint32_t seed, float off,
-                                 float* ox, float* oy) {
+                                 float* ox, float* oy, int grid) {
+  if (grid > 0) {
+    const float st = grid_step(grid);
+    *ox = (float)(smp % grid) * st;
+    *oy = (float)(smp / grid) * st;
+    return;
+  }
   if (spp <= 1) { *ox = off; *oy = off; return; }
   uint32_t h1 = hash32(p * 0x9E3779B9u ^ hash32((uint32_t)smp * 0x85EBCA6Bu + seed));
   uint32_t h2 = hash32(h1 ^ 0x68E31DA4u);
   *ox = (float)(h1 >> 8) * (1.0f / 16777216.0f);
   *oy = (float)(h2 >> 8) * (1.0f / 16777216.0f);
+}
+
+/* Weight of a sample in its pixel: 1 / spp, or the grid's inv_aaSamplesSquared (:212). */
+static inline float sample_weight(int spp, int grid) {
+  if (grid > 0) { const float st = grid_step(grid); return st * st; }
+  return 1.0f / (float)spp;
 }
 
 static inline v3f primary_dir(const float* cam, int w, int hgt, int x, int y, float ox, float oy) {
@@ -625,10 +643,117 @@ static v3f trace_path(const oscene* s, const float* cam, v3f o, v3f d, int trace
   return c;
 }
 
+/* ---------------------------------------------------------------- ray trees
+ * A material that is both reflective and transparent makes the reference trace the
+ * mirror ray (src/RayTracer.cpp:339-351) and then the transparent bounce's ray (:353-407)
+ * from the same hit, so a path is a binary tree of rays.  Nodes in heap order: node 0 the
+ * primary ray, node j's mirror child 2j + 1 and transparent child 2j + 2 (node j lies at
+ * bounce floor(log2(j + 1))); a record holds 2^(trace_depth + 1) - 1 nodes.  Colour of a
+ * node as :410 sums it: (phong + refl c_mirror) + (K c_t + (1 - K) c_t), an absent term
+ * being 0; a child beyond trace_depth is not traced and contributes 0 (:275-276). */
+static v3f trace_node(const oscene* s, const float* cam, v3f o, v3f d, int depth, int node, int trace_depth,
+                      int32_t* hits, uint32_t* shadows, uint32_t* flags, counts_t* cnt) {
+  const v3f zero = V3(0.0f, 0.0f, 0.0f);
+  if (depth > trace_depth) return zero;
+  const float eps = 1e-3f;
+  v3f campos = V3(cam[0], cam[1], cam[2]);
+  if (depth == 0) cnt->prim++; else cnt->second++;
+  if (d.x == 0.0f || d.y == 0.0f || d.z == 0.0f) *flags |= FLAG_AXIS_PARALLEL;
+  chit h = closest(s, o, d);
+  if (h.pos < 0) { hits[node] = HIT_NONE; return zero; }
+  hits[node] = h.gid;
+  if (h.t2 < FLT_MAX && fbits(h.t2) - fbits(h.t) <= 2u) *flags |= FLAG_TIE;
+  if (h.t < 1e-3f || h.t > 999.0f) *flags |= FLAG_OUT_OF_RANGE;
+  v3f P, N;
+  int ob;
+  hit_shading(s, &h, o, d, &P, &N, &ob);
+  const float* m = s->mats + OMAT * ob;
+  v3f phong = zero;
+  uint32_t mask = 0;
+  for (int li = 0; li < s->nl; ++li) {
+    const float* l = s->lights + 6 * li;
+    v3f sd = vnorm(vsub(V3(l[0], l[1], l[2]), P));
+    v3f so = vadd(P, vscale(eps, sd));
+    cnt->shadow++;
+    if (sd.x == 0.0f || sd.y == 0.0f || sd.z == 0.0f) *flags |= FLAG_AXIS_PARALLEL;
+    if (any_hit(s, so, sd)) {
+      mask |= 1u << li;
+      chit sh = closest(s, so, sd);
+      if (sh.pos >= 0 && sh.t < 1e-3f) *flags |= FLAG_NEAR_ORIGIN;
+    } else {
+      phong = vadd(phong, phong_one(m, l, P, N, campos));
+    }
+  }
+  shadows[node] = mask;
+  v3f reflected = zero, refracted = zero;
+  if (m[7] > 0.0f) {  /* mirror ray (:339-351) */
+    v3f rd = vnorm(reflect_f(d, N));
+    v3f ro = vadd(P, vscale(eps, rd));
+    v3f c = trace_node(s, cam, ro, rd, depth + 1, 2 * node + 1, trace_depth, hits, shadows, flags, cnt);
+    reflected = vscale(m[7], c);
+  }
+  if (m[8] > 0.0f) {  /* transparent: the mirror ray about the incident-side normal, traced for both halves of the mix */
+    v3f inc = vnorm(d);
+    v3f n = N;
+    float n1 = s->ambient, n2 = m[9];
+    if (!(vdot(inc, N) < 0.0f)) {
+      n1 = m[9];
+      n2 = s->ambient;
+      n = vsub(zero, N);
+    }
+    float K = fresnel_f(inc, n, n1, n2);
+    v3f rd = vnorm(reflect_f(d, n));
+    v3f ro = vadd(P, vscale(eps, n));
+    v3f c = trace_node(s, cam, ro, rd, depth + 1, 2 * node + 2, trace_depth, hits, shadows, flags, cnt);
+    refracted = vadd(vscale(K, c), vscale(1.0f - K, c));
+  }
+  return vadd(vadd(phong, reflected), refracted);
+}
+
+/* As oracle_render with ray trees: hits / shadows [npix*spp, 2^(trace_depth+1) - 1] in heap
+ * order (nodes not reached: HIT_UNTRACED, mask 0). */
+int oracle_render_tree(void* h, const float* cam, int w, int hgt, float pixel_offset, int trace_depth,
+                       int spp, uint32_t jitter_seed, const int32_t* pix, int npix, int nthreads,
+                       float* rgb, int32_t* hits, uint32_t* shadows, uint32_t* flags, long long* counts, int grid) {
+  const oscene* s = (const oscene*)h;
+  if (trace_depth < 0 || trace_depth >= MAXB) return -1;
+  const int nn = (1 << (trace_depth + 1)) - 1;
+  int n = pix ? npix : w * hgt;
+  if (spp < 1) spp = 1;
+  long long c0 = 0, c1 = 0, c2 = 0;
+#pragma omp parallel for schedule(dynamic, 32) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : c0, c1, c2)
+  for (int i = 0; i < n; ++i) {
+    int p = pix ? pix[i] : i;
+    int x = p % w, y = p / w;
+    v3f sum = V3(0, 0, 0);
+    counts_t cnt = {0, 0, 0};
+    int32_t hh[(1 << MAXB) - 1];
+    uint32_t ss[(1 << MAXB) - 1];
+    for (int smp = 0; smp < spp; ++smp) {
+      size_t r = (size_t)i * spp + smp;
+      uint32_t fl = 0;
+      for (int k = 0; k < nn; ++k) { hh[k] = HIT_UNTRACED; ss[k] = 0; }
+      float ox, oy;
+      sample_offset((uint32_t)p, smp, spp, jitter_seed, pixel_offset, &ox, &oy, grid);
+      v3f d = primary_dir(cam, w, hgt, x, y, ox, oy);
+      v3f c = trace_node(s, cam, V3(cam[0], cam[1], cam[2]), d, 0, 0, trace_depth, hh, ss, &fl, &cnt);
+      sum = vadd(sum, c);
+      if (hits) memcpy(hits + r * nn, hh, sizeof(int32_t) * nn);
+      if (shadows) memcpy(shadows + r * nn, ss, sizeof(uint32_t) * nn);
+      if (flags) flags[r] = fl;
+    }
+    if (spp > 1 || grid > 0) sum = vscale(sample_weight(spp, grid), sum);
+    rgb[3 * (size_t)i] = sum.x; rgb[3 * (size_t)i + 1] = sum.y; rgb[3 * (size_t)i + 2] = sum.z;
+    c0 += cnt.prim; c1 += cnt.shadow; c2 += cnt.second;
+  }
+  if (counts) { counts[0] = c0; counts[1] = c1; counts[2] = c2; }
+  return 0;
+}
+
 /* rgb [npix,3]; hits/shadows [npix*spp, 8]; flags [npix*spp]; counts [3]. */
 int oracle_render(void* h, const float* cam, int w, int hgt, float pixel_offset, int trace_depth,
                   int spp, uint32_t jitter_seed, const int32_t* pix, int npix, int nthreads,
-                  float* rgb, int32_t* hits, uint32_t* shadows, uint32_t* flags, long long* counts) {
+                  float* rgb, int32_t* hits, uint32_t* shadows, uint32_t* flags, long long* counts, int grid) {
   const oscene* s = (const oscene*)h;
   int n = pix ? npix : w * hgt;
   if (spp < 1) spp = 1;
@@ -644,7 +769,7 @@ int oracle_render(void* h, const float* cam, int w, int hgt, float pixel_offset,
       int32_t hh[MAXB]; uint32_t ss[MAXB]; uint32_t fl = 0;
       for (int k = 0; k < MAXB; ++k) { hh[k] = HIT_UNTRACED; ss[k] = 0; }
       float ox, oy;
-      sample_offset((uint32_t)p, smp, spp, jitter_seed, pixel_offset, &ox, &oy);
+      sample_offset((uint32_t)p, smp, spp, jitter_seed, pixel_offset, &ox, &oy, grid);
       v3f d = primary_dir(cam, w, hgt, x, y, ox, oy);
       v3f c = trace_path(s, cam, V3(cam[0], cam[1], cam[2]), d, trace_depth, hh, ss, &fl, &cnt);
       sum = vadd(sum, c);
@@ -652,7 +777,7 @@ int oracle_render(void* h, const float* cam, int w, int hgt, float pixel_offset,
       if (shadows) memcpy(shadows + r * MAXB, ss, sizeof ss);
       if (flags) flags[r] = fl;
     }
-    if (spp > 1) sum = vscale(1.0f / (float)spp, sum);
+    if (spp > 1 || grid > 0) sum = vscale(sample_weight(spp, grid), sum);
     rgb[3 * (size_t)i] = sum.x; rgb[3 * (size_t)i + 1] = sum.y; rgb[3 * (size_t)i + 2] = sum.z;
     c0 += cnt.prim; c1 += cnt.shadow; c2 += cnt.second;
   }
@@ -721,145 +846,157 @@ typedef struct {
   const double* lp;  /* nl x 6 */
 } f64ctx;
 
-/* One frozen path in FP64: re-derive each bounce's hit from the stored triangle id and
- * shade it; when g != NULL accumulate the adjoint of <g, colour>. */
-static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, int y, float ox,
-                    float oy, const int32_t* hits, const uint32_t* shadows, int trace_depth,
-                    const double* g, double* gm, double* gl) {
+/* One node of a frozen path in FP64: re-derive the hit from the stored triangle id, shade
+ * it and recurse into the secondary rays; when g != NULL accumulate the adjoint of
+ * <g, colour>.  T = the product of the weights from the primary ray: reflectivity for a
+ * mirror edge, 1 for a transparent one (its Fresnel mix K c + (1 - K) c of one colour).
+ * Records: chain form (tree = 0, slot = bounce k; one secondary ray per hit, the mirror
+ * ray before the transparent one as the chain renderer takes them) or tree form (tree = 1,
+ * slot = heap node: mirror child 2j + 1, transparent child 2j + 2, both traced). */
+static void f64_node(const f64ctx* c, v3d campos, v3d o, v3d d, int k, int node, double T, const int32_t* hits,
+                     const uint32_t* shadows, int tree, int trace_depth, const double* g, double* gm, double* gl,
+                     v3d* col) {
   const oscene* s = c->s;
+  const int slot = tree ? node : k;
+  const int id = hits[slot];
+  if (id < 0) return;
+  const uint32_t mask = shadows[slot];
+  /* the triangle: flat scene, or (two-level) the instance holding global id `id`, its
+   * mesh, the ray in object space (o' = Minv [o, 1], d' = Minv [d, 0]: t is the same
+   * parameter) and the normal back through Minv^T */
+  const oscene* ms = s;
+  const float* minv = NULL;
+  int base = 0, local = id;
+  if (s->ninst) {
+    int lo = 0, hi = s->ninst - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (s->inst_id_off[mid] <= id) lo = mid; else hi = mid - 1;
+    }
+    ms = (const oscene*)s->inst_mesh[lo];
+    minv = s->inst_minv + 12 * lo;
+    base = s->inst_mat_base[lo];
+    local = id - s->inst_id_off[lo];
+  }
+  int p = ms->pos_of_id[local];
+  v3d oo = o, od = d;
+  if (minv) {
+    oo = D3(minv[0] * o.x + minv[1] * o.y + minv[2] * o.z + minv[3],
+            minv[4] * o.x + minv[5] * o.y + minv[6] * o.z + minv[7],
+            minv[8] * o.x + minv[9] * o.y + minv[10] * o.z + minv[11]);
+    od = D3(minv[0] * d.x + minv[1] * d.y + minv[2] * d.z, minv[4] * d.x + minv[5] * d.y + minv[6] * d.z,
+            minv[8] * d.x + minv[9] * d.y + minv[10] * d.z);
+  }
+  v3d v1 = f2d(ms->v1[p]), e1 = f2d(ms->e1[p]), e2 = f2d(ms->e2[p]);
+  v3d Pm = dcross(od, e2);
+  double det = ddot(e1, Pm);
+  v3d Tv = dsub(oo, v1);
+  v3d Q = dcross(Tv, e1);
+  double t = ddot(e2, Q) / det, u = ddot(Tv, Pm) / det, v = ddot(od, Q) / det;
+  v3d P = dadd(o, dsc(t, d));
+  v3d n = dadd(dadd(dsc(1.0 - u - v, f2d(ms->n1[p])), dsc(u, f2d(ms->n2[p]))), dsc(v, f2d(ms->n3[p])));
+  if (minv) {
+    n = dnorm(n);
+    n = D3(minv[0] * n.x + minv[4] * n.y + minv[8] * n.z, minv[1] * n.x + minv[5] * n.y + minv[9] * n.z,
+           minv[2] * n.x + minv[6] * n.y + minv[10] * n.z);
+  }
+  v3d N = dnorm(n);
+  int ob = (int)ms->obj[p] + base;
+  const double* m = c->mp + OMAT * ob;
+  double shin = exp(m[6]);
+  v3d V = dnorm(dsub(campos, P));
+  for (int li = 0; li < s->nl; ++li) {
+    if (mask & (1u << li)) continue;
+    const double* l = c->lp + 6 * li;
+    v3d uvec = dsub(D3(l[0], l[1], l[2]), P);
+    double ul = dlen(uvec);
+    v3d L = dsc(1.0 / ul, uvec);
+    double ndl = ddot(N, L);
+    v3d wv = dsub(dsc(2.0 * ndl, N), L);
+    double wl = dlen(wv);
+    v3d R = dsc(1.0 / wl, wv);
+    double fd = ndl > 0.0 ? ndl : 0.0;
+    double vr = ddot(V, R);
+    double fs = vr > 0.0 ? pow(vr, shin) : 0.0;
+    double C[3] = {l[3], l[4], l[5]};
+    col->x += T * (fd * m[0] * C[0] + fs * C[0] * m[3]);
+    col->y += T * (fd * m[1] * C[1] + fs * C[1] * m[4]);
+    col->z += T * (fd * m[2] * C[2] + fs * C[2] * m[5]);
+    if (!g) continue;
+    double* gmo = gm + 7 * ob;
+    double* glo = gl + 6 * li;
+    double a = 0.0, b = 0.0, sl = 0.0;
+    for (int ch = 0; ch < 3; ++ch) {
+      double gc = g[ch] * T;
+      gmo[ch] += gc * fd * C[ch];
+      gmo[3 + ch] += gc * fs * C[ch];
+      glo[ch] += gc * (fd * m[ch] + fs * m[3 + ch]);
+      a += gc * C[ch] * m[ch];
+      b += gc * C[ch] * m[3 + ch];
+    }
+    if (vr > 0.0) {
+      sl = b * fs * log(vr) * shin;
+      gmo[6] += sl;
+    }
+    v3d gp = D3(0, 0, 0);
+    if (ndl > 0.0) {
+      v3d gd = dsc(1.0 / ul, dsub(N, dsc(ndl, L)));
+      gp = dadd(gp, dsc(a, gd));
+    }
+    if (vr > 0.0) {
+      v3d q = dsc(1.0 / wl, dsub(V, dsc(vr, R)));
+      v3d q2 = dsub(dsc(2.0 * ddot(N, q), N), q);
+      v3d gs = dsc(1.0 / ul, dsub(q2, dsc(ddot(L, q2), L)));
+      double dfs = shin * pow(vr, shin - 1.0);
+      gp = dadd(gp, dsc(b * dfs, gs));
+    }
+    glo[3] += gp.x; glo[4] += gp.y; glo[5] += gp.z;
+  }
+  if (k + 1 > trace_depth) return;
+  if (m[7] > 0.0) {
+    v3d rd = dnorm(dsub(d, dsc(2.0 * ddot(N, d), N)));
+    f64_node(c, campos, dadd(P, dsc(1e-3, rd)), rd, k + 1, 2 * node + 1, T * m[7], hits, shadows, tree,
+             trace_depth, g, gm, gl, col);
+    if (!tree) return;
+  }
+  if (m[8] > 0.0) {
+    v3d n = ddot(dnorm(d), N) < 0.0 ? N : dsc(-1.0, N);
+    v3d rd = dnorm(dsub(d, dsc(2.0 * ddot(n, d), n)));
+    f64_node(c, campos, dadd(P, dsc(1e-3, n)), rd, k + 1, 2 * node + 2, T, hits, shadows, tree, trace_depth, g,
+             gm, gl, col);
+  }
+}
+
+/* One frozen path in FP64 from its primary ray (see f64_node). */
+static v3d f64_path(const f64ctx* c, const float* cam, int w, int hgt, int x, int y, float ox,
+                    float oy, const int32_t* hits, const uint32_t* shadows, int tree, int trace_depth,
+                    const double* g, double* gm, double* gl) {
   double nw = w / 2.0, nh = hgt / 2.0;
   double aa = ((x + (double)ox) - nw) / nw, bb = ((y + (double)oy) - nh) / nh;
   v3d campos = D3(cam[0], cam[1], cam[2]);
   v3d d = dnorm(dadd(dadd(dsc(aa, D3(cam[6], cam[7], cam[8])), dsc(bb, D3(cam[9], cam[10], cam[11]))),
                      D3(cam[3], cam[4], cam[5])));
-  v3d o = campos;
   v3d col = D3(0, 0, 0);
-  double T = 1.0;
-  for (int k = 0; k <= trace_depth && k < MAXB; ++k) {
-    int id = hits[k];
-    if (id < 0) break;
-    /* the triangle: flat scene, or (two-level) the instance holding global id `id`, its
-     * mesh, the ray in object space (o' = Minv [o, 1], d' = Minv [d, 0]: t is the same
-     * parameter) and the normal back through Minv^T */
-    const oscene* ms = s;
-    const float* minv = NULL;
-    int base = 0, local = id;
-    if (s->ninst) {
-      int lo = 0, hi = s->ninst - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (s->inst_id_off[mid] <= id) lo = mid; else hi = mid - 1;
-      }
-      ms = (const oscene*)s->inst_mesh[lo];
-      minv = s->inst_minv + 12 * lo;
-      base = s->inst_mat_base[lo];
-      local = id - s->inst_id_off[lo];
-    }
-    int p = ms->pos_of_id[local];
-    v3d oo = o, od = d;
-    if (minv) {
-      oo = D3(minv[0] * o.x + minv[1] * o.y + minv[2] * o.z + minv[3],
-              minv[4] * o.x + minv[5] * o.y + minv[6] * o.z + minv[7],
-              minv[8] * o.x + minv[9] * o.y + minv[10] * o.z + minv[11]);
-      od = D3(minv[0] * d.x + minv[1] * d.y + minv[2] * d.z, minv[4] * d.x + minv[5] * d.y + minv[6] * d.z,
-              minv[8] * d.x + minv[9] * d.y + minv[10] * d.z);
-    }
-    v3d v1 = f2d(ms->v1[p]), e1 = f2d(ms->e1[p]), e2 = f2d(ms->e2[p]);
-    v3d Pm = dcross(od, e2);
-    double det = ddot(e1, Pm);
-    v3d Tv = dsub(oo, v1);
-    v3d Q = dcross(Tv, e1);
-    double t = ddot(e2, Q) / det, u = ddot(Tv, Pm) / det, v = ddot(od, Q) / det;
-    v3d P = dadd(o, dsc(t, d));
-    v3d n = dadd(dadd(dsc(1.0 - u - v, f2d(ms->n1[p])), dsc(u, f2d(ms->n2[p]))), dsc(v, f2d(ms->n3[p])));
-    if (minv) {
-      n = dnorm(n);
-      n = D3(minv[0] * n.x + minv[4] * n.y + minv[8] * n.z, minv[1] * n.x + minv[5] * n.y + minv[9] * n.z,
-             minv[2] * n.x + minv[6] * n.y + minv[10] * n.z);
-    }
-    v3d N = dnorm(n);
-    int ob = (int)ms->obj[p] + base;
-    const double* m = c->mp + OMAT * ob;
-    double shin = exp(m[6]);
-    v3d V = dnorm(dsub(campos, P));
-    for (int li = 0; li < s->nl; ++li) {
-      if (shadows[k] & (1u << li)) continue;
-      const double* l = c->lp + 6 * li;
-      v3d uvec = dsub(D3(l[0], l[1], l[2]), P);
-      double ul = dlen(uvec);
-      v3d L = dsc(1.0 / ul, uvec);
-      double ndl = ddot(N, L);
-      v3d wv = dsub(dsc(2.0 * ndl, N), L);
-      double wl = dlen(wv);
-      v3d R = dsc(1.0 / wl, wv);
-      double fd = ndl > 0.0 ? ndl : 0.0;
-      double vr = ddot(V, R);
-      double fs = vr > 0.0 ? pow(vr, shin) : 0.0;
-      double C[3] = {l[3], l[4], l[5]};
-      col.x += T * (fd * m[0] * C[0] + fs * C[0] * m[3]);
-      col.y += T * (fd * m[1] * C[1] + fs * C[1] * m[4]);
-      col.z += T * (fd * m[2] * C[2] + fs * C[2] * m[5]);
-      if (!g) continue;
-      double* gmo = gm + 7 * ob;
-      double* glo = gl + 6 * li;
-      double a = 0.0, b = 0.0, sl = 0.0;
-      for (int ch = 0; ch < 3; ++ch) {
-        double gc = g[ch] * T;
-        gmo[ch] += gc * fd * C[ch];
-        gmo[3 + ch] += gc * fs * C[ch];
-        glo[ch] += gc * (fd * m[ch] + fs * m[3 + ch]);
-        a += gc * C[ch] * m[ch];
-        b += gc * C[ch] * m[3 + ch];
-      }
-      if (vr > 0.0) {
-        sl = b * fs * log(vr) * shin;
-        gmo[6] += sl;
-      }
-      v3d gp = D3(0, 0, 0);
-      if (ndl > 0.0) {
-        v3d gd = dsc(1.0 / ul, dsub(N, dsc(ndl, L)));
-        gp = dadd(gp, dsc(a, gd));
-      }
-      if (vr > 0.0) {
-        v3d q = dsc(1.0 / wl, dsub(V, dsc(vr, R)));
-        v3d q2 = dsub(dsc(2.0 * ddot(N, q), N), q);
-        v3d gs = dsc(1.0 / ul, dsub(q2, dsc(ddot(L, q2), L)));
-        double dfs = shin * pow(vr, shin - 1.0);
-        gp = dadd(gp, dsc(b * dfs, gs));
-      }
-      glo[3] += gp.x; glo[4] += gp.y; glo[5] += gp.z;
-    }
-    if (k + 1 > trace_depth) break;
-    if (m[7] > 0.0) {
-      T *= m[7];
-      v3d rd = dnorm(dsub(d, dsc(2.0 * ddot(N, d), N)));
-      o = dadd(P, dsc(1e-3, rd));
-      d = rd;
-    } else if (m[8] > 0.0) {
-      /* transparent: the Fresnel mix K c + (1 - K) c of one colour, weight 1 */
-      v3d n = ddot(dnorm(d), N) < 0.0 ? N : dsc(-1.0, N);
-      v3d rd = dnorm(dsub(d, dsc(2.0 * ddot(n, d), n)));
-      o = dadd(P, dsc(1e-3, n));
-      d = rd;
-    } else {
-      break;
-    }
-  }
+  f64_node(c, campos, campos, d, 0, 0, 1.0, hits, shadows, tree, trace_depth, g, gm, gl, &col);
   return col;
 }
 
 /* Frozen-visibility FP64 render of n_views cameras (cams: n_views x 12; every view has
- * w x hgt pixels and spp == 1 at pixel_offset).  hits / shadows: [n_views*w*hgt, 8].
+ * w x hgt pixels, spp samples from seed at pixel_offset).  hits / shadows:
+ * [n_views*w*hgt*spp, 8] (chain records) or [.., 2^(trace_depth+1) - 1] (tree = 1).
  * rgb_out: [n_views*w*hgt, 3].  If g is non-NULL, also writes gradients of <g, rgb>. */
 int oracle_frozen_f64(void* h, const float* cams, int n_views, int w, int hgt, float pixel_offset,
                       int spp, uint32_t seed, int trace_depth, const int32_t* hits, const uint32_t* shadows,
                       const double* mat_params, const double* light_params, double* rgb_out,
-                      const double* g, double* grad_mat, double* grad_light, int nthreads) {
+                      const double* g, double* grad_mat, double* grad_light, int nthreads, int tree, int grid) {
   /* Paths are per sample (pixel-major, samples of a pixel consecutive, the forward's
-   * order); a pixel's colour is the sample mean, so each sample's adjoint is g / spp. */
+   * order); a pixel's colour is the sample mean (on the reference's grid: the sum times
+   * (1/n)^2), so each sample's adjoint is g times that weight. */
   const oscene* s = (const oscene*)h;
   f64ctx c = {s, mat_params, light_params};
   size_t npx = (size_t)w * hgt;
+  /* record slots per path: 8 bounces (chain form) or the 2^(trace_depth+1) - 1 tree nodes */
+  const long long rec = tree ? (1ll << (trace_depth + 1)) - 1 : MAXB;
   if (spp < 1) spp = 1;
   int nth = nthreads > 0 ? nthreads : 1;
   size_t gms = (size_t)7 * s->nobj, gls = (size_t)6 * s->nl;
@@ -874,17 +1011,18 @@ int oracle_frozen_f64(void* h, const float* cams, int n_views, int w, int hgt, f
       int p = (int)(i % (long long)npx);
       const float* cam = cams + 12 * view;
       double gs[3];
-      if (g) for (int k = 0; k < 3; ++k) gs[k] = g[3 * i + k] / spp;
+      const double wsmp = grid > 0 ? (double)sample_weight(spp, grid) : 1.0 / spp;
+      if (g) for (int k = 0; k < 3; ++k) gs[k] = g[3 * i + k] * wsmp;
       v3d sum = D3(0, 0, 0);
       for (int smp = 0; smp < spp; ++smp) {
         float ox, oy;
-        sample_offset((uint32_t)p, smp, spp, seed, pixel_offset, &ox, &oy);
+        sample_offset((uint32_t)p, smp, spp, seed, pixel_offset, &ox, &oy, grid);
         long long path = i * spp + smp;
-        v3d col = f64_path(&c, cam, w, hgt, p % w, p / w, ox, oy, hits + MAXB * path, shadows + MAXB * path,
+        v3d col = f64_path(&c, cam, w, hgt, p % w, p / w, ox, oy, hits + rec * path, shadows + rec * path, tree,
                            trace_depth, g ? gs : NULL, g ? gmt + gms * tid : NULL, g ? glt + gls * tid : NULL);
         sum = dadd(sum, col);
       }
-      sum = dsc(1.0 / spp, sum);
+      sum = dsc(wsmp, sum);
       if (rgb_out) { rgb_out[3 * i] = sum.x; rgb_out[3 * i + 1] = sum.y; rgb_out[3 * i + 2] = sum.z; }
     }
   }

@@ -196,6 +196,55 @@ void scan_leaves(RefScene* rs) {
     if (nodes[i].type == BVH_LEAF) rs->max_leaf = std::max(rs->max_leaf, nodes[i].numSurfacesEncapulated);
 }
 
+// Ray tree of one primary ray, node j's mirror child 2j + 1 and transparent child 2j + 2:
+// the same queries and rays as RayTracer::rayTrace / shadeIntersection, which for a
+// material that is both reflective and transparent traces the mirror ray (:339-351) and
+// then the transparent bounce's ray (:353-407) from the same hit.
+void replay_node(const RefScene& rs, const Ray& ray, int depth, int node, int trace_depth, int32_t* hits,
+                 uint32_t* shadows, long long* cnt) {
+  const float epsilon = 1e-3f;
+  if (depth > trace_depth) return;
+  const Scene& scene = rs.scene;
+  RayIntersection isect;
+  cnt[depth == 0 ? 0 : 2]++;
+  if (!scene.findMinDistanceIntersectionBVH(ray, isect)) {
+    hits[node] = kHitNone;
+    return;
+  }
+  const int id = isect.getMaterialIndex();
+  hits[node] = id;
+  const glm::vec3& P = isect.getPoint();
+  uint32_t mask = 0;
+  for (int i = 0; i < scene.getNumLightSources(); ++i) {
+    const LightSource* light = scene.getLightSource(i);
+    glm::vec3 sd = glm::normalize(glm::vec3(light->getPosition()) - P);
+    Ray sray;
+    sray.setOrigin(P + epsilon * sd);
+    sray.setDirection(sd);
+    cnt[1]++;
+    if (scene.shadowRayVisibilityBVH(sray)) mask |= 1u << i;
+  }
+  shadows[node] = mask;
+  const Material& m = scene.getMaterialAtIndex(id);
+  if (m.isReflective()) {
+    glm::vec3 rd = glm::normalize(glm::reflect(ray.getDirection(), isect.getNormal()));
+    Ray r;
+    r.setOrigin(P + epsilon * rd);
+    r.setDirection(rd);
+    replay_node(rs, r, depth + 1, 2 * node + 1, trace_depth, hits, shadows, cnt);
+  }
+  if (m.isTransparent()) {
+    glm::vec3 incident = glm::normalize(ray.getDirection());
+    glm::vec3 n = isect.getNormal();
+    if (!(glm::dot(incident, n) < 0.0f)) n = glm::vec3(0.0f) - isect.getNormal();
+    glm::vec3 rd = glm::normalize(glm::reflect(ray.getDirection(), n));
+    Ray r;
+    r.setOrigin(P + epsilon * n);
+    r.setDirection(rd);
+    replay_node(rs, r, depth + 1, 2 * node + 2, trace_depth, hits, shadows, cnt);
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -368,14 +417,99 @@ int eosref_render(void* h, const float* cam12, int w, int hgt, float pixel_offse
   return 0;
 }
 
-// The reference's own frame call, RayTracer::render (src/RayTracer.cpp:85-174), into a
-// caller-owned RGBA8 buffer.  This is what the CPU baseline times.
-int eosref_render_rgba8(void* h, const float* cam12, int w, int hgt, int trace_depth, int nthreads,
-                        unsigned char* out, double* seconds) {
+// As eosref_render with ray-tree records: hits / shadows [npix, 2^(trace_depth+1) - 1] in
+// heap order (replay_node).
+int eosref_render_tree(void* h, const float* cam12, int w, int hgt, float pixel_offset, int trace_depth,
+                       int nthreads, const int32_t* pix, int npix, float* rgb, int32_t* hits, uint32_t* shadows,
+                       long long* counts) {
   RefScene* rs = (RefScene*)h;
   Camera cam = make_camera(cam12, w, hgt);
   RayTracer rt;
   rt.setAASamples(RAYTRACER_NO_AA);
+  rt.setTracedDepth(trace_depth);
+  if (rt.getTracedDepth() != trace_depth || trace_depth >= kMaxBounces) return -1;
+  const int nn = (1 << (trace_depth + 1)) - 1;
+  int n = pix ? npix : w * hgt;
+  long long c0 = 0, c1 = 0, c2 = 0;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : c0, c1, c2)
+  for (int i = 0; i < n; ++i) {
+    int p = pix ? pix[i] : i;
+    int x = p % w, y = p / w;
+    Ray ray = primary_ray(cam, x, y, pixel_offset, pixel_offset);
+    glm::vec4 c = rt.rayTrace(rs->scene, cam, ray, 0);
+    rgb[3 * i] = c.x;
+    rgb[3 * i + 1] = c.y;
+    rgb[3 * i + 2] = c.z;
+    int32_t* hh = hits + (size_t)nn * i;
+    uint32_t* ss = shadows + (size_t)nn * i;
+    for (int k = 0; k < nn; ++k) { hh[k] = kHitUntraced; ss[k] = 0; }
+    long long cnt[3] = {0, 0, 0};
+    replay_node(*rs, ray, 0, 0, trace_depth, hh, ss, cnt);
+    c0 += cnt[0];
+    c1 += cnt[1];
+    c2 += cnt[2];
+  }
+  if (counts) { counts[0] = c0; counts[1] = c1; counts[2] = c2; }
+  return 0;
+}
+
+// Colours and paths on the reference's anti-aliasing grid (RayTracer::renderWithAA,
+// src/RayTracer.cpp:176-265): per pixel aa x aa samples at ((p + ksi) / aa, (q + ksi) / aa),
+// ksi = rand() / RAND_MAX = 0 in its integer arithmetic, summed in that order and scaled by
+// inv_aaSamples^2.  hits / shadows [npix * aa * aa, 8], samples of a pixel consecutive.
+int eosref_render_aa(void* h, const float* cam12, int w, int hgt, int trace_depth, int aa, int nthreads,
+                     const int32_t* pix, int npix, float* rgb, int32_t* hits, uint32_t* shadows,
+                     long long* counts) {
+  RefScene* rs = (RefScene*)h;
+  Camera cam = make_camera(cam12, w, hgt);
+  RayTracer rt;
+  rt.setAASamples(aa);
+  rt.setTracedDepth(trace_depth);
+  if (rt.getTracedDepth() != trace_depth || aa < 1) return -1;
+  const float inv = 1.0 / (float)aa;
+  const float inv2 = inv * inv;
+  const int n = pix ? npix : w * hgt;
+  long long c0 = 0, c1 = 0, c2 = 0;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : c0, c1, c2)
+  for (int i = 0; i < n; ++i) {
+    int p0 = pix ? pix[i] : i;
+    int x = p0 % w, y = p0 / w;
+    glm::vec4 sum(0.0f);
+    for (int q = 0; q < aa; ++q) {
+      for (int p = 0; p < aa; ++p) {
+        const float ksi = 0.0f;
+        Ray ray = primary_ray(cam, x, y, (p + ksi) * inv, (q + ksi) * inv);
+        sum += rt.rayTrace(rs->scene, cam, ray, 0);
+        if (hits) {
+          const size_t r = (size_t)i * aa * aa + q * aa + p;
+          int32_t* hh = hits + kMaxBounces * r;
+          uint32_t* ss = shadows + kMaxBounces * r;
+          for (int k = 0; k < kMaxBounces; ++k) { hh[k] = kHitUntraced; ss[k] = 0; }
+          long long cnt[3] = {0, 0, 0};
+          replay_path(*rs, ray, trace_depth, hh, ss, cnt);
+          c0 += cnt[0];
+          c1 += cnt[1];
+          c2 += cnt[2];
+        }
+      }
+    }
+    sum = sum * inv2;
+    rgb[3 * i] = sum.x;
+    rgb[3 * i + 1] = sum.y;
+    rgb[3 * i + 2] = sum.z;
+  }
+  if (counts) { counts[0] = c0; counts[1] = c1; counts[2] = c2; }
+  return 0;
+}
+
+// The reference's own frame call, RayTracer::render (src/RayTracer.cpp:85-265), into a
+// caller-owned RGBA8 buffer; aa > 0 = setAASamples(aa), its anti-aliasing grid.
+int eosref_render_rgba8(void* h, const float* cam12, int w, int hgt, int trace_depth, int nthreads,
+                        unsigned char* out, double* seconds, int aa) {
+  RefScene* rs = (RefScene*)h;
+  Camera cam = make_camera(cam12, w, hgt);
+  RayTracer rt;
+  rt.setAASamples(aa > 0 ? aa : RAYTRACER_NO_AA);
   rt.setTracedDepth(trace_depth);
   int prev = omp_get_max_threads();
   omp_set_num_threads(nthreads > 0 ? nthreads : 1);

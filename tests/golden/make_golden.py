@@ -7,6 +7,8 @@ tests read these files there.
 
     python tests/golden/make_golden.py            (all fixtures)
     python tests/golden/make_golden.py config2    (the 1.06M-triangle sample only)
+    python tests/golden/make_golden.py trees      (the ray-tree scene only)
+    python tests/golden/make_golden.py aa         (the anti-aliasing grid case only)
 """
 from __future__ import annotations
 
@@ -47,6 +49,41 @@ def morton_case():
     print("morton3", codes[:10])
 
 
+def tree_scene():
+    """Spheres whose materials are both reflective and transparent (each hit on them spawns
+    two secondary rays) beside a transparent one and mirrors, in air."""
+    return scenes.small_random_scene(91, n_spheres=7, level=2, lights=3, refl=0.5, transparent=1, both=3,
+                                     ambient_index=1.0002)
+
+
+def tree_case():
+    """Ray-tree records (heap order) and FP32 colours of the reference on tree_scene()."""
+    sc = tree_scene()
+    cam = scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 96, 72)
+    td = 3
+    ref = oracle.RefRenderer(sc, build_threads=1)
+    r = ref.render_tree(cam, td, pixel_offset=0.0, nthreads=os.cpu_count())
+    np.savez_compressed(os.path.join(HERE, "both91.npz"), rgb=r["rgb"], hits=r["hits"],
+                        shadows=r["shadows"].astype(np.uint8), counts=r["counts"], cam=cam.as_array(),
+                        size=np.array([cam.width, cam.height, td]), ref_nodes=np.array([ref.n_nodes, ref.max_leaf]))
+    print("both91", r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
+
+
+def aa_case():
+    """The reference's anti-aliasing grid (RayTracer::setAASamples(3), renderWithAA): FP32
+    colours, per-sample paths and the reference's own RGBA8 frame."""
+    sc = scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 48, 36)
+    td, n = 2, 3
+    ref = oracle.RefRenderer(sc, build_threads=1)
+    r = ref.render_aa(cam, td, n, nthreads=os.cpu_count())
+    rgba8, _ = ref.render_rgba8(cam, td, nthreads=os.cpu_count(), aa=n)
+    np.savez_compressed(os.path.join(HERE, "aa3_small12.npz"), rgb=r["rgb"], hits=r["hits"][:, :td + 1],
+                        shadows=r["shadows"][:, :td + 1].astype(np.uint8), counts=r["counts"], rgba8=rgba8,
+                        cam=cam.as_array(), size=np.array([cam.width, cam.height, td, n]))
+    print("aa3_small12", r["counts"])
+
+
 def config2_case(n_sample=30_000):
     """30,000 seeded pixels of the 1080p view of the 1,056,768-triangle scene (depth 3, 4
     lights, pixel centres) through the reference's renderer, with the tree its own builder
@@ -72,6 +109,12 @@ def main():
     if sys.argv[1:] == ["config2"]:
         config2_case()
         return
+    if sys.argv[1:] == ["trees"]:
+        tree_case()
+        return
+    if sys.argv[1:] == ["aa"]:
+        aa_case()
+        return
     morton_case()
     render_case("config1_128", scenes.config1_scene(), scenes.config1_camera(128, 128), 1)
     for seed in (11, 12):
@@ -81,6 +124,8 @@ def main():
     # transparent spheres (Fresnel-mixed secondary rays) in air
     sc = scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3, ambient_index=1.0002)
     render_case("transp61", sc, scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 96, 72), 4)
+    tree_case()
+    aa_case()
     config2_case()
 
 

@@ -295,3 +295,105 @@ def test_ploc_restatement_small_cases():
         leaves[k] = s
         p = np.sort(pos[s])
         assert p[-1] - p[0] + 1 == len(s) == count[k]  # each subtree a contiguous range
+
+
+# ----------------------------------------------------------------------------- ray trees
+def tree_scene():
+    return scenes.small_random_scene(91, n_spheres=7, level=2, lights=3, refl=0.5, transparent=1, both=3,
+                                     ambient_index=1.0002)
+
+
+def test_oracle_tree_matches_reference_golden():
+    """Materials both reflective and transparent: the reference traces both secondary rays
+    (src/RayTracer.cpp:339-407).  The oracle's ray trees (heap order) and FP32 colours vs
+    the reference's own renderer (golden file both91.npz): bit-exact."""
+    g = load("both91")
+    W, H, td = (int(v) for v in g["size"])
+    cam = scenes.CameraData(*[g["cam"][3 * i:3 * i + 3] for i in range(4)], W, H)
+    r = oracle.Oracle(tree_scene()).render_tree(cam, td, pixel_offset=0.0)
+    assert r["hits"].shape[1] == oracle.tree_nodes(td) == 15
+    mm = (r["hits"] != g["hits"]).any(1) | (r["shadows"] != g["shadows"]).any(1)
+    c = classify(mm, r["flags"])
+    assert c["unexplained"] == 0 and c["mismatch"] == 0, c
+    assert np.array_equal(r["rgb"].view(np.uint32), g["rgb"].view(np.uint32))
+    assert np.array_equal(r["counts"], g["counts"])
+    # the case is exercised: paths whose hits on both children of one node were traced
+    both = ((r["hits"][:, 1:15:2] != -2) & (r["hits"][:, 2:15:2] != -2)).any(1)
+    assert both.sum() > 50
+
+
+def test_oracle_tree_render_equals_chain_render_on_chain_scenes():
+    """Without such materials the tree form holds the chain: same colours bit for bit, same
+    ray counts, and every chain bounce's record at its node."""
+    sc = scenes.small_random_scene(11, n_spheres=5, level=2, lights=3, refl=0.6, transparent=2)
+    cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 64, 48)
+    orc = oracle.Oracle(sc)
+    a = orc.render(cam, 3, pixel_offset=0.5)
+    b = orc.render_tree(cam, 3, pixel_offset=0.5)
+    assert np.array_equal(a["rgb"].view(np.uint32), b["rgb"].view(np.uint32))
+    assert np.array_equal(a["counts"], b["counts"])
+    mats = sc.materials[sc.tri_obj]  # per-triangle material rows
+    for p in range(a["hits"].shape[0]):
+        node = 0
+        for k in range(4):
+            assert b["hits"][p, node] == a["hits"][p, k] and b["shadows"][p, node] == a["shadows"][p, k]
+            h = a["hits"][p, k]
+            if h < 0 or k == 3:
+                break
+            node = 2 * node + (1 if mats[h, 7] > 0 else 2)
+
+
+def test_frozen_f64_tree_adjoint_matches_central_differences():
+    """The FP64 adjoint over ray trees (mirror edge weight = reflectivity, transparent edge
+    weight 1) vs central differences of the FP64 frozen tree render, and its colours vs the
+    FP32 tree render."""
+    sc = tree_scene()
+    cams = [scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 24, 20)]
+    orc = oracle.Oracle(sc)
+    td = 3
+    r = orc.render_tree(cams[0], td, pixel_offset=0.5)
+    hits, shadows = r["hits"], r["shadows"]
+    mp = sc.materials.astype(np.float64).copy()
+    mp[:, 6] = np.log(mp[:, 6])
+    lp = sc.lights.astype(np.float64).copy()
+    target = np.random.default_rng(4).uniform(0, 0.5, (24 * 20, 3))
+
+    def loss(m, l):
+        rgb = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, m, l, tree=True)
+        return float(((rgb - target) ** 2).sum()), rgb
+
+    L0, rgb = loss(mp, lp)
+    assert np.abs(rgb - r["rgb"]).max() < 1e-3
+    g = 2.0 * (rgb - target)
+    _, gm, gl = orc.frozen_f64(cams, 24, 20, 0.5, td, hits, shadows, mp, lp, g=g, tree=True)
+    h = 1e-3
+    for kind, i, col in [("m", 1, 0), ("m", 2, 4), ("m", 3, 6), ("m", 7, 1), ("l", 0, 3), ("l", 1, 0), ("l", 2, 5)]:
+        m2, l2 = mp.copy(), lp.copy()
+        arr = m2 if kind == "m" else l2
+        orig = arr[i, col]
+        arr[i, col] = orig + h
+        Lp, _ = loss(m2, l2)
+        arr[i, col] = orig - h
+        Lm, _ = loss(m2, l2)
+        fd = (Lp - Lm) / (2 * h)
+        an = gm[i, col] if kind == "m" else gl[i, col - 3 if col >= 3 else col + 3]
+        assert abs(fd - an) <= 1e-3 * max(1.0, abs(fd)), (kind, i, col, fd, an)
+
+
+def test_oracle_aa_grid_matches_reference_golden():
+    """The reference's anti-aliasing grid (RayTracer::renderWithAA, src/RayTracer.cpp:176-265,
+    3 x 3 samples): per-sample paths and FP32 colours bit-exact, and the reference's own
+    RGBA8 frame equals the oracle's colours quantised (golden aa3_small12.npz)."""
+    g = load("aa3_small12")
+    W, H, td, n = (int(v) for v in g["size"])
+    cam = scenes.CameraData(*[g["cam"][3 * i:3 * i + 3] for i in range(4)], W, H)
+    sc = scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)
+    o = oracle.Oracle(sc).render(cam, td, spp=n * n, aa_grid=True)
+    assert np.array_equal(o["hits"][:, :td + 1], g["hits"]) and np.array_equal(o["shadows"][:, :td + 1], g["shadows"])
+    assert np.array_equal(o["rgb"].view(np.uint32), g["rgb"].view(np.uint32))
+    assert np.array_equal(o["counts"], g["counts"])
+    c = o["rgb"].reshape(H, W, 3).astype(np.float64)
+    q = np.floor(np.where(c == 1.0, 255, np.minimum(c * 256.0, 255.0))).astype(np.uint8)
+    assert np.array_equal(q, g["rgba8"][..., :3])
+    with pytest.raises(ValueError):
+        oracle.grid_side(5)

@@ -126,8 +126,12 @@ def test_noalloc_refuses_unknown_flags(ctx):
     dsc = api.DeviceScene(ctx, sc)
     cam = scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 32, 32)
     rgb = torch.zeros((32 * 32, 3), device="cuda")
-    for bad in (2, 4, 1 << 30):
+    for bad in (8, 1 << 30):
         code, _ = _noalloc(ctx, dsc, cam, 1, rgb, None, flags=bad)
         assert code == 1, bad
+    code, _ = _noalloc(ctx, dsc, cam, 1, rgb, None, flags=L.FLAG_TREE_RECORDS)  # needs ray-tree queues
+    assert code == 7
     code, st = _noalloc(ctx, dsc, cam, 1, rgb, None, flags=1)  # stage timing is accepted and ignored
     assert code == 0 and st.primary_rays == 32 * 32
+    code, st = _noalloc(ctx, dsc, cam, 1, rgb, None, spp=4, flags=L.FLAG_AA_GRID)  # the reference's 2x2 grid
+    assert code == 0 and st.primary_rays == 4 * 32 * 32
