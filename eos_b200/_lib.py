@@ -55,6 +55,7 @@ class RenderParams(Structure):
 FLAG_STAGE_TIMING = 1
 FLAG_TREE_RECORDS = 2
 FLAG_AA_GRID = 4
+FLAG_ASYNC = 8
 
 
 class Tuning(Structure):

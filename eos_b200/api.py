@@ -96,7 +96,12 @@ class Context:
                 "eos_ctx_set_stream")
 
     def synchronize(self):
+        """Waits for the context (the copies of asynchronous batches included); raises the first
+        device error of the asynchronous batches since the last call and returns their stats
+        dicts in issue order."""
+        pending, self._async_stats = getattr(self, "_async_stats", []), []
         L.check(self.lib.eos_ctx_synchronize(self.h), "eos_ctx_synchronize")
+        return [stats_dict(st) for st in pending]
 
     def set_limits(self, queue_entries: int = 0, work_budget: int = 0, small_stack: bool = False):
         """Test limits of the wavefront kernels (eos_ctx_set_limits); no arguments clears them."""
@@ -299,9 +304,12 @@ def make_batch_outputs(jobs: list[BatchJob], outputs=("rgb",), tree_records: boo
     return outs
 
 
-def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning) -> dict:
+def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], async_outputs: bool = False,
+                 **tuning) -> dict | None:
     """All jobs through one wavefront pass (graph-captured); outputs are device tensors or host
-    arrays (host outputs are filled when the call returns)."""
+    arrays (host outputs are filled when the call returns).  async_outputs=True
+    (EOS_FLAG_ASYNC): returns None once the batch is queued; host outputs (pinned) are
+    filled, and the call's stats returned, by ctx.synchronize()."""
     arr = (L.Job * len(jobs))()
     for i, (j, o) in enumerate(zip(jobs, outs)):
         arr[i].scene = j.scene.h
@@ -316,8 +324,15 @@ def render_batch(ctx: Context, jobs: list[BatchJob], outs: list[dict], **tuning)
         if j.rows is not None:
             arr[i].row_begin, arr[i].row_end = int(j.rows[0]), int(j.rows[1])
     p = params_struct(mode="wavefront", **tuning)
+    if async_outputs:
+        p.flags |= L.FLAG_ASYNC
     st = L.Stats()
     L.check(ctx.lib.eos_render_batch(ctx.h, arr, len(jobs), byref(p), byref(st)), "eos_render_batch")
+    if async_outputs:
+        if not hasattr(ctx, "_async_stats"):
+            ctx._async_stats = []
+        ctx._async_stats.append(st)  # filled by eos_ctx_synchronize: kept alive until then
+        return None
     return stats_dict(st)
 
 

@@ -12,6 +12,13 @@
 using namespace eos;
 
 eos_ctx::~eos_ctx() {
+  if (copy_stream) cudaStreamSynchronize(copy_stream);
+  for (AsyncSlot& a : async) {
+    if (a.rendered) cudaEventDestroy(a.rendered);
+    if (a.copied) cudaEventDestroy(a.copied);
+  }
+  if (async_host) cudaFreeHost(async_host);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);
@@ -154,7 +161,8 @@ eos_status check_params(const eos_render_params* p) {
   if (p->trace_depth < 0 || p->trace_depth >= EOS_MAX_BOUNCES) return EOS_ERR_INVALID_ARG;
   if (p->spp < 1 || p->spp > 1024) return EOS_ERR_INVALID_ARG;
   if (p->mode != EOS_MODE_PLAIN && p->mode != EOS_MODE_WAVEFRONT) return EOS_ERR_INVALID_ARG;
-  if (p->flags & ~(EOS_FLAG_STAGE_TIMING | EOS_FLAG_TREE_RECORDS | EOS_FLAG_AA_GRID)) return EOS_ERR_INVALID_ARG;
+  if (p->flags & ~(EOS_FLAG_STAGE_TIMING | EOS_FLAG_TREE_RECORDS | EOS_FLAG_AA_GRID | EOS_FLAG_ASYNC))
+    return EOS_ERR_INVALID_ARG;
   if ((p->flags & EOS_FLAG_AA_GRID) && aa_grid_side(p->spp) == 0) return EOS_ERR_INVALID_ARG;
   return EOS_OK;
 }
@@ -172,6 +180,53 @@ int band_rows(int h, int rb, int re) { return re > 0 ? re - rb : h; }
 eos_status set_device(eos_ctx* ctx) {
   EOS_CUDA(cudaSetDevice(ctx->device));
   return EOS_OK;
+}
+
+// Copy stream, events and pinned read-back of asynchronous batches (made on first use).
+eos_status async_setup(eos_ctx* ctx) {
+  if (ctx->copy_stream) return EOS_OK;
+  EOS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  for (eos_ctx::AsyncSlot& a : ctx->async) {
+    EOS_CUDA(cudaEventCreateWithFlags(&a.rendered, cudaEventDisableTiming));
+    EOS_CUDA(cudaEventCreateWithFlags(&a.copied, cudaEventDisableTiming));
+  }
+  EOS_CUDA(cudaHostAlloc((void**)&ctx->async_host, 2 * (kCounters + 1) * sizeof(unsigned long long),
+                         cudaHostAllocDefault));
+  return EOS_OK;
+}
+
+// Waits for a pending asynchronous slot's copies and folds in its error word and counters.
+eos_status async_finish(eos_ctx* ctx, int k) {
+  eos_ctx::AsyncSlot& a = ctx->async[k];
+  if (!a.pending) return EOS_OK;
+  a.pending = false;
+  EOS_CUDA(cudaEventSynchronize(a.copied));
+  const unsigned long long* h = ctx->async_host + k * (kCounters + 1);
+  const int err = (int)h[kCounters];
+  if (a.stats) {
+    eos_stats* st = a.stats;
+    std::memset(st, 0, sizeof *st);
+    st->primary_rays = h[0];
+    st->shadow_rays = h[1];
+    st->secondary_rays = h[2];
+    st->nodes_closest = h[3];
+    st->tests_closest = h[4];
+    st->nodes_shadow = h[5];
+    st->tests_shadow = h[6];
+    st->shaded_hits = h[7];
+    st->error_flags = err;
+    st->kernel_launches = a.launches;
+  }
+  return err_to_status(err);
+}
+
+// Folds every pending asynchronous slot, oldest first; the first error wins.
+eos_status async_drain(eos_ctx* ctx) {
+  const int first = (ctx->async[0].pending && ctx->async[1].pending)
+                        ? (ctx->async[0].seq < ctx->async[1].seq ? 0 : 1) : (ctx->async[0].pending ? 0 : 1);
+  eos_status s0 = async_finish(ctx, first);
+  eos_status s1 = async_finish(ctx, first ^ 1);
+  return s0 != EOS_OK ? s0 : s1;
 }
 
 // Tuned entry for a scene of n triangles (zeros when the table has none).
@@ -264,6 +319,7 @@ eos_status eos_ctx_destroy(eos_ctx* ctx) {
   if (!ctx) return EOS_ERR_INVALID_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   delete ctx;
   return EOS_OK;
 }
@@ -276,8 +332,13 @@ eos_status eos_ctx_set_stream(eos_ctx* ctx, void* stream) {
 
 eos_status eos_ctx_synchronize(eos_ctx* ctx) {
   if (!ctx) return EOS_ERR_INVALID_ARG;
+  EOS_CUDA(cudaSetDevice(ctx->device));
   EOS_CUDA(cudaStreamSynchronize(ctx->stream));
-  return EOS_OK;
+  if (ctx->copy_stream) EOS_CUDA(cudaStreamSynchronize(ctx->copy_stream));
+  const eos_status drained = async_drain(ctx);
+  const eos_status st = ctx->async_status != EOS_OK ? ctx->async_status : drained;
+  ctx->async_status = EOS_OK;
+  return st;
 }
 
 eos_status eos_ctx_set_tuning(eos_ctx* ctx, uint32_t min_tris, const eos_tuning* t) {
@@ -511,6 +572,18 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     if ((p->flags & EOS_FLAG_AA_GRID) && aa_grid_side(jb.spp) == 0) return EOS_ERR_INVALID_ARG;
   }
   if ((st = set_device(ctx)) != EOS_OK) return st;
+  const bool async = (p->flags & EOS_FLAG_ASYNC) != 0;
+  int slot = 0;
+  if (async) {
+    if ((st = async_setup(ctx)) != EOS_OK) return st;
+    slot = ctx->async_next;
+    // the slot's previous call (two calls ago) must have finished copying out of its
+    // staging buffer; its status is kept for the next synchronize
+    if (ctx->async[slot].pending) {
+      const eos_status prev = async_finish(ctx, slot);
+      if (ctx->async_status == EOS_OK) ctx->async_status = prev;
+    }
+  }
   // host output buffers are staged through one device buffer and copied back at the end
   struct HostOut {
     void* user;
@@ -532,7 +605,7 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   }
   char* stage = nullptr;
   if (staged) {
-    stage = (char*)scratch(ctx, "batch.host_out", staged, &st);
+    stage = (char*)scratch(ctx, async ? (slot ? "batch.async1" : "batch.async0") : "batch.host_out", staged, &st);
     if (st != EOS_OK) return st;
     size_t k = 0;
     auto swap_in = [&](auto*& ptr) {
@@ -552,6 +625,27 @@ eos_status eos_render_batch(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   st = render_wavefront(ctx, dj.data(), n_jobs, with_tuning(ctx, *p, largest),
                         (p->flags & EOS_FLAG_STAGE_TIMING) == 0);
   if (st != EOS_OK) return st;
+  if (async) {
+    // read-back of this call's error word and counters (ordered before the next call's
+    // clearing), then the output copies on the copy stream, behind the render
+    eos_ctx::AsyncSlot& a = ctx->async[slot];
+    unsigned long long* hb = ctx->async_host + slot * (kCounters + 1);
+    EOS_CUDA(cudaMemcpyAsync(hb, ctx->d_counts, kCounters * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    EOS_CUDA(cudaMemsetAsync(hb + kCounters, 0, sizeof(unsigned long long), ctx->stream));
+    EOS_CUDA(cudaMemcpyAsync(hb + kCounters, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    EOS_CUDA(cudaEventRecord(a.rendered, ctx->stream));
+    EOS_CUDA(cudaStreamWaitEvent(ctx->copy_stream, a.rendered, 0));
+    for (const HostOut& h : host_outs)
+      EOS_CUDA(cudaMemcpyAsync(h.user, stage + h.off, h.bytes, cudaMemcpyDeviceToHost, ctx->copy_stream));
+    EOS_CUDA(cudaEventRecord(a.copied, ctx->copy_stream));
+    a.pending = true;
+    a.seq = ++ctx->async_seq;
+    a.stats = stats;
+    a.launches = ctx->launches;
+    ctx->async_next = slot ^ 1;
+    return EOS_OK;
+  }
   EOS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   for (const HostOut& h : host_outs)
     EOS_CUDA(cudaMemcpyAsync(h.user, stage + h.off, h.bytes, cudaMemcpyDeviceToHost, ctx->stream));

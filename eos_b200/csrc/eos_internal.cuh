@@ -113,6 +113,23 @@ struct eos_ctx {
   std::map<uint32_t, eos_tuning> tuning;
   // test limits of the wavefront kernels (eos_ctx_set_limits); zeros = none
   eos_limits limits{0, 0, 0};
+  // asynchronous batches (EOS_FLAG_ASYNC): two slots used in turn, each with its staging
+  // buffer ("batch.async<k>"), the events that order its copies, and a pinned read-back of
+  // its error word and counters; eos_ctx_synchronize folds pending slots in issue order
+  struct AsyncSlot {
+    cudaEvent_t rendered = nullptr;  // recorded on the render stream after the read-back
+    cudaEvent_t copied = nullptr;    // recorded on copy_stream after the output copies
+    bool pending = false;
+    long long seq = 0;               // issue order
+    eos_stats* stats = nullptr;      // caller's stats, filled at synchronize
+    uint32_t launches = 0;
+  };
+  cudaStream_t copy_stream = nullptr;
+  AsyncSlot async[2];
+  int async_next = 0;
+  long long async_seq = 0;
+  unsigned long long* async_host = nullptr;  // pinned [2][kCounters + 1] (counters, error word)
+  eos_status async_status = EOS_OK;          // first error of slots folded before a synchronize
   // per-call bookkeeping reported in eos_stats
   uint32_t launches = 0;
   float stage_ms[3] = {0, 0, 0};

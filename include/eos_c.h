@@ -136,6 +136,14 @@ typedef struct eos_render_params {
  * float order; pixel_offset and jitter_seed are not used.  spp must be a square
  * (EOS_ERR_INVALID_ARG otherwise).  Without the flag, spp > 1 samples at hashed jitter. */
 #define EOS_FLAG_AA_GRID 4
+/* eos_render_batch only: return once the batch is queued.  Host output buffers are copied on
+ * a second stream of the context from one of two staging buffers, so one call's copy to the
+ * host overlaps the next call's rendering; they are complete, and the call's device errors
+ * and stats (when stats is not NULL; the pointer must stay valid) are known, when
+ * eos_ctx_synchronize returns, which reports the first error of the pending calls.  At
+ * most two calls are in flight: a third waits for the first one's copies.  Host outputs
+ * should be pinned memory (pageable copies do not overlap). */
+#define EOS_FLAG_ASYNC 8
 /* Other flag bits are refused (EOS_ERR_INVALID_ARG). */
 
 /* Tuned launch / layout parameters of one scene-size bucket (see eos_ctx_set_tuning). */
@@ -254,6 +262,9 @@ eos_status eos_ctx_create(int32_t device, eos_ctx** out);
 eos_status eos_ctx_destroy(eos_ctx* ctx);
 /* Use a caller stream (a cudaStream_t) instead of the context's own; NULL restores it. */
 eos_status eos_ctx_set_stream(eos_ctx* ctx, void* stream);
+/* Waits for all work of the context, the copies of asynchronous batches included; returns
+ * the first device error of the asynchronous calls since the last synchronize (EOS_OK if
+ * none) and fills their stats. */
 eos_status eos_ctx_synchronize(eos_ctx* ctx);
 /* Autotuner table (no reference counterpart): parameters for scenes of at least min_tris
  * triangles.  A render / scene-create parameter left at 0 takes the entry with the largest

@@ -42,3 +42,42 @@ def test_config3_style_batch_matches_plain_and_oracle(ctx):
         p = o["paths"].cpu().numpy()[pix]
         assert np.array_equal(p[:, :8], r["hits"])
         assert np.array_equal(p[:, 8:].view(np.uint32), r["shadows"])
+
+
+def test_async_batches_equal_synchronous_ones(ctx):
+    """EOS_FLAG_ASYNC: three batches in a row into pinned host images (each call's copy to
+    the host overlaps the next call's rendering) give the synchronous call's images and
+    stats once the context is synchronized; a device error of an asynchronous call is
+    reported by the synchronize, and the context stays usable."""
+    import torch
+    from eos_b200._lib import EosError
+    sc = scenes.small_random_scene(41, n_spheres=6, level=3, lights=3, refl=0.6)
+    dsc = api.DeviceScene(ctx, sc)
+    cams = [scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 160, 120),
+            scenes.look_at((-6.0, 4.0, 6.0), (0, -0.5, 0), 50.0, 96, 64)]
+    jobs = [api.BatchJob(dsc, c, 2, 0.5) for c in cams]
+    ref_outs = [{"rgba8": np.zeros((c.height, c.width, 4), np.uint8)} for c in cams]
+    ref_st = api.render_batch(ctx, jobs, ref_outs)
+    host = [[{"rgba8": torch.zeros((c.height, c.width, 4), dtype=torch.uint8).pin_memory()} for c in cams]
+            for _ in range(3)]
+    for outs in host:
+        assert api.render_batch(ctx, jobs, [{"rgba8": o["rgba8"].numpy()} for o in outs], async_outputs=True) is None
+    stats = ctx.synchronize()
+    assert len(stats) == 3
+    for outs, st in zip(host, stats):
+        for o, r in zip(outs, ref_outs):
+            assert np.array_equal(o["rgba8"].numpy(), r["rgba8"])
+        for k in ("primary_rays", "shadow_rays", "secondary_rays"):
+            assert st[k] == ref_st[k]
+    # a device error of an asynchronous call surfaces at the synchronize
+    ctx.set_limits(queue_entries=16)
+    try:
+        api.render_batch(ctx, jobs, [{"rgba8": o["rgba8"].numpy()} for o in host[0]], async_outputs=True)
+        with pytest.raises(EosError) as e:
+            ctx.synchronize()
+        assert e.value.code == 6
+    finally:
+        ctx.set_limits()
+    out = [{"rgba8": np.zeros((c.height, c.width, 4), np.uint8)} for c in cams]
+    api.render_batch(ctx, jobs, out)
+    assert all(np.array_equal(a["rgba8"], b["rgba8"]) for a, b in zip(out, ref_outs))
