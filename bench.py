@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--views", type=int, default=4)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's own GPU megakernel as a comparison point")
     ap.add_argument("--no-config3", action="store_true", help="skip the 80-job batching workload")
     ap.add_argument("--no-config5", action="store_true", help="skip the 4.5M-triangle 4K stress workload")
     ap.add_argument("--profile", action="store_true",
@@ -82,6 +84,7 @@ def parse():
     a = ap.parse_args()
     if a.profile:
         a.views, a.no_adjoint, a.no_cpu_baseline, a.no_config3, a.no_config5 = 1, True, True, True, True
+        a.no_reference_gpu = True
     return a
 
 
@@ -339,6 +342,21 @@ def port_baseline(sc, cam, trace_depth, budget_s=15.0):
     return {"value": total_rays / total_t / 1e6, "unit": "Mrays/s", "cores": nthreads, "kind": "port",
             "sample": f"{rows_done} rows x {W} px of the 1080p view (oracle C port, {nthreads} threads)",
             "rays": total_rays, "seconds": total_t}
+
+
+def reference_gpu_point(scene: str, reps: int = 5, timeout_s: int = 300):
+    """The reference's own GPU megakernel (primary rays and local Phong only) on this GPU, as
+    a comparison point: `python -m oracle.ref_gpu` in a process of its own (the reference
+    exits on any CUDA error)."""
+    try:
+        r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", "--scene", scene, "--reps", str(reps)],
+                           cwd=ROOT, capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"timed out after {timeout_s} s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": f"exit {r.returncode}: " + (r.stderr.strip().splitlines() or [""])[-1][:200]}
+    return json.loads(lines[-1])
 
 
 def run_reference(args, rank, world):
@@ -599,6 +617,13 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sc, cams[0], td)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = {"config2_1080p": reference_gpu_point("config2"), "config1_512": reference_gpu_point("config1")}
+        ref_gpu["note"] = ("the reference's __rayTrace_MegaKernel compiled for sm_100a (oracle/_ref/libeosref_gpu.so): "
+                           "one primary ray per pixel and local Phong over all lights, no shadow or mirror rays, on "
+                           "its own tree; a comparison point, not this line's workload (which traces shadow and "
+                           "mirror rays as the reference's CPU renderer does)")
 
     npx_step = sum(c.width * c.height for c in cams)
     line = {
@@ -648,6 +673,8 @@ def run_ours(args, rank, world, local):
         line["config3_batch"] = batch3
     if stress5:
         line["config5_stress"] = stress5
+    if ref_gpu:
+        line["reference_gpu_kernel"] = ref_gpu
     if cpu:
         line["cpu_baseline"] = {k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in cpu.items()
                                 if k in ("value", "unit", "cores", "kind", "sample", "cpu", "port", "note")}

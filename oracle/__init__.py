@@ -20,6 +20,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
+import sys
 from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_longlong, c_uint32, c_uint8, c_void_p
 
 import numpy as np
@@ -54,6 +55,16 @@ def grid_side(spp: int) -> int:
 def tree_nodes(trace_depth: int) -> int:
     """Nodes of a tree record: 2^(trace_depth + 1) - 1 (heap order)."""
     return (1 << (trace_depth + 1)) - 1
+
+
+def build_reference_gpu() -> None:
+    """The reference's GPU megakernel for sm_100a (oracle/_ref/libeosref_gpu.so, a comparison
+    point run by oracle/ref_gpu.py) and the cached config-1 tree it renders with."""
+    if not os.path.isdir(REF_SRC):
+        return
+    subprocess.run(["make", "-s", "-C", HERE, "refgpu", f"REF={REF_SRC}"], check=True)
+    subprocess.run([sys.executable, "-m", "oracle.make_ref_tree", "--scene", "config1"], cwd=os.path.dirname(HERE),
+                   check=True, capture_output=True)
 
 
 def _p(a, ct):

@@ -347,6 +347,9 @@ void* eosref_scene_create_from_tree(const float* verts, const float* normals, in
   return rs;
 }
 
+// The harness scene's reference Scene (for the GPU harness, ref_gpu_harness.cu).
+void* eosref_scene_ptr(void* h) { return &((RefScene*)h)->scene; }
+
 // Boxes of the flat node buffer, [n_nodes * 6] min xyz, max xyz (to check a restore).
 void eosref_tree_boxes(void* h, float* boxes) {
   RefScene* rs = (RefScene*)h;
