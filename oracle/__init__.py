@@ -123,6 +123,11 @@ def lib_ref():
         L.eosref_scene_create.argtypes = [POINTER(c_float), POINTER(c_float), c_int, POINTER(c_uint32),
                                           POINTER(c_uint32), c_int, POINTER(c_float), c_int,
                                           POINTER(c_float), c_int, c_int, POINTER(c_double)]
+        L.eosref_scene_create_transformed.restype = c_void_p
+        L.eosref_scene_create_transformed.argtypes = [POINTER(c_float), POINTER(c_float), POINTER(c_uint32),
+                                                      POINTER(c_uint32), c_int, POINTER(c_float), c_int,
+                                                      POINTER(c_float), c_int, POINTER(c_int32), POINTER(c_float),
+                                                      c_int, c_int]
         L.eosref_scene_destroy.argtypes = [c_void_p]
         L.eosref_scene_set_ambient.argtypes = [c_void_p, c_float]
         L.eosref_scene_stats.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int)]
@@ -331,13 +336,25 @@ class RefRenderer:
     """The reference's own CPU renderer, compiled from its sources, over one scene.
 
     tree: (perm, nodes) from :meth:`export_tree` of an earlier build of the same scene;
-    the tree is then restored instead of built (see :func:`ref_tree_cached`)."""
+    the tree is then restored instead of built (see :func:`ref_tree_cached`).
+    transforms: (tri_xf [n_tris] int32, xforms [K, 12] row-major 3x4) for a scene of
+    object-space triangles, each placed by one transformation (eosref_scene_create_transformed;
+    the reference's builder bounds the placed triangles, its CPU renderer ignores them)."""
 
-    def __init__(self, scene, build_threads: int = 1, tree=None):
+    def __init__(self, scene, build_threads: int = 1, tree=None, transforms=None):
         L = lib_ref()
         self.scene = scene
         secs = c_double(0.0)
-        if tree is None:
+        if transforms is not None:
+            tri_xf = np.ascontiguousarray(transforms[0], np.int32)
+            xf = np.ascontiguousarray(transforms[1], np.float32).reshape(-1, 12)
+            a = _scene_args(scene)
+            self.h = L.eosref_scene_create_transformed(a[0], a[1], a[3], a[4], a[5], a[6], a[7], a[8], a[9],
+                                                       _p(tri_xf, c_int32), _p(xf, c_float), xf.shape[0],
+                                                       build_threads)
+            if not self.h:
+                raise ValueError("transformation index out of range")
+        elif tree is None:
             self.h = L.eosref_scene_create(*_scene_args(scene), build_threads, ctypes.byref(secs))
         else:
             perm = np.ascontiguousarray(tree[0], np.int32)

@@ -54,6 +54,9 @@ struct RefScene {
   glm::mat4 identity_inv{1.0f};
   glm::mat4 identity_inv_t{1.0f};
   std::vector<Material> object_materials;
+  // per-object transformations of eosref_scene_create_transformed (sized once: the
+  // triangles keep pointers into them)
+  std::vector<glm::mat4> xf, xf_inv, xf_inv_t;
   std::vector<Triangle*> triangles;
   std::vector<LightSource*> lights;
   int max_leaf = 0;
@@ -264,6 +267,52 @@ void* eosref_scene_create(const float* verts, const float* normals, int nv, cons
   double t1 = getRealTime();
   omp_set_num_threads(prev);
   if (build_seconds) *build_seconds = t1 - t0;
+  scan_leaves(rs);
+  return rs;
+}
+
+// A scene whose triangles carry per-object transformations, built the way the reference's
+// main program places a transformed mesh (src/main.cpp:388-394, src/triangleMesh.cpp:140-150):
+// object-space vertices and normals, triangle i placed by transformation tri_xf[i] of
+// xforms [nx][12] (world-from-object, row-major 3 x 4), each registered in order with
+// Scene::addTransformation (src/Scene.cpp:96-106, which the GPU path reads) and pointed to
+// by the triangle (which the builder reads: BVH::computeBoxWithSurfaces transforms every
+// triangle's local box, src/BVH.cpp:144-159).  Built by the reference's builder with
+// build_threads threads.  The reference's CPU renderer ignores the transformations
+// (src/Triangle.cpp:26-54); only its GPU path renders such a scene.
+void* eosref_scene_create_transformed(const float* verts, const float* normals, const uint32_t* tris,
+                                      const uint32_t* tri_obj, int nt, const float* mats, int nobj,
+                                      const float* lights, int nl, const int32_t* tri_xf, const float* xforms,
+                                      int nx, int build_threads) {
+  if (nx < 1) return nullptr;
+  for (int i = 0; i < nt; ++i)
+    if (tri_xf[i] < 0 || tri_xf[i] >= nx) return nullptr;
+  RefScene* rs = make_scene(verts, normals, tris, tri_obj, nt, mats, nobj, lights, nl);
+  rs->xf.assign(nx, glm::mat4(1.0f));
+  rs->xf_inv.assign(nx, glm::mat4(1.0f));
+  rs->xf_inv_t.assign(nx, glm::mat4(1.0f));
+  for (int k = 0; k < nx; ++k) {
+    const float* m = xforms + 12 * k;
+    glm::mat4 M(1.0f);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 4; ++c) M[c][r] = m[4 * r + c];  // glm: column c, row r
+    rs->xf[k] = M;
+    rs->xf_inv[k] = glm::inverse(M);
+    rs->xf_inv_t[k] = glm::inverse(glm::transpose(M));
+    rs->scene.addTransformation(M);
+  }
+  for (int i = 0; i < nt; ++i) {
+    Triangle* tri = rs->triangles[i];
+    const int k = tri_xf[i];
+    tri->setTransformation(rs->xf[k]);
+    tri->setInverseTransformation(rs->xf_inv[k]);
+    tri->setInverseTransposeTransformation(rs->xf_inv_t[k]);
+    tri->setTransformationIndex(k);
+  }
+  int prev = omp_get_max_threads();
+  omp_set_num_threads(build_threads > 0 ? build_threads : 1);
+  rs->scene.flush();
+  omp_set_num_threads(prev);
   scan_leaves(rs);
   return rs;
 }

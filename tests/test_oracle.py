@@ -235,6 +235,45 @@ def test_instanced_oracle_agrees_with_the_flattened_scene():
     assert (a["hits"][:, 0] >= 0).mean() > 0.2
 
 
+def test_reference_builder_bounds_placed_triangles():
+    """The reference's own builder over object-space triangles with per-object
+    transformations (eosref_scene_create_transformed, as its main program places a mesh):
+    every leaf box holds its placed triangles under translations and axis scales (the
+    placements the GPU comparison uses), and not under a rotation -- its
+    Box::transformBoundingBox moves only the local box's two corners (src/Box.cu:84-135)."""
+    if not oracle.ref_available():
+        pytest.skip("reference CPU build unavailable")
+    from oracle import ref_gpu
+    d, _ = ref_gpu.transformed_case()
+    verts, normals, tris, tri_mat, tri_xf, xf = ref_gpu.object_space_arrays(d)
+    sc = scenes.SceneData(verts, normals, tris, tri_mat, d.materials, d.lights)
+
+    def leaves_outside(xforms):
+        """Placed triangles outside their leaf's box, and the root box."""
+        r = oracle.RefRenderer(sc, transforms=(tri_xf, xforms))
+        perm, nodes = r.export_tree()
+        boxes = r.boxes().astype(np.float64)
+        M = np.asarray(xforms, np.float64).reshape(-1, 3, 4)
+        out = 0
+        for i in np.nonzero(nodes[:, 0] == 1)[0]:  # BVH_LEAF (src/BVH.h:34-37)
+            ids = perm[nodes[i, 4]:nodes[i, 4] + nodes[i, 1]]
+            for t in ids:
+                p = verts[tris[t]].astype(np.float64) @ M[tri_xf[t], :, :3].T + M[tri_xf[t], :, 3]
+                out += int(((p < boxes[i, :3] - 1e-5) | (p > boxes[i, 3:] + 1e-5)).any())
+        return out, boxes[0]
+
+    out, root = leaves_outside(xf)
+    assert out == 0
+    world = d.flatten().verts.astype(np.float64)
+    assert np.allclose(root[:3], world.min(0), rtol=0, atol=1e-5)
+    assert np.allclose(root[3:], world.max(0), rtol=0, atol=1e-5)
+    c, s_ = np.cos(np.pi / 4), np.sin(np.pi / 4)
+    xr = xf.copy().reshape(-1, 3, 4)
+    xr[4, :, :3] = xr[4, :, :3] @ np.array([[c, 0, s_], [0, 1, 0], [-s_, 0, c]], np.float32)
+    out_r, _ = leaves_outside(xr.reshape(-1, 12))
+    assert out_r > 0
+
+
 def test_instanced_frozen_f64_adjoint_matches_central_differences():
     """The FP64 adjoint of a two-level scene (hits replayed in each instance's object space,
     normals through the inverse transpose) against central differences of its own FP64
