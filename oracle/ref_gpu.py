@@ -39,15 +39,22 @@ def transformed_case(seed: int = 7, size: int = 256):
     Placements are translations and axis scales, non-uniform and mirrored ones among them:
     the reference bounds a transformed triangle by transforming its local box's two
     corners only (Box::transformBoundingBox, src/Box.cu:84-135), which holds the triangle
-    under those placements and not under rotations.  The lights are on the camera's side
-    of the origin, so that the megakernel's specular term of a ray that hits nothing is 0
-    (src/kernelInvocations.cu:246-300 shades misses with a zero point and normal)."""
+    under those placements and not under rotations.  The ground is a slightly warped quad:
+    the kernel's box test asks tmin < tmax (src/kernelInvocations.h:60-73), which a box of
+    zero thickness never passes, so it cannot see a triangle lying in an axis plane.  The
+    lights are on the camera's side of the origin, so that the megakernel's specular term
+    of a ray that hits nothing is 0 (src/kernelInvocations.cu:246-300 shades misses with a
+    zero point and normal)."""
     sys.path.insert(0, ROOT)
     from eos_b200 import scenes
     rng = scenes.rng_for(seed)
     grey = [scenes.material((0.5, 0.5, 0.5), 0.2, 16, 0.0)]
     v, f = scenes.icosphere(2)
     qv, qn, qf = scenes.ground_quad(4.0, 0.0)
+    qv[:, 1] = (0.0, 0.15, 0.05, 0.2)  # warped: no triangle lies in an axis plane
+    qn = np.cross(qv[qf[:, 1]] - qv[qf[:, 0]], qv[qf[:, 2]] - qv[qf[:, 0]])
+    qn = np.repeat(qn / np.linalg.norm(qn, axis=1, keepdims=True), 3, axis=0)
+    qv, qf = qv[qf.reshape(-1)], np.arange(6).reshape(2, 3)  # flat-shaded: vertices per triangle
     cv, cn, cf = scenes.foliage_cluster(300, rng, radius=1.0)
     meshes = [scenes.SceneData(v, v, f, np.zeros(len(f)), grey, np.zeros((0, 6))),
               scenes.SceneData(qv, qn, qf, np.zeros(len(qf)), grey, np.zeros((0, 6))),
