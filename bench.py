@@ -46,17 +46,34 @@ METRIC = "Mrays/s @1080p 1M tris, batched vs plain GPU; fwd+adjoint ms/view"
 TUNING = os.path.join(ROOT, "eos_b200", "tuning_b200.json")
 
 
-def run_autotune():
-    """Tunes one representative workload per scene-size bucket and writes the table."""
+def run_autotune(only=None, out=None):
+    """Tunes one representative workload per scene-size bucket and writes the table (to
+    `out`, default the committed table); `only`: names of the workloads to tune, the other
+    buckets are kept as they are."""
     import numpy as np
     from eos_b200 import api, autotune, scenes
     ctx = api.Context(0)
     rng = scenes.rng_for(4242)
-    work = [(scenes.config1_scene(), [scenes.config1_camera()]),
-            (scenes.mixed_scene(rng, 60_000, "mixed60k"), [scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 512, 512)]),
-            (scenes.mixed_scene(rng, 300_000, "mixed300k"), [scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 512, 512)]),
-            (scenes.config2_scene(), views_for(0, 4))]
-    table = autotune.tune(ctx, work, path=TUNING, trace_depth=2)
+    work = {"config1": lambda: (scenes.config1_scene(), [scenes.config1_camera()]),
+            "mixed60k": lambda: (scenes.mixed_scene(rng, 60_000, "mixed60k"),
+                                 [scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 512, 512)]),
+            "mixed300k": lambda: (scenes.mixed_scene(rng, 300_000, "mixed300k"),
+                                  [scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 512, 512)]),
+            "config2": lambda: (scenes.config2_scene(), views_for(0, 4)),
+            # the 4K stress view: depth 4 (trace depth 3), 2 jittered samples per pixel
+            "config5": lambda: (scenes.config5_scene(), [scenes.config5_camera()], 3, 2)}
+    names = list(work) if not only else [n for n in work if n in only]
+    if only and len(names) != len(set(only)):
+        raise SystemExit(f"--autotune-only takes {', '.join(work)}")
+    if only:  # the generators draw from one stream: make the skipped ones too, in order
+        items = []
+        for n in work:
+            w = work[n]()
+            if n in names:
+                items.append(w)
+    else:
+        items = [work[n]() for n in names]
+    table = autotune.tune(ctx, items, path=out or TUNING, trace_depth=2, base=TUNING)
     print(json.dumps({str(k): {"setting": v["setting"], "mrays": round(v["mrays"], 1),
                                "default_mrays": round(v["default_mrays"], 1)} for k, v in table.items()}))
     del np
@@ -80,6 +97,9 @@ def parse():
     ap.add_argument("--autotune", action="store_true",
                     help=f"tune block / queue chunk / stack depth / leaf size per scene-size bucket and "
                          f"write {os.path.relpath(TUNING, ROOT)}")
+    ap.add_argument("--autotune-only", nargs="+", default=None,
+                    help="with --autotune: the workloads to tune (config1 mixed60k mixed300k config2 config5)")
+    ap.add_argument("--tuning-out", default=None, help="with --autotune: write the table here instead")
     ap.add_argument("--no-tuning", action="store_true", help="ignore the committed tuning table")
     a = ap.parse_args()
     if a.profile:
@@ -415,7 +435,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     if args.autotune:
         if rank == 0:
-            run_autotune()
+            run_autotune(args.autotune_only, args.tuning_out)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

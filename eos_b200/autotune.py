@@ -55,8 +55,9 @@ def _time_batch(ctx, jobs, outs, params, reps=3) -> float:
     return rays / (best * 1e-3) / 1e6  # Mrays/s
 
 
-def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log=None) -> dict:
-    """Coordinate descent for one scene; returns the best setting and its Mrays/s."""
+def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log=None, spp=1) -> dict:
+    """Coordinate descent for one scene (its views rendered with `spp` jittered samples
+    per pixel); returns the best setting and its Mrays/s."""
     best = dict(DEFAULT)
     scenes_by_leaf = {}
 
@@ -69,7 +70,7 @@ def tune_scene(ctx, scene_data, cameras, trace_depth=2, reps=3, margin=0.02, log
 
     def measure(setting):
         dsc = scene_for(setting["builder"], setting["width"], setting["layout"], setting["leaf_size"])
-        jobs = [api.BatchJob(dsc, c, trace_depth, 0.5) for c in cameras]
+        jobs = [api.BatchJob(dsc, c, trace_depth, 0.5, spp, 7) for c in cameras]
         outs = api.make_batch_outputs(jobs, ("rgba8",))
         p = {k: setting[k] for k in ("block_size", "stack_depth", "queue_chunk")}
         return _time_batch(ctx, jobs, outs, p, reps)
@@ -123,14 +124,20 @@ def load_table(path: str) -> dict:
     return {int(k): v for k, v in d.get("buckets", {}).items()}
 
 
-def tune(ctx, workloads, path=None, trace_depth=2, log=print) -> dict:
-    """workloads: list of (scene_data, cameras).  Returns and optionally saves the table."""
-    table = load_table(path) if path else {}
-    for sc, cams in workloads:
+def tune(ctx, workloads, path=None, trace_depth=2, log=print, base=None) -> dict:
+    """workloads: list of (scene_data, cameras) or (scene_data, cameras, trace_depth, spp).
+    The buckets tuned replace those of the table at `base` (default `path`); returns the
+    table and saves it at `path` when given."""
+    src = base or path
+    table = load_table(src) if src else {}
+    for w in workloads:
+        sc, cams = w[0], w[1]
+        td = w[2] if len(w) > 2 else trace_depth
+        spp = w[3] if len(w) > 3 else 1
         b = bucket_of(sc.n_tris)
         if log:
-            log(f"bucket {b}: {sc.name} ({sc.n_tris} tris), {len(cams)} views")
-        table[b] = tune_scene(ctx, sc, cams, trace_depth, log=log)
+            log(f"bucket {b}: {sc.name} ({sc.n_tris} tris), {len(cams)} views, trace depth {td}, {spp} spp")
+        table[b] = tune_scene(ctx, sc, cams, td, log=log, spp=spp)
     if path:
         save_table(table, path)
     apply_table(ctx, table)
