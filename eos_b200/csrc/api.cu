@@ -19,6 +19,12 @@ eos_ctx::~eos_ctx() {
   }
   if (async_host) cudaFreeHost(async_host);
   if (copy_stream) cudaStreamDestroy(copy_stream);
+  if (side_stream) cudaStreamSynchronize(side_stream);
+  for (int k = 0; k < eos::kMaxBounces; ++k) {
+    if (ev_closest[k]) cudaEventDestroy(ev_closest[k]);
+    if (ev_shaded[k]) cudaEventDestroy(ev_shaded[k]);
+  }
+  if (side_stream) cudaStreamDestroy(side_stream);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);

@@ -126,6 +126,12 @@ struct eos_ctx {
   };
   cudaStream_t copy_stream = nullptr;
   AsyncSlot async[2];
+  // batched renders: the stream that runs bounce k's shadow and shading stages while the
+  // render stream runs bounce k+1's nearest-hit stage, with the events that order them
+  // (made on first use)
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_closest[eos::kMaxBounces] = {};
+  cudaEvent_t ev_shaded[eos::kMaxBounces] = {};
   int async_next = 0;
   long long async_seq = 0;
   unsigned long long* async_host = nullptr;  // pinned [2][kCounters + 1] (counters, error word)

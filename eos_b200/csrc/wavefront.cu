@@ -30,7 +30,7 @@ namespace eos {
 namespace {
 
 constexpr long long kChunkPathsMax = 1ll << 24;
-constexpr long long kQueueBudget = 8ll << 30;  // bytes of queues and accumulators per chunk
+constexpr long long kQueueBudget = 16ll << 30;  // bytes of queues and accumulators per chunk
 constexpr int kTileW = 8, kTileH = 4;  // one warp = 8 x 4 pixels
 
 struct DevJob {
@@ -523,12 +523,30 @@ struct StageKernels {
   }
 };
 
+// Overlapped bounces: bounce k's shadow and shading stages depend on its nearest-hit stage
+// only, and bounce k+1's nearest-hit stage on bounce k's nearest-hit stage only (its rays
+// and counters), so the two run at the same time, on `side` and on the render stream; each
+// fills the other's tail of straggling warps.  Bounces alternate between two sets of hit
+// records, shadow masks and shadow queues (set k & 1; `hits1` etc. is the second), and the
+// nearest-hit stage of bounce k+2, which reuses bounce k's set, waits for bounce k's
+// shading (ev_shaded[k]).  side == nullptr: one stream, strictly in order.
+struct Overlap {
+  cudaStream_t side = nullptr;
+  cudaEvent_t* ev_closest = nullptr;  // [kMaxBounces]
+  cudaEvent_t* ev_shaded = nullptr;   // [kMaxBounces]
+  HitQ* hits1 = nullptr;
+  uint32_t* masks1 = nullptr;
+  ShadowQ* sq1 = nullptr;
+};
+
 template <int SH>
 eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, const Chunk* chunks, int n_chunks,
                            int depth, int block, int grid_closest, int grid_any, int* ctr, size_t smem,
-                           bool small_stack, bool tree, StageTimer tm, uint32_t& launches) {
+                           bool small_stack, bool tree, StageTimer tm, const Overlap& ov, uint32_t& launches) {
   const int grid_lin = num_sms * 8;
   const StageKernels<SH> K = StageKernels<SH>::get(small_stack, tree);
+  const bool split = ov.side != nullptr && !tm.on;  // stage timing times the stages one by one
+  cudaStream_t st2 = split ? ov.side : st;
   for (int ci = 0; ci < n_chunks; ++ci) {
     const Chunk& c = chunks[ci];
     WfArgs A = base;
@@ -545,18 +563,30 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
       A.k = k;
       A.rin = rin;
       A.rout = bufs[k & 1];
+      const bool second = split && (k & 1);
+      A.hits = second ? ov.hits1 : base.hits;
+      A.masks = second ? ov.masks1 : base.masks;
+      A.sq = second ? ov.sq1 : base.sq;
+      if (split && k >= 2) EOS_CUDA(cudaStreamWaitEvent(st, ov.ev_shaded[k - 2], 0));
       EOS_TRY(tm.begin());
       (k == 0 ? K.closest_primary : K.closest)<<<grid_closest, block, smem, st>>>(A);
       EOS_TRY(tm.end(0));
+      if (split) {
+        EOS_CUDA(cudaEventRecord(ov.ev_closest[k], st));
+        EOS_CUDA(cudaStreamWaitEvent(st2, ov.ev_closest[k], 0));
+      }
       EOS_TRY(tm.begin());
-      K.any<<<grid_any, block, smem, st>>>(A);
+      K.any<<<grid_any, block, smem, st2>>>(A);
       EOS_TRY(tm.end(1));
       EOS_TRY(tm.begin());
-      K.shade<<<grid_lin, 256, 0, st>>>(A);
+      K.shade<<<grid_lin, 256, 0, st2>>>(A);
       EOS_TRY(tm.end(2));
+      if (split) EOS_CUDA(cudaEventRecord(ov.ev_shaded[k], st2));
       launches += 3;
       rin = A.rout;
     }
+    // the side stream's last shading (it ran every bounce's in order) joins the render stream
+    if (split) EOS_CUDA(cudaStreamWaitEvent(st, ov.ev_shaded[depth], 0));
     EOS_TRY(tm.begin());
     K.resolve<<<grid_lin, 256, 0, st>>>(A);
     EOS_TRY(tm.end(2));
@@ -635,15 +665,15 @@ LaunchConfig launch_config(const eos_render_params& p, int num_sms, bool small_s
 }
 
 eos_status run_sequence(cudaStream_t st, int num_sms, const LaunchConfig& lc, const WfArgs& A, const Chunk* chunks,
-                        int n_chunks, int depth, StageTimer tm, uint32_t& launches) {
+                        int n_chunks, int depth, StageTimer tm, const Overlap& ov, uint32_t& launches) {
   if (lc.sh == 8)
     return launch_sequence<8>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                              lc.small_stack, lc.tree, tm, launches);
+                              lc.small_stack, lc.tree, tm, ov, launches);
   if (lc.sh == 16)
     return launch_sequence<16>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr,
-                               lc.smem, false, lc.tree, tm, launches);
+                               lc.smem, false, lc.tree, tm, ov, launches);
   return launch_sequence<32>(st, num_sms, A, chunks, n_chunks, depth, lc.block, lc.grid_c, lc.grid_a, A.ctr, lc.smem,
-                             false, lc.tree, tm, launches);
+                             false, lc.tree, tm, ov, launches);
 }
 
 }  // namespace
@@ -662,11 +692,13 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     max_lights = std::max(max_lights, (int)jobs[j].scene->dev.n_lights);
     tree = tree || jobs[j].scene->branching;
   }
-  // Per path: rays per bounce (1, or up to 2^depth in tree mode) x (two ray queues, hit
-  // record, mask, shadow queue) + accumulators (one per bounce, or per tree node).
+  // Per path: rays per bounce (1, or up to 2^depth in tree mode) x (two ray queues, two
+  // sets of hit record, mask and shadow queue: Overlap) + accumulators (one per bounce, or
+  // per tree node).
   const long long width = tree ? 1ll << depth : 1;
   const int nn = EOS_TREE_NODES(depth);
-  const long long per_path = width * (3ll * 32 + 4 + 32ll * std::max(1, max_lights)) + 16ll * (tree ? nn : depth + 1);
+  const long long per_path =
+      width * (2ll * 32 + 2 * (32 + 4 + 32ll * std::max(1, max_lights))) + 16ll * (tree ? nn : depth + 1);
   const long long chunk_paths = std::max(1ll << 16, std::min(kChunkPathsMax, kQueueBudget / per_path));
   for (uint32_t j = 0; j < n_jobs; ++j) {
     DevJob& d = dj[j];
@@ -699,6 +731,21 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   ShadowQ* sq = (ShadowQ*)scratch(ctx, "wf.sq", sizeof(ShadowQ) * cap_s, &es);
   float4* acc = (float4*)scratch(ctx, "wf.acc", 16 * (size_t)max_chunk * (tree ? nn : depth + 1), &es);
   int* ctr = (int*)scratch(ctx, "wf.ctr", sizeof(int) * kCtr * (depth + 1), &es);
+  Overlap ov;
+  const bool timing = (p.flags & EOS_FLAG_STAGE_TIMING) != 0;
+  if (depth > 0 && !timing) {  // the second set of per-bounce buffers, the side stream and its events
+    ov.hits1 = (HitQ*)scratch(ctx, "wf.hits1", sizeof(HitQ) * cap_q, &es);
+    ov.masks1 = (uint32_t*)scratch(ctx, "wf.masks1", 4 * cap_q, &es);
+    ov.sq1 = (ShadowQ*)scratch(ctx, "wf.sq1", sizeof(ShadowQ) * cap_s, &es);
+    if (!ctx->side_stream) EOS_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < kMaxBounces; ++k) {
+      if (!ctx->ev_closest[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_closest[k], cudaEventDisableTiming));
+      if (!ctx->ev_shaded[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_shaded[k], cudaEventDisableTiming));
+    }
+    ov.side = ctx->side_stream;
+    ov.ev_closest = ctx->ev_closest;
+    ov.ev_shaded = ctx->ev_shaded;
+  }
   if (es != EOS_OK) return es;
   EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
 
@@ -733,7 +780,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   uint32_t launches = 0;
   StageTimer tm{!use_graph && (p.flags & EOS_FLAG_STAGE_TIMING) != 0, ctx->stream, ctx->ev0, ctx->ev1, ctx->stage_ms};
   auto run = [&]() -> eos_status {
-    return run_sequence(ctx->stream, ctx->num_sms, lc, A, merged.data(), (int)merged.size(), depth, tm, launches);
+    return run_sequence(ctx->stream, ctx->num_sms, lc, A, merged.data(), (int)merged.size(), depth, tm, ov,
+                        launches);
   };
   if (!use_graph) {
     eos_status rs = run();
@@ -746,7 +794,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
                                 (long long)lc.tree, A.cap_r, A.cap_s, A.work_limit,
                                 (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
-                                (long long)(size_t)acc};
+                                (long long)(size_t)acc, (long long)(size_t)hits, (long long)(size_t)ov.hits1,
+                                (long long)(size_t)ov.sq1, (long long)(size_t)masks, (long long)(size_t)ov.masks1};
   for (const Chunk& c : merged) {
     key.push_back(c.c0);
     key.push_back(c.n);
@@ -922,7 +971,7 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
   Chunk ch{0, (int)job.n_paths};
   StageTimer tm{false, s, nullptr, nullptr, nullptr};
   uint32_t launches = 1;
-  st = run_sequence(s, num_sms, lc, A, &ch, 1, A.depth, tm, launches);
+  st = run_sequence(s, num_sms, lc, A, &ch, 1, A.depth, tm, Overlap{}, launches);
   if (st != EOS_OK) return st;
 
   struct {
