@@ -96,6 +96,8 @@ struct WfArgs {
   int nn;         // tree mode: nodes per path (EOS_TREE_NODES of the deepest job)
   int qchunk;
   int work_limit;  // queue entries a persistent launch traces (test limit; INT_MAX = all)
+  int init_in_primary;  // chain mode without a work budget: the primary nearest-hit stage
+                        // does k_wf_init's clearing for its own paths (no init launch)
   int* err;
   unsigned long long* counts;
 };
@@ -208,6 +210,12 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
             path = i;
           } else {
             valid = false;
+            if (!TREE && A.init_in_primary) {  // tile padding: the mark k_wf_init writes
+              HitQ hq;
+              hq.a = make_float4(0, 0, 0, __int_as_float(-1));
+              hq.b = make_float4(0, 0, 0, __int_as_float(-1));
+              A.hits[i] = hq;
+            }
           }
         } else {
           RayQ r = A.rin[i];
@@ -249,17 +257,35 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
             }
           }
         } else {
+          const bool whole = PRIMARY && A.init_in_primary;  // this stage writes the whole record / row
           if (J.paths) {
             int x, y, smp;
             path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
-            J.paths[((size_t)y * J.w + x) * J.spp + smp].hit[A.k] = hit ? h.id : EOS_HIT_NONE;
+            eos_path_record* rec = J.paths + ((size_t)y * J.w + x) * J.spp + smp;
+            if (whole) {
+              eos_path_record r;
+              for (int k = 0; k < kMaxBounces; ++k) {
+                r.hit[k] = EOS_HIT_UNTRACED;
+                r.shadow[k] = 0u;
+              }
+              r.hit[0] = hit ? h.id : EOS_HIT_NONE;
+              *rec = r;
+            } else {
+              rec->hit[A.k] = hit ? h.id : EOS_HIT_NONE;
+            }
           }
+          float w = 0.0f;
           if (hit) {
             hit_geometry(J.s, o, d, h, P, N, obj);
-            float w;
             refl = secondary_ray(J.s.mats + kMatStride * obj, J.s.ambient_index, d, P, N, ro, rd, w);
-            reinterpret_cast<float*>(A.acc + (size_t)path * (A.depth + 1) + A.k)[3] = w;
             refl = refl && A.k < J.trace_depth;
+          }
+          float4* row = A.acc + (size_t)path * (A.depth + 1);
+          if (whole) {
+            row[0] = make_float4(0, 0, 0, w);
+            for (int k = 1; k <= A.depth; ++k) row[k] = make_float4(0, 0, 0, 0);
+          } else if (hit) {
+            reinterpret_cast<float*>(row + A.k)[3] = w;
           }
         }
         HitQ hq;
@@ -553,10 +579,12 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
     A.c0 = c.c0;
     A.n_chunk = c.n;
     EOS_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int) * kCtr * (depth + 1), st));
-    EOS_TRY(tm.begin());
-    K.init<<<grid_lin, 256, 0, st>>>(A);
-    EOS_TRY(tm.end(2));
-    ++launches;
+    if (!A.init_in_primary) {
+      EOS_TRY(tm.begin());
+      K.init<<<grid_lin, 256, 0, st>>>(A);
+      EOS_TRY(tm.end(2));
+      ++launches;
+    }
     const RayQ* rin = nullptr;
     RayQ* bufs[2] = {base.rout, const_cast<RayQ*>(base.rin)};
     for (int k = 0; k <= depth; ++k) {
@@ -774,6 +802,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   }
   A.qchunk = qchunk;
   A.work_limit = lim.work_budget > 0 ? lim.work_budget : 0x7fffffff;
+  A.init_in_primary = !tree && lim.work_budget <= 0;  // a budget leaves primary entries untraced
   A.err = ctx->d_err;
   A.counts = ctx->d_counts;
 
@@ -791,7 +820,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
 
   // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
   std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
-                                (long long)lc.tree, A.cap_r, A.cap_s, A.work_limit,
+                                (long long)lc.tree, A.cap_r, A.cap_s, A.work_limit, (long long)A.init_in_primary,
                                 (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
                                 (long long)(size_t)acc, (long long)(size_t)hits, (long long)(size_t)ov.hits1,
@@ -966,6 +995,7 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
       launch_config(with_tuning(scene->ctx, *params, (uint32_t)scene->dev.n_tris), num_sms, false, false);
   A.qchunk = lc.qchunk;
   A.work_limit = 0x7fffffff;
+  A.init_in_primary = 1;
   A.err = (int*)(base + kNaErr);
   A.counts = (unsigned long long*)(base + kNaCounts);
   Chunk ch{0, (int)job.n_paths};
