@@ -20,11 +20,14 @@ eos_ctx::~eos_ctx() {
   if (async_host) cudaFreeHost(async_host);
   if (copy_stream) cudaStreamDestroy(copy_stream);
   if (side_stream) cudaStreamSynchronize(side_stream);
+  if (shade_stream) cudaStreamSynchronize(shade_stream);
   for (int k = 0; k < eos::kMaxBounces; ++k) {
     if (ev_closest[k]) cudaEventDestroy(ev_closest[k]);
+    if (ev_any[k]) cudaEventDestroy(ev_any[k]);
     if (ev_shaded[k]) cudaEventDestroy(ev_shaded[k]);
   }
   if (side_stream) cudaStreamDestroy(side_stream);
+  if (shade_stream) cudaStreamDestroy(shade_stream);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);

@@ -126,11 +126,13 @@ struct eos_ctx {
   };
   cudaStream_t copy_stream = nullptr;
   AsyncSlot async[2];
-  // batched renders: the stream that runs bounce k's shadow and shading stages while the
-  // render stream runs bounce k+1's nearest-hit stage, with the events that order them
-  // (made on first use)
+  // batched renders: the streams that run bounce k's shadow stage and its shading stage
+  // while the render stream runs bounce k+1's nearest-hit stage, with the events that
+  // order them (made on first use)
   cudaStream_t side_stream = nullptr;
+  cudaStream_t shade_stream = nullptr;
   cudaEvent_t ev_closest[eos::kMaxBounces] = {};
+  cudaEvent_t ev_any[eos::kMaxBounces] = {};
   cudaEvent_t ev_shaded[eos::kMaxBounces] = {};
   int async_next = 0;
   long long async_seq = 0;

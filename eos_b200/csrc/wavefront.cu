@@ -68,6 +68,9 @@ struct HitQ {
 // path's tree bottom-up.  Paths of a chunk are < 2^24 and nodes < 2^8, so a hit record
 // packs both into one word.
 constexpr uint32_t kTreePad = 0xFFFFFFFFu;
+// Chain mode: object id bit of a hit record whose path ends at this bounce (no secondary
+// ray follows); a miss (object id -1) ends its path too.
+constexpr int kEndsBit = 1 << 30;
 __device__ __forceinline__ uint32_t tree_pack(int path, int node) { return (uint32_t)path | ((uint32_t)node << 24); }
 struct ShadowQ {
   float4 a;  // origin xyz, hit index (int)
@@ -97,7 +100,10 @@ struct WfArgs {
   int qchunk;
   int work_limit;  // queue entries a persistent launch traces (test limit; INT_MAX = all)
   int init_in_primary;  // chain mode without a work budget: the primary nearest-hit stage
-                        // does k_wf_init's clearing for its own paths (no init launch)
+                        // does k_wf_init's clearing for its own paths (no init launch), and
+                        // the shading stage writes the pixel of a one-sample path when the
+                        // path ends (k_wf_resolve skips those jobs)
+  int resolve;          // host side: some job needs k_wf_resolve
   int* err;
   unsigned long long* counts;
 };
@@ -290,7 +296,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
         }
         HitQ hq;
         hq.a = make_float4(P.x, P.y, P.z, TREE ? __uint_as_float(tree_pack(path, node)) : __int_as_float(path));
-        hq.b = make_float4(N.x, N.y, N.z, __int_as_float(hit ? obj : -1));
+        hq.b = make_float4(N.x, N.y, N.z, __int_as_float(hit ? (TREE || refl ? obj : obj | kEndsBit) : -1));
         A.hits[i] = hq;
         A.masks[i] = 0u;
       }
@@ -367,6 +373,20 @@ __global__ void __launch_bounds__(256, 4) k_wf_any(WfArgs A) {
   warp_add_count(&A.counts[kCntTestsA], tests);
 }
 
+// The output pixel of path gp (its first sample): FP32 RGB and / or RGBA8.
+__device__ __forceinline__ void write_pixel(const DevJob& J, long long gp, f3 c) {
+  int x, y, smp;
+  path_pixel(J, gp - J.path_off, x, y, smp);
+  const size_t pix = (size_t)y * J.w + x;
+  if (J.rgb) {
+    J.rgb[3 * pix] = c.x;
+    J.rgb[3 * pix + 1] = c.y;
+    J.rgb[3 * pix + 2] = c.z;
+  }
+  if (J.rgba8)
+    reinterpret_cast<uchar4*>(J.rgba8)[pix] = make_uchar4(quantize(c.x), quantize(c.y), quantize(c.z), 255);
+}
+
 template <bool TREE = false>
 __global__ void k_wf_shade(WfArgs A) {
   int* ctr = A.ctr + A.k * kCtr;
@@ -385,24 +405,44 @@ __global__ void k_wf_shade(WfArgs A) {
       if (path < 0) continue;  // tile padding (primary only)
     }
     int obj = __float_as_int(hq.b.w);
+    bool ends = false;
+    if constexpr (!TREE) {
+      ends = obj < 0 || (obj & kEndsBit) != 0;
+      if (obj >= 0) obj &= ~kEndsBit;
+    }
     const DevJob& J = A.jobs[find_job(A.jobs, A.n_jobs, A.c0 + path)];
-    if (obj < 0) continue;
-    f3 P = mk3(hq.a.x, hq.a.y, hq.a.z), N = mk3(hq.b.x, hq.b.y, hq.b.z);
-    f3 cam = mk3(J.cam[0], J.cam[1], J.cam[2]);
-    const float* m = J.s.mats + kMatStride * obj;
-    uint32_t mask = A.masks[i];
-    f3 acc = mk3(0, 0, 0);
-    for (int l = 0; l < J.s.n_lights; ++l)
-      if (!(mask & (1u << l))) acc = add3(acc, phong_light(m, J.s.lights + 6 * l, P, N, cam));
-    // .w: the bounce weight (tree mode: the weight of the edge into the node), set by the hit stage
-    float4* e = TREE ? A.acc + (size_t)path * A.nn + node : A.acc + (size_t)path * (A.depth + 1) + A.k;
-    *e = make_float4(acc.x, acc.y, acc.z, e->w);
-    if (J.paths || (TREE && J.tree)) {
-      int x, y, smp;
-      path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
-      const size_t rec = ((size_t)y * J.w + x) * J.spp + smp;
-      if (TREE) J.tree[rec * J.tree_nn + node].shadow = mask;
-      else J.paths[rec].shadow[A.k] = mask;
+    if (obj >= 0) {
+      f3 P = mk3(hq.a.x, hq.a.y, hq.a.z), N = mk3(hq.b.x, hq.b.y, hq.b.z);
+      f3 cam = mk3(J.cam[0], J.cam[1], J.cam[2]);
+      const float* m = J.s.mats + kMatStride * obj;
+      uint32_t mask = A.masks[i];
+      f3 acc = mk3(0, 0, 0);
+      for (int l = 0; l < J.s.n_lights; ++l)
+        if (!(mask & (1u << l))) acc = add3(acc, phong_light(m, J.s.lights + 6 * l, P, N, cam));
+      // .w: the bounce weight (tree mode: the weight of the edge into the node), set by the hit stage
+      float4* e = TREE ? A.acc + (size_t)path * A.nn + node : A.acc + (size_t)path * (A.depth + 1) + A.k;
+      *e = make_float4(acc.x, acc.y, acc.z, e->w);
+      if (J.paths || (TREE && J.tree)) {
+        int x, y, smp;
+        path_pixel(J, A.c0 + path - J.path_off, x, y, smp);
+        const size_t rec = ((size_t)y * J.w + x) * J.spp + smp;
+        if (TREE) J.tree[rec * J.tree_nn + node].shadow = mask;
+        else J.paths[rec].shadow[A.k] = mask;
+      }
+    }
+    if constexpr (!TREE) {
+      // the path's colour is final: slots beyond this bounce hold zeros, which the fold of
+      // k_wf_resolve passes through unchanged (0 + 0 * 0 = +0), so folding from here gives
+      // its colour bit for bit
+      if (ends && A.init_in_primary && J.spp == 1 && J.grid == 0) {
+        const float4* a = A.acc + (size_t)path * (A.depth + 1);
+        f3 c = mk3(0, 0, 0);
+        for (int k = A.k; k >= 0; --k) {
+          const float4 e = a[k];
+          c = fold_colour(mk3(e.x, e.y, e.z), e.w, c);
+        }
+        write_pixel(J, A.c0 + path, c);
+      }
     }
   }
 }
@@ -471,19 +511,13 @@ __global__ void k_wf_resolve(WfArgs A) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_chunk; i += gridDim.x * blockDim.x) {
     long long gp = A.c0 + i;
     const DevJob& J = A.jobs[find_job(A.jobs, A.n_jobs, gp)];
+    if (!TREE && A.init_in_primary && J.spp == 1 && J.grid == 0) continue;  // written by k_wf_shade
     int x, y, smp;
     if (!path_pixel(J, gp - J.path_off, x, y, smp) || smp != 0) continue;
     f3 sum = mk3(0, 0, 0);
     for (int s = 0; s < J.spp; ++s) sum = add3(sum, path_colour<TREE>(A, i + s));
     if (J.spp > 1 || J.grid > 0) sum = scale3(sample_weight(J.spp, J.grid), sum);
-    size_t pix = (size_t)y * J.w + x;
-    if (J.rgb) {
-      J.rgb[3 * pix] = sum.x;
-      J.rgb[3 * pix + 1] = sum.y;
-      J.rgb[3 * pix + 2] = sum.z;
-    }
-    if (J.rgba8)
-      reinterpret_cast<uchar4*>(J.rgba8)[pix] = make_uchar4(quantize(sum.x), quantize(sum.y), quantize(sum.z), 255);
+    write_pixel(J, gp, sum);
   }
 }
 
@@ -549,16 +583,20 @@ struct StageKernels {
   }
 };
 
-// Overlapped bounces: bounce k's shadow and shading stages depend on its nearest-hit stage
-// only, and bounce k+1's nearest-hit stage on bounce k's nearest-hit stage only (its rays
-// and counters), so the two run at the same time, on `side` and on the render stream; each
-// fills the other's tail of straggling warps.  Bounces alternate between two sets of hit
-// records, shadow masks and shadow queues (set k & 1; `hits1` etc. is the second), and the
-// nearest-hit stage of bounce k+2, which reuses bounce k's set, waits for bounce k's
-// shading (ev_shaded[k]).  side == nullptr: one stream, strictly in order.
+// Overlapped bounces: bounce k's shadow stage depends on its nearest-hit stage only, its
+// shading stage on its shadow stage, and bounce k+1's nearest-hit stage on bounce k's
+// nearest-hit stage only (its rays and counters).  So the nearest-hit stages run in order
+// on the render stream, the shadow stages on `side` and the shading stages on `shade`, each
+// as soon as its inputs are there; the stages fill each other's tails of straggling warps.
+// Bounces alternate between two sets of hit records, shadow masks and shadow queues (set
+// k & 1; `hits1` etc. is the second), and the nearest-hit stage of bounce k+2, which reuses
+// bounce k's set, waits for bounce k's shading (ev_shaded[k]), which followed its shadow
+// stage.  side == nullptr: one stream, strictly in order.
 struct Overlap {
   cudaStream_t side = nullptr;
+  cudaStream_t shade = nullptr;
   cudaEvent_t* ev_closest = nullptr;  // [kMaxBounces]
+  cudaEvent_t* ev_any = nullptr;      // [kMaxBounces]
   cudaEvent_t* ev_shaded = nullptr;   // [kMaxBounces]
   HitQ* hits1 = nullptr;
   uint32_t* masks1 = nullptr;
@@ -572,7 +610,7 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
   const int grid_lin = num_sms * 8;
   const StageKernels<SH> K = StageKernels<SH>::get(small_stack, tree);
   const bool split = ov.side != nullptr && !tm.on;  // stage timing times the stages one by one
-  cudaStream_t st2 = split ? ov.side : st;
+  cudaStream_t st2 = split ? ov.side : st, st3 = split ? ov.shade : st;
   for (int ci = 0; ci < n_chunks; ++ci) {
     const Chunk& c = chunks[ci];
     WfArgs A = base;
@@ -606,19 +644,29 @@ eos_status launch_sequence(cudaStream_t st, int num_sms, const WfArgs& base, con
       EOS_TRY(tm.begin());
       K.any<<<grid_any, block, smem, st2>>>(A);
       EOS_TRY(tm.end(1));
+      if (split) {
+        EOS_CUDA(cudaEventRecord(ov.ev_any[k], st2));
+        EOS_CUDA(cudaStreamWaitEvent(st3, ov.ev_any[k], 0));
+      }
       EOS_TRY(tm.begin());
-      K.shade<<<grid_lin, 256, 0, st2>>>(A);
+      K.shade<<<grid_lin, 256, 0, st3>>>(A);
       EOS_TRY(tm.end(2));
-      if (split) EOS_CUDA(cudaEventRecord(ov.ev_shaded[k], st2));
+      if (split) EOS_CUDA(cudaEventRecord(ov.ev_shaded[k], st3));
       launches += 3;
       rin = A.rout;
     }
-    // the side stream's last shading (it ran every bounce's in order) joins the render stream
-    if (split) EOS_CUDA(cudaStreamWaitEvent(st, ov.ev_shaded[depth], 0));
-    EOS_TRY(tm.begin());
-    K.resolve<<<grid_lin, 256, 0, st>>>(A);
-    EOS_TRY(tm.end(2));
-    ++launches;
+    // both side streams end with this chunk's last bounce (each ran its stages in order)
+    // and join the render stream
+    if (split) {
+      EOS_CUDA(cudaStreamWaitEvent(st, ov.ev_any[depth], 0));
+      EOS_CUDA(cudaStreamWaitEvent(st, ov.ev_shaded[depth], 0));
+    }
+    if (A.resolve) {
+      EOS_TRY(tm.begin());
+      K.resolve<<<grid_lin, 256, 0, st>>>(A);
+      EOS_TRY(tm.end(2));
+      ++launches;
+    }
   }
   EOS_CUDA(cudaGetLastError());
   return EOS_OK;
@@ -766,12 +814,16 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     ov.masks1 = (uint32_t*)scratch(ctx, "wf.masks1", 4 * cap_q, &es);
     ov.sq1 = (ShadowQ*)scratch(ctx, "wf.sq1", sizeof(ShadowQ) * cap_s, &es);
     if (!ctx->side_stream) EOS_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+    if (!ctx->shade_stream) EOS_CUDA(cudaStreamCreateWithFlags(&ctx->shade_stream, cudaStreamNonBlocking));
     for (int k = 0; k < kMaxBounces; ++k) {
       if (!ctx->ev_closest[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_closest[k], cudaEventDisableTiming));
+      if (!ctx->ev_any[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_any[k], cudaEventDisableTiming));
       if (!ctx->ev_shaded[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_shaded[k], cudaEventDisableTiming));
     }
     ov.side = ctx->side_stream;
+    ov.shade = ctx->shade_stream;
     ov.ev_closest = ctx->ev_closest;
+    ov.ev_any = ctx->ev_any;
     ov.ev_shaded = ctx->ev_shaded;
   }
   if (es != EOS_OK) return es;
@@ -803,6 +855,8 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   A.qchunk = qchunk;
   A.work_limit = lim.work_budget > 0 ? lim.work_budget : 0x7fffffff;
   A.init_in_primary = !tree && lim.work_budget <= 0;  // a budget leaves primary entries untraced
+  A.resolve = !A.init_in_primary;
+  for (uint32_t j = 0; j < n_jobs; ++j) A.resolve |= dj[j].spp > 1 || dj[j].grid > 0;
   A.err = ctx->d_err;
   A.counts = ctx->d_counts;
 
@@ -821,6 +875,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
   std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
                                 (long long)lc.tree, A.cap_r, A.cap_s, A.work_limit, (long long)A.init_in_primary,
+                                (long long)A.resolve,
                                 (long long)(size_t)d_jobs,
                                 (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
                                 (long long)(size_t)acc, (long long)(size_t)hits, (long long)(size_t)ov.hits1,
@@ -996,6 +1051,7 @@ extern "C" eos_status eos_render_noalloc(const eos_scene* scene, const eos_camer
   A.qchunk = lc.qchunk;
   A.work_limit = 0x7fffffff;
   A.init_in_primary = 1;
+  A.resolve = job.spp > 1 || job.grid > 0;
   A.err = (int*)(base + kNaErr);
   A.counts = (unsigned long long*)(base + kNaCounts);
   Chunk ch{0, (int)job.n_paths};
