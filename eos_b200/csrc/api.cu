@@ -19,15 +19,19 @@ eos_ctx::~eos_ctx() {
   }
   if (async_host) cudaFreeHost(async_host);
   if (copy_stream) cudaStreamDestroy(copy_stream);
-  if (side_stream) cudaStreamSynchronize(side_stream);
-  if (shade_stream) cudaStreamSynchronize(shade_stream);
-  for (int k = 0; k < eos::kMaxBounces; ++k) {
-    if (ev_closest[k]) cudaEventDestroy(ev_closest[k]);
-    if (ev_any[k]) cudaEventDestroy(ev_any[k]);
-    if (ev_shaded[k]) cudaEventDestroy(ev_shaded[k]);
+  for (WfLane& l : wf_lane) {
+    for (cudaStream_t s : {l.main, l.side, l.shade})
+      if (s) cudaStreamSynchronize(s);
+    for (int k = 0; k < eos::kMaxBounces; ++k) {
+      if (l.ev_closest[k]) cudaEventDestroy(l.ev_closest[k]);
+      if (l.ev_any[k]) cudaEventDestroy(l.ev_any[k]);
+      if (l.ev_shaded[k]) cudaEventDestroy(l.ev_shaded[k]);
+    }
+    for (cudaStream_t s : {l.main, l.side, l.shade})
+      if (s) cudaStreamDestroy(s);
   }
-  if (side_stream) cudaStreamDestroy(side_stream);
-  if (shade_stream) cudaStreamDestroy(shade_stream);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);

@@ -126,14 +126,19 @@ struct eos_ctx {
   };
   cudaStream_t copy_stream = nullptr;
   AsyncSlot async[2];
-  // batched renders: the streams that run bounce k's shadow stage and its shading stage
-  // while the render stream runs bounce k+1's nearest-hit stage, with the events that
-  // order them (made on first use)
-  cudaStream_t side_stream = nullptr;
-  cudaStream_t shade_stream = nullptr;
-  cudaEvent_t ev_closest[eos::kMaxBounces] = {};
-  cudaEvent_t ev_any[eos::kMaxBounces] = {};
-  cudaEvent_t ev_shaded[eos::kMaxBounces] = {};
+  // batched renders run as up to two lanes (halves of the paths) at once; a lane's
+  // nearest-hit stages run on its main stream (lane 0: the context's stream), its shadow
+  // and shading stages on two more streams, ordered by events (all made on first use)
+  struct WfLane {
+    cudaStream_t main = nullptr;  // lane 1 only
+    cudaStream_t side = nullptr;
+    cudaStream_t shade = nullptr;
+    cudaEvent_t ev_closest[eos::kMaxBounces] = {};
+    cudaEvent_t ev_any[eos::kMaxBounces] = {};
+    cudaEvent_t ev_shaded[eos::kMaxBounces] = {};
+  };
+  WfLane wf_lane[2];
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int async_next = 0;
   long long async_seq = 0;
   unsigned long long* async_host = nullptr;  // pinned [2][kCounters + 1] (counters, error word)

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "trace.cuh"
@@ -31,6 +32,7 @@ namespace {
 
 constexpr long long kChunkPathsMax = 1ll << 24;
 constexpr long long kQueueBudget = 16ll << 30;  // bytes of queues and accumulators per chunk
+constexpr long long kLaneSplitMin = 1ll << 20;  // paths of a chunk from which it runs as two lanes
 constexpr int kTileW = 8, kTileH = 4;  // one warp = 8 x 4 pixels
 
 struct DevJob {
@@ -793,78 +795,137 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     else
       merged.push_back(c);
   }
-  int max_chunk = 0;
-  for (const Chunk& c : merged) max_chunk = std::max(max_chunk, c.n);
+  // Two lanes: the paths of a large pass are split in halves (at a whole pixel) that run at
+  // the same time, each on its own streams and buffers, so that one half's start and its
+  // tails of straggling warps overlap the other half's busy stages.
+  const bool timing = (p.flags & EOS_FLAG_STAGE_TIMING) != 0;
+  long long biggest = 0;
+  for (const Chunk& c : merged) biggest = std::max<long long>(biggest, c.n);
+  std::vector<Chunk> lane_chunks[2];
+  if (timing || depth == 0 || !use_graph || biggest < kLaneSplitMin) {
+    lane_chunks[0] = merged;
+  } else {
+    for (const Chunk& c : merged) {
+      const long long mid = c.c0 + c.n / 2;
+      int j = 0;  // the job holding the middle path
+      for (int lo = 0, hi = (int)n_jobs - 1; lo <= hi;) {
+        const int m = (lo + hi) / 2;
+        if (dj[m].path_off <= mid) {
+          j = m;
+          lo = m + 1;
+        } else {
+          hi = m - 1;
+        }
+      }
+      const long long unit = 32ll * dj[j].spp;
+      const long long cut = dj[j].path_off + ((mid - dj[j].path_off) / unit) * unit;
+      if (cut <= c.c0 || cut >= c.c0 + c.n) {
+        lane_chunks[0].push_back(c);
+        continue;
+      }
+      lane_chunks[0].push_back({c.c0, (int)(cut - c.c0)});
+      lane_chunks[1].push_back({cut, (int)(c.c0 + c.n - cut)});
+    }
+  }
+  const int n_lanes = lane_chunks[1].empty() ? 1 : 2;
 
   eos_status es = EOS_OK;
   DevJob* d_jobs = (DevJob*)scratch(ctx, "wf.jobs", sizeof(DevJob) * n_jobs, &es);
-  const size_t cap_q = (size_t)max_chunk * width;  // rays of one bounce
-  RayQ* r0 = (RayQ*)scratch(ctx, "wf.r0", sizeof(RayQ) * cap_q, &es);
-  RayQ* r1 = (RayQ*)scratch(ctx, "wf.r1", sizeof(RayQ) * cap_q, &es);
-  HitQ* hits = (HitQ*)scratch(ctx, "wf.hits", sizeof(HitQ) * cap_q, &es);
-  uint32_t* masks = (uint32_t*)scratch(ctx, "wf.masks", 4 * cap_q, &es);
-  size_t cap_s = cap_q * std::max(1, max_lights);
-  ShadowQ* sq = (ShadowQ*)scratch(ctx, "wf.sq", sizeof(ShadowQ) * cap_s, &es);
-  float4* acc = (float4*)scratch(ctx, "wf.acc", 16 * (size_t)max_chunk * (tree ? nn : depth + 1), &es);
-  int* ctr = (int*)scratch(ctx, "wf.ctr", sizeof(int) * kCtr * (depth + 1), &es);
-  Overlap ov;
-  const bool timing = (p.flags & EOS_FLAG_STAGE_TIMING) != 0;
-  if (depth > 0 && !timing) {  // the second set of per-bounce buffers, the side stream and its events
-    ov.hits1 = (HitQ*)scratch(ctx, "wf.hits1", sizeof(HitQ) * cap_q, &es);
-    ov.masks1 = (uint32_t*)scratch(ctx, "wf.masks1", 4 * cap_q, &es);
-    ov.sq1 = (ShadowQ*)scratch(ctx, "wf.sq1", sizeof(ShadowQ) * cap_s, &es);
-    if (!ctx->side_stream) EOS_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
-    if (!ctx->shade_stream) EOS_CUDA(cudaStreamCreateWithFlags(&ctx->shade_stream, cudaStreamNonBlocking));
-    for (int k = 0; k < kMaxBounces; ++k) {
-      if (!ctx->ev_closest[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_closest[k], cudaEventDisableTiming));
-      if (!ctx->ev_any[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_any[k], cudaEventDisableTiming));
-      if (!ctx->ev_shaded[k]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_shaded[k], cudaEventDisableTiming));
-    }
-    ov.side = ctx->side_stream;
-    ov.shade = ctx->shade_stream;
-    ov.ev_closest = ctx->ev_closest;
-    ov.ev_any = ctx->ev_any;
-    ov.ev_shaded = ctx->ev_shaded;
-  }
-  if (es != EOS_OK) return es;
-  EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
-
   const eos_limits& lim = ctx->limits;
   const LaunchConfig lc = launch_config(p, ctx->num_sms, lim.small_stack != 0, tree);
   const int block = lc.block, sh = lc.sh, qchunk = lc.qchunk;
 
-  WfArgs A;
-  memset(&A, 0, sizeof A);
-  A.jobs = d_jobs;
-  A.n_jobs = (int)n_jobs;
-  A.depth = depth;
-  A.rin = r1;
-  A.rout = r0;
-  A.hits = hits;
-  A.masks = masks;
-  A.sq = sq;
-  A.acc = acc;
-  A.ctr = ctr;
-  A.cap_r = (int)std::min<size_t>(cap_q, 0x7fffffff);
-  A.cap_s = (int)std::min<size_t>(cap_s, 0x7fffffff);
-  A.nn = nn;
-  if (lim.queue_entries > 0) {
-    A.cap_r = std::min(A.cap_r, (int)lim.queue_entries);
-    A.cap_s = std::min(A.cap_s, (int)lim.queue_entries);
+  WfArgs A[2];
+  Overlap ov[2];
+  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
+                                (long long)lc.tree, n_lanes, (long long)(size_t)d_jobs};
+  for (int l = 0; l < n_lanes; ++l) {
+    int max_chunk = 0;
+    for (const Chunk& c : lane_chunks[l]) max_chunk = std::max(max_chunk, c.n);
+    const std::string tag = l == 0 ? "wf." : "wf.b.";
+    auto buf = [&](const char* name, size_t bytes) { return scratch(ctx, (tag + name).c_str(), bytes, &es); };
+    const size_t cap_q = (size_t)max_chunk * width;  // rays of one bounce
+    const size_t cap_s = cap_q * std::max(1, max_lights);
+    WfArgs& a = A[l];
+    memset(&a, 0, sizeof a);
+    a.jobs = d_jobs;
+    a.n_jobs = (int)n_jobs;
+    a.depth = depth;
+    a.rout = (RayQ*)buf("r0", sizeof(RayQ) * cap_q);
+    a.rin = (RayQ*)buf("r1", sizeof(RayQ) * cap_q);
+    a.hits = (HitQ*)buf("hits", sizeof(HitQ) * cap_q);
+    a.masks = (uint32_t*)buf("masks", 4 * cap_q);
+    a.sq = (ShadowQ*)buf("sq", sizeof(ShadowQ) * cap_s);
+    a.acc = (float4*)buf("acc", 16 * (size_t)max_chunk * (tree ? nn : depth + 1));
+    a.ctr = (int*)buf("ctr", sizeof(int) * kCtr * (depth + 1));
+    a.cap_r = (int)std::min<size_t>(cap_q, 0x7fffffff);
+    a.cap_s = (int)std::min<size_t>(cap_s, 0x7fffffff);
+    a.nn = nn;
+    if (lim.queue_entries > 0) {
+      a.cap_r = std::min(a.cap_r, (int)lim.queue_entries);
+      a.cap_s = std::min(a.cap_s, (int)lim.queue_entries);
+    }
+    a.qchunk = qchunk;
+    a.work_limit = lim.work_budget > 0 ? lim.work_budget : 0x7fffffff;
+    a.init_in_primary = !tree && lim.work_budget <= 0;  // a budget leaves primary entries untraced
+    a.resolve = !a.init_in_primary;
+    for (uint32_t j = 0; j < n_jobs; ++j) a.resolve |= dj[j].spp > 1 || dj[j].grid > 0;
+    a.err = ctx->d_err;
+    a.counts = ctx->d_counts;
+    eos_ctx::WfLane& ln = ctx->wf_lane[l];
+    if (depth > 0 && !timing) {  // the second set of per-bounce buffers, the side streams and their events
+      ov[l].hits1 = (HitQ*)buf("hits1", sizeof(HitQ) * cap_q);
+      ov[l].masks1 = (uint32_t*)buf("masks1", 4 * cap_q);
+      ov[l].sq1 = (ShadowQ*)buf("sq1", sizeof(ShadowQ) * cap_s);
+      if (l == 1 && !ln.main) EOS_CUDA(cudaStreamCreateWithFlags(&ln.main, cudaStreamNonBlocking));
+      if (!ln.side) EOS_CUDA(cudaStreamCreateWithFlags(&ln.side, cudaStreamNonBlocking));
+      if (!ln.shade) EOS_CUDA(cudaStreamCreateWithFlags(&ln.shade, cudaStreamNonBlocking));
+      for (int k = 0; k < kMaxBounces; ++k) {
+        if (!ln.ev_closest[k]) EOS_CUDA(cudaEventCreateWithFlags(&ln.ev_closest[k], cudaEventDisableTiming));
+        if (!ln.ev_any[k]) EOS_CUDA(cudaEventCreateWithFlags(&ln.ev_any[k], cudaEventDisableTiming));
+        if (!ln.ev_shaded[k]) EOS_CUDA(cudaEventCreateWithFlags(&ln.ev_shaded[k], cudaEventDisableTiming));
+      }
+      ov[l].side = ln.side;
+      ov[l].shade = ln.shade;
+      ov[l].ev_closest = ln.ev_closest;
+      ov[l].ev_any = ln.ev_any;
+      ov[l].ev_shaded = ln.ev_shaded;
+    }
+    if (es != EOS_OK) return es;
+    for (long long v : {(long long)a.cap_r, (long long)a.cap_s, (long long)a.work_limit, (long long)a.init_in_primary,
+                        (long long)a.resolve, (long long)(size_t)a.rout, (long long)(size_t)a.rin,
+                        (long long)(size_t)a.hits, (long long)(size_t)a.masks, (long long)(size_t)a.sq,
+                        (long long)(size_t)a.acc, (long long)(size_t)a.ctr, (long long)(size_t)ov[l].hits1,
+                        (long long)(size_t)ov[l].masks1, (long long)(size_t)ov[l].sq1})
+      key.push_back(v);
+    for (const Chunk& c : lane_chunks[l]) {
+      key.push_back(c.c0);
+      key.push_back(c.n);
+    }
   }
-  A.qchunk = qchunk;
-  A.work_limit = lim.work_budget > 0 ? lim.work_budget : 0x7fffffff;
-  A.init_in_primary = !tree && lim.work_budget <= 0;  // a budget leaves primary entries untraced
-  A.resolve = !A.init_in_primary;
-  for (uint32_t j = 0; j < n_jobs; ++j) A.resolve |= dj[j].spp > 1 || dj[j].grid > 0;
-  A.err = ctx->d_err;
-  A.counts = ctx->d_counts;
+  if (n_lanes == 2 && !ctx->ev_fork) {
+    EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
+  EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
 
   uint32_t launches = 0;
-  StageTimer tm{!use_graph && (p.flags & EOS_FLAG_STAGE_TIMING) != 0, ctx->stream, ctx->ev0, ctx->ev1, ctx->stage_ms};
+  StageTimer tm{!use_graph && timing, ctx->stream, ctx->ev0, ctx->ev1, ctx->stage_ms};
   auto run = [&]() -> eos_status {
-    return run_sequence(ctx->stream, ctx->num_sms, lc, A, merged.data(), (int)merged.size(), depth, tm, ov,
-                        launches);
+    cudaStream_t s1 = ctx->wf_lane[1].main;
+    if (n_lanes == 2) {  // lane 1 forks from the context's stream and joins it at the end
+      EOS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+      EOS_CUDA(cudaStreamWaitEvent(s1, ctx->ev_fork, 0));
+    }
+    EOS_TRY(run_sequence(ctx->stream, ctx->num_sms, lc, A[0], lane_chunks[0].data(), (int)lane_chunks[0].size(),
+                         depth, tm, ov[0], launches));
+    if (n_lanes == 2) {
+      EOS_TRY(run_sequence(s1, ctx->num_sms, lc, A[1], lane_chunks[1].data(), (int)lane_chunks[1].size(), depth,
+                           tm, ov[1], launches));
+      EOS_CUDA(cudaEventRecord(ctx->ev_join, s1));
+      EOS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    }
+    return EOS_OK;
   };
   if (!use_graph) {
     eos_status rs = run();
@@ -872,18 +933,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     return rs;
   }
 
-  // graph cache: the sequence depends on the chunk plan, depth, buffers and tuning only
-  std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
-                                (long long)lc.tree, A.cap_r, A.cap_s, A.work_limit, (long long)A.init_in_primary,
-                                (long long)A.resolve,
-                                (long long)(size_t)d_jobs,
-                                (long long)(size_t)r0, (long long)(size_t)r1, (long long)(size_t)sq,
-                                (long long)(size_t)acc, (long long)(size_t)hits, (long long)(size_t)ov.hits1,
-                                (long long)(size_t)ov.sq1, (long long)(size_t)masks, (long long)(size_t)ov.masks1};
-  for (const Chunk& c : merged) {
-    key.push_back(c.c0);
-    key.push_back(c.n);
-  }
+  // graph cache: the sequence depends on the lanes' chunk plans, depth, buffers and tuning only
   for (auto& g : ctx->graphs)
     if (g->key == key) {
       EOS_CUDA(cudaGraphLaunch(g->exec, ctx->stream));
