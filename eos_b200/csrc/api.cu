@@ -31,7 +31,8 @@ eos_ctx::~eos_ctx() {
       if (s) cudaStreamDestroy(s);
   }
   if (ev_fork) cudaEventDestroy(ev_fork);
-  if (ev_join) cudaEventDestroy(ev_join);
+  for (cudaEvent_t e : ev_join)
+    if (e) cudaEventDestroy(e);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);

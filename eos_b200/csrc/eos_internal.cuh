@@ -126,7 +126,7 @@ struct eos_ctx {
   };
   cudaStream_t copy_stream = nullptr;
   AsyncSlot async[2];
-  // batched renders run as up to two lanes (halves of the paths) at once; a lane's
+  // batched renders run as up to kWfLanes lanes (parts of the paths) at once; a lane's
   // nearest-hit stages run on its main stream (lane 0: the context's stream), its shadow
   // and shading stages on two more streams, ordered by events (all made on first use)
   struct WfLane {
@@ -137,8 +137,10 @@ struct eos_ctx {
     cudaEvent_t ev_any[eos::kMaxBounces] = {};
     cudaEvent_t ev_shaded[eos::kMaxBounces] = {};
   };
-  WfLane wf_lane[2];
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  static constexpr int kWfLanes = 4;
+  WfLane wf_lane[kWfLanes];
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kWfLanes] = {};
   int async_next = 0;
   long long async_seq = 0;
   unsigned long long* async_host = nullptr;  // pinned [2][kCounters + 1] (counters, error word)

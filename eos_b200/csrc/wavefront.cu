@@ -32,7 +32,8 @@ namespace {
 
 constexpr long long kChunkPathsMax = 1ll << 24;
 constexpr long long kQueueBudget = 16ll << 30;  // bytes of queues and accumulators per chunk
-constexpr long long kLaneSplitMin = 1ll << 20;  // paths of a chunk from which it runs as two lanes
+constexpr long long kLaneSplitMin = 1ll << 20;  // paths of a chunk from which it runs as several lanes
+constexpr int kLanes = 2;                       // lanes of such a chunk (<= eos_ctx::kWfLanes)
 constexpr int kTileW = 8, kTileH = 4;  // one warp = 8 x 4 pixels
 
 struct DevJob {
@@ -795,39 +796,41 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
     else
       merged.push_back(c);
   }
-  // Two lanes: the paths of a large pass are split in halves (at a whole pixel) that run at
-  // the same time, each on its own streams and buffers, so that one half's start and its
-  // tails of straggling warps overlap the other half's busy stages.
+  // Lanes: the paths of a large pass are split in kLanes parts (at whole pixels) that run
+  // at the same time, each on its own streams and buffers, so that one part's start and its
+  // tails of straggling warps overlap the other parts' busy stages.
+  static_assert(kLanes >= 1 && kLanes <= eos_ctx::kWfLanes, "lane count");
   const bool timing = (p.flags & EOS_FLAG_STAGE_TIMING) != 0;
   long long biggest = 0;
   for (const Chunk& c : merged) biggest = std::max<long long>(biggest, c.n);
-  std::vector<Chunk> lane_chunks[2];
+  std::vector<Chunk> lane_chunks[kLanes];
   if (timing || depth == 0 || !use_graph || biggest < kLaneSplitMin) {
     lane_chunks[0] = merged;
   } else {
     for (const Chunk& c : merged) {
-      const long long mid = c.c0 + c.n / 2;
-      int j = 0;  // the job holding the middle path
-      for (int lo = 0, hi = (int)n_jobs - 1; lo <= hi;) {
-        const int m = (lo + hi) / 2;
-        if (dj[m].path_off <= mid) {
-          j = m;
-          lo = m + 1;
-        } else {
-          hi = m - 1;
+      std::vector<long long> cuts = {c.c0};
+      for (int part = 1; part < kLanes; ++part) {
+        const long long at = c.c0 + (long long)c.n * part / kLanes;
+        int j = 0;  // the job holding path `at`
+        for (int lo = 0, hi = (int)n_jobs - 1; lo <= hi;) {
+          const int m = (lo + hi) / 2;
+          if (dj[m].path_off <= at) {
+            j = m;
+            lo = m + 1;
+          } else {
+            hi = m - 1;
+          }
         }
+        const long long unit = 32ll * dj[j].spp;
+        const long long cut = dj[j].path_off + ((at - dj[j].path_off) / unit) * unit;
+        if (cut > cuts.back() && cut < c.c0 + c.n) cuts.push_back(cut);
       }
-      const long long unit = 32ll * dj[j].spp;
-      const long long cut = dj[j].path_off + ((mid - dj[j].path_off) / unit) * unit;
-      if (cut <= c.c0 || cut >= c.c0 + c.n) {
-        lane_chunks[0].push_back(c);
-        continue;
-      }
-      lane_chunks[0].push_back({c.c0, (int)(cut - c.c0)});
-      lane_chunks[1].push_back({cut, (int)(c.c0 + c.n - cut)});
+      cuts.push_back(c.c0 + c.n);
+      for (size_t l = 0; l + 1 < cuts.size(); ++l) lane_chunks[l].push_back({cuts[l], (int)(cuts[l + 1] - cuts[l])});
     }
   }
-  const int n_lanes = lane_chunks[1].empty() ? 1 : 2;
+  int n_lanes = 1;
+  while (n_lanes < kLanes && !lane_chunks[n_lanes].empty()) ++n_lanes;
 
   eos_status es = EOS_OK;
   DevJob* d_jobs = (DevJob*)scratch(ctx, "wf.jobs", sizeof(DevJob) * n_jobs, &es);
@@ -835,14 +838,14 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
   const LaunchConfig lc = launch_config(p, ctx->num_sms, lim.small_stack != 0, tree);
   const int block = lc.block, sh = lc.sh, qchunk = lc.qchunk;
 
-  WfArgs A[2];
-  Overlap ov[2];
+  WfArgs A[kLanes];
+  Overlap ov[kLanes];
   std::vector<long long> key = {(long long)n_jobs, depth, max_lights, block, sh, qchunk, (long long)lc.small_stack,
                                 (long long)lc.tree, n_lanes, (long long)(size_t)d_jobs};
   for (int l = 0; l < n_lanes; ++l) {
     int max_chunk = 0;
     for (const Chunk& c : lane_chunks[l]) max_chunk = std::max(max_chunk, c.n);
-    const std::string tag = l == 0 ? "wf." : "wf.b.";
+    const std::string tag = l == 0 ? std::string("wf.") : "wf." + std::to_string(l) + ".";
     auto buf = [&](const char* name, size_t bytes) { return scratch(ctx, (tag + name).c_str(), bytes, &es); };
     const size_t cap_q = (size_t)max_chunk * width;  // rays of one bounce
     const size_t cap_s = cap_q * std::max(1, max_lights);
@@ -877,7 +880,7 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
       ov[l].hits1 = (HitQ*)buf("hits1", sizeof(HitQ) * cap_q);
       ov[l].masks1 = (uint32_t*)buf("masks1", 4 * cap_q);
       ov[l].sq1 = (ShadowQ*)buf("sq1", sizeof(ShadowQ) * cap_s);
-      if (l == 1 && !ln.main) EOS_CUDA(cudaStreamCreateWithFlags(&ln.main, cudaStreamNonBlocking));
+      if (l > 0 && !ln.main) EOS_CUDA(cudaStreamCreateWithFlags(&ln.main, cudaStreamNonBlocking));
       if (!ln.side) EOS_CUDA(cudaStreamCreateWithFlags(&ln.side, cudaStreamNonBlocking));
       if (!ln.shade) EOS_CUDA(cudaStreamCreateWithFlags(&ln.shade, cudaStreamNonBlocking));
       for (int k = 0; k < kMaxBounces; ++k) {
@@ -903,27 +906,25 @@ eos_status render_wavefront(eos_ctx* ctx, const eos_job* jobs, uint32_t n_jobs, 
       key.push_back(c.n);
     }
   }
-  if (n_lanes == 2 && !ctx->ev_fork) {
-    EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-    EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
-  }
+  if (n_lanes > 1 && !ctx->ev_fork) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  for (int l = 1; l < n_lanes; ++l)
+    if (!ctx->ev_join[l]) EOS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join[l], cudaEventDisableTiming));
   EOS_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, ctx->stream));
 
   uint32_t launches = 0;
   StageTimer tm{!use_graph && timing, ctx->stream, ctx->ev0, ctx->ev1, ctx->stage_ms};
   auto run = [&]() -> eos_status {
-    cudaStream_t s1 = ctx->wf_lane[1].main;
-    if (n_lanes == 2) {  // lane 1 forks from the context's stream and joins it at the end
-      EOS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
-      EOS_CUDA(cudaStreamWaitEvent(s1, ctx->ev_fork, 0));
+    // lanes 1.. fork from the context's stream and join it at the end
+    if (n_lanes > 1) EOS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    for (int l = 1; l < n_lanes; ++l) EOS_CUDA(cudaStreamWaitEvent(ctx->wf_lane[l].main, ctx->ev_fork, 0));
+    for (int l = 0; l < n_lanes; ++l) {
+      cudaStream_t s_l = l == 0 ? ctx->stream : ctx->wf_lane[l].main;
+      EOS_TRY(run_sequence(s_l, ctx->num_sms, lc, A[l], lane_chunks[l].data(), (int)lane_chunks[l].size(), depth, tm,
+                           ov[l], launches));
     }
-    EOS_TRY(run_sequence(ctx->stream, ctx->num_sms, lc, A[0], lane_chunks[0].data(), (int)lane_chunks[0].size(),
-                         depth, tm, ov[0], launches));
-    if (n_lanes == 2) {
-      EOS_TRY(run_sequence(s1, ctx->num_sms, lc, A[1], lane_chunks[1].data(), (int)lane_chunks[1].size(), depth,
-                           tm, ov[1], launches));
-      EOS_CUDA(cudaEventRecord(ctx->ev_join, s1));
-      EOS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    for (int l = 1; l < n_lanes; ++l) {
+      EOS_CUDA(cudaEventRecord(ctx->ev_join[l], ctx->wf_lane[l].main));
+      EOS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join[l], 0));
     }
     return EOS_OK;
   };
