@@ -7,9 +7,10 @@
 //                          per warp
 //   any      (persistent)  any-hit of every shadow ray in S_k; blocked -> bit in the hit's
 //                          light mask
-//   shade                  Phong over the unblocked lights, in light order, per hit
+//   shade                  Phong over the unblocked lights, in light order, per hit; for a
+//                          one-sample job, the colour and pixel of each path ending here
 //   resolve                colour fold c_k = phong_k + refl_k c_k+1 per path, sample mean,
-//                          RGB / RGBA8 / path records to each job's buffers
+//                          RGB / RGBA8 to each job's buffers (jobs of several samples, trees)
 //
 // The semantics are those of the reference's CPU renderer (src/RayTracer.cpp:268-458),
 // identical to the plain renderer (render.cu) bit for bit: the same hits, masks and
@@ -17,8 +18,11 @@
 // rays of uneven cost balance across the SMs.  Paths are processed in chunks of at most
 // kChunkPathsMax, fewer when the queues of a chunk would exceed kQueueBudget bytes: one
 // large chunk keeps the persistent kernels' tails short (8.3M paths in one chunk ran the
-// config-2 batch 25 % faster than four chunks of 2M).  The whole sequence for a batch is captured once as a
-// CUDA graph and replayed; the job table is uploaded before each replay.
+// config-2 batch 25 % faster than four chunks of 2M).  Bounce k's shadow and shading stages
+// run beside bounce k+1's nearest-hit stage (Overlap), and a large chunk runs as kLanes
+// parts side by side (render_wavefront), so that stages fill each other's tails.  The whole
+// sequence for a batch is captured once as a CUDA graph and replayed; the job table is
+// uploaded before each replay.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
