@@ -64,6 +64,24 @@ def test_limit_gives_its_status_and_the_context_stays_usable(ctx, big, lim, code
     assert np.array_equal(outs[0]["rgb"].cpu().numpy(), ref["rgb"])
 
 
+@pytest.mark.parametrize("lim,code", [(dict(queue_entries=64), QUEUE), (dict(work_budget=1000), TIMEOUT),
+                                      (dict(small_stack=True), STACK)])
+def test_limits_on_a_pass_of_two_lanes(ctx, big, lim, code):
+    """A view of more than 2^20 paths runs as two lanes (halves of its paths side by side):
+    each limit still gives its status, and the same context then renders the plain
+    renderer's image."""
+    import torch
+    dsc, _, _ = big
+    cam = scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 1280, 960)
+    ref = api.render(ctx, dsc, cam, 2, mode="plain", outputs=("rgb",), device=True)
+    jobs = [api.BatchJob(dsc, cam, 2, 0.5)]
+    outs = api.make_batch_outputs(jobs, ("rgb",))
+    assert _limited(ctx, lambda: api.render_batch(ctx, jobs, outs), **lim) == code
+    api.render_batch(ctx, jobs, outs)
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0]["rgb"], ref["rgb"])
+
+
 def test_work_budget_leaves_untraced_paths_marked(ctx, big):
     """Past the budget the queue entries stay untraced: their path records keep
     EOS_HIT_UNTRACED (-2) and the traced ones equal the unlimited render's."""
