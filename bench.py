@@ -611,11 +611,12 @@ def run_ours(args, rank, world, local):
     st = api.render_batch(ctx, jobs, outs, stage_timing=True)
     shadow_bytes, closest_bytes = algorithmic_bytes(st, info["width"])
     stage = st["stage_ms"]
-    # one launch per bounce per chunk; the library's chunk rule: at most 2^24 paths (8x4-pixel
-    # tiles) and at most 8 GB of queues at (3 x 32 + 4 + 32 x lights + 16 x (depth + 1)) B per path
+    # the stage-timed run launches its stages one by one in a single lane: one launch per
+    # bounce per chunk; the library's chunk rule: at most 2^24 paths (8x4-pixel tiles) and at
+    # most 16 GB of queues at (2 x 32 + 2 x (36 + 32 x lights) + 16 x (depth + 1)) B per path
     paths = sum(((c.width + 7) // 8) * ((c.height + 3) // 4) * 32 for c in cams)
-    per_path = 3 * 32 + 4 + 32 * max(1, sc.n_lights) + 16 * (td + 1)
-    chunk = max(1 << 16, min(1 << 24, (8 << 30) // per_path))
+    per_path = 2 * 32 + 2 * (36 + 32 * max(1, sc.n_lights)) + 16 * (td + 1)
+    chunk = max(1 << 16, min(1 << 24, (16 << 30) // per_path))
     launches_stage = (td + 1) * int(np.ceil(paths / float(chunk)))
     sm_hz = (clk.summary()["sm_mhz"] or 1965.0) * 1e6
     roof = roofline(profile_traffic(), st, stage, shadow_bytes, closest_bytes, launches_stage, sm_hz)
