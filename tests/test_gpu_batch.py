@@ -54,7 +54,8 @@ def test_async_batches_equal_synchronous_ones(ctx):
     sc = scenes.small_random_scene(41, n_spheres=6, level=3, lights=3, refl=0.6)
     dsc = api.DeviceScene(ctx, sc)
     cams = [scenes.look_at((0.5, 3.0, 9.0), (0, -0.5, 0), 55.0, 160, 120),
-            scenes.look_at((-6.0, 4.0, 6.0), (0, -0.5, 0), 50.0, 96, 64)]
+            scenes.look_at((-6.0, 4.0, 6.0), (0, -0.5, 0), 50.0, 96, 64),
+            scenes.look_at((3.0, 2.0, 7.0), (0, -0.5, 0), 55.0, 1280, 960)]  # the pass runs as two lanes
     jobs = [api.BatchJob(dsc, c, 2, 0.5) for c in cams]
     ref_outs = [{"rgba8": np.zeros((c.height, c.width, 4), np.uint8)} for c in cams]
     ref_st = api.render_batch(ctx, jobs, ref_outs)
