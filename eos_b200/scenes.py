@@ -451,6 +451,34 @@ def small_random_scene(seed: int, n_spheres: int = 4, level: int = 2, lights: in
     return sc
 
 
+def mirror_hall_scene(seed: int = 71) -> SceneData:
+    """Two parallel mirrors with four spheres between them over a reflective floor, under
+    eight lights: paths down to the deepest trace depth (7: eight hits) and eight shadow
+    bits per hit."""
+    rng = rng_for(seed)
+    V, N, F, O = [], [], [], []
+
+    def add(v, n, f, obj):
+        F.append(np.asarray(f) + sum(len(x) for x in V))
+        V.append(np.asarray(v, np.float64))
+        N.append(np.asarray(n, np.float64))
+        O.append(np.full(len(f), obj))
+
+    for obj, x in ((0, -2.0), (1, 2.0)):  # mirrors facing each other
+        v = [[x, -2, -6], [x, -2, 6], [x, 3, 6], [x, 3, -6]]
+        add(v, [[-np.sign(x), 0, 0]] * 4, [[0, 1, 2], [0, 2, 3]] if x > 0 else [[0, 2, 1], [0, 3, 2]], obj)
+    add([[-2, -2, -6], [2, -2, -6], [2, -2, 6], [-2, -2, 6]], [[0, 1, 0]] * 4, [[0, 2, 1], [0, 3, 2]], 2)
+    iv, ifc = icosphere(2)
+    for k, c in enumerate(([-0.8, -1.2, -1.0], [0.9, -0.9, -2.5], [0.0, -0.4, -4.0], [-1.0, 0.2, -3.2])):
+        add(iv * 0.6 + c, iv, ifc, 3 + k)
+    mats = [material((0.05, 0.05, 0.05), 0.3, 64, 0.95), material((0.05, 0.05, 0.05), 0.3, 64, 0.9),
+            material((0.4, 0.4, 0.4), 0.2, 16, 0.3)]
+    mats += [material(rng.uniform(0, 1, 3), 0.4, 32, 0.7) for _ in range(4)]
+    lights = [[*rng.uniform([-1.8, 1.0, -5.0], [1.8, 2.8, 3.0]), 0.3, 0.3, 0.3] for _ in range(8)]
+    return SceneData(np.concatenate(V), np.concatenate(N), np.concatenate(F), np.concatenate(O), mats,
+                     np.array(lights), f"mirrors{seed}")
+
+
 # ----------------------------------------------------------------------------- instancing
 @dataclass
 class InstancedData:

@@ -9,6 +9,7 @@ tests read these files there.
     python tests/golden/make_golden.py config2    (the 1.06M-triangle sample only)
     python tests/golden/make_golden.py trees      (the ray-tree scene only)
     python tests/golden/make_golden.py aa         (the anti-aliasing grid case only)
+    python tests/golden/make_golden.py deep       (the deepest paths: trace depth 7, 8 lights)
 """
 from __future__ import annotations
 
@@ -84,6 +85,10 @@ def aa_case():
     print("aa3_small12", r["counts"])
 
 
+def deep_case():
+    render_case("deep71", scenes.mirror_hall_scene(71), scenes.look_at((-0.3, 0.5, 5.0), (1.2, -0.6, -3.0), 60.0, 80, 60), 7)
+
+
 def config2_case(n_sample=30_000):
     """30,000 seeded pixels of the 1080p view of the 1,056,768-triangle scene (depth 3, 4
     lights, pixel centres) through the reference's renderer, with the tree its own builder
@@ -115,6 +120,9 @@ def main():
     if sys.argv[1:] == ["aa"]:
         aa_case()
         return
+    if sys.argv[1:] == ["deep"]:
+        deep_case()
+        return
     morton_case()
     render_case("config1_128", scenes.config1_scene(), scenes.config1_camera(128, 128), 1)
     for seed in (11, 12):
@@ -126,6 +134,7 @@ def main():
     render_case("transp61", sc, scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 96, 72), 4)
     tree_case()
     aa_case()
+    deep_case()
     config2_case()
 
 

@@ -95,6 +95,7 @@ def test_plain_matches_compiled_reference_config1(ctx, c1):
     ("small12", lambda: scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)),
     ("transp61", lambda: scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3,
                                                    ambient_index=1.0002)),
+    ("deep71", lambda: scenes.mirror_hall_scene(71)),  # trace depth 7, 8 lights
 ])
 def test_plain_matches_reference_golden(ctx, name, scene_fn):
     gd = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -112,6 +113,28 @@ def test_plain_matches_reference_golden(ctx, name, scene_fn):
     assert np.abs(g["rgb"] - gd["rgb"]).max(1)[~mm].max() <= RGB_TOL
     # and bit-exact against the oracle everywhere
     assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+
+
+def test_deepest_paths_in_every_mode(ctx):
+    """The reference's deepest paths (golden deep71: trace depth 7, eight hits, eight
+    lights) in plain, wavefront and batched mode: the same records and colours, and 2-spp
+    paths of the same depth equal in plain and batched mode."""
+    gd = np.load(os.path.join(GOLDEN, "deep71.npz"))
+    W, H, td = (int(v) for v in gd["size"])
+    cam = scenes.CameraData(*[gd["cam"][3 * i:3 * i + 3] for i in range(4)], W, H)
+    dsc = api.DeviceScene(ctx, scenes.mirror_hall_scene(71))
+    a = gpu_render(ctx, dsc, cam, td, 0.0)
+    assert (paths_split(a["paths"])[0][:, 7] >= 0).sum() > 30  # paths with an eighth hit
+    b = gpu_render(ctx, dsc, cam, td, 0.0, mode="wavefront")
+    assert np.array_equal(a["paths"], b["paths"]) and np.array_equal(a["rgb"], b["rgb"])
+    jobs = [api.BatchJob(dsc, cam, td, 0.0), api.BatchJob(dsc, cam, td, 0.5, 2, 3)]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    api.render_batch(ctx, jobs, outs)
+    assert np.array_equal(outs[0]["paths"].cpu().numpy(), a["paths"])
+    assert np.array_equal(outs[0]["rgb"].cpu().numpy(), a["rgb"])
+    c = gpu_render(ctx, dsc, cam, td, 0.5, spp=2, jitter_seed=3)
+    assert np.array_equal(outs[1]["paths"].cpu().numpy(), c["paths"])
+    assert np.array_equal(outs[1]["rgb"].cpu().numpy(), c["rgb"])
 
 
 @pytest.mark.parametrize("spp,td", [(1, 1), (2, 3)])

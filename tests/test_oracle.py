@@ -52,6 +52,7 @@ def test_oracle_morton_order_is_stable_sort():
     ("small12", lambda: scenes.small_random_scene(12, n_spheres=5, level=2, lights=3, refl=0.6)),
     ("transp61", lambda: scenes.small_random_scene(61, n_spheres=6, level=2, lights=3, refl=0.5, transparent=3,
                                                    ambient_index=1.0002)),
+    ("deep71", lambda: scenes.mirror_hall_scene(71)),  # trace depth 7, 8 lights
 ])
 def test_oracle_matches_reference_golden(name, scene_fn):
     """Oracle paths and colours vs the reference's own renderer output (golden file)."""
