@@ -318,19 +318,22 @@ __global__ void __launch_bounds__(256, 4) k_wf_closest(WfArgs A) {
         int wbase = 0;
         if (lane == 0) wbase = atomicAdd(&ctr[2], total);
         wbase = __shfl_sync(0xffffffffu, wbase, 0);
-        bool fits = wbase + total <= A.cap_s;
-        if (!fits && lane == 0) atomicOr(A.err, kErrQueue);
+        // past the capacity the queue overflows (error bit); the entries below it are all
+        // written, also those of a block that only partly fits, because the shadow stage
+        // reads every entry below min(count, capacity)
+        if (wbase + total > A.cap_s && lane == 0) atomicOr(A.err, kErrQueue);
         int prefix = 0;
         for (int l = 0; l < maxl; ++l) {
           uint32_t bl = __ballot_sync(0xffffffffu, l < nl);
-          if (l < nl && fits) {
+          const int pos = wbase + prefix + __popc(bl & lanemask_lt());
+          if (l < nl && pos < A.cap_s) {
             const float* lp = J.s.lights + 6 * l;
             f3 sd = norm3(sub3(mk3(lp[0], lp[1], lp[2]), P));
             f3 so = add3(P, scale3(kRayEps, sd));
             ShadowQ s;
             s.a = make_float4(so.x, so.y, so.z, __int_as_float(i));
             s.b = make_float4(sd.x, sd.y, sd.z, __int_as_float((jb << 5) | l));
-            A.sq[wbase + prefix + __popc(bl & lanemask_lt())] = s;
+            A.sq[pos] = s;
           }
           prefix += __popc(bl);
         }

@@ -28,12 +28,25 @@ def big(ctx):
     return dsc, cam, ref
 
 
+class _Status(int):
+    """The status of a limited call; its repr carries the library's error detail, so that a
+    failed comparison shows which CUDA call or device error it was."""
+
+    def __new__(cls, err):
+        obj = super().__new__(cls, err.code)
+        obj.detail = str(err)
+        return obj
+
+    def __repr__(self):
+        return f"{int(self)} ({self.detail})"
+
+
 def _limited(ctx, fn, **lim):
     ctx.set_limits(**lim)
     try:
         with pytest.raises(EosError) as e:
             fn()
-        return e.value.code
+        return _Status(e.value)
     finally:
         ctx.set_limits()
 
@@ -69,11 +82,19 @@ def test_limit_gives_its_status_and_the_context_stays_usable(ctx, big, lim, code
 def test_limits_on_a_pass_of_two_lanes(ctx, big, lim, code):
     """A view of more than 2^20 paths runs as two lanes (halves of its paths side by side):
     each limit still gives its status, and the same context then renders the plain
-    renderer's image."""
+    renderer's image.  Before the limited call a batch of four jobs on a scene that is then
+    destroyed fills the queues: a limited call reads none of those stale entries (a shadow
+    queue entry names its job and hit, which would point into the destroyed scene)."""
     import torch
     dsc, _, _ = big
     cam = scenes.look_at((0, 25, 60), (0, 0, 0), 60.0, 1280, 960)
     ref = api.render(ctx, dsc, cam, 2, mode="plain", outputs=("rgb",), device=True)
+    tmp = api.DeviceScene(ctx, scenes.small_random_scene(44, n_spheres=6, level=3, lights=8, refl=0.6))
+    pre = [api.BatchJob(tmp, scenes.look_at((0.5 * k, 3.0, 9.0), (0, -0.5, 0), 55.0, 1280, 960), 2, 0.5)
+           for k in range(4)]
+    api.render_batch(ctx, pre, api.make_batch_outputs(pre, ("rgb",)))
+    torch.cuda.synchronize()
+    tmp.close()
     jobs = [api.BatchJob(dsc, cam, 2, 0.5)]
     outs = api.make_batch_outputs(jobs, ("rgb",))
     assert _limited(ctx, lambda: api.render_batch(ctx, jobs, outs), **lim) == code
