@@ -88,6 +88,21 @@ def test_trees_two_samples_and_modes_agree(ctx):
     assert np.array_equal(th[:, 0], c["paths"][:, 0])
 
 
+def test_trees_in_a_pass_of_two_lanes(ctx):
+    """A ray-tree view of more than 2^20 paths (halves side by side, the init and resolve
+    passes of tree mode in each): tree records and colours equal the plain renderer's."""
+    import torch
+    dsc = api.DeviceScene(ctx, tree_scene())
+    cam = scenes.look_at((1.0, 2.5, 8.0), (0, -0.5, 0), 55.0, 1280, 960)
+    jobs = [api.BatchJob(dsc, cam, 3, 0.5)]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"), tree_records=True)
+    api.render_batch(ctx, jobs, outs, tree_records=True)
+    ref = api.render(ctx, dsc, cam, 3, pixel_offset=0.5, outputs=("rgb", "paths"), device=True, tree_records=True)
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0]["paths"], ref["paths"])
+    assert torch.equal(outs[0]["rgb"], ref["rgb"])
+
+
 def test_tree_kernels_equal_chain_kernels_on_chain_scenes(ctx):
     """Tree records on a scene without such materials: the ray-tree kernels give the chain
     kernels' colours bit for bit and the chain bounces at their nodes."""
