@@ -26,7 +26,9 @@ from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_longlong, c_uin
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ORACLE_SO = os.path.join(HERE, "liboracle.so")
+# EOS_ORACLE_LIB: another build of eos_oracle.c (the sanitizer test loads one built with
+# AddressSanitizer and UBSan)
+ORACLE_SO = os.environ.get("EOS_ORACLE_LIB") or os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libeosref.so")
 # the reference's source tree, present where the checkers are built (not on the GPU box)
 REF_ROOT = os.environ.get("EOS_REFERENCE_ROOT", "/root/reference")
