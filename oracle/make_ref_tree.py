@@ -11,7 +11,7 @@ eosref_scene_create_from_tree, which recomputes every box with the builder's own
 BVH::computeBoxWithSurfaces.  The file lives beside the compiled reference in
 oracle/_ref/ (ignored by git, shipped with the built libraries).
 
-    python -m oracle.make_ref_tree [--scene config1|config2] [--force]
+    python -m oracle.make_ref_tree [--scene config1|config2|config5] [--force]
 """
 from __future__ import annotations
 
@@ -54,9 +54,9 @@ def main() -> None:
     from eos_b200 import scenes
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
-    ap.add_argument("--scene", default="config2", choices=["config1", "config2"])
+    ap.add_argument("--scene", default="config2", choices=["config1", "config2", "config5"])
     a = ap.parse_args()
-    sc = scenes.config2_scene() if a.scene == "config2" else scenes.config1_scene()
+    sc = {"config1": scenes.config1_scene, "config2": scenes.config2_scene, "config5": scenes.config5_scene}[a.scene]()
     path = tree_file(a.scene)
     if not a.force and load(sc, a.scene) is not None:
         print(f"{path}: up to date")

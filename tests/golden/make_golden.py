@@ -10,6 +10,7 @@ tests read these files there.
     python tests/golden/make_golden.py trees      (the ray-tree scene only)
     python tests/golden/make_golden.py aa         (the anti-aliasing grid case only)
     python tests/golden/make_golden.py deep       (the deepest paths: trace depth 7, 8 lights)
+    python tests/golden/make_golden.py config5    (the 4.5M-triangle 4K sample only)
 """
 from __future__ import annotations
 
@@ -109,6 +110,27 @@ def config2_case(n_sample=30_000):
     print("config2_sample", r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
 
 
+def config5_case(n_sample=3_000):
+    """3,000 seeded pixel centres of the 4K view of the 4,524,288-triangle stress scene
+    (depth 4, 8 lights; one sample at each pixel centre -- the reference has no jittered
+    samples) through the reference's renderer, with the tree its own builder made (saved
+    once by `python -m oracle.make_ref_tree --scene config5`)."""
+    from oracle import make_ref_tree
+    sc = scenes.config5_scene()
+    tree = make_ref_tree.load(sc, "config5")
+    if tree is None:
+        raise SystemExit("run `python -m oracle.make_ref_tree --scene config5` first")
+    ref = oracle.RefRenderer(sc, tree=tree)
+    cam = scenes.config5_camera()
+    rng = np.random.default_rng(5005)
+    pix = np.sort(rng.choice(cam.width * cam.height, n_sample, replace=False)).astype(np.int32)
+    r = ref.render(cam, 3, pixel_offset=0.5, pixels=pix, nthreads=os.cpu_count())
+    np.savez_compressed(os.path.join(HERE, "config5_sample.npz"), pixels=pix, rgb=r["rgb"], hits=r["hits"][:, :4],
+                        shadows=r["shadows"][:, :4].astype(np.uint8), counts=r["counts"], cam=cam.as_array(),
+                        size=np.array([cam.width, cam.height, 3]), ref_nodes=np.array([ref.n_nodes, ref.max_leaf]))
+    print("config5_sample", r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
+
+
 def main():
     oracle.build(ref=True)
     if sys.argv[1:] == ["config2"]:
@@ -123,6 +145,9 @@ def main():
     if sys.argv[1:] == ["deep"]:
         deep_case()
         return
+    if sys.argv[1:] == ["config5"]:
+        config5_case()
+        return
     morton_case()
     render_case("config1_128", scenes.config1_scene(), scenes.config1_camera(128, 128), 1)
     for seed in (11, 12):
@@ -136,6 +161,7 @@ def main():
     aa_case()
     deep_case()
     config2_case()
+    config5_case()
 
 
 if __name__ == "__main__":

@@ -422,6 +422,39 @@ def test_config2_sampled_pixels_match_oracle(ctx, width):
     assert st["shadow_rays"] > st["primary_rays"]
 
 
+def test_config5_sample_matches_reference_golden(ctx):
+    """The reference's own renderer on the 4,524,288-triangle 4K stress view (3,000 seeded
+    pixel centres, depth 4, 8 lights, thin foliage triangles; tests/golden/config5_sample.npz
+    with the tree the reference's builder made): hit ids and bounce paths bit-exact except
+    the classes the oracle flags, colours within RGB_TOL on every other path; the plain and
+    batched paths agree."""
+    path = os.path.join(GOLDEN, "config5_sample.npz")
+    if not os.path.exists(path):
+        pytest.skip("config5_sample.npz not generated")
+    gd = np.load(path)
+    pix = gd["pixels"]
+    sc = scenes.config5_scene()
+    dsc = api.DeviceScene(ctx, sc, inputs_on_device=True)
+    cam = scenes.config5_camera()
+    import torch
+    idx = torch.as_tensor(pix, dtype=torch.long, device="cuda")
+    g = api.render(ctx, dsc, cam, 3, pixel_offset=0.5, outputs=("rgb", "paths"), device=True)
+    jobs = [api.BatchJob(dsc, cam, 3, 0.5)]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    api.render_batch(ctx, jobs, outs)
+    assert torch.equal(outs[0]["paths"], g["paths"]) and torch.equal(outs[0]["rgb"], g["rgb"])
+    gp = g["paths"][idx].cpu().numpy()
+    gh, gs = paths_split(gp)
+    o = oracle.Oracle(sc).render(cam, 3, pixel_offset=0.5, pixels=pix)
+    mm = path_mismatch(gh, gs, gd["hits"], gd["shadows"], 4)
+    c = classify(mm, o["flags"])
+    print("config5 3k sample vs reference:", c)
+    assert c["unexplained"] == 0, c
+    assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 10, c
+    assert np.abs(g["rgb"][idx].cpu().numpy() - gd["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+
+
 def test_config2_sample_matches_reference_golden(ctx):
     """The reference's own renderer on the 1,056,768-triangle 1080p view (30,000 seeded pixel
     centres, depth 3, 4 lights; tests/golden/config2_sample.npz, from make_golden.py with the

@@ -91,6 +91,25 @@ def test_oracle_matches_reference_config2_sample():
     assert np.array_equal(r["counts"][0], g["counts"][0])
 
 
+def test_oracle_matches_reference_config5_sample():
+    """The oracle against the reference's renderer on 3,000 sampled paths of the
+    4,524,288-triangle 4K stress view (depth 4, 8 lights, thin foliage triangles; golden file
+    recorded with the reference's own tree)."""
+    path = os.path.join(os.path.dirname(__file__), "golden", "config5_sample.npz")
+    if not os.path.exists(path):
+        pytest.skip("config5_sample.npz not generated")
+    g = np.load(path)
+    sc = scenes.config5_scene()
+    cam = scenes.config5_camera()
+    r = oracle.Oracle(sc).render(cam, 3, pixel_offset=0.5, pixels=g["pixels"])
+    mm = path_mismatch(r["hits"], r["shadows"], g["hits"], g["shadows"], 4)
+    c = classify(mm, r["flags"])
+    print("oracle vs reference, config 5 sample:", c)
+    assert c["unexplained"] == 0, c
+    assert np.abs(r["rgb"] - g["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    assert np.array_equal(r["counts"][0], g["counts"][0])
+
+
 def test_reference_tree_restore_equals_build():
     """The reference's tree exported after its own build and restored (boxes recomputed by
     BVH::computeBoxWithSurfaces) gives the same node buffer boxes and the same renders."""
