@@ -11,6 +11,7 @@ tests read these files there.
     python tests/golden/make_golden.py aa         (the anti-aliasing grid case only)
     python tests/golden/make_golden.py deep       (the deepest paths: trace depth 7, 8 lights)
     python tests/golden/make_golden.py config5    (the 4.5M-triangle 4K sample only)
+    python tests/golden/make_golden.py config3    (two jobs of the batching workload only)
 """
 from __future__ import annotations
 
@@ -131,6 +132,37 @@ def config5_case(n_sample=3_000):
     print("config5_sample", r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
 
 
+def config3_case(n_sample=20_000):
+    """Two jobs of the batching workload (scenes.config3_jobs): its largest mixed scene
+    (job 69, 361,330 triangles, 512^2, 20,000 seeded pixel centres) and its first view of
+    the config-1 scene (job 0, 1920x1080 from 120 units away, 20,000 seeded pixel centres of
+    the central 600 x 600 pixels, where the scene is), depth 3, through the reference's
+    renderer on trees its own builder made (single-threaded; config 1's from oracle/_ref)."""
+    from oracle import make_ref_tree
+    jobs = scenes.config3_jobs()
+    rng = np.random.default_rng(3003)
+    for k, name in ((69, "config3_job69"), (0, "config3_job0")):
+        j = jobs[k]
+        tree = make_ref_tree.load(j.scene, "config1") if k == 0 else None
+        ref = oracle.RefRenderer(j.scene, build_threads=1, tree=tree)
+        cam = j.camera
+        if k == 0:
+            xs, ys = np.meshgrid(np.arange(cam.width // 2 - 300, cam.width // 2 + 300),
+                                 np.arange(cam.height // 2 - 300, cam.height // 2 + 300))
+            pool = (ys * cam.width + xs).reshape(-1)
+        else:
+            pool = np.arange(cam.width * cam.height)
+        pix = np.sort(rng.choice(pool, n_sample, replace=False)).astype(np.int32)
+        r = ref.render(cam, j.trace_depth, pixel_offset=j.pixel_offset, pixels=pix, nthreads=os.cpu_count())
+        nb = j.trace_depth + 1
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), job=np.array(k), pixels=pix, rgb=r["rgb"],
+                            hits=r["hits"][:, :nb], shadows=r["shadows"][:, :nb].astype(np.uint8),
+                            counts=r["counts"], cam=cam.as_array(),
+                            size=np.array([cam.width, cam.height, j.trace_depth]),
+                            ref_nodes=np.array([ref.n_nodes, ref.max_leaf]))
+        print(name, r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
+
+
 def main():
     oracle.build(ref=True)
     if sys.argv[1:] == ["config2"]:
@@ -148,6 +180,9 @@ def main():
     if sys.argv[1:] == ["config5"]:
         config5_case()
         return
+    if sys.argv[1:] == ["config3"]:
+        config3_case()
+        return
     morton_case()
     render_case("config1_128", scenes.config1_scene(), scenes.config1_camera(128, 128), 1)
     for seed in (11, 12):
@@ -162,6 +197,7 @@ def main():
     deep_case()
     config2_case()
     config5_case()
+    config3_case()
 
 
 if __name__ == "__main__":

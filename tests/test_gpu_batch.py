@@ -111,3 +111,45 @@ def test_batch_over_several_chunks_equals_single_renders(ctx):
         ref = api.render(ctx, dsc, c, 2, 0.5, spp=2, jitter_seed=11, outputs=("rgb", "paths"), device=False)
         assert np.array_equal(o["rgb"].cpu().numpy(), ref["rgb"])
         assert np.array_equal(o["paths"].cpu().numpy(), ref["paths"])
+
+
+def test_batching_workload_matches_reference_goldens(ctx):
+    """Jobs of the batching workload (scenes.config3_jobs: 8 views of the config-1 scene and
+    its 16 mixed scenes, one batch): the reference's own renderer recorded 20,000 sampled
+    paths of job 69 (its largest mixed scene) and of job 0 (a 1080p view of the config-1
+    scene) -- the batch equals them on every path but the classes the oracle flags, and
+    equals the oracle everywhere."""
+    import os
+    from tests.parity import RGB_TOL, classify, path_mismatch
+    golden = os.path.join(os.path.dirname(__file__), "golden")
+    if not all(os.path.exists(os.path.join(golden, f"config3_job{k}.npz")) for k in (0, 69)):
+        pytest.skip("config3 goldens not generated")
+    spec = scenes.config3_jobs()
+    keep = list(range(8)) + [k for k, j in enumerate(spec) if j.scene.name.startswith("mixed")]
+    dev = {}
+    jobs = []
+    for k in keep:
+        j = spec[k]
+        if id(j.scene) not in dev:
+            dev[id(j.scene)] = api.DeviceScene(ctx, j.scene)
+        jobs.append(api.BatchJob(dev[id(j.scene)], j.camera, j.trace_depth, j.pixel_offset))
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    api.render_batch(ctx, jobs, outs)
+    for k in (0, 69):
+        gd = np.load(os.path.join(golden, f"config3_job{k}.npz"))
+        pix = gd["pixels"]
+        o_k = outs[keep.index(k)]
+        p = o_k["paths"].cpu().numpy()[pix]
+        gh, gs = p[:, :8], p[:, 8:].view(np.uint32)
+        j = spec[k]
+        o = oracle.Oracle(j.scene).render(j.camera, j.trace_depth, pixel_offset=j.pixel_offset, pixels=pix)
+        mm = path_mismatch(gh, gs, gd["hits"], gd["shadows"], j.trace_depth + 1)
+        c = classify(mm, o["flags"])
+        print(f"config3 job {k} vs reference:", c)
+        assert c["unexplained"] == 0, c
+        assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 10, c
+        assert np.abs(o_k["rgb"].cpu().numpy()[pix] - gd["rgb"]).max(1)[~mm].max() <= RGB_TOL
+        assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+        ref = api.render(ctx, jobs[keep.index(k)].scene, j.camera, j.trace_depth, j.pixel_offset,
+                         outputs=("rgb", "paths"), device=False)
+        assert np.array_equal(o_k["paths"].cpu().numpy(), ref["paths"])

@@ -110,6 +110,26 @@ def test_oracle_matches_reference_config5_sample():
     assert np.array_equal(r["counts"][0], g["counts"][0])
 
 
+@pytest.mark.parametrize("name", ["config3_job69", "config3_job0"])
+def test_oracle_matches_reference_config3_jobs(name):
+    """The oracle against the reference's renderer on 20,000 sampled paths of two jobs of
+    the batching workload (its largest mixed scene, 361,330 triangles, and a 1080p view of
+    the config-1 scene)."""
+    path = os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"{name}.npz not generated")
+    g = np.load(path)
+    j = scenes.config3_jobs()[int(g["job"])]
+    r = oracle.Oracle(j.scene).render(j.camera, j.trace_depth, pixel_offset=j.pixel_offset, pixels=g["pixels"])
+    mm = path_mismatch(r["hits"], r["shadows"], g["hits"], g["shadows"], j.trace_depth + 1)
+    c = classify(mm, r["flags"])
+    print(f"oracle vs reference, {name}:", c)
+    assert c["unexplained"] == 0, c
+    assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 10, c
+    assert np.abs(r["rgb"] - g["rgb"]).max(1)[~mm].max() <= RGB_TOL
+    assert np.array_equal(r["counts"][0], g["counts"][0])
+
+
 def test_reference_tree_restore_equals_build():
     """The reference's tree exported after its own build and restored (boxes recomputed by
     BVH::computeBoxWithSurfaces) gives the same node buffer boxes and the same renders."""
