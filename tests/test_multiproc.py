@@ -105,7 +105,7 @@ def _band_worker(rank, world, port, out):
 def test_split_frame_bands_gather_to_the_whole_frame():
     world = 3  # 12 rows over 3 ranks: 4 + 4 + 4; and a remainder case below
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_band_worker, args=(world, port, out), nprocs=world, start_method="spawn")
     sc, cams = _setup()
