@@ -385,6 +385,16 @@ def config4_scene(seed: int = 1004, hidden: bool = True) -> SceneData:
     return sc
 
 
+def integer_shininess(sc: SceneData) -> SceneData:
+    """The same scene with every shininess rounded down to an integer (at least 1).  The
+    reference's Material holds its shininess as an int (src/Material.h:47,72), so this is
+    the scene its renderer draws when given config 4's continuous shininess."""
+    m = sc.materials.copy()
+    m[:, 6] = np.maximum(np.floor(m[:, 6]), 1.0)
+    return SceneData(sc.verts, sc.normals, sc.tris, sc.tri_obj, m, sc.lights, sc.name + "-intshin",
+                     sc.ambient_index)
+
+
 def perturb_params(sc: SceneData, rng: np.random.Generator, frac: float) -> SceneData:
     m = sc.materials.astype(np.float64).copy()
     l = sc.lights.astype(np.float64).copy()

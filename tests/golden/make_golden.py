@@ -12,6 +12,7 @@ tests read these files there.
     python tests/golden/make_golden.py deep       (the deepest paths: trace depth 7, 8 lights)
     python tests/golden/make_golden.py config5    (the 4.5M-triangle 4K sample only)
     python tests/golden/make_golden.py config3    (two jobs of the batching workload only)
+    python tests/golden/make_golden.py config4    (the differentiation workload's 8 views only)
 """
 from __future__ import annotations
 
@@ -163,8 +164,37 @@ def config3_case(n_sample=20_000):
         print(name, r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
 
 
+def config4_case(n_per_view=4_000):
+    """The differentiation workload's forward render: all 8 views at 256^2 of config 4's
+    scene (50 level-3 icospheres on a ground quad, 3 lights, depth 2 = trace depth 1),
+    4,000 seeded pixel centres per view, through the reference's renderer on the tree its
+    own builder makes (single-threaded).  The reference's shininess is an int, so the scene
+    is config 4 with each shininess rounded down (scenes.integer_shininess)."""
+    sc = scenes.integer_shininess(scenes.config4_scene())
+    cams = scenes.config4_cameras(8, 256)
+    ref = oracle.RefRenderer(sc, build_threads=1)
+    rng = np.random.default_rng(4004)
+    out = {k: [] for k in ("view", "pixels", "rgb", "hits", "shadows")}
+    counts = np.zeros(3, np.int64)
+    for v, cam in enumerate(cams):
+        pix = np.sort(rng.choice(cam.width * cam.height, n_per_view, replace=False)).astype(np.int32)
+        r = ref.render(cam, 1, pixel_offset=0.5, pixels=pix, nthreads=os.cpu_count())
+        out["view"].append(np.full(n_per_view, v, np.int32))
+        out["pixels"].append(pix)
+        out["rgb"].append(r["rgb"])
+        out["hits"].append(r["hits"][:, :2])
+        out["shadows"].append(r["shadows"][:, :2].astype(np.uint8))
+        counts += np.asarray(r["counts"][:3], np.int64)
+    np.savez_compressed(os.path.join(HERE, "config4_views.npz"), **{k: np.concatenate(v) for k, v in out.items()},
+                        counts=counts, size=np.array([256, 256, 1]), ref_nodes=np.array([ref.n_nodes, ref.max_leaf]))
+    print("config4_views", counts, "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
+
+
 def main():
     oracle.build(ref=True)
+    if sys.argv[1:] == ["config4"]:
+        config4_case()
+        return
     if sys.argv[1:] == ["config2"]:
         config2_case()
         return
@@ -198,6 +228,7 @@ def main():
     config2_case()
     config5_case()
     config3_case()
+    config4_case()
 
 
 if __name__ == "__main__":

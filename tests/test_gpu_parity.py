@@ -484,3 +484,34 @@ def test_config2_sample_matches_reference_golden(ctx):
     assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 30, c
     assert np.abs(g["rgb"].cpu().numpy()[pix] - gd["rgb"]).max(1)[~mm].max() <= RGB_TOL
     assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"])
+
+
+def test_config4_views_match_reference_golden(ctx):
+    """The reference's own renderer on the differentiation workload's forward render: the 8
+    views at 256^2 of config 4's scene (shininess rounded down to the reference's int; 4,000
+    seeded pixel centres per view, tests/golden/config4_views.npz): the 8 views as one
+    batch, as the adjoint timing renders them, and one plain call per view give the same
+    frames, and on the sampled paths hit ids and shadow masks equal the reference's and the
+    colours are within RGB_TOL."""
+    import torch
+    gd = np.load(os.path.join(GOLDEN, "config4_views.npz"))
+    sc = scenes.integer_shininess(scenes.config4_scene())
+    dsc = api.DeviceScene(ctx, sc)
+    cams = scenes.config4_cameras(8, 256)
+    jobs = [api.BatchJob(dsc, c, 1, 0.5) for c in cams]
+    outs = api.make_batch_outputs(jobs, ("rgb", "paths"))
+    api.render_batch(ctx, jobs, outs)
+    o = oracle.Oracle(sc)
+    for v, cam in enumerate(cams):
+        g = api.render(ctx, dsc, cam, 1, pixel_offset=0.5, outputs=("rgb", "paths"), device=True)
+        assert torch.equal(outs[v]["paths"], g["paths"]) and torch.equal(outs[v]["rgb"], g["rgb"]), v
+        sel = gd["view"] == v
+        pix = gd["pixels"][sel]
+        gh, gs = paths_split(g["paths"].cpu().numpy()[pix])
+        r = o.render(cam, 1, pixel_offset=0.5, pixels=pix)
+        mm = path_mismatch(gh, gs, gd["hits"][sel], gd["shadows"][sel], 2)
+        c = classify(mm, r["flags"])
+        assert c["unexplained"] == 0, (v, c)
+        assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 5, (v, c)
+        assert np.abs(g["rgb"].cpu().numpy()[pix] - gd["rgb"][sel]).max(1)[~mm].max() <= RGB_TOL, v
+        assert np.array_equal(gh, r["hits"]) and np.array_equal(gs, r["shadows"]), v

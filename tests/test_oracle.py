@@ -130,6 +130,27 @@ def test_oracle_matches_reference_config3_jobs(name):
     assert np.array_equal(r["counts"][0], g["counts"][0])
 
 
+def test_oracle_matches_reference_config4_views():
+    """The oracle against the reference's renderer on the differentiation workload's forward
+    render: 4,000 sampled paths of each of its 8 views at 256^2 (config 4's scene with the
+    shininess rounded down to the reference's int)."""
+    g = load("config4_views")
+    sc = scenes.integer_shininess(scenes.config4_scene())
+    cams = scenes.config4_cameras(8, 256)
+    o = oracle.Oracle(sc)
+    shadow_rays = 0
+    for v, cam in enumerate(cams):
+        sel = g["view"] == v
+        r = o.render(cam, 1, pixel_offset=0.5, pixels=g["pixels"][sel])
+        mm = path_mismatch(r["hits"], r["shadows"], g["hits"][sel], g["shadows"][sel], 2)
+        c = classify(mm, r["flags"])
+        assert c["unexplained"] == 0, (v, c)
+        assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 5, (v, c)
+        assert np.abs(r["rgb"] - g["rgb"][sel]).max(1)[~mm].max() <= RGB_TOL, v
+        shadow_rays += int(r["counts"][1])
+    assert shadow_rays == int(g["counts"][1])
+
+
 def test_reference_tree_restore_equals_build():
     """The reference's tree exported after its own build and restored (boxes recomputed by
     BVH::computeBoxWithSurfaces) gives the same node buffer boxes and the same renders."""
