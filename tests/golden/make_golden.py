@@ -13,6 +13,7 @@ tests read these files there.
     python tests/golden/make_golden.py config5    (the 4.5M-triangle 4K sample only)
     python tests/golden/make_golden.py config3    (two jobs of the batching workload only)
     python tests/golden/make_golden.py config4    (the differentiation workload's 8 views only)
+    python tests/golden/make_golden.py config3mixed  (the other 15 mixed scenes of the batching workload)
 """
 from __future__ import annotations
 
@@ -164,6 +165,40 @@ def config3_case(n_sample=20_000):
         print(name, r["counts"], "nodes", ref.n_nodes, "max leaf", ref.max_leaf)
 
 
+def _config3_mixed_job(args):
+    """One mixed scene of the batching workload through the reference's renderer (run in a
+    worker process: the reference's builder is single-threaded)."""
+    k, n_sample = args
+    j = scenes.config3_jobs()[k]
+    ref = oracle.RefRenderer(j.scene, build_threads=1)
+    cam = j.camera
+    pix = np.sort(np.random.default_rng(3100 + k).choice(cam.width * cam.height, n_sample,
+                                                          replace=False)).astype(np.int32)
+    r = ref.render(cam, j.trace_depth, pixel_offset=j.pixel_offset, pixels=pix, nthreads=1)
+    nb = j.trace_depth + 1
+    return (k, pix, r["rgb"], r["hits"][:, :nb], r["shadows"][:, :nb].astype(np.uint8), np.asarray(r["counts"]),
+            ref.n_nodes, ref.max_leaf)
+
+
+def config3_mixed_case(n_sample=2_000):
+    """The other 15 mixed scenes of the batching workload (jobs 64-79 but 69, 25k-315k
+    triangles, 512^2, depth 3, 2 lights): 2,000 seeded pixel centres of each through the
+    reference's renderer on the tree its own builder makes, one worker process per scene."""
+    import multiprocessing as mp
+    jobs = scenes.config3_jobs()
+    ks = [k for k, j in enumerate(jobs) if j.scene.name.startswith("mixed") and k != 69]
+    with mp.get_context("spawn").Pool(min(len(ks), os.cpu_count() or 1)) as pool:
+        res = pool.map(_config3_mixed_job, [(k, n_sample) for k in ks])
+    res.sort(key=lambda t: t[0])
+    out = dict(job=np.concatenate([np.full(len(t[1]), t[0], np.int32) for t in res]),
+               pixels=np.concatenate([t[1] for t in res]), rgb=np.concatenate([t[2] for t in res]),
+               hits=np.concatenate([t[3] for t in res]), shadows=np.concatenate([t[4] for t in res]),
+               counts=np.stack([t[5] for t in res]), ref_nodes=np.array([[t[6], t[7]] for t in res]))
+    np.savez_compressed(os.path.join(HERE, "config3_mixed.npz"), **out)
+    for t in res:
+        print("config3 job", t[0], t[5], "nodes", t[6], "max leaf", t[7])
+
+
 def config4_case(n_per_view=4_000):
     """The differentiation workload's forward render: all 8 views at 256^2 of config 4's
     scene (50 level-3 icospheres on a ground quad, 3 lights, depth 2 = trace depth 1),
@@ -194,6 +229,9 @@ def main():
     oracle.build(ref=True)
     if sys.argv[1:] == ["config4"]:
         config4_case()
+        return
+    if sys.argv[1:] == ["config3mixed"]:
+        config3_mixed_case()
         return
     if sys.argv[1:] == ["config2"]:
         config2_case()
@@ -228,6 +266,7 @@ def main():
     config2_case()
     config5_case()
     config3_case()
+    config3_mixed_case()
     config4_case()
 
 

@@ -117,8 +117,8 @@ def test_batching_workload_matches_reference_goldens(ctx):
     """Jobs of the batching workload (scenes.config3_jobs: 8 views of the config-1 scene and
     its 16 mixed scenes, one batch): the reference's own renderer recorded 20,000 sampled
     paths of job 69 (its largest mixed scene) and of job 0 (a 1080p view of the config-1
-    scene) -- the batch equals them on every path but the classes the oracle flags, and
-    equals the oracle everywhere."""
+    scene), and 2,000 of each of the other 15 mixed scenes -- the batch equals them on every
+    path but the classes the oracle flags, and equals the oracle everywhere."""
     import os
     from tests.parity import RGB_TOL, classify, path_mismatch
     golden = os.path.join(os.path.dirname(__file__), "golden")
@@ -153,3 +153,20 @@ def test_batching_workload_matches_reference_goldens(ctx):
         ref = api.render(ctx, jobs[keep.index(k)].scene, j.camera, j.trace_depth, j.pixel_offset,
                          outputs=("rgb", "paths"), device=False)
         assert np.array_equal(o_k["paths"].cpu().numpy(), ref["paths"])
+    # the other 15 mixed scenes: 2,000 sampled paths of each from the reference's renderer
+    gm = np.load(os.path.join(golden, "config3_mixed.npz"))
+    for k in np.unique(gm["job"]):
+        k = int(k)
+        sel = gm["job"] == k
+        pix = gm["pixels"][sel]
+        o_k = outs[keep.index(k)]
+        p = o_k["paths"].cpu().numpy()[pix]
+        gh, gs = p[:, :8], p[:, 8:].view(np.uint32)
+        j = spec[k]
+        o = oracle.Oracle(j.scene).render(j.camera, j.trace_depth, pixel_offset=j.pixel_offset, pixels=pix)
+        mm = path_mismatch(gh, gs, gm["hits"][sel], gm["shadows"][sel], j.trace_depth + 1)
+        c = classify(mm, o["flags"])
+        assert c["unexplained"] == 0, (k, c)
+        assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 5, (k, c)
+        assert np.abs(o_k["rgb"].cpu().numpy()[pix] - gm["rgb"][sel]).max(1)[~mm].max() <= RGB_TOL, k
+        assert np.array_equal(gh, o["hits"]) and np.array_equal(gs, o["shadows"]), k

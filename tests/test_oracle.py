@@ -130,6 +130,24 @@ def test_oracle_matches_reference_config3_jobs(name):
     assert np.array_equal(r["counts"][0], g["counts"][0])
 
 
+def test_oracle_matches_reference_config3_mixed_scenes():
+    """The oracle against the reference's renderer on the other 15 mixed scenes of the
+    batching workload (25k-315k triangles; 2,000 sampled paths of each, recorded on the
+    trees the reference's builder made)."""
+    g = load("config3_mixed")
+    spec = scenes.config3_jobs()
+    for k in np.unique(g["job"]):
+        j = spec[int(k)]
+        sel = g["job"] == k
+        r = oracle.Oracle(j.scene).render(j.camera, j.trace_depth, pixel_offset=j.pixel_offset,
+                                          pixels=g["pixels"][sel])
+        mm = path_mismatch(r["hits"], r["shadows"], g["hits"][sel], g["shadows"][sel], j.trace_depth + 1)
+        c = classify(mm, r["flags"])
+        assert c["unexplained"] == 0, (int(k), c)
+        assert c["axis_parallel_not_tie"] + c["near_origin_not_tie"] <= 5, (int(k), c)
+        assert np.abs(r["rgb"] - g["rgb"][sel]).max(1)[~mm].max() <= RGB_TOL, int(k)
+
+
 def test_oracle_matches_reference_config4_views():
     """The oracle against the reference's renderer on the differentiation workload's forward
     render: 4,000 sampled paths of each of its 8 views at 256^2 (config 4's scene with the
